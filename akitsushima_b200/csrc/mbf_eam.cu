@@ -1,0 +1,468 @@
+// Alloy EAM: density kernel (rho-bar, F, F') and force kernel, lane group
+// per atom over the two-way CSR, no atomics.
+//
+// Replaces engine/eam.py:174-256 and engine/_eam_kernels.py:231-307.  The
+// reference evaluates each half pair once and scatters through a serial
+// two-way CSR; here each atom gathers over its own row (owner computes), so
+// a pair's functions are evaluated from both sides and nothing is written
+// twice.  rho-bar is accumulated and clamped in float64 and F(rho-bar) is
+// evaluated in float64 in both precisions.
+#include "mbf_util.cuh"
+
+namespace mbf {
+
+constexpr int EAM_NZ = 20;         // Zhou parameters per element row
+constexpr int EAM_NCOL = 2 * EAM_NZ + 3;
+constexpr int EAM_MAXSP = 8;       // species staged in shared memory (fused path)
+constexpr int EAM_BLOCK = 128;
+
+enum { F_SPLINE = 1, F_SPLINE_R = 2, F_Z_DENS = 3, F_Z_PAIR = 4, F_Z_CROSS = 5, F_Z_EMB = 6 };
+
+struct EamDev {
+    int ns, nf, nX;
+    const int *codes;
+    const double *P;
+    const int *xo, *nx;
+    const double *X, *C;
+    const int *rho_f, *F_f, *phi_f;
+    double r_cut;
+};
+
+// ---- generic function evaluation (engine/_eam_kernels.py:129-228) -------
+
+template <typename T>
+__device__ __forceinline__ void spline_eval(const EamDev &E, int f, double r, T &v, T &dv) {
+    int o = E.xo[f], n = E.nx[f];
+    const double *X = E.X + o;
+    int lo = 0, hi = n;
+    while (lo < hi) {  // searchsorted(side='right')
+        int mid = (lo + hi) >> 1;
+        if (X[mid] <= r) lo = mid + 1; else hi = mid;
+    }
+    int i = lo - 1;
+    i = i < 0 ? 0 : (i > n - 2 ? n - 2 : i);
+    T dx = (T)(r - X[i]);
+    T c0 = (T)E.C[o + i], c1 = (T)E.C[E.nX + o + i];
+    T c2 = (T)E.C[2 * E.nX + o + i], c3 = (T)E.C[3 * E.nX + o + i];
+    v = ((c0 * dx + c1) * dx + c2) * dx + c3;
+    dv = (T(3) * c0 * dx + T(2) * c1) * dx + c2;
+}
+
+template <typename T>
+__device__ __forceinline__ void zdecay(T r, T re, T pre, T expo, T shift, T &val, T &dval) {
+    T x = r / re;
+    T e = pre * RT<T>::ex(-expo * (x - T(1)));
+    T u19;
+    T den = T(1) + pow20(x - shift, u19);
+    val = e / den;
+    dval = (-expo * e / den - e * T(20) * u19 / (den * den)) / re;
+}
+
+template <typename T>
+__device__ __forceinline__ void zdens(const double *p, T r, T &v, T &dv) {
+    zdecay<T>(r, (T)p[0], (T)p[1], (T)p[5], (T)p[9], v, dv);
+}
+
+template <typename T>
+__device__ __forceinline__ void zpair(const double *p, T r, T &v, T &dv) {
+    T a, da, b, db;
+    zdecay<T>(r, (T)p[0], (T)p[6], (T)p[4], (T)p[8], a, da);
+    zdecay<T>(r, (T)p[0], (T)p[7], (T)p[5], (T)p[9], b, db);
+    v = a - b;
+    dv = da - db;
+}
+
+template <typename T>
+__device__ __forceinline__ void zswitch(T r, T rc, T w, T &S, T &dS) {
+    T s = (r - (rc - w)) / w;
+    s = s < T(0) ? T(0) : (s > T(1) ? T(1) : s);
+    S = T(1) - s * s * s * (T(10) - T(15) * s + T(6) * s * s);
+    dS = T(-30) * s * s * (T(1) - s) * (T(1) - s) / w;
+}
+
+// Zhou embedding, eqs. (A6)-(A8) (engine/_eam_kernels.py:180-196); float64.
+__device__ __forceinline__ void zembed(const double *p, double rho, double &F, double &dF) {
+    double re = p[2], rs = p[3], eta = p[18];
+    double rn = 0.85 * re;
+    if (rho < rn) {
+        double z = rho / rn - 1.0;
+        F = p[10] + p[11] * z + p[12] * z * z + p[13] * z * z * z;
+        dF = (p[11] + 2 * p[12] * z + 3 * p[13] * z * z) / rn;
+    } else if (rho >= 1.15 * re) {
+        double t = rho / rs;
+        double lt = log(t);
+        F = p[19] * (1.0 - eta * lt) * pow(t, eta);
+        dF = -p[19] * eta * eta * lt * pow(t, eta - 1.0) / rs;
+    } else {
+        double z = rho / re - 1.0;
+        F = p[14] + p[15] * z + p[16] * z * z + p[17] * z * z * z;
+        dF = (p[15] + 2 * p[16] * z + 3 * p[17] * z * z) / re;
+    }
+}
+
+template <typename T>
+__device__ void feval(const EamDev &E, int f, double r, T &v, T &dv) {
+    int code = E.codes[f];
+    const double *P = E.P + (size_t)f * EAM_NCOL;
+    if (code == F_SPLINE) {
+        spline_eval<T>(E, f, r, v, dv);
+        return;
+    }
+    if (code == F_SPLINE_R) {
+        T s, ds;
+        spline_eval<T>(E, f, r, s, ds);
+        T rr = (T)r;
+        v = s / rr;
+        dv = (ds * rr - s) / (rr * rr);
+        return;
+    }
+    if (code == F_Z_EMB) {
+        double F, dF;
+        zembed(P, r, F, dF);
+        v = (T)F;
+        dv = (T)dF;
+        return;
+    }
+    T rr = (T)r, val, dval;
+    if (code == F_Z_DENS) {
+        zdens<T>(P, rr, val, dval);
+    } else if (code == F_Z_PAIR) {
+        zpair<T>(P, rr, val, dval);
+    } else {
+        T fa, dfa, fb, dfb, ua, dua, ub, dub;
+        zdens<T>(P, rr, fa, dfa);
+        zdens<T>(P + EAM_NZ, rr, fb, dfb);
+        zpair<T>(P, rr, ua, dua);
+        zpair<T>(P + EAM_NZ, rr, ub, dub);
+        T k = (T)P[2 * EAM_NZ + 2];
+        T q = fb / fa;
+        T dq = (dfb * fa - fb * dfa) / (fa * fa);
+        val = T(0.5) * k * (q * ua + ub / q);
+        dval = T(0.5) * k * (dq * ua + q * dua + dub / q - ub * dq / (q * q));
+    }
+    T S, dS;
+    zswitch<T>(rr, (T)P[2 * EAM_NZ], (T)P[2 * EAM_NZ + 1], S, dS);
+    v = val * S;
+    dv = dval * S + val * dS;
+}
+
+// Embedding F(rho) always in float64.
+__device__ __forceinline__ void embed64(const EamDev &E, int f, double rho, double &F, double &dF) {
+    if (E.codes[f] == F_Z_EMB) {
+        zembed(E.P + (size_t)f * EAM_NCOL, rho, F, dF);
+    } else {
+        feval<double>(E, f, rho, F, dF);
+    }
+}
+
+// ---- fused Zhou alloy path ----------------------------------------------
+// One element's density f and pair phi_aa share exp(-beta (x - 1)) and the
+// denominator 1 + (x - lambda)^20, so a species costs two exponentials.
+
+template <typename T>
+struct ZSp {
+    T re, fe, beta, lam, A, alpha, kappa, B;
+};
+
+template <typename T>
+struct ZTab {
+    ZSp<T> sp[EAM_MAXSP];
+    T chi[EAM_MAXSP * EAM_MAXSP];
+    T rc, w;
+};
+
+template <typename T>
+__device__ __forceinline__ void zspecies(const ZSp<T> &p, T r, T &f, T &df, T &pr, T &dpr) {
+    T x = r / p.re;
+    T xm1 = x - T(1);
+    T eB = RT<T>::ex(-p.beta * xm1);
+    T eA = RT<T>::ex(-p.alpha * xm1);
+    T u19B, u19A;
+    T dB = T(1) + pow20(x - p.lam, u19B);
+    T dA = T(1) + pow20(x - p.kappa, u19A);
+    T gB = eB / dB, gA = eA / dA;
+    T dgB = -p.beta * gB - gB * T(20) * u19B / dB;
+    T dgA = -p.alpha * gA - gA * T(20) * u19A / dA;
+    f = p.fe * gB;
+    df = p.fe * dgB / p.re;
+    pr = p.A * gA - p.B * gB;
+    dpr = (p.A * dgA - p.B * dgB) / p.re;
+}
+
+template <typename T>
+__device__ __forceinline__ T zdens_only(const ZSp<T> &p, T r) {
+    T x = r / p.re;
+    T u19;
+    T d = T(1) + pow20(x - p.lam, u19);
+    return p.fe * RT<T>::ex(-p.beta * (x - T(1))) / d;
+}
+
+template <typename T>
+__device__ void load_ztab(const EamDev &E, ZTab<T> &Z) {
+    for (int s = threadIdx.x; s < E.ns; s += blockDim.x) {
+        const double *p = E.P + (size_t)E.rho_f[s] * EAM_NCOL;
+        ZSp<T> q;
+        q.re = (T)p[0]; q.fe = (T)p[1]; q.beta = (T)p[5]; q.lam = (T)p[9];
+        q.A = (T)p[6]; q.alpha = (T)p[4]; q.kappa = (T)p[8]; q.B = (T)p[7];
+        Z.sp[s] = q;
+    }
+    for (int ab = threadIdx.x; ab < E.ns * E.ns; ab += blockDim.x) {
+        int a = ab / E.ns, b = ab % E.ns;
+        T k = T(1);
+        if (a != b) k = (T)E.P[(size_t)E.phi_f[a * E.ns + b] * EAM_NCOL + 2 * EAM_NZ + 2];
+        Z.chi[a * EAM_MAXSP + b] = k;
+    }
+    if (threadIdx.x == 0) {
+        const double *p = E.P + (size_t)E.rho_f[0] * EAM_NCOL;
+        Z.rc = (T)p[2 * EAM_NZ];
+        Z.w = (T)p[2 * EAM_NZ + 1];
+    }
+    __syncthreads();
+}
+
+// phi_{si,sj}, rho'_{sj}, rho'_{si} at r (fused Zhou path).
+template <typename T>
+__device__ __forceinline__ void zhou_pair_terms(const ZTab<T> &Z, int si, int sj, T r, T &phi,
+                                                T &dphi, T &drho_j, T &drho_i) {
+    T S, dS;
+    zswitch<T>(r, Z.rc, Z.w, S, dS);
+    if (si == sj) {
+        T f, df, pr, dpr;
+        zspecies<T>(Z.sp[si], r, f, df, pr, dpr);
+        phi = pr * S;
+        dphi = dpr * S + pr * dS;
+        drho_j = df * S + f * dS;
+        drho_i = drho_j;
+    } else {
+        int a = si < sj ? si : sj, b = si < sj ? sj : si;
+        T fa, dfa, ua, dua, fb, dfb, ub, dub;
+        zspecies<T>(Z.sp[a], r, fa, dfa, ua, dua);
+        zspecies<T>(Z.sp[b], r, fb, dfb, ub, dub);
+        T k = Z.chi[a * EAM_MAXSP + b];
+        T q = fb / fa;
+        T dq = (dfb * fa - fb * dfa) / (fa * fa);
+        T v = T(0.5) * k * (q * ua + ub / q);
+        T dv = T(0.5) * k * (dq * ua + q * dua + dub / q - ub * dq / (q * q));
+        phi = v * S;
+        dphi = dv * S + v * dS;
+        T dra = dfa * S + fa * dS, drb = dfb * S + fb * dS;
+        drho_j = sj == a ? dra : drb;
+        drho_i = si == a ? dra : drb;
+    }
+}
+
+// Fast minimum image for the force kernels (fused multiply-add allowed).
+__device__ __forceinline__ void mic_fast(const double *__restrict__ c, double rx, double ry, double rz,
+                                         double &dx, double &dy, double &dz) {
+    double sx = rx * c[9] + ry * c[12] + rz * c[15];
+    double sy = rx * c[10] + ry * c[13] + rz * c[16];
+    double sz = rx * c[11] + ry * c[14] + rz * c[17];
+    sx -= rint(sx);
+    sy -= rint(sy);
+    sz -= rint(sz);
+    dx = sx * c[0] + sy * c[3] + sz * c[6];
+    dy = sx * c[1] + sy * c[4] + sz * c[7];
+    dz = sx * c[2] + sy * c[5] + sz * c[8];
+}
+
+// ---- kernels --------------------------------------------------------------
+
+template <typename T, int LPA, bool ZHOU>
+__global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *__restrict__ row_off,
+                                                         const int *__restrict__ nbr, EamDev E,
+                                                         double *__restrict__ aux) {
+    __shared__ ZTab<T> Z;
+    if (ZHOU) load_ztab<T>(E, Z);
+    const int sub = threadIdx.x & (LPA - 1);
+    const int gpb = EAM_BLOCK / LPA;
+    const double rc = E.r_cut;
+    for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
+        int i = base + threadIdx.x / LPA;
+        double acc = 0.0;
+        int si = 0;
+        if (i < S.n_atoms) {
+            si = S.types[i];
+            const double *cell = cell_of(S, i);
+            double xi = S.pos[3 * (size_t)i], yi = S.pos[3 * (size_t)i + 1], zi = S.pos[3 * (size_t)i + 2];
+            int end = row_off[i + 1];
+            for (int s = row_off[i] + sub; s < end; s += LPA) {
+                int j = nbr[s];
+                double dx, dy, dz;
+                mic_fast(cell, S.pos[3 * (size_t)j] - xi, S.pos[3 * (size_t)j + 1] - yi,
+                         S.pos[3 * (size_t)j + 2] - zi, dx, dy, dz);
+                double r = sqrt(dx * dx + dy * dy + dz * dz);
+                if (!(r < rc && r > 1e-12)) continue;
+                int sj = S.types[j];
+                if (ZHOU) {
+                    T Sw, dSw;
+                    zswitch<T>((T)r, Z.rc, Z.w, Sw, dSw);
+                    acc += (double)(zdens_only<T>(Z.sp[sj], (T)r) * Sw);
+                } else {
+                    T v, dv;
+                    feval<T>(E, E.rho_f[sj], r, v, dv);
+                    acc += (double)v;
+                }
+            }
+        }
+        acc = group_sum<LPA>(acc);
+        if (sub == 0 && i < S.n_atoms) {
+            double rb = acc > 0.0 ? acc : 0.0;
+            double F, dF;
+            embed64(E, E.F_f[si], rb, F, dF);
+            aux[2 * (size_t)i] = dF;
+            aux[2 * (size_t)i + 1] = F;
+        }
+    }
+}
+
+template <typename T, int LPA, bool ZHOU>
+__global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__restrict__ row_off,
+                                                       const int *__restrict__ nbr, EamDev E,
+                                                       const double *__restrict__ aux,
+                                                       double *__restrict__ forces,
+                                                       double *__restrict__ per_atom) {
+    __shared__ ZTab<T> Z;
+    if (ZHOU) load_ztab<T>(E, Z);
+    const int sub = threadIdx.x & (LPA - 1);
+    const int gpb = EAM_BLOCK / LPA;
+    const double rc = E.r_cut;
+    for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
+        int i = base + threadIdx.x / LPA;
+        double fx = 0, fy = 0, fz = 0, e = 0, npair = 0;
+        double vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+        if (i < S.n_atoms) {
+            int si = S.types[i];
+            double Fp_i = aux[2 * (size_t)i];
+            const double *cell = cell_of(S, i);
+            double xi = S.pos[3 * (size_t)i], yi = S.pos[3 * (size_t)i + 1], zi = S.pos[3 * (size_t)i + 2];
+            int end = row_off[i + 1];
+            for (int s = row_off[i] + sub; s < end; s += LPA) {
+                int j = nbr[s];
+                double dx, dy, dz;
+                mic_fast(cell, S.pos[3 * (size_t)j] - xi, S.pos[3 * (size_t)j + 1] - yi,
+                         S.pos[3 * (size_t)j + 2] - zi, dx, dy, dz);
+                double r = sqrt(dx * dx + dy * dy + dz * dz);
+                if (!(r < rc && r > 1e-12)) continue;
+                int sj = S.types[j];
+                npair += 1.0;
+                T phi, dphi, drho_j, drho_i;
+                if (ZHOU) {
+                    zhou_pair_terms<T>(Z, si, sj, (T)r, phi, dphi, drho_j, drho_i);
+                } else {
+                    T rj, ri;
+                    feval<T>(E, E.phi_f[si * E.ns + sj], r, phi, dphi);
+                    feval<T>(E, E.rho_f[sj], r, rj, drho_j);
+                    feval<T>(E, E.rho_f[si], r, ri, drho_i);
+                }
+                double Fp_j = aux[2 * (size_t)j];
+                T c = dphi + (T)Fp_i * drho_j + (T)Fp_j * drho_i;
+                double sc = (double)(c / (T)r);
+                double px = sc * dx, py = sc * dy, pz = sc * dz;
+                fx += px;
+                fy += py;
+                fz += pz;
+                e += 0.5 * (double)phi;
+                vxx -= 0.5 * px * dx;
+                vyy -= 0.5 * py * dy;
+                vzz -= 0.5 * pz * dz;
+                vxy -= 0.5 * px * dy;
+                vxz -= 0.5 * px * dz;
+                vyz -= 0.5 * py * dz;
+            }
+        }
+        fx = group_sum<LPA>(fx);
+        fy = group_sum<LPA>(fy);
+        fz = group_sum<LPA>(fz);
+        e = group_sum<LPA>(e);
+        vxx = group_sum<LPA>(vxx);
+        vyy = group_sum<LPA>(vyy);
+        vzz = group_sum<LPA>(vzz);
+        vxy = group_sum<LPA>(vxy);
+        vxz = group_sum<LPA>(vxz);
+        vyz = group_sum<LPA>(vyz);
+        npair = group_sum<LPA>(npair);
+        if (sub == 0 && i < S.n_atoms) {
+            forces[3 * (size_t)i] = fx;
+            forces[3 * (size_t)i + 1] = fy;
+            forces[3 * (size_t)i + 2] = fz;
+            double *pa = per_atom + (size_t)i * ATOM_ACC;
+            pa[0] = e + aux[2 * (size_t)i + 1];
+            pa[1] = vxx; pa[2] = vxy; pa[3] = vxz;
+            pa[4] = vxy; pa[5] = vyy; pa[6] = vyz;
+            pa[7] = vxz; pa[8] = vyz; pa[9] = vzz;
+            pa[10] = npair;
+        }
+    }
+}
+
+template <typename T, int LPA, bool ZHOU>
+static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, double *aux,
+                      double *forces, double *per_atom, cudaStream_t st) {
+    int gpb = EAM_BLOCK / LPA;
+    int blocks = (S.n_atoms + gpb - 1) / gpb;
+    int g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_density<T, LPA, ZHOU>);
+    PROF_BEGIN("eam_density", st);
+    eam_density<T, LPA, ZHOU><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, E, aux);
+    PROF_END("eam_density", st);
+    MBF_CHECK_LAUNCH();
+    g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_force<T, LPA, ZHOU>);
+    PROF_BEGIN("eam_force", st);
+    eam_force<T, LPA, ZHOU><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, E, aux, forces, per_atom);
+    PROF_END("eam_force", st);
+    MBF_CHECK_LAUNCH();
+    return MBF_OK;
+}
+
+template <typename T, bool ZHOU>
+static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E,
+                            double *aux, double *forces, double *per_atom, cudaStream_t st) {
+    switch (lpa) {
+        case 4: return eam_launch<T, 4, ZHOU>(S, nl, E, aux, forces, per_atom, st);
+        case 8: return eam_launch<T, 8, ZHOU>(S, nl, E, aux, forces, per_atom, st);
+        case 16: return eam_launch<T, 16, ZHOU>(S, nl, E, aux, forces, per_atom, st);
+        case 32: return eam_launch<T, 32, ZHOU>(S, nl, E, aux, forces, per_atom, st);
+        default: return MBF_ERR_ARGUMENT;
+    }
+}
+
+}  // namespace mbf
+
+using namespace mbf;
+
+extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                            const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
+                            void *workspace, size_t workspace_bytes, double *forces, double *energy,
+                            double *virial, void *stream) {
+    if (!sys || !nl || !tab || !plan || !workspace || !forces || !energy || !virial) return MBF_ERR_ARGUMENT;
+    if (precision != MBF_FP64 && precision != MBF_MIXED) return MBF_ERR_ARGUMENT;
+    if (nl->n_atoms != sys->n_atoms || tab->ns <= 0) return MBF_ERR_ARGUMENT;
+    EvalLayout L = eval_layout(sys->n_atoms, nl->n_slots, plan->n_chunks);
+    if (workspace_bytes < L.total) return MBF_ERR_WORKSPACE;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (sys->n_atoms == 0) {
+        if (cudaMemsetAsync(energy, 0, sizeof(double) * sys->n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
+        if (cudaMemsetAsync(virial, 0, sizeof(double) * 9 * sys->n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
+        return MBF_OK;
+    }
+    SysView S = make_view(sys);
+    EamDev E;
+    E.ns = tab->ns; E.nf = tab->nf; E.nX = tab->nX;
+    E.codes = tab->codes; E.P = tab->P; E.xo = tab->xo; E.nx = tab->nx;
+    E.X = tab->X; E.C = tab->C;
+    E.rho_f = tab->rho_f; E.F_f = tab->F_f; E.phi_f = tab->phi_f;
+    E.r_cut = tab->r_cut;
+    double *aux = ws_at<double>(workspace, L.atom_aux);
+    double *per_atom = ws_at<double>(workspace, L.per_atom);
+    double *partial = ws_at<double>(workspace, L.partial);
+    int lpa = lanes_per_atom > 0 ? lanes_per_atom : 8;
+    bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
+    int rc;
+    if (precision == MBF_FP64)
+        rc = zhou ? eam_dispatch_lpa<double, true>(lpa, S, nl, E, aux, forces, per_atom, st)
+                  : eam_dispatch_lpa<double, false>(lpa, S, nl, E, aux, forces, per_atom, st);
+    else
+        rc = zhou ? eam_dispatch_lpa<float, true>(lpa, S, nl, E, aux, forces, per_atom, st)
+                  : eam_dispatch_lpa<float, false>(lpa, S, nl, E, aux, forces, per_atom, st);
+    if (rc != MBF_OK) return rc;
+    return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
+}

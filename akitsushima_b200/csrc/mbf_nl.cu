@@ -1,0 +1,423 @@
+// Cell-list neighbour list: binning by integer counting sort, two-way CSR
+// by count -> scan -> fill, rows sorted ascending, reverse-slot index.
+//
+// Replaces engine/neighborlist.py:935-1024 (_build_cell_linked), :312-373
+// (_cell_linked_pairs_numpy), :1166-1181 (_canonical_pair_order) and the
+// two-way CSR of engine/tersoff.py:1297-1307.  The pair test reproduces the
+// reference's rounding exactly (mic_exact), so the pair set is bit-exact.
+#include "mbf_util.cuh"
+
+namespace mbf {
+
+constexpr int NL_WARPS = 4;        // warps per block in the search kernels
+constexpr int NL_MAXROW = 1024;    // longest row the sort stages in shared memory
+
+struct NlLayout {
+    size_t err, atom_cell, cell_count, cell_start, cursor, cell_atoms, row_cnt, maxrow, scan, total;
+};
+
+static NlLayout nl_layout(int n_atoms, int n_cells) {
+    NlLayout L;
+    size_t o = 0;
+    L.err = o;
+    o = align256(o + 64);
+    L.atom_cell = o;
+    o = align256(o + sizeof(int) * (size_t)n_atoms);
+    L.cell_count = o;
+    o = align256(o + sizeof(int) * (size_t)n_cells);
+    L.cell_start = o;
+    o = align256(o + sizeof(int) * ((size_t)n_cells + 1));
+    L.cursor = o;
+    o = align256(o + sizeof(int) * (size_t)n_cells);
+    L.cell_atoms = o;
+    o = align256(o + sizeof(int) * (size_t)n_atoms);
+    L.row_cnt = o;
+    o = align256(o + sizeof(int) * (size_t)n_atoms);
+    L.maxrow = o;
+    o = align256(o + 64);
+    L.scan = o;
+    int nmax = n_atoms > n_cells ? n_atoms : n_cells;
+    o = align256(o + sizeof(int) * scan_workspace_ints(nmax + 1));
+    L.total = o;
+    return L;
+}
+
+// Bin every atom: fractional coordinate wrapped to [0, 1), sub-cell index
+// floor(frac * nc) clipped to [0, nc - 1] (engine/neighborlist.py:982-989).
+__global__ void nl_assign(SysView S, const int *__restrict__ grids, int *__restrict__ atom_cell,
+                          int *__restrict__ cell_count) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= S.n_atoms) return;
+    int s = S.n_struct > 1 ? S.atom_struct[a] : 0;
+    const int *g = grids + 8 * s;
+    const double *inv = S.cells + 18 * (size_t)s + 9;
+    double x = S.pos[3 * (size_t)a], y = S.pos[3 * (size_t)a + 1], z = S.pos[3 * (size_t)a + 2];
+    int ci[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double f = x * inv[k] + y * inv[3 + k] + z * inv[6 + k];
+        f = f - floor(f);
+        int c = (int)floor(f * (double)g[k]);
+        c = c < 0 ? 0 : (c > g[k] - 1 ? g[k] - 1 : c);
+        ci[k] = c;
+    }
+    int cell = g[3] + (ci[0] * g[1] + ci[1]) * g[2] + ci[2];
+    atom_cell[a] = cell;
+    atomicAdd(cell_count + cell, 1);
+}
+
+__global__ void nl_fill_cells(int n_atoms, const int *__restrict__ atom_cell, int *__restrict__ cursor,
+                              int *__restrict__ cell_atoms) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    int p = atomicAdd(cursor + atom_cell[a], 1);
+    cell_atoms[p] = a;
+}
+
+// Each cell's atoms in ascending index order, so the traversal below (and
+// the rows it produces) do not depend on the order of the atomics above.
+__global__ void nl_sort_cells(int n_cells, const int *__restrict__ cell_start, int *__restrict__ cell_atoms) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_cells) return;
+    int b = cell_start[c], e = cell_start[c + 1];
+    for (int i = b + 1; i < e; ++i) {
+        int v = cell_atoms[i];
+        int j = i - 1;
+        while (j >= b && cell_atoms[j] > v) {
+            cell_atoms[j + 1] = cell_atoms[j];
+            --j;
+        }
+        cell_atoms[j + 1] = v;
+    }
+}
+
+// Stencil of atom a's cell: up to 27 neighbour cells (per-axis offsets
+// {0} for nc = 1, {0, 1} for nc = 2, {-1, 0, 1} otherwise -- the reference's
+// _axis_offsets, engine/neighborlist.py:270-299), visited in (da, db, dc)
+// order.  Lane k < K describes cell k; returns the warp-wide candidate count.
+struct Stencil {
+    int start[32];
+    int pre[33];
+};
+
+__device__ int build_stencil(const SysView &S, const int *__restrict__ grids,
+                             const int *__restrict__ cell_start, const int *__restrict__ atom_cell,
+                             int a, Stencil &st) {
+    int lane = threadIdx.x & 31;
+    int s = S.n_struct > 1 ? S.atom_struct[a] : 0;
+    const int *g = grids + 8 * s;
+    int nc0 = g[0], nc1 = g[1], nc2 = g[2], first = g[3];
+    int w0 = g[4], w1 = g[5], w2 = g[6];
+    int local = atom_cell[a] - first;
+    int c2 = local % nc2, c1 = (local / nc2) % nc1, c0 = local / (nc1 * nc2);
+    int K = w0 * w1 * w2;
+    int len = 0, start = 0;
+    if (lane < K) {
+        int i0 = lane / (w1 * w2), i1 = (lane / w2) % w1, i2 = lane % w2;
+        int o0 = w0 == 3 ? i0 - 1 : i0, o1 = w1 == 3 ? i1 - 1 : i1, o2 = w2 == 3 ? i2 - 1 : i2;
+        int j0 = (c0 + o0 + nc0) % nc0, j1 = (c1 + o1 + nc1) % nc1, j2 = (c2 + o2 + nc2) % nc2;
+        int cell = first + (j0 * nc1 + j1) * nc2 + j2;
+        start = cell_start[cell];
+        len = cell_start[cell + 1] - start;
+    }
+    int inc = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(MBF_FULL, inc, o);
+        if (lane >= o) inc += t;
+    }
+    st.start[lane] = start;
+    st.pre[lane] = inc - len;
+    int total = __shfl_sync(MBF_FULL, inc, 31);
+    if (lane == 0) st.pre[32] = total;
+    __syncwarp();
+    return total;
+}
+
+// Candidate t of the stencil -> atom index (binary search over the prefix).
+__device__ __forceinline__ int stencil_atom(const Stencil &st, const int *__restrict__ cell_atoms, int t) {
+    int lo = 0, hi = 31;
+    while (lo < hi) {  // largest k with pre[k] <= t
+        int mid = (lo + hi + 1) >> 1;
+        if (st.pre[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    // skip empty cells that share the same prefix value
+    return cell_atoms[st.start[lo] + (t - st.pre[lo])];
+}
+
+__device__ __forceinline__ bool is_pair(const SysView &S, const double *cell, int a, int b, double rl2) {
+    if (b == a) return false;
+    double dx, dy, dz;
+    pair_vec(S, cell, a, b, dx, dy, dz);
+    double r2 = r2_exact(dx, dy, dz);
+    return r2 < rl2 && r2 > 1e-20;
+}
+
+// Warp per atom: count the neighbours within r_list.
+__global__ void nl_count(SysView S, const int *__restrict__ grids, const int *__restrict__ cell_start,
+                         const int *__restrict__ cell_atoms, const int *__restrict__ atom_cell,
+                         double rl2, int *__restrict__ row_cnt, int *__restrict__ max_row) {
+    __shared__ Stencil sst[NL_WARPS];
+    int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Stencil &st = sst[wid];
+    for (int a = blockIdx.x * NL_WARPS + wid; a < S.n_atoms; a += gridDim.x * NL_WARPS) {
+        int total = build_stencil(S, grids, cell_start, atom_cell, a, st);
+        const double *cell = cell_of(S, a);
+        int cnt = 0;
+        for (int t = lane; t < total; t += 32) {
+            // stencil_atom needs pre[] sorted; empty cells have pre equal to the
+            // next cell's, and the search returns the last such cell, whose
+            // range contains t.
+            int b = stencil_atom(st, cell_atoms, t);
+            cnt += is_pair(S, cell, a, b, rl2) ? 1 : 0;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(MBF_FULL, cnt, o);
+        if (lane == 0) {
+            row_cnt[a] = cnt;
+            atomicMax(max_row, cnt);
+        }
+        __syncwarp();
+    }
+}
+
+// Warp per atom: write the neighbours (traversal order, by ballot), then
+// sort the row ascending by rank in shared memory.
+__global__ void nl_fill(SysView S, const int *__restrict__ grids, const int *__restrict__ cell_start,
+                        const int *__restrict__ cell_atoms, const int *__restrict__ atom_cell, double rl2,
+                        const int *__restrict__ row_off, int *__restrict__ nbr, int *__restrict__ err) {
+    __shared__ Stencil sst[NL_WARPS];
+    __shared__ int srow[NL_WARPS][NL_MAXROW];
+    int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Stencil &st = sst[wid];
+    int *row = srow[wid];
+    for (int a = blockIdx.x * NL_WARPS + wid; a < S.n_atoms; a += gridDim.x * NL_WARPS) {
+        int total = build_stencil(S, grids, cell_start, atom_cell, a, st);
+        const double *cell = cell_of(S, a);
+        int beg = row_off[a], n = row_off[a + 1] - beg;
+        int w = 0;
+        int rounds = (total + 31) & ~31;
+        for (int t = lane; t < rounds; t += 32) {
+            int b = -1;
+            bool hit = false;
+            if (t < total) {
+                b = stencil_atom(st, cell_atoms, t);
+                hit = is_pair(S, cell, a, b, rl2);
+            }
+            unsigned m = __ballot_sync(MBF_FULL, hit);
+            if (hit) {
+                int pos = w + __popc(m & ((1u << lane) - 1u));
+                if (pos < n) nbr[beg + pos] = b;
+            }
+            w += __popc(m);
+        }
+        __syncwarp();
+        if (n > NL_MAXROW) {
+            if (lane == 0) atomicOr(err, MBF_DEV_ROW_TOO_LONG);
+            continue;
+        }
+        for (int k = lane; k < n; k += 32) row[k] = nbr[beg + k];
+        __syncwarp();
+        for (int k = lane; k < n; k += 32) {
+            int v = row[k], rank = 0;
+            for (int q = 0; q < n; ++q) rank += row[q] < v ? 1 : 0;
+            nbr[beg + rank] = v;
+        }
+        __syncwarp();
+    }
+}
+
+// Reverse slot of every slot: rows are sorted, so binary search for a in
+// the row of b.
+__global__ void nl_reverse(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ nbr,
+                           int *__restrict__ rev, int *__restrict__ err) {
+    int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int a = blockIdx.x * NL_WARPS + wid; a < n_atoms; a += gridDim.x * NL_WARPS) {
+        for (int s = row_off[a] + lane; s < row_off[a + 1]; s += 32) {
+            int b = nbr[s];
+            int lo = row_off[b], hi = row_off[b + 1] - 1, found = -1;
+            while (lo <= hi) {
+                int mid = (lo + hi) >> 1;
+                int v = nbr[mid];
+                if (v == a) { found = mid; break; }
+                if (v < a) lo = mid + 1; else hi = mid - 1;
+            }
+            if (found < 0) {
+                atomicOr(err, MBF_DEV_BAD_INDEX);
+                found = s;
+            }
+            rev[s] = found;
+        }
+    }
+}
+
+// Per-structure largest minimum-image displacement from the reference
+// positions mapped by the lattice change (engine/neighborlist.py:661-668).
+__global__ void nl_max_disp(SysView S, const double *__restrict__ ref, const double *__restrict__ maps,
+                            unsigned long long *__restrict__ dmax_bits) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= S.n_atoms) return;
+    int s = S.n_struct > 1 ? S.atom_struct[a] : 0;
+    const double *M = maps + 9 * (size_t)s;
+    const double *r0 = ref + 3 * (size_t)a;
+    double ax = r0[0] * M[0] + r0[1] * M[3] + r0[2] * M[6];
+    double ay = r0[0] * M[1] + r0[1] * M[4] + r0[2] * M[7];
+    double az = r0[0] * M[2] + r0[1] * M[5] + r0[2] * M[8];
+    double dx, dy, dz;
+    mic_exact(S.cells + 18 * (size_t)s, S.pos[3 * (size_t)a] - ax, S.pos[3 * (size_t)a + 1] - ay,
+              S.pos[3 * (size_t)a + 2] - az, dx, dy, dz);
+    double d = sqrt(dx * dx + dy * dy + dz * dz);
+    atomicMax(dmax_bits + s, (unsigned long long)__double_as_longlong(d));
+}
+
+__global__ void nl_upper_count(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ nbr,
+                               int *__restrict__ up) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    int c = 0;
+    for (int s = row_off[a]; s < row_off[a + 1]; ++s) c += nbr[s] > a ? 1 : 0;
+    up[a] = c;
+}
+
+__global__ void nl_upper_write(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ nbr,
+                               const int *__restrict__ up_off, int *__restrict__ pi, int *__restrict__ pj) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    int o = up_off[a];
+    for (int s = row_off[a]; s < row_off[a + 1]; ++s) {
+        int b = nbr[s];
+        if (b > a) {
+            pi[o] = a;
+            pj[o] = b;
+            ++o;
+        }
+    }
+}
+
+}  // namespace mbf
+
+using namespace mbf;
+
+extern "C" {
+
+size_t mbf_nl_workspace_bytes(int n_atoms, int n_cells_total) {
+    return nl_layout(n_atoms, n_cells_total).total;
+}
+
+int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total, double r_list,
+                 void *workspace, size_t workspace_bytes, int *row_off, int *nbr, int *rev,
+                 long long nbr_capacity, long long *n_slots, int *max_row, void *stream) {
+    if (!sys || !grids || !workspace || !row_off || !n_slots || !max_row || sys->n_atoms < 0 ||
+        n_cells_total <= 0 || !(r_list > 0.0))
+        return MBF_ERR_ARGUMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    int N = sys->n_atoms;
+    NlLayout L = nl_layout(N, n_cells_total);
+    if (workspace_bytes < L.total) return MBF_ERR_WORKSPACE;
+    SysView S = make_view(sys);
+    int *err = ws_at<int>(workspace, L.err);
+    int *atom_cell = ws_at<int>(workspace, L.atom_cell);
+    int *cell_count = ws_at<int>(workspace, L.cell_count);
+    int *cell_start = ws_at<int>(workspace, L.cell_start);
+    int *cursor = ws_at<int>(workspace, L.cursor);
+    int *cell_atoms = ws_at<int>(workspace, L.cell_atoms);
+    int *row_cnt = ws_at<int>(workspace, L.row_cnt);
+    int *mrow = ws_at<int>(workspace, L.maxrow);
+    int *scan_ws = ws_at<int>(workspace, L.scan);
+    if (cudaMemsetAsync(err, 0, 64, st) != cudaSuccess) return MBF_ERR_CUDA;
+    if (cudaMemsetAsync(mrow, 0, sizeof(int), st) != cudaSuccess) return MBF_ERR_CUDA;
+    if (cudaMemsetAsync(cell_count, 0, sizeof(int) * (size_t)n_cells_total, st) != cudaSuccess)
+        return MBF_ERR_CUDA;
+    if (N == 0) {
+        if (cudaMemsetAsync(row_off, 0, sizeof(int), st) != cudaSuccess) return MBF_ERR_CUDA;
+        *n_slots = 0;
+        *max_row = 0;
+        return MBF_OK;
+    }
+    PROF_BEGIN("nl_assign", st);
+    nl_assign<<<(N + 255) / 256, 256, 0, st>>>(S, grids, atom_cell, cell_count);
+    PROF_END("nl_assign", st);
+    MBF_CHECK_LAUNCH();
+    int rc = exclusive_scan(cell_count, cell_start, n_cells_total, scan_ws, st);
+    if (rc != MBF_OK) return rc;
+    if (cudaMemcpyAsync(cursor, cell_start, sizeof(int) * (size_t)n_cells_total,
+                        cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return MBF_ERR_CUDA;
+    nl_fill_cells<<<(N + 255) / 256, 256, 0, st>>>(N, atom_cell, cursor, cell_atoms);
+    nl_sort_cells<<<(n_cells_total + 127) / 128, 128, 0, st>>>(n_cells_total, cell_start, cell_atoms);
+    MBF_CHECK_LAUNCH();
+    double rl2 = r_list * r_list;
+    int blocks = (N + NL_WARPS - 1) / NL_WARPS;
+    int g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_count);
+    PROF_BEGIN("nl_count", st);
+    nl_count<<<g, 32 * NL_WARPS, 0, st>>>(S, grids, cell_start, cell_atoms, atom_cell, rl2, row_cnt, mrow);
+    PROF_END("nl_count", st);
+    MBF_CHECK_LAUNCH();
+    rc = exclusive_scan(row_cnt, row_off, N, scan_ws, st);
+    if (rc != MBF_OK) return rc;
+    int host[2];
+    if (cudaMemcpyAsync(&host[0], row_off + N, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(&host[1], mrow, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return MBF_ERR_CUDA;
+    *n_slots = host[0];
+    *max_row = host[1];
+    if ((long long)host[0] > nbr_capacity || !nbr || !rev) return MBF_ERR_CAPACITY;
+    if (host[1] > NL_MAXROW) return MBF_ERR_ROW_TOO_LONG;
+    g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_fill);
+    PROF_BEGIN("nl_fill", st);
+    nl_fill<<<g, 32 * NL_WARPS, 0, st>>>(S, grids, cell_start, cell_atoms, atom_cell, rl2, row_off, nbr, err);
+    PROF_END("nl_fill", st);
+    MBF_CHECK_LAUNCH();
+    g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_reverse);
+    PROF_BEGIN("nl_reverse", st);
+    nl_reverse<<<g, 32 * NL_WARPS, 0, st>>>(N, row_off, nbr, rev, err);
+    PROF_END("nl_reverse", st);
+    MBF_CHECK_LAUNCH();
+    int herr = 0;
+    if (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return MBF_ERR_CUDA;
+    if (herr & MBF_DEV_ROW_TOO_LONG) return MBF_ERR_ROW_TOO_LONG;
+    if (herr) return MBF_ERR_ARGUMENT;
+    return MBF_OK;
+}
+
+int mbf_nl_max_displacement(const mbf_system *sys, const double *ref_positions, const double *maps,
+                            double *d_max, void *stream) {
+    if (!sys || !ref_positions || !maps || !d_max) return MBF_ERR_ARGUMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    SysView S = make_view(sys);
+    if (cudaMemsetAsync(d_max, 0, sizeof(double) * (size_t)sys->n_struct, st) != cudaSuccess)
+        return MBF_ERR_CUDA;
+    if (sys->n_atoms == 0) return MBF_OK;
+    nl_max_disp<<<(sys->n_atoms + 255) / 256, 256, 0, st>>>(S, ref_positions, maps,
+                                                            (unsigned long long *)d_max);
+    MBF_CHECK_LAUNCH();
+    return MBF_OK;
+}
+
+size_t mbf_nl_half_workspace_bytes(int n_atoms) {
+    return sizeof(int) * ((size_t)2 * n_atoms + 2 + scan_workspace_ints(n_atoms + 1)) + 256;
+}
+
+int mbf_nl_half_pairs(const mbf_nlist *nl, int *pair_i, int *pair_j, void *workspace,
+                      size_t workspace_bytes, void *stream) {
+    if (!nl || !pair_i || !pair_j || !workspace) return MBF_ERR_ARGUMENT;
+    int N = nl->n_atoms;
+    if (workspace_bytes < mbf_nl_half_workspace_bytes(N)) return MBF_ERR_WORKSPACE;
+    if (N == 0) return MBF_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    int *up = (int *)workspace;
+    int *up_off = up + N;
+    int *scan_ws = up_off + N + 2;
+    nl_upper_count<<<(N + 255) / 256, 256, 0, st>>>(N, nl->row_off, nl->nbr, up);
+    MBF_CHECK_LAUNCH();
+    int rc = exclusive_scan(up, up_off, N, scan_ws, st);
+    if (rc != MBF_OK) return rc;
+    nl_upper_write<<<(N + 255) / 256, 256, 0, st>>>(N, nl->row_off, nl->nbr, up_off, pair_i, pair_j);
+    MBF_CHECK_LAUNCH();
+    return MBF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,220 @@
+// Scan, per-structure reduction and small utilities shared by the kernels.
+#include "mbf_util.cuh"
+
+namespace mbf {
+
+int persistent_grid(int blocks_needed, int block, const void *kernel, size_t smem) {
+    static int n_sm = 0;
+    if (n_sm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+        if (n_sm <= 0) n_sm = 148;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess ||
+        per_sm <= 0)
+        per_sm = 1;
+    int g = n_sm * per_sm;
+    if (blocks_needed < g) g = blocks_needed;
+    return g > 0 ? g : 1;
+}
+
+// ---- exclusive scan of int32 (n + 1 outputs: out[n] = total) -------------
+
+constexpr int SCAN_BLOCK = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
+
+__device__ __forceinline__ int warp_incl_scan(int v) {
+    int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(MBF_FULL, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan of one value per thread; returns the block total.
+__device__ int block_excl_scan(int v, int &excl) {
+    __shared__ int warp_tot[32];
+    __shared__ int block_tot;
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int inc = warp_incl_scan(v);
+    if (lane == 31) warp_tot[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = blockDim.x >> 5;
+        int t = lane < nw ? warp_tot[lane] : 0;
+        int ti = warp_incl_scan(t);
+        if (lane < nw) warp_tot[lane] = ti - t;
+        if (lane == 31) block_tot = ti;  // nw <= 32
+    }
+    __syncthreads();
+    excl = inc - v + warp_tot[wid];
+    int total = block_tot;
+    __syncthreads();
+    return total;
+}
+
+__global__ void scan_tiles(const int *__restrict__ in, int *__restrict__ out, int n,
+                           int *__restrict__ tile_sums) {
+    int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        v[k] = (base + k < n) ? in[base + k] : 0;
+        s += v[k];
+    }
+    int excl;
+    int total = block_excl_scan(s, excl);
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        if (base + k < n) out[base + k] = excl;
+        excl += v[k];
+    }
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// One block: exclusive scan of the tile sums in place; writes the grand
+// total to *total.
+__global__ void scan_tile_sums(int *__restrict__ tile_sums, int n_tiles, int *__restrict__ total) {
+    int carry = 0;
+    for (int base = 0; base < n_tiles; base += blockDim.x) {
+        int i = base + threadIdx.x;
+        int v = i < n_tiles ? tile_sums[i] : 0;
+        int excl;
+        int t = block_excl_scan(v, excl);
+        if (i < n_tiles) tile_sums[i] = excl + carry;
+        carry += t;
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void scan_add(int *__restrict__ out, int n, const int *__restrict__ tile_sums,
+                         const int *__restrict__ total) {
+    int base = blockIdx.x * SCAN_TILE;
+    int add = tile_sums[blockIdx.x];
+    for (int k = threadIdx.x; k < SCAN_TILE; k += blockDim.x) {
+        int i = base + k;
+        if (i < n) out[i] += add;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = *total;
+}
+
+size_t scan_workspace_ints(int n) { return (size_t)(n + SCAN_TILE - 1) / SCAN_TILE + 2; }
+
+int exclusive_scan(const int *in, int *out, int n, int *ws, cudaStream_t st) {
+    int n_tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (n_tiles == 0) n_tiles = 1;
+    int *tile_sums = ws;
+    int *total = ws + n_tiles;
+    scan_tiles<<<n_tiles, SCAN_BLOCK, 0, st>>>(in, out, n, tile_sums);
+    scan_tile_sums<<<1, SCAN_BLOCK, 0, st>>>(tile_sums, n_tiles, total);
+    scan_add<<<n_tiles, 256, 0, st>>>(out, n, tile_sums, total);
+    MBF_CHECK_LAUNCH();
+    return MBF_OK;
+}
+
+// ---- per-structure reduction of per-atom (energy, virial[9]) -------------
+
+constexpr int RED_BLOCK = 256;
+
+__global__ void reduce_chunks(const double *__restrict__ per_atom, const int *__restrict__ chunk,
+                              int n_chunks, double *__restrict__ partial) {
+    __shared__ double sh[RED_BLOCK];
+    int c = blockIdx.x;
+    if (c >= n_chunks) return;
+    int a0 = chunk[3 * c + 1], a1 = chunk[3 * c + 2];
+    for (int q = 0; q < ATOM_ACC; ++q) {
+        double s = 0.0;
+        for (int a = a0 + threadIdx.x; a < a1; a += RED_BLOCK) s += per_atom[(size_t)a * ATOM_ACC + q];
+        sh[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = RED_BLOCK / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) partial[(size_t)c * ATOM_ACC + q] = sh[0];
+        __syncthreads();
+    }
+}
+
+__global__ void reduce_structs(const double *__restrict__ partial, const int *__restrict__ chunk_first,
+                               int n_struct, double *__restrict__ energy, double *__restrict__ virial) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_struct) return;
+    double acc[ATOM_ACC];
+    for (int q = 0; q < ATOM_ACC; ++q) acc[q] = 0.0;
+    for (int c = chunk_first[s]; c < chunk_first[s + 1]; ++c)
+        for (int q = 0; q < ATOM_ACC; ++q) acc[q] += partial[(size_t)c * ATOM_ACC + q];
+    energy[s] = acc[10] > 0.0 ? acc[0] : 0.0;
+    for (int q = 0; q < 9; ++q) virial[9 * s + q] = acc[1 + q];
+}
+
+int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, int n_struct,
+                         double *partial, double *energy, double *virial, cudaStream_t st) {
+    if (plan->n_chunks <= 0) return MBF_ERR_ARGUMENT;
+    PROF_BEGIN("reduce_chunks", st);
+    reduce_chunks<<<plan->n_chunks, RED_BLOCK, 0, st>>>(per_atom, plan->chunk, plan->n_chunks, partial);
+    PROF_END("reduce_chunks", st);
+    reduce_structs<<<(n_struct + 127) / 128, 128, 0, st>>>(partial, plan->chunk_first, n_struct,
+                                                           energy, virial);
+    MBF_CHECK_LAUNCH();
+    return MBF_OK;
+}
+
+// Gather the three-body forces a centre left on its neighbours: F_a +=
+// sum over slots (a -> x) of G[rev(a -> x)], the force on a from centre x.
+__global__ void gather_slot_forces(int n_atoms, const int *__restrict__ row_off,
+                                   const int *__restrict__ rev, const double *__restrict__ G,
+                                   const double *__restrict__ f_local, double *__restrict__ forces) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    double fx = f_local[3 * (size_t)a], fy = f_local[3 * (size_t)a + 1], fz = f_local[3 * (size_t)a + 2];
+    for (int s = row_off[a]; s < row_off[a + 1]; ++s) {
+        int r = rev[s];
+        fx += G[3 * (size_t)r];
+        fy += G[3 * (size_t)r + 1];
+        fz += G[3 * (size_t)r + 2];
+    }
+    forces[3 * (size_t)a] = fx;
+    forces[3 * (size_t)a + 1] = fy;
+    forces[3 * (size_t)a + 2] = fz;
+}
+
+int gather_forces(int n_atoms, const int *row_off, const int *rev, const double *G,
+                  const double *f_local, double *forces, cudaStream_t st) {
+    PROF_BEGIN("gather_forces", st);
+    gather_slot_forces<<<(n_atoms + 255) / 256, 256, 0, st>>>(n_atoms, row_off, rev, G, f_local, forces);
+    PROF_END("gather_forces", st);
+    MBF_CHECK_LAUNCH();
+    return MBF_OK;
+}
+
+}  // namespace mbf
+
+extern "C" {
+
+const char *mbf_error_string(int code) {
+    switch (code) {
+        case MBF_OK: return "ok";
+        case MBF_ERR_ARGUMENT: return "invalid argument";
+        case MBF_ERR_CUDA: return "CUDA runtime error";
+        case MBF_ERR_CAPACITY: return "neighbour capacity too small";
+        case MBF_ERR_ROW_TOO_LONG: return "neighbour row longer than the kernel's staging limit";
+        case MBF_ERR_WORKSPACE: return "workspace too small";
+        case MBF_ERR_SCRATCH_LIMIT: return "size beyond the no-allocation entry point's limit";
+        default: return "unknown error";
+    }
+}
+
+int mbf_version(void) { return 10000; }
+
+size_t mbf_eval_workspace_bytes(int n_atoms, long long n_slots, int n_chunks) {
+    return mbf::eval_layout(n_atoms, n_slots, n_chunks).total;
+}
+
+}  // extern "C"

@@ -1,0 +1,79 @@
+// Internal helpers shared by the kernel files (scan, reductions, layouts).
+#pragma once
+
+#include "mbf_common.cuh"
+
+namespace mbf {
+
+// Per-atom accumulators written by every evaluation: energy, virial[9] and
+// the number of neighbours inside the cutoff.  A structure with no pair
+// inside the cutoff gets energy 0, as the reference returns early then
+// (engine/eam.py:237-238, engine/tersoff.py:1293-1294).
+constexpr int ATOM_ACC = 11;
+
+size_t scan_workspace_ints(int n);
+// Exclusive scan of n ints into out[0..n]; out[n] is the total.  `ws` needs
+// scan_workspace_ints(n) ints.
+int exclusive_scan(const int *in, int *out, int n, int *ws, cudaStream_t st);
+
+int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, int n_struct,
+                         double *partial, double *energy, double *virial, cudaStream_t st);
+
+int gather_forces(int n_atoms, const int *row_off, const int *rev, const double *G,
+                  const double *f_local, double *forces, cudaStream_t st);
+
+// Layout of the evaluation workspace (all offsets 256-byte aligned):
+//   err      device error word (int)
+//   per_atom (n_atoms, ATOM_ACC) doubles
+//   f_local  (n_atoms, 3) doubles (three-body potentials: centre-local force)
+//   atom_aux (n_atoms, 2) doubles (EAM F'(rho), F(rho))
+//   slot     (n_slots, 3) doubles (three-body force left on each neighbour)
+//   slot_b   (n_slots, 2) doubles (Tersoff bond order and its derivative)
+//   partial  (n_chunks, ATOM_ACC) doubles
+struct EvalLayout {
+    size_t err, per_atom, f_local, atom_aux, slot, slot_b, partial, total;
+};
+
+static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static inline EvalLayout eval_layout(int n_atoms, long long n_slots, int n_chunks) {
+    EvalLayout L;
+    size_t o = 0;
+    L.err = o;
+    o = align256(o + 64);
+    L.per_atom = o;
+    o = align256(o + sizeof(double) * (size_t)n_atoms * ATOM_ACC);
+    L.f_local = o;
+    o = align256(o + sizeof(double) * (size_t)n_atoms * 3);
+    L.atom_aux = o;
+    o = align256(o + sizeof(double) * (size_t)n_atoms * 2);
+    L.slot = o;
+    o = align256(o + sizeof(double) * (size_t)n_slots * 3);
+    L.slot_b = o;
+    o = align256(o + sizeof(double) * (size_t)n_slots * 2);
+    L.partial = o;
+    o = align256(o + sizeof(double) * (size_t)(n_chunks > 0 ? n_chunks : 1) * ATOM_ACC);
+    L.total = o;
+    return L;
+}
+
+template <typename T>
+static inline T *ws_at(void *ws, size_t off) {
+    return reinterpret_cast<T *>(static_cast<char *>(ws) + off);
+}
+
+}  // namespace mbf
+
+// ---- launch profiler (CUDA events on the launching stream) -----------------
+// Off by default; mbf_profile_begin() turns it on.  Each PROF_LAUNCH records
+// an event pair around one kernel launch; mbf_profile_end() synchronises and
+// returns per-kernel counts and total milliseconds.
+namespace mbf {
+void prof_mark(const char *name, cudaStream_t st, bool start);
+extern bool g_prof_on;
+}  // namespace mbf
+
+#define PROF_BEGIN(name, st) \
+    do { if (mbf::g_prof_on) mbf::prof_mark(name, st, true); } while (0)
+#define PROF_END(name, st) \
+    do { if (mbf::g_prof_on) mbf::prof_mark(name, st, false); } while (0)

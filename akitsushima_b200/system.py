@@ -1,0 +1,216 @@
+"""Structures on the device: one or many periodic cells concatenated.
+
+A :class:`Batch` holds the flattened atom arrays of ``n_struct`` structures
+(positions, species ids, structure id per atom), the per-structure lattice and
+inverse, and the per-structure reduction plan the kernels use to sum energy
+and virial.  A single structure is a batch of one.  Torch supplies the device
+memory and the stream; every computation runs in libmbforce.so.
+"""
+import numpy as np
+import torch
+
+from . import _lib
+
+# Atoms per reduction chunk (the per-structure energy/virial sums).
+REDUCE_CHUNK = 4096
+
+
+def cell_metrics(lattice):
+    """Perpendicular widths d_i = V / |a_j x a_k| and sigma_min of a lattice
+    (rows are lattice vectors); the reference's engine/neighborlist.py:170-267.
+    Raises ValueError for a degenerate cell."""
+    lat = np.asarray(lattice, dtype=float)
+    if lat.shape != (3, 3):
+        raise ValueError(f"NeighbourList: lattice must have shape (3, 3), got {lat.shape}.")
+    volume = abs(float(np.linalg.det(lat)))
+    cross = np.array([np.linalg.norm(np.cross(lat[(i + 1) % 3], lat[(i + 2) % 3]))
+                      for i in range(3)])
+    if volume <= 0.0 or not np.all(cross > 0.0) or not np.isfinite(volume):
+        raise ValueError(
+            f"NeighbourList: degenerate (singular) lattice with volume {volume:.6g} A^3 -- "
+            "the three lattice vectors must be linearly independent for a minimum-image "
+            "convention to exist.")
+    return volume / cross, float(np.linalg.svd(lat, compute_uv=False)[-1])
+
+
+def check_min_image(lattice, r_list, caller="NeighbourList"):
+    """Refuse r_list >= half the smallest perpendicular width
+    (engine/neighborlist.py:98-132 and :489-572)."""
+    widths, _ = cell_metrics(lattice)
+    if r_list >= float(np.min(widths)) / 2.0:
+        lengths = np.linalg.norm(np.asarray(lattice, float), axis=1)
+        raise ValueError(
+            f"{caller}: cutoff radius ({r_list:.4f} A) must be < half the smallest "
+            f"perpendicular cell width ({float(np.min(widths)) / 2.0:.4f} A) for the "
+            f"minimum-image convention to be valid. Perpendicular widths are "
+            f"[{widths[0]:.4f}, {widths[1]:.4f}, {widths[2]:.4f}] A for lattice vector "
+            f"lengths [{lengths[0]:.4f}, {lengths[1]:.4f}, {lengths[2]:.4f}] A.")
+
+
+def cell_grid(lattice, r_list):
+    """Sub-cell counts nc_i = max(1, floor(d_i / r_list))
+    (engine/neighborlist.py:976-978) and the stencil width per axis."""
+    widths, _ = cell_metrics(lattice)
+    nc = np.maximum(1, np.floor(widths / r_list).astype(int))
+    w = np.where(nc == 1, 1, np.where(nc == 2, 2, 3))
+    return nc, w
+
+
+def default_device():
+    if not torch.cuda.is_available():
+        raise RuntimeError("akitsushima_b200 needs a CUDA device (B200); none is visible.")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def species_ids(atom_types, species):
+    """Species index of every atom.  ``atom_types`` is a list / array of
+    symbols, or an integer array of indices into ``species``."""
+    a = np.asarray(atom_types)
+    if a.dtype.kind in "iu":
+        ids = a.astype(np.int32, copy=False)
+        if len(ids) and (ids.min() < 0 or ids.max() >= len(species)):
+            raise ValueError("atom type index out of range of the potential's species")
+        return ids
+    index = {s: k for k, s in enumerate(species)}
+    if len(a) == 0:
+        return np.zeros(0, np.int32)
+    uniq, inv = np.unique(a.astype(str), return_inverse=True)
+    try:
+        lut = np.array([index[str(u)] for u in uniq], np.int32)
+    except KeyError as exc:
+        raise ValueError(f"atom type {exc.args[0]!r} is not among the potential's species "
+                         f"{list(species)}") from None
+    return lut[inv.reshape(-1)]
+
+
+class Batch:
+    """``n_struct`` periodic structures flattened on one device.
+
+    Parameters
+    ----------
+    lattices  : sequence of (3, 3) row-vector lattices [A].
+    positions : sequence of (N_s, 3) Cartesian positions [A] (numpy or torch).
+    type_ids  : sequence of (N_s,) integer species ids.
+    """
+
+    def __init__(self, lattices, positions, type_ids, device=None):
+        self.device = torch.device(device) if device is not None else default_device()
+        lats = [np.asarray(l, dtype=np.float64).reshape(3, 3) for l in lattices]
+        if len(lats) == 0:
+            raise ValueError("Batch: no structures")
+        if not (len(lats) == len(positions) == len(type_ids)):
+            raise ValueError("Batch: lattices, positions and type_ids differ in length")
+        counts = [int(len(p)) for p in positions]
+        self.n_struct = len(lats)
+        self.n_atoms = int(sum(counts))
+        self.counts = np.array(counts, np.int64)
+        off = np.zeros(self.n_struct + 1, np.int64)
+        off[1:] = np.cumsum(counts)
+        self.offsets = off
+        self.lattices = np.stack(lats)
+        for lat in lats:
+            cell_metrics(lat)
+        self.volumes = np.abs(np.linalg.det(self.lattices))
+        invs = np.linalg.inv(self.lattices)
+        cells = np.concatenate([self.lattices.reshape(-1, 9), invs.reshape(-1, 9)], axis=1)
+        dev = self.device
+        self.cells = torch.as_tensor(np.ascontiguousarray(cells), device=dev)
+        self.struct_off = torch.as_tensor(off.astype(np.int32), device=dev)
+        self.atom_struct = torch.as_tensor(
+            np.repeat(np.arange(self.n_struct, dtype=np.int32), counts), device=dev)
+        self.pos = torch.empty((self.n_atoms, 3), dtype=torch.float64, device=dev)
+        self.types = torch.empty(self.n_atoms, dtype=torch.int32, device=dev)
+        self.set_positions(positions)
+        self.set_types(type_ids)
+        # reduction plan: chunks of REDUCE_CHUNK atoms inside one structure
+        chunk, first = [], [0]
+        for s in range(self.n_struct):
+            a0, a1 = int(off[s]), int(off[s + 1])
+            for c0 in range(a0, a1, REDUCE_CHUNK):
+                chunk.append((s, c0, min(a1, c0 + REDUCE_CHUNK)))
+            if a1 == a0:
+                chunk.append((s, a0, a0))
+            first.append(len(chunk))
+        self.chunk = torch.as_tensor(np.array(chunk, np.int32).reshape(-1, 3), device=dev)
+        self.chunk_first = torch.as_tensor(np.array(first, np.int32), device=dev)
+
+    @classmethod
+    def single(cls, lattice, positions, type_ids, device=None):
+        return cls([lattice], [positions], [type_ids], device=device)
+
+    def set_positions(self, positions):
+        """Copy new positions in place: one (N, 3) array or tensor for the
+        whole batch, or a sequence of (N_s, 3) arrays, one per structure."""
+        if isinstance(positions, torch.Tensor):
+            src = positions.reshape(-1, 3)
+        elif isinstance(positions, np.ndarray) and positions.ndim == 2:
+            arr = np.ascontiguousarray(positions, dtype=np.float64)
+            if not np.isfinite(arr).all():
+                raise ValueError("positions contain NaN or inf")
+            src = torch.from_numpy(arr)
+        else:
+            parts = [torch.as_tensor(np.asarray(p, np.float64)).reshape(-1, 3)
+                     if not isinstance(p, torch.Tensor) else p.reshape(-1, 3).to("cpu", torch.float64)
+                     for p in positions]
+            src = torch.cat(parts) if parts else torch.zeros((0, 3), dtype=torch.float64)
+        if tuple(src.shape) != (self.n_atoms, 3):
+            raise ValueError(f"positions have shape {tuple(src.shape)}, expected ({self.n_atoms}, 3)")
+        self.pos.copy_(src.to(torch.float64), non_blocking=src.device.type != "cpu")
+
+    def set_types(self, type_ids):
+        if isinstance(type_ids, torch.Tensor):
+            self.types.copy_(type_ids.to(torch.int32))
+            return
+        arr = np.concatenate([np.asarray(t, np.int32).reshape(-1) for t in type_ids]) \
+            if len(type_ids) else np.zeros(0, np.int32)
+        if arr.shape != (self.n_atoms,):
+            raise ValueError("type_ids do not match the atom count")
+        self.types.copy_(torch.from_numpy(arr))
+
+    def set_lattice(self, s, lattice):
+        lat = np.asarray(lattice, np.float64).reshape(3, 3)
+        cell_metrics(lat)
+        self.lattices[s] = lat
+        self.volumes[s] = abs(np.linalg.det(lat))
+        row = np.concatenate([lat.reshape(9), np.linalg.inv(lat).reshape(9)])
+        self.cells[s].copy_(torch.from_numpy(row))
+
+    def mbf_system(self):
+        s = _lib.MbfSystem(self.n_atoms, self.n_struct, _lib.ptr(self.pos), _lib.ptr(self.types),
+                           _lib.ptr(self.atom_struct), _lib.ptr(self.struct_off),
+                           _lib.ptr(self.cells))
+        return s
+
+    def reduce_plan(self):
+        return _lib.MbfReducePlan(int(self.chunk.shape[0]), _lib.ptr(self.chunk),
+                                  _lib.ptr(self.chunk_first))
+
+    @property
+    def n_chunks(self):
+        return int(self.chunk.shape[0])
+
+
+def replicate_thin(lattice, positions, type_ids, r_list):
+    """Replicate a cell along every axis whose perpendicular width is below
+    2 r_list, so the minimum image holds; returns (lattice, positions, types,
+    reps).  Energy of the original = supercell energy / prod(reps); the
+    forces of the first N atoms and the stress are unchanged (exact periodic
+    physics)."""
+    lat = np.asarray(lattice, float)
+    widths, _ = cell_metrics(lat)
+    reps = np.ones(3, int)
+    for k in range(3):
+        while widths[k] * reps[k] / 2.0 <= r_list:
+            reps[k] += 1
+    if np.all(reps == 1):
+        return lat, np.asarray(positions, float), np.asarray(type_ids, np.int32), reps
+    shifts = np.array([[a, b, c] for a in range(reps[0]) for b in range(reps[1])
+                       for c in range(reps[2])], float)
+    pos = np.asarray(positions, float)
+    big = (pos[None, :, :] + (shifts @ lat)[:, None, :]).reshape(-1, 3)
+    types = np.tile(np.asarray(type_ids, np.int32), len(shifts))
+    return lat * reps[:, None], big, types, reps
+
+
+__all__ = ["Batch", "cell_metrics", "check_min_image", "cell_grid", "species_ids",
+           "replicate_thin", "default_device"]

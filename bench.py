@@ -1,0 +1,305 @@
+"""Benchmark of the force path: atom-force-evaluations per second.
+
+Workload (default, --workload eam_cuni_256k): fcc Cu-Ni random 50/50 alloy,
+40x40x40 cubic cells = 256,000 atoms, a = 3.58 A, Gaussian displacements
+sigma = 0.08 A, Zhou (2004) alloy EAM, mixed precision (float32 pair terms,
+float64 wrap / rho-bar / embedding argument / accumulation).  Synthetic, seeded
+data in the shape of the reference's benchmarks/bench_force.py generator.
+
+A step is one energy + force + virial evaluation of the whole structure with
+a prebuilt device neighbour list (the reference's call_nl_s methodology,
+benchmarks/bench_force.py:372-409).  value = atoms / step time on the device
+(CUDA events, L2 flushed between steps outside the events), whole job over all
+ranks; e2e = the same through the public force_fn API with host numpy arrays
+(host->device positions + species, device->host forces, energy, stress inside
+the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With --gpus N > 1 (torchrun), every rank evaluates its own replica of the
+structure ("replicas only": one structure does not shard) and the time is the
+max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FCC = np.array([[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0]], float)
+METRIC = "atom-force-evals/s"
+
+
+def make_cuni(n_cells=40, a=3.58, sigma=0.08, seed=0):
+    rng = np.random.default_rng(seed)
+    g = np.arange(n_cells)
+    cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    frac = (FCC[None] + cells[:, None]).reshape(-1, 3)
+    pos = frac * a + rng.normal(0.0, sigma, frac.shape)
+    ids = np.random.default_rng(seed + 1).integers(0, 2, len(pos)).astype(np.int32)
+    return np.eye(3) * a * n_cells, pos, ids
+
+
+def cpu_count():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def clocks_start(path):
+    cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+           "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+           "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+           "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"]
+    try:
+        fh = open(path, "w")
+        return subprocess.Popen(cmd, stdout=fh, stderr=subprocess.DEVNULL), fh
+    except (OSError, FileNotFoundError):
+        return None, None
+
+
+def clocks_stop(proc_fh, path, gpu_index):
+    proc, fh = proc_fh
+    if proc is None:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+    proc.terminate()
+    try:
+        proc.wait(timeout=5)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+    fh.close()
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    with open(path) as f:
+        for line in f:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9 or p[0] != str(gpu_index):
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+    return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def time_reference(lat, pos, ids, steps, warmup):
+    """The CPU port of the reference's numba path (oracle/): numpy prep and
+    C kernels under OpenMP with every host thread, prebuilt neighbour list."""
+    import oracle
+    from akitsushima_b200.published_parameters import ZHOU_2004
+    threads = cpu_count()
+    oracle.set_threads(threads)
+    spec = oracle.zhou_spec({s: ZHOU_2004[s] for s in ("Cu", "Ni")}, ["Cu", "Ni"])
+    types = np.array(["Cu", "Ni"])[ids]
+    i, j, _, _ = oracle.nl_build(lat, pos, spec.r_cut, 0.3)
+    for _ in range(max(1, warmup)):
+        oracle.eam(spec, lat, pos, types, (i, j))
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        oracle.eam(spec, lat, pos, types, (i, j))
+        ts.append(time.perf_counter() - t0)
+    return float(np.mean(ts)), threads
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--cells", type=int, default=40)
+    ap.add_argument("--lanes", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    lat, pos, ids = make_cuni(args.cells)
+    n_atoms = len(pos)
+    workload = f"eam_zhou_cuni_fcc{args.cells}^3_{n_atoms}_atoms"
+    cfg = {"workload": workload, "potential": "Zhou 2004 EAM Cu-Ni", "n_atoms": n_atoms,
+           "a": 3.58, "sigma": 0.08, "skin": 0.3, "precision": args.precision,
+           "l2": "256 MB scratch write between steps, outside the timed events",
+           "parallelism": f"replicas{world}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        t, threads = time_reference(lat, pos, ids, args.steps, args.warmup)
+        v = n_atoms / t
+        line = {"metric": METRIC, "value": v, "unit": "atoms/s", "impl": "reference",
+                "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": dict(cfg, precision="fp64"),
+                "cpu_baseline": {"value": v, "unit": "atoms/s", "cores": threads, "kind": "port",
+                                 "sample": f"{args.steps} full force calls of the {n_atoms}-atom "
+                                           "structure, prebuilt neighbour list"},
+                "e2e": {"value": v, "unit": "atoms/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    import akitsushima_b200 as ak
+    from akitsushima_b200 import _lib, roofline
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    fn = ak.force_fn_from_config({"type": "EAM", "form": "zhou2004", "elements": ["Cu", "Ni"]},
+                                 precision=args.precision)
+    pot = fn.engine.potentials[0]
+    pot.lanes_per_atom = args.lanes
+    batch = ak.Batch.single(lat, pos, ids, device=dev)
+    dnl = ak.DeviceNeighbourList(pot.r_cut + 0.3).build(batch)
+    out = pot.evaluate(batch, dnl)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        pot.evaluate(batch, dnl, out=out)
+    torch.cuda.synchronize()
+
+    # timed region
+    clk_path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
+    os.makedirs(os.path.dirname(clk_path), exist_ok=True)
+    clk = clocks_start(clk_path)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.zero_()
+        ev[k][0].record()
+        pot.evaluate(batch, dnl, out=out)
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = clocks_stop(clk, clk_path, local)
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n_atoms / (ms * 1e-3)
+
+    # per-kernel breakdown: a second identical pass under the launch profiler
+    _lib.profile_begin()
+    for k in range(args.steps):
+        flush.zero_()
+        pot.evaluate(batch, dnl, out=out)
+    prof = _lib.profile_end()
+    launches_per_step = sum(c for c, _ in prof.values()) / args.steps
+
+    # algorithmic work of the dominant kernel (the force pass)
+    pi, pj = dnl.half_pairs()
+    pi, pj = pi.long(), pj.long()
+    d = batch.pos[pj] - batch.pos[pi]
+    cell = torch.as_tensor(lat, device=dev)
+    s = d @ torch.linalg.inv(cell)
+    s -= torch.round(s)
+    r = torch.linalg.norm(s @ cell, dim=1)
+    inside = (r < pot.r_cut) & (r > 1e-12)
+    tp = batch.types
+    cross = (tp[pi] != tp[pj]) & inside
+    n_in = int(inside.sum().item())
+    n_cross = int(cross.sum().item())
+    force_flops = roofline.eam_force_flops(n_in - n_cross, n_cross)
+    force_bytes = roofline.eam_force_bytes(n_atoms, dnl.n_slots)
+    dom = "eam_force"
+    cnt, tot = prof.get(dom, (1, float("nan")))
+    t_dom = tot / cnt * 1e-3
+    scratch = torch.empty(148 * 8 * 256 * 8 * 4, dtype=torch.uint8, device=dev)
+    peak = _lib._d(0.0)
+    pcode = _lib.MBF_MIXED if args.precision == "mixed" else _lib.MBF_FP64
+    _lib.check(_lib.lib().mbf_peak_probe(pcode, _lib.ptr(scratch), scratch.numel(), peak,
+                                         torch.cuda.current_stream().cuda_stream), "peak probe")
+    peak_tf = peak.value / 1e12
+    ach_tf = force_flops / t_dom / 1e12
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            hbm_peak = float(json.load(f)["hbm_gbs"])
+            hbm_src = "MEASURED_PEAKS.json"
+    except (OSError, KeyError, ValueError):
+        hbm_peak, hbm_src = 6650.0, "fallback"
+    ach_gbs = force_bytes / t_dom / 1e9
+    roof = {"kernel": dom, "bound": "fp32" if args.precision == "mixed" else "fp64",
+            "achieved": ach_tf, "peak": peak_tf, "unit": "TFLOP/s", "frac": ach_tf / peak_tf,
+            "peak_source": "measured live on this GPU: mbf_peak_probe FMA chains",
+            "algorithmic_flops_per_launch": force_flops, "launch_ms": t_dom * 1e3,
+            "traffic": None,
+            "hbm_view": {"achieved": ach_gbs, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": ach_gbs / hbm_peak, "peak_source": hbm_src,
+                         "algorithmic_bytes_per_launch": force_bytes},
+            "kernels": {k: {"launches": c, "ms_per_launch": t / c} for k, (c, t) in prof.items()}}
+
+    # end to end through the public API, host arrays in and out
+    nl = ak.NeighbourList(fn.r_cut, skin_width=0.3, device=dev)
+    nl.build_batch(batch)
+    pos_host = np.ascontiguousarray(pos)
+    fn(lat, pos_host, ids, nl)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e, f, st = fn(lat, pos_host, ids, nl)
+    t_e2e = (time.perf_counter() - t0) / args.e2e_steps
+    if dist:
+        t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = {"value": world * n_atoms / t_e2e, "unit": "atoms/s",
+           "h2d_bytes_per_step": n_atoms * (24 + 4), "d2h_bytes_per_step": n_atoms * 24 + 8 + 72,
+           "ms_per_step": t_e2e * 1e3, "path": "force_fn(lattice, numpy positions, species ids, "
+                                             "NeighbourList) -> numpy"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t_cpu, threads = time_reference(lat, pos, ids, steps=2, warmup=1)
+        cpu = {"value": n_atoms / t_cpu, "unit": "atoms/s", "cores": threads, "kind": "port",
+               "sample": "2 full force calls of the same structure (after 1 warm-up), oracle port "
+                         "of the reference's numba EAM path, prebuilt neighbour list"}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+            "config": cfg, "gpu_launches": int(round(launches_per_step * args.steps)),
+            "gpu_launches_per_step": launches_per_step, "clocks": clocks, "roofline": roof,
+            "e2e": e2e, "cpu_baseline": cpu,
+            "check": {"energy_per_atom": e / n_atoms, "max_abs_force_sum": float(np.abs(f.sum(0)).max())}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,220 @@
+/*
+ * mbforce.h -- C ABI of the B200 many-body force path (libmbforce.so).
+ *
+ * Plain pointers and sizes only.  Every array argument is DEVICE memory unless
+ * its comment says "host"; `stream` is a cudaStream_t passed as void*.  The
+ * library allocates nothing: callers pass workspaces sized by the *_bytes
+ * queries.  Every function returns MBF_OK (0) or a negative MBF_ERR_* code;
+ * mbf_error_string() names it.
+ *
+ * Each entry point replaces one interface of the reference (akitsushima
+ * 0.4.0a4, Python + numba); the citation is given beside it.  The reference
+ * has no native ABI of its own, so these functions are what a ctypes / cffi
+ * binding from its Python layer would call.
+ *
+ * Units: A, eV, eV/A; the virial returned is sum over pairs of -f (x) r
+ * (eV), NOT divided by the volume -- the caller divides, as the reference does
+ * (engine/tersoff.py:1512, engine/eam.py:253).
+ *
+ * Layouts:
+ *   positions  (n_atoms, 3) float64 row-major, Cartesian
+ *   types      (n_atoms,)   int32 species index
+ *   cells      (n_struct, 18) float64: lattice rows a0 a1 a2 (9), then the
+ *              inverse lattice (9); cart = frac @ lattice
+ *   struct_off (n_struct + 1) int32 atom offsets (atoms of structure s are
+ *              struct_off[s] .. struct_off[s+1]-1); atom_struct (n_atoms,)
+ *              int32 structure id of each atom
+ *   grids      (n_struct, 8) int32: nc0 nc1 nc2, first global cell, and the
+ *              per-axis stencil widths (1 if nc == 1, 2 if nc == 2, else 3)
+ *   neighbour list: two-way CSR, row_off (n_atoms + 1) int32, nbr (n_slots)
+ *              int32 with every row sorted ascending, rev (n_slots) int32 the
+ *              slot of the reverse direction (rev[slot(a->b)] = slot(b->a)).
+ */
+#ifndef MBFORCE_H
+#define MBFORCE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MBF_OK 0
+#define MBF_ERR_ARGUMENT -1     /* bad size, null pointer or bad precision */
+#define MBF_ERR_CUDA -2         /* a CUDA runtime call failed */
+#define MBF_ERR_CAPACITY -3     /* nbr capacity too small; *n_slots holds the need */
+#define MBF_ERR_ROW_TOO_LONG -4 /* a neighbour row exceeds the kernel's staging */
+#define MBF_ERR_WORKSPACE -5    /* workspace too small */
+#define MBF_ERR_SCRATCH_LIMIT -6 /* size beyond the no-allocation entry's limit */
+
+#define MBF_FP64 0   /* all arithmetic in float64 */
+#define MBF_MIXED 1  /* bond terms in float32; wrap, accumulation, EAM rho-bar in float64 */
+
+typedef struct mbf_system {
+    int n_atoms;
+    int n_struct;
+    const double *positions;   /* (n_atoms, 3) */
+    const int *types;          /* (n_atoms,) */
+    const int *atom_struct;    /* (n_atoms,) */
+    const int *struct_off;     /* (n_struct + 1) */
+    const double *cells;       /* (n_struct, 18) */
+} mbf_system;
+
+typedef struct mbf_nlist {
+    int n_atoms;
+    long long n_slots;
+    int max_row;               /* host copy of the longest row */
+    const int *row_off;        /* (n_atoms + 1) */
+    const int *nbr;            /* (n_slots,) */
+    const int *rev;            /* (n_slots,) */
+} mbf_nlist;
+
+/* Per-structure reduction table: chunks of atoms that lie in one structure.
+ * chunk (n_chunks, 3) int32 rows (struct id, first atom, end atom);
+ * chunk_first (n_struct + 1) int32: chunks of structure s are
+ * chunk_first[s] .. chunk_first[s+1]-1. */
+typedef struct mbf_reduce_plan {
+    int n_chunks;
+    const int *chunk;
+    const int *chunk_first;
+} mbf_reduce_plan;
+
+const char *mbf_error_string(int code);
+int mbf_version(void);
+
+/* ---- neighbour list ---------------------------------------------------
+ * Replaces NeighbourList.build / _build_cell_linked / _canonical_pair_order
+ * (engine/neighborlist.py:574-585, :935-1024, :1166-1181) and the two-way CSR
+ * every potential derives from it (engine/tersoff.py:1297-1307).  A pair
+ * (a, b) is listed iff it lies in the cell stencil and r2 < r_list^2,
+ * r2 > 1e-20, with r2 from the minimum-image displacement evaluated in the
+ * reference's operation order without fused multiply-add
+ * (engine/neighborlist.py:350-363), so the pair set equals the reference's
+ * bit for bit.  n_cells_total = sum over structures of nc0*nc1*nc2.      */
+size_t mbf_nl_workspace_bytes(int n_atoms, int n_cells_total);
+
+/* Counts, scans and fills.  If nbr_capacity < the number of slots it stops
+ * after the count, stores the need in *n_slots (host) and returns
+ * MBF_ERR_CAPACITY; call again with a larger nbr/rev.  *n_slots and
+ * *max_row are host outputs.  Synchronises `stream` once (to read the
+ * count). */
+int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total,
+                 double r_list, void *workspace, size_t workspace_bytes,
+                 int *row_off, int *nbr, int *rev, long long nbr_capacity,
+                 long long *n_slots, int *max_row, void *stream);
+
+/* Largest minimum-image displacement of any atom from its reference
+ * position mapped by the lattice change (engine/neighborlist.py:653-668):
+ * writes max_i |MIC(r_i - r_ref_i @ M_s)| per structure to d_max (n_struct),
+ * M_s = inv(lattice_build_s) @ lattice_now_s given per structure as
+ * maps (n_struct, 9). */
+int mbf_nl_max_displacement(const mbf_system *sys, const double *ref_positions,
+                            const double *maps, double *d_max, void *stream);
+
+/* Canonical half list (i < j sorted by (i, j), the reference's
+ * get_candidate_pairs(), engine/neighborlist.py:679-714) extracted from the
+ * two-way CSR: pair_i/pair_j sized n_slots / 2; the workspace needs
+ * mbf_nl_half_workspace_bytes(n_atoms). */
+size_t mbf_nl_half_workspace_bytes(int n_atoms);
+int mbf_nl_half_pairs(const mbf_nlist *nl, int *pair_i, int *pair_j, void *workspace,
+                      size_t workspace_bytes, void *stream);
+
+/* ---- per-structure reduction workspace --------------------------------- */
+/* Bytes of the workspace every *_eval below needs (per-atom accumulators,
+ * per-slot three-body forces and bond orders, reduction partials). */
+size_t mbf_eval_workspace_bytes(int n_atoms, long long n_slots, int n_chunks);
+
+/* ---- EAM --------------------------------------------------------------
+ * Replaces EAMPotential.compute's numba branch (engine/eam.py:174-256) and
+ * _eam_kernel (engine/_eam_kernels.py:231-307): alloy EAM, rho-bar at an
+ * atom from its neighbours' species densities, clamped at 0.
+ * Function tables (device) as engine/_eam_kernels.py:77-121 lays them out:
+ *   codes (nf,) int32: 1 spline, 2 spline/r, 3 Zhou density, 4 Zhou pair,
+ *         5 Zhou cross pair, 6 Zhou embedding
+ *   P     (nf, 43) float64 parameter rows; spline xo/nx (nf,) int32,
+ *         X (nX,), C (4, nX)
+ *   rho_f, F_f (ns,) int32 and phi_f (ns, ns) int32 function ids.        */
+typedef struct mbf_eam_tables {
+    int ns;
+    int nf;
+    int nX;
+    const int *codes;
+    const double *P;
+    const int *xo;
+    const int *nx;
+    const double *X;
+    const double *C;
+    const int *rho_f;
+    const int *F_f;
+    const int *phi_f;
+    double r_cut;
+    /* 1 when every function is a Zhou form (codes 3..6) sharing one switch
+     * (r_c, width) and ns <= 8: the kernels then evaluate an element's
+     * density and pair function from shared exponentials.  0: generic. */
+    int zhou_fused;
+} mbf_eam_tables;
+
+int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                 const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
+                 void *workspace, size_t workspace_bytes,
+                 double *forces, double *energy, double *virial, void *stream);
+
+/* ---- Tersoff ----------------------------------------------------------
+ * Replaces TersoffPotential.compute (engine/tersoff.py:1208-1711): both the
+ * single-species flat form (m = 3, gamma = 1; :1233-1513) and the
+ * multi-species record form (:1518-1711), given as dense species tables
+ * (:1606-1653).  tb (ns*ns, 10) float64 rows [valid, A, B, lambda1, lambda2,
+ * R, D, beta, n, unused]; tri (ns*ns*ns, 8) rows [valid, c, d, h, lambda3,
+ * m, gamma, unused]. r_cut = the largest R + D.                           */
+typedef struct mbf_tersoff_tables {
+    int ns;
+    const double *tb;
+    const double *tri;
+    double r_cut;
+} mbf_tersoff_tables;
+
+int mbf_tersoff_eval(const mbf_system *sys, const mbf_nlist *nl,
+                     const mbf_tersoff_tables *tab, const mbf_reduce_plan *plan,
+                     int precision, void *workspace, size_t workspace_bytes,
+                     double *forces, double *energy, double *virial, void *stream);
+
+/* ---- Stillinger-Weber -------------------------------------------------
+ * Replaces StillingerWeberPotential.compute (engine/stillinger_weber.py:
+ * 900-1451), single- and multi-species.  tb (ns*ns, 8) rows [valid, eps,
+ * sigma, a, A, B, p, q] of the two-body records; leg (ns*ns, 4) rows
+ * [sigma, a, gamma, unused]; tri (ns*ns*ns, 4) rows [valid, eps*lambda/2,
+ * costheta0, unused].  A single-species parameter dict is the ns = 1 case
+ * with lambda halved over both neighbour orders.                         */
+typedef struct mbf_sw_tables {
+    int ns;
+    const double *tb;
+    const double *leg;
+    const double *tri;
+    double r_cut;
+} mbf_sw_tables;
+
+int mbf_sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables *tab,
+                const mbf_reduce_plan *plan, int precision, void *workspace,
+                size_t workspace_bytes, double *forces, double *energy,
+                double *virial, void *stream);
+
+/* ---- measurement ------------------------------------------------------
+ * Launch profiler: between begin and end every kernel launch of this library
+ * is bracketed by CUDA events on its stream; end() synchronises the device
+ * and writes "name launches total_ms" lines to buf.  Returns the number of
+ * kernels listed.  No counterpart in the reference (its timing is
+ * benchmarks/bench_force.py's wall clock).                                */
+void mbf_profile_begin(void);
+int mbf_profile_end(char *buf, size_t cap);
+
+/* Sustained FMA throughput (FLOP/s, 2 per FMA) of the current GPU in
+ * float64 (precision 0) or float32 (1): the compute roofline denominator.
+ * scratch >= 148 * 8 * 256 * 8 bytes of device memory. */
+int mbf_peak_probe(int precision, void *scratch, size_t scratch_bytes, double *flops,
+                   void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MBFORCE_H */
