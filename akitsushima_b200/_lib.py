@@ -31,7 +31,7 @@ class MbfSystem(ctypes.Structure):
 
 class MbfNlist(ctypes.Structure):
     _fields_ = [("n_atoms", _i), ("n_slots", _ll), ("max_row", _i), ("row_off", _vp),
-                ("nbr", _vp), ("rev", _vp)]
+                ("nbr", _vp), ("rev", _vp), ("upper", _vp)]
 
 
 class MbfReducePlan(ctypes.Structure):
@@ -67,7 +67,7 @@ _SIGS = {
     "mbf_error_string": (ctypes.c_char_p, [_i]),
     "mbf_version": (_i, []),
     "mbf_nl_workspace_bytes": (_sz, [_i, _i]),
-    "mbf_nl_build": (_i, [ctypes.POINTER(MbfSystem), _vp, _i, _d, _vp, _sz, _vp, _vp, _vp, _ll,
+    "mbf_nl_build": (_i, [ctypes.POINTER(MbfSystem), _vp, _i, _d, _vp, _sz, _vp, _vp, _vp, _vp, _ll,
                           ctypes.POINTER(_ll), ctypes.POINTER(_i), _vp]),
     "mbf_nl_max_displacement": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _vp]),
     "mbf_nl_half_workspace_bytes": (_sz, [_i]),

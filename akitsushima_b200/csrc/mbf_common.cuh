@@ -43,6 +43,15 @@ static inline SysView make_view(const mbf_system *s) {
     return v;
 }
 
+// Round half to even for |x| < 2^51 by the 1.5 * 2^52 shift: the sum's
+// spacing is exactly 1, so the add rounds x to the nearest integer (ties to
+// even) and the subtraction is exact.  Equal to rint(x) there, and cheaper
+// than the conversion unit's rounding.
+__device__ __forceinline__ double rint_shift(double x) {
+    const double M = 6755399441055744.0;
+    return __dsub_rn(__dadd_rn(x, M), M);
+}
+
 // Minimum-image displacement of r = (rx, ry, rz) in the cell `c` (lattice
 // rows c[0..8], inverse c[9..17]) evaluated exactly as the reference's
 // neighbour-list kernel does (engine/neighborlist.py:350-362): each dot
@@ -58,9 +67,9 @@ __device__ __forceinline__ void mic_exact(const double *__restrict__ c, double r
                           __dmul_rn(rz, __ldg(inv + 7)));
     double sz = __dadd_rn(__dadd_rn(__dmul_rn(rx, __ldg(inv + 2)), __dmul_rn(ry, __ldg(inv + 5))),
                           __dmul_rn(rz, __ldg(inv + 8)));
-    sx = __dsub_rn(sx, rint(sx));
-    sy = __dsub_rn(sy, rint(sy));
-    sz = __dsub_rn(sz, rint(sz));
+    sx = __dsub_rn(sx, rint_shift(sx));
+    sy = __dsub_rn(sy, rint_shift(sy));
+    sz = __dsub_rn(sz, rint_shift(sz));
     dx = __dadd_rn(__dadd_rn(__dmul_rn(sx, __ldg(c + 0)), __dmul_rn(sy, __ldg(c + 3))),
                    __dmul_rn(sz, __ldg(c + 6)));
     dy = __dadd_rn(__dadd_rn(__dmul_rn(sx, __ldg(c + 1)), __dmul_rn(sy, __ldg(c + 4))),
@@ -123,6 +132,12 @@ __device__ __forceinline__ T clamped_exp(T x) {
     if (x < T(-500)) return T(0);
     return RT<T>::ex(x);
 }
+
+// Division: IEEE in float64; the fast approximate quotient (2 ulp) in
+// float32, whose callers are the mixed-precision terms only.
+template <typename T> __device__ __forceinline__ T fdiv(T a, T b);
+template <> __device__ __forceinline__ double fdiv<double>(double a, double b) { return a / b; }
+template <> __device__ __forceinline__ float fdiv<float>(float a, float b) { return __fdividef(a, b); }
 
 // Integer power by repeated multiplication for the small fixed exponents
 // used by the potentials.

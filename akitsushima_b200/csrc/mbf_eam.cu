@@ -161,40 +161,48 @@ __device__ __forceinline__ void embed64(const EamDev &E, int f, double rho, doub
 
 template <typename T>
 struct ZSp {
-    T re, fe, beta, lam, A, alpha, kappa, B;
+    T inv_re, fe, beta, lam, A, alpha, kappa, B;
 };
 
 template <typename T>
 struct ZTab {
     ZSp<T> sp[EAM_MAXSP];
     T chi[EAM_MAXSP * EAM_MAXSP];
-    T rc, w;
+    T rc, w, inv_w;
 };
 
 template <typename T>
 __device__ __forceinline__ void zspecies(const ZSp<T> &p, T r, T &f, T &df, T &pr, T &dpr) {
-    T x = r / p.re;
+    T x = r * p.inv_re;
     T xm1 = x - T(1);
     T eB = RT<T>::ex(-p.beta * xm1);
     T eA = RT<T>::ex(-p.alpha * xm1);
     T u19B, u19A;
-    T dB = T(1) + pow20(x - p.lam, u19B);
-    T dA = T(1) + pow20(x - p.kappa, u19A);
-    T gB = eB / dB, gA = eA / dA;
-    T dgB = -p.beta * gB - gB * T(20) * u19B / dB;
-    T dgA = -p.alpha * gA - gA * T(20) * u19A / dA;
+    T rdB = fdiv<T>(T(1), T(1) + pow20(x - p.lam, u19B));
+    T rdA = fdiv<T>(T(1), T(1) + pow20(x - p.kappa, u19A));
+    T gB = eB * rdB, gA = eA * rdA;
+    T dgB = gB * (-p.beta - T(20) * u19B * rdB);
+    T dgA = gA * (-p.alpha - T(20) * u19A * rdA);
     f = p.fe * gB;
-    df = p.fe * dgB / p.re;
+    df = p.fe * dgB * p.inv_re;
     pr = p.A * gA - p.B * gB;
-    dpr = (p.A * dgA - p.B * dgB) / p.re;
+    dpr = (p.A * dgA - p.B * dgB) * p.inv_re;
 }
 
 template <typename T>
 __device__ __forceinline__ T zdens_only(const ZSp<T> &p, T r) {
-    T x = r / p.re;
+    T x = r * p.inv_re;
     T u19;
     T d = T(1) + pow20(x - p.lam, u19);
-    return p.fe * RT<T>::ex(-p.beta * (x - T(1))) / d;
+    return fdiv<T>(p.fe * RT<T>::ex(-p.beta * (x - T(1))), d);
+}
+
+template <typename T>
+__device__ __forceinline__ void zswitch_fast(T r, const ZTab<T> &Z, T &S, T &dS) {
+    T s = (r - (Z.rc - Z.w)) * Z.inv_w;
+    s = s < T(0) ? T(0) : (s > T(1) ? T(1) : s);
+    S = T(1) - s * s * s * (T(10) - T(15) * s + T(6) * s * s);
+    dS = T(-30) * s * s * (T(1) - s) * (T(1) - s) * Z.inv_w;
 }
 
 template <typename T>
@@ -202,7 +210,7 @@ __device__ void load_ztab(const EamDev &E, ZTab<T> &Z) {
     for (int s = threadIdx.x; s < E.ns; s += blockDim.x) {
         const double *p = E.P + (size_t)E.rho_f[s] * EAM_NCOL;
         ZSp<T> q;
-        q.re = (T)p[0]; q.fe = (T)p[1]; q.beta = (T)p[5]; q.lam = (T)p[9];
+        q.inv_re = (T)(1.0 / p[0]); q.fe = (T)p[1]; q.beta = (T)p[5]; q.lam = (T)p[9];
         q.A = (T)p[6]; q.alpha = (T)p[4]; q.kappa = (T)p[8]; q.B = (T)p[7];
         Z.sp[s] = q;
     }
@@ -216,6 +224,7 @@ __device__ void load_ztab(const EamDev &E, ZTab<T> &Z) {
         const double *p = E.P + (size_t)E.rho_f[0] * EAM_NCOL;
         Z.rc = (T)p[2 * EAM_NZ];
         Z.w = (T)p[2 * EAM_NZ + 1];
+        Z.inv_w = (T)(1.0 / p[2 * EAM_NZ + 1]);
     }
     __syncthreads();
 }
@@ -225,7 +234,7 @@ template <typename T>
 __device__ __forceinline__ void zhou_pair_terms(const ZTab<T> &Z, int si, int sj, T r, T &phi,
                                                 T &dphi, T &drho_j, T &drho_i) {
     T S, dS;
-    zswitch<T>(r, Z.rc, Z.w, S, dS);
+    zswitch_fast<T>(r, Z, S, dS);
     if (si == sj) {
         T f, df, pr, dpr;
         zspecies<T>(Z.sp[si], r, f, df, pr, dpr);
@@ -239,10 +248,12 @@ __device__ __forceinline__ void zhou_pair_terms(const ZTab<T> &Z, int si, int sj
         zspecies<T>(Z.sp[a], r, fa, dfa, ua, dua);
         zspecies<T>(Z.sp[b], r, fb, dfb, ub, dub);
         T k = Z.chi[a * EAM_MAXSP + b];
-        T q = fb / fa;
-        T dq = (dfb * fa - fb * dfa) / (fa * fa);
-        T v = T(0.5) * k * (q * ua + ub / q);
-        T dv = T(0.5) * k * (dq * ua + q * dua + dub / q - ub * dq / (q * q));
+        T rfa = fdiv<T>(T(1), fa);
+        T q = fb * rfa;
+        T rq = fdiv<T>(T(1), q);
+        T dq = (dfb * fa - fb * dfa) * rfa * rfa;
+        T v = T(0.5) * k * (q * ua + ub * rq);
+        T dv = T(0.5) * k * (dq * ua + q * dua + dub * rq - ub * dq * rq * rq);
         phi = v * S;
         dphi = dv * S + v * dS;
         T dra = dfa * S + fa * dS, drb = dfb * S + fb * dS;
@@ -251,22 +262,30 @@ __device__ __forceinline__ void zhou_pair_terms(const ZTab<T> &Z, int si, int sj
     }
 }
 
-// Fast minimum image for the force kernels (fused multiply-add allowed).
+// Minimum image for the force kernels (fused multiply-add allowed).
 __device__ __forceinline__ void mic_fast(const double *__restrict__ c, double rx, double ry, double rz,
                                          double &dx, double &dy, double &dz) {
     double sx = rx * c[9] + ry * c[12] + rz * c[15];
     double sy = rx * c[10] + ry * c[13] + rz * c[16];
     double sz = rx * c[11] + ry * c[14] + rz * c[17];
-    sx -= rint(sx);
-    sy -= rint(sy);
-    sz -= rint(sz);
+    sx -= rint_shift(sx);
+    sy -= rint_shift(sy);
+    sz -= rint_shift(sz);
     dx = sx * c[0] + sy * c[3] + sz * c[6];
     dy = sx * c[1] + sy * c[4] + sz * c[7];
     dz = sx * c[2] + sy * c[5] + sz * c[8];
 }
 
+// Distance of a minimum-imaged displacement in the working precision: the
+// wrap and the square stay float64; the root is taken in T.
+template <typename T>
+__device__ __forceinline__ T pair_dist(double r2);
+template <> __device__ __forceinline__ double pair_dist<double>(double r2) { return sqrt(r2); }
+template <> __device__ __forceinline__ float pair_dist<float>(double r2) { return sqrtf((float)r2); }
+
 // ---- kernels --------------------------------------------------------------
 
+// rho-bar_i over the full row, F(rho-bar_i) and F'(rho-bar_i) in float64.
 template <typename T, int LPA, bool ZHOU>
 __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *__restrict__ row_off,
                                                          const int *__restrict__ nbr, EamDev E,
@@ -275,7 +294,7 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *_
     if (ZHOU) load_ztab<T>(E, Z);
     const int sub = threadIdx.x & (LPA - 1);
     const int gpb = EAM_BLOCK / LPA;
-    const double rc = E.r_cut;
+    const double rc = E.r_cut, rc2 = rc * rc;
     for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
         int i = base + threadIdx.x / LPA;
         double acc = 0.0;
@@ -290,16 +309,17 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *_
                 double dx, dy, dz;
                 mic_fast(cell, S.pos[3 * (size_t)j] - xi, S.pos[3 * (size_t)j + 1] - yi,
                          S.pos[3 * (size_t)j + 2] - zi, dx, dy, dz);
-                double r = sqrt(dx * dx + dy * dy + dz * dz);
-                if (!(r < rc && r > 1e-12)) continue;
+                double r2 = dx * dx + dy * dy + dz * dz;
+                if (!(r2 < rc2 && r2 > 1e-24)) continue;
                 int sj = S.types[j];
                 if (ZHOU) {
+                    T r = pair_dist<T>(r2);
                     T Sw, dSw;
-                    zswitch<T>((T)r, Z.rc, Z.w, Sw, dSw);
-                    acc += (double)(zdens_only<T>(Z.sp[sj], (T)r) * Sw);
+                    zswitch_fast<T>(r, Z, Sw, dSw);
+                    acc += (double)(zdens_only<T>(Z.sp[sj], r) * Sw);
                 } else {
                     T v, dv;
-                    feval<T>(E, E.rho_f[sj], r, v, dv);
+                    feval<T>(E, E.rho_f[sj], sqrt(r2), v, dv);
                     acc += (double)v;
                 }
             }
@@ -315,17 +335,23 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *_
     }
 }
 
+// Force pass over the upper half of every row: each unordered pair once.
+// The pair force on i is accumulated here; the one on j (its negative) is
+// stored in slot (i -> j) for j's gather.  Energy phi and the virial of the
+// pair go to i, the lower index.
 template <typename T, int LPA, bool ZHOU>
 __global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__restrict__ row_off,
+                                                       const int *__restrict__ upper,
                                                        const int *__restrict__ nbr, EamDev E,
                                                        const double *__restrict__ aux,
-                                                       double *__restrict__ forces,
+                                                       double *__restrict__ slot_f,
+                                                       double *__restrict__ f_local,
                                                        double *__restrict__ per_atom) {
     __shared__ ZTab<T> Z;
     if (ZHOU) load_ztab<T>(E, Z);
     const int sub = threadIdx.x & (LPA - 1);
     const int gpb = EAM_BLOCK / LPA;
-    const double rc = E.r_cut;
+    const double rc = E.r_cut, rc2 = rc * rc;
     for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
         int i = base + threadIdx.x / LPA;
         double fx = 0, fy = 0, fz = 0, e = 0, npair = 0;
@@ -336,38 +362,48 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__r
             const double *cell = cell_of(S, i);
             double xi = S.pos[3 * (size_t)i], yi = S.pos[3 * (size_t)i + 1], zi = S.pos[3 * (size_t)i + 2];
             int end = row_off[i + 1];
-            for (int s = row_off[i] + sub; s < end; s += LPA) {
+            for (int s = upper[i] + sub; s < end; s += LPA) {
                 int j = nbr[s];
                 double dx, dy, dz;
                 mic_fast(cell, S.pos[3 * (size_t)j] - xi, S.pos[3 * (size_t)j + 1] - yi,
                          S.pos[3 * (size_t)j + 2] - zi, dx, dy, dz);
-                double r = sqrt(dx * dx + dy * dy + dz * dz);
-                if (!(r < rc && r > 1e-12)) continue;
-                int sj = S.types[j];
-                npair += 1.0;
-                T phi, dphi, drho_j, drho_i;
-                if (ZHOU) {
-                    zhou_pair_terms<T>(Z, si, sj, (T)r, phi, dphi, drho_j, drho_i);
-                } else {
-                    T rj, ri;
-                    feval<T>(E, E.phi_f[si * E.ns + sj], r, phi, dphi);
-                    feval<T>(E, E.rho_f[sj], r, rj, drho_j);
-                    feval<T>(E, E.rho_f[si], r, ri, drho_i);
+                double r2 = dx * dx + dy * dy + dz * dz;
+                double px = 0, py = 0, pz = 0;
+                if (r2 < rc2 && r2 > 1e-24) {
+                    int sj = S.types[j];
+                    npair += 1.0;
+                    T r = pair_dist<T>(r2);
+                    T phi, dphi, drho_j, drho_i;
+                    if (ZHOU) {
+                        zhou_pair_terms<T>(Z, si, sj, r, phi, dphi, drho_j, drho_i);
+                    } else {
+                        double rr = sqrt(r2);
+                        T rj, ri;
+                        feval<T>(E, E.phi_f[si * E.ns + sj], rr, phi, dphi);
+                        feval<T>(E, E.rho_f[sj], rr, rj, drho_j);
+                        feval<T>(E, E.rho_f[si], rr, ri, drho_i);
+                    }
+                    double Fp_j = aux[2 * (size_t)j];
+                    T c = dphi + (T)Fp_i * drho_j + (T)Fp_j * drho_i;
+                    double sc = (double)fdiv<T>(c, r);
+                    px = sc * dx;
+                    py = sc * dy;
+                    pz = sc * dz;
+                    fx += px;
+                    fy += py;
+                    fz += pz;
+                    e += (double)phi;
+                    vxx -= px * dx;
+                    vyy -= py * dy;
+                    vzz -= pz * dz;
+                    vxy -= px * dy;
+                    vxz -= px * dz;
+                    vyz -= py * dz;
                 }
-                double Fp_j = aux[2 * (size_t)j];
-                T c = dphi + (T)Fp_i * drho_j + (T)Fp_j * drho_i;
-                double sc = (double)(c / (T)r);
-                double px = sc * dx, py = sc * dy, pz = sc * dz;
-                fx += px;
-                fy += py;
-                fz += pz;
-                e += 0.5 * (double)phi;
-                vxx -= 0.5 * px * dx;
-                vyy -= 0.5 * py * dy;
-                vzz -= 0.5 * pz * dz;
-                vxy -= 0.5 * px * dy;
-                vxz -= 0.5 * px * dz;
-                vyz -= 0.5 * py * dz;
+                size_t o = 3 * (size_t)s;
+                slot_f[o] = px;
+                slot_f[o + 1] = py;
+                slot_f[o + 2] = pz;
             }
         }
         fx = group_sum<LPA>(fx);
@@ -382,9 +418,9 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__r
         vyz = group_sum<LPA>(vyz);
         npair = group_sum<LPA>(npair);
         if (sub == 0 && i < S.n_atoms) {
-            forces[3 * (size_t)i] = fx;
-            forces[3 * (size_t)i + 1] = fy;
-            forces[3 * (size_t)i + 2] = fz;
+            f_local[3 * (size_t)i] = fx;
+            f_local[3 * (size_t)i + 1] = fy;
+            f_local[3 * (size_t)i + 2] = fz;
             double *pa = per_atom + (size_t)i * ATOM_ACC;
             pa[0] = e + aux[2 * (size_t)i + 1];
             pa[1] = vxx; pa[2] = vxy; pa[3] = vxz;
@@ -395,9 +431,27 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__r
     }
 }
 
+// F_a = (pairs above a) - sum of the forces stored by the lower neighbours.
+__global__ void eam_gather(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ upper,
+                           const int *__restrict__ rev, const double *__restrict__ slot_f,
+                           const double *__restrict__ f_local, double *__restrict__ forces) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n_atoms) return;
+    double fx = f_local[3 * (size_t)a], fy = f_local[3 * (size_t)a + 1], fz = f_local[3 * (size_t)a + 2];
+    for (int s = row_off[a]; s < upper[a]; ++s) {
+        size_t o = 3 * (size_t)rev[s];
+        fx -= slot_f[o];
+        fy -= slot_f[o + 1];
+        fz -= slot_f[o + 2];
+    }
+    forces[3 * (size_t)a] = fx;
+    forces[3 * (size_t)a + 1] = fy;
+    forces[3 * (size_t)a + 2] = fz;
+}
+
 template <typename T, int LPA, bool ZHOU>
-static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, double *aux,
-                      double *forces, double *per_atom, cudaStream_t st) {
+static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, double *aux, double *slot_f,
+                      double *f_local, double *forces, double *per_atom, cudaStream_t st) {
     int gpb = EAM_BLOCK / LPA;
     int blocks = (S.n_atoms + gpb - 1) / gpb;
     int g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_density<T, LPA, ZHOU>);
@@ -407,20 +461,27 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, do
     MBF_CHECK_LAUNCH();
     g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_force<T, LPA, ZHOU>);
     PROF_BEGIN("eam_force", st);
-    eam_force<T, LPA, ZHOU><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, E, aux, forces, per_atom);
+    eam_force<T, LPA, ZHOU><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, E, aux, slot_f,
+                                                     f_local, per_atom);
     PROF_END("eam_force", st);
+    MBF_CHECK_LAUNCH();
+    PROF_BEGIN("eam_gather", st);
+    eam_gather<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S.n_atoms, nl->row_off, nl->upper, nl->rev, slot_f,
+                                                         f_local, forces);
+    PROF_END("eam_gather", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;
 }
 
 template <typename T, bool ZHOU>
-static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E,
-                            double *aux, double *forces, double *per_atom, cudaStream_t st) {
+static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E, double *aux,
+                            double *slot_f, double *f_local, double *forces, double *per_atom,
+                            cudaStream_t st) {
     switch (lpa) {
-        case 4: return eam_launch<T, 4, ZHOU>(S, nl, E, aux, forces, per_atom, st);
-        case 8: return eam_launch<T, 8, ZHOU>(S, nl, E, aux, forces, per_atom, st);
-        case 16: return eam_launch<T, 16, ZHOU>(S, nl, E, aux, forces, per_atom, st);
-        case 32: return eam_launch<T, 32, ZHOU>(S, nl, E, aux, forces, per_atom, st);
+        case 4: return eam_launch<T, 4, ZHOU>(S, nl, E, aux, slot_f, f_local, forces, per_atom, st);
+        case 8: return eam_launch<T, 8, ZHOU>(S, nl, E, aux, slot_f, f_local, forces, per_atom, st);
+        case 16: return eam_launch<T, 16, ZHOU>(S, nl, E, aux, slot_f, f_local, forces, per_atom, st);
+        case 32: return eam_launch<T, 32, ZHOU>(S, nl, E, aux, slot_f, f_local, forces, per_atom, st);
         default: return MBF_ERR_ARGUMENT;
     }
 }
@@ -451,18 +512,21 @@ extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mb
     E.X = tab->X; E.C = tab->C;
     E.rho_f = tab->rho_f; E.F_f = tab->F_f; E.phi_f = tab->phi_f;
     E.r_cut = tab->r_cut;
+    if (!nl->upper) return MBF_ERR_ARGUMENT;
     double *aux = ws_at<double>(workspace, L.atom_aux);
     double *per_atom = ws_at<double>(workspace, L.per_atom);
     double *partial = ws_at<double>(workspace, L.partial);
+    double *slot_f = ws_at<double>(workspace, L.slot);
+    double *f_local = ws_at<double>(workspace, L.f_local);
     int lpa = lanes_per_atom > 0 ? lanes_per_atom : 8;
     bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
     int rc;
     if (precision == MBF_FP64)
-        rc = zhou ? eam_dispatch_lpa<double, true>(lpa, S, nl, E, aux, forces, per_atom, st)
-                  : eam_dispatch_lpa<double, false>(lpa, S, nl, E, aux, forces, per_atom, st);
+        rc = zhou ? eam_dispatch_lpa<double, true>(lpa, S, nl, E, aux, slot_f, f_local, forces, per_atom, st)
+                  : eam_dispatch_lpa<double, false>(lpa, S, nl, E, aux, slot_f, f_local, forces, per_atom, st);
     else
-        rc = zhou ? eam_dispatch_lpa<float, true>(lpa, S, nl, E, aux, forces, per_atom, st)
-                  : eam_dispatch_lpa<float, false>(lpa, S, nl, E, aux, forces, per_atom, st);
+        rc = zhou ? eam_dispatch_lpa<float, true>(lpa, S, nl, E, aux, slot_f, f_local, forces, per_atom, st)
+                  : eam_dispatch_lpa<float, false>(lpa, S, nl, E, aux, slot_f, f_local, forces, per_atom, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
 }

@@ -185,7 +185,8 @@ __global__ void nl_count(SysView S, const int *__restrict__ grids, const int *__
 // sort the row ascending by rank in shared memory.
 __global__ void nl_fill(SysView S, const int *__restrict__ grids, const int *__restrict__ cell_start,
                         const int *__restrict__ cell_atoms, const int *__restrict__ atom_cell, double rl2,
-                        const int *__restrict__ row_off, int *__restrict__ nbr, int *__restrict__ err) {
+                        const int *__restrict__ row_off, int *__restrict__ nbr, int *__restrict__ upper,
+                        int *__restrict__ err) {
     __shared__ Stencil sst[NL_WARPS];
     __shared__ int srow[NL_WARPS][NL_MAXROW];
     int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -213,16 +214,24 @@ __global__ void nl_fill(SysView S, const int *__restrict__ grids, const int *__r
         }
         __syncwarp();
         if (n > NL_MAXROW) {
-            if (lane == 0) atomicOr(err, MBF_DEV_ROW_TOO_LONG);
+            if (lane == 0) {
+                atomicOr(err, MBF_DEV_ROW_TOO_LONG);
+                upper[a] = beg;
+            }
             continue;
         }
         for (int k = lane; k < n; k += 32) row[k] = nbr[beg + k];
         __syncwarp();
+        int lower = 0;
         for (int k = lane; k < n; k += 32) {
             int v = row[k], rank = 0;
             for (int q = 0; q < n; ++q) rank += row[q] < v ? 1 : 0;
             nbr[beg + rank] = v;
+            lower += v < a ? 1 : 0;
         }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lower += __shfl_xor_sync(MBF_FULL, lower, o);
+        if (lane == 0) upper[a] = beg + lower;
         __syncwarp();
     }
 }
@@ -305,7 +314,7 @@ size_t mbf_nl_workspace_bytes(int n_atoms, int n_cells_total) {
 }
 
 int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total, double r_list,
-                 void *workspace, size_t workspace_bytes, int *row_off, int *nbr, int *rev,
+                 void *workspace, size_t workspace_bytes, int *row_off, int *nbr, int *rev, int *upper,
                  long long nbr_capacity, long long *n_slots, int *max_row, void *stream) {
     if (!sys || !grids || !workspace || !row_off || !n_slots || !max_row || sys->n_atoms < 0 ||
         n_cells_total <= 0 || !(r_list > 0.0))
@@ -363,10 +372,11 @@ int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total, dou
     *n_slots = host[0];
     *max_row = host[1];
     if ((long long)host[0] > nbr_capacity || !nbr || !rev) return MBF_ERR_CAPACITY;
+    if (!upper) return MBF_ERR_ARGUMENT;
     if (host[1] > NL_MAXROW) return MBF_ERR_ROW_TOO_LONG;
     g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_fill);
     PROF_BEGIN("nl_fill", st);
-    nl_fill<<<g, 32 * NL_WARPS, 0, st>>>(S, grids, cell_start, cell_atoms, atom_cell, rl2, row_off, nbr, err);
+    nl_fill<<<g, 32 * NL_WARPS, 0, st>>>(S, grids, cell_start, cell_atoms, atom_cell, rl2, row_off, nbr, upper, err);
     PROF_END("nl_fill", st);
     MBF_CHECK_LAUNCH();
     g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_reverse);

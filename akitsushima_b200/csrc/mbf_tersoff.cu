@@ -49,6 +49,16 @@ __device__ __forceinline__ T te_arg(T l3, T u, T m) {
     return RT<T>::pw(l3, m) * RT<T>::pw(u, m);
 }
 
+// Angular function g = 1 + c^2/d^2 - c^2/(d^2 + (h - cos)^2), written as
+// 1 + c^2 (h - cos)^2 / (d^2 (d^2 + (h - cos)^2)): the same value without
+// the cancellation of two ~c^2/d^2 terms (c^2/d^2 ~ 4e7 for silicon), which
+// float32 cannot afford.
+template <typename T>
+__device__ __forceinline__ T te_g(T c, T d, T hc) {
+    T d2 = d * d, hc2 = hc * hc;
+    return T(1) + (c * c) * hc2 / (d2 * (d2 + hc2));
+}
+
 // Analytic gradient of one zeta term (engine/tersoff.py:161-202).
 template <typename T>
 __device__ __forceinline__ void te_zgrad(T rijx, T rijy, T rijz, T r_ij, T rikx, T riky, T rikz, T r_ik,
@@ -58,7 +68,7 @@ __device__ __forceinline__ void te_zgrad(T rijx, T rijy, T rijz, T r_ij, T rikx,
     T cos_t = (rijx * rikx + rijy * riky + rijz * rikz) * inv_ij * inv_ik;
     T hc = h - cos_t;
     T q = d * d + hc * hc;
-    T g = T(1) + c * c / (d * d) - c * c / q;
+    T g = te_g<T>(c, d, hc);
     T dg = T(-2) * c * c * hc / (q * q);
     T u = r_ij - r_ik;
     T ex = clamped_exp<T>(te_arg<T>(l3, u, m));
@@ -152,7 +162,7 @@ __global__ void te_zeta(SysView S, const int *__restrict__ row_off, const int *_
                             T cos_t = (R.x[s] * R.x[k] + R.y[s] * R.y[k] + R.z[s] * R.z[k]) / (rs * R.r[k]);
                             T c = (T)t3[1], d = (T)t3[2], h = (T)t3[3];
                             T hc = h - cos_t;
-                            T g = T(1) + c * c / (d * d) - c * c / (d * d + hc * hc);
+                            T g = te_g<T>(c, d, hc);
                             zeta += (T)t3[6] * fc * g * clamped_exp<T>(te_arg<T>((T)t3[4], rs - R.r[k], (T)t3[5]));
                         }
                         const double *tij = P.tb + 10 * (si * ns + sj);
@@ -202,9 +212,19 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
         int si = live ? S.types[i] : 0;
         // pass 1: pair terms and the zeta-gradient coefficients
         double cxs[(MAXN + TE_LPA - 1) / TE_LPA];
+        double pair_r[(MAXN + TE_LPA - 1) / TE_LPA];
         if (live) {
+            const double *cell = cell_of(S, i);
+            double xi = S.pos[3 * (size_t)i], yi = S.pos[3 * (size_t)i + 1], zi = S.pos[3 * (size_t)i + 2];
             int q = 0;
             for (int s = sub; s < n; s += TE_LPA, ++q) {
+                {
+                    int j = nbr[beg + s];
+                    double dx, dy, dz;
+                    mic_exact(cell, S.pos[3 * (size_t)j] - xi, S.pos[3 * (size_t)j + 1] - yi,
+                              S.pos[3 * (size_t)j + 2] - zi, dx, dy, dz);
+                    pair_r[q] = sqrt(dx * dx + dy * dy + dz * dz);
+                }
                 T coef = T(0);
                 double cx = 0.0;
                 if (R.ok[s]) {
@@ -217,18 +237,19 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
                         double db_own = slot_b[2 * (size_t)(beg + s) + 1];
                         double b_rev = slot_b[2 * (size_t)rev[beg + s]];
                         double bavg = i < j ? 0.5 * (b_own + b_rev) : 0.5 * (b_rev + b_own);
-                        T r = R.r[s];
-                        T Rr = (T)tp[5], Dd = (T)tp[6];
-                        T fc = te_fc<T>(r, Rr, Dd), dfc = te_dfc<T>(r, Rr, Dd);
-                        if (fc != T(0) || dfc != T(0)) {
-                            T l1 = (T)tp[3], l2 = (T)tp[4];
-                            T fr = (T)tp[1] * clamped_exp<T>(-l1 * r);
-                            T fa = -(T)tp[2] * clamped_exp<T>(-l2 * r);
-                            T bv = (T)bavg;
-                            e += 0.5 * (double)(fc * (fr + bv * fa));
-                            T dEdr = dfc * (fr + bv * fa) + fc * (-l1 * fr + bv * (-l2 * fa));
-                            cx = (double)(dEdr / r);
-                            if (fabs(db_own) > 1e-30) coef = T(0.5) * fc * fa * (T)db_own;
+                        // the two-body part is per bond, not per angle: float64
+                        // in both precisions
+                        double r = pair_r[q];
+                        double Rr = tp[5], Dd = tp[6];
+                        double fc = te_fc<double>(r, Rr, Dd), dfc = te_dfc<double>(r, Rr, Dd);
+                        if (fc != 0.0 || dfc != 0.0) {
+                            double l1 = tp[3], l2 = tp[4];
+                            double fr = tp[1] * clamped_exp<double>(-l1 * r);
+                            double fa = -tp[2] * clamped_exp<double>(-l2 * r);
+                            e += 0.5 * (fc * (fr + bavg * fa));
+                            double dEdr = dfc * (fr + bavg * fa) + fc * (-l1 * fr + bavg * (-l2 * fa));
+                            cx = dEdr / r;
+                            if (fabs(db_own) > 1e-30) coef = (T)(0.5 * fc * fa * db_own);
                         }
                     }
                 }

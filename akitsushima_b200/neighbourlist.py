@@ -37,6 +37,7 @@ class DeviceNeighbourList:
         self.row_off = None
         self.nbr = None
         self.rev = None
+        self.upper = None
         self._ws = None
         self._grids = None
         self.device = None
@@ -64,6 +65,7 @@ class DeviceNeighbourList:
             self._ws = torch.empty(need, dtype=torch.uint8, device=dev)
         if self.row_off is None or self.row_off.numel() < N + 1 or self.row_off.device != dev:
             self.row_off = torch.empty(N + 1, dtype=torch.int32, device=dev)
+            self.upper = torch.empty(max(N, 1), dtype=torch.int32, device=dev)
         if self.nbr is None or self.nbr.device != dev:
             cap = max(1024, int(N * 8))
             self.nbr = torch.empty(cap, dtype=torch.int32, device=dev)
@@ -75,7 +77,7 @@ class DeviceNeighbourList:
         for _ in range(3):
             rc = L.mbf_nl_build(sysd, _lib.ptr(self._grids), n_cells, self.r_list, _lib.ptr(self._ws),
                                 need, _lib.ptr(self.row_off), _lib.ptr(self.nbr), _lib.ptr(self.rev),
-                                self.nbr.numel(), n_slots, max_row, stream)
+                                _lib.ptr(self.upper), self.nbr.numel(), n_slots, max_row, stream)
             if rc == _lib.MBF_ERR_CAPACITY:
                 cap = int(n_slots.value * 1.25) + 1024
                 self.nbr = torch.empty(cap, dtype=torch.int32, device=dev)
@@ -91,7 +93,7 @@ class DeviceNeighbourList:
 
     def mbf_nlist(self):
         return _lib.MbfNlist(self.n_atoms, self.n_slots, self.max_row, _lib.ptr(self.row_off),
-                             _lib.ptr(self.nbr), _lib.ptr(self.rev))
+                             _lib.ptr(self.nbr), _lib.ptr(self.rev), _lib.ptr(self.upper))
 
     def half_pairs(self):
         """Canonical (i < j, sorted by (i, j)) pairs as device int32 tensors."""
@@ -134,6 +136,9 @@ class DeviceNeighbourList:
         self.row_off = row_off.to(torch.int32)
         self.nbr = nbr.to(torch.int32)
         self.rev = rev.to(torch.int32)
+        lower = torch.zeros(n_atoms, dtype=torch.int64, device=device)
+        lower.index_add_(0, src[order], (nbr < src[order]).to(torch.int64))
+        self.upper = (row_off[:-1] + lower).to(torch.int32)
         return self
 
 

@@ -67,6 +67,7 @@ typedef struct mbf_nlist {
     const int *row_off;        /* (n_atoms + 1) */
     const int *nbr;            /* (n_slots,) */
     const int *rev;            /* (n_slots,) */
+    const int *upper;          /* (n_atoms,) first slot of row a whose neighbour is > a */
 } mbf_nlist;
 
 /* Per-structure reduction table: chunks of atoms that lie in one structure.
@@ -100,7 +101,7 @@ size_t mbf_nl_workspace_bytes(int n_atoms, int n_cells_total);
  * count). */
 int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total,
                  double r_list, void *workspace, size_t workspace_bytes,
-                 int *row_off, int *nbr, int *rev, long long nbr_capacity,
+                 int *row_off, int *nbr, int *rev, int *upper, long long nbr_capacity,
                  long long *n_slots, int *max_row, void *stream);
 
 /* Largest minimum-image displacement of any atom from its reference
