@@ -285,10 +285,25 @@ template <> __device__ __forceinline__ float pair_dist<float>(double r2) { retur
 
 // ---- kernels --------------------------------------------------------------
 
+// Per-atom record read by every neighbour: position and, once the density
+// pass has run, F'(rho-bar) -- one 32-byte sector per neighbour gather.
+__global__ void eam_pack(SysView S, double4 *__restrict__ pk) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n_atoms) return;
+    pk[i] = make_double4(S.pos[3 * (size_t)i], S.pos[3 * (size_t)i + 1], S.pos[3 * (size_t)i + 2], 0.0);
+}
+
+__device__ __forceinline__ double4 ld_pack(const double4 *__restrict__ pk, int j) {
+    const double2 *p = reinterpret_cast<const double2 *>(pk + j);
+    double2 a = __ldg(p), b = __ldg(p + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
 // rho-bar_i over the full row, F(rho-bar_i) and F'(rho-bar_i) in float64.
 template <typename T, int LPA, bool ZHOU>
 __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *__restrict__ row_off,
                                                          const int *__restrict__ nbr, EamDev E,
+                                                         double4 *__restrict__ pk,
                                                          double *__restrict__ aux) {
     __shared__ ZTab<T> Z;
     if (ZHOU) load_ztab<T>(E, Z);
@@ -302,16 +317,16 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *_
         if (i < S.n_atoms) {
             si = S.types[i];
             const double *cell = cell_of(S, i);
-            double xi = S.pos[3 * (size_t)i], yi = S.pos[3 * (size_t)i + 1], zi = S.pos[3 * (size_t)i + 2];
+            double4 pi = ld_pack(pk, i);
             int end = row_off[i + 1];
             for (int s = row_off[i] + sub; s < end; s += LPA) {
                 int j = nbr[s];
+                double4 pj = ld_pack(pk, j);
+                int sj = __ldg(S.types + j);
                 double dx, dy, dz;
-                mic_fast(cell, S.pos[3 * (size_t)j] - xi, S.pos[3 * (size_t)j + 1] - yi,
-                         S.pos[3 * (size_t)j + 2] - zi, dx, dy, dz);
+                mic_fast(cell, pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
                 double r2 = dx * dx + dy * dy + dz * dz;
                 if (!(r2 < rc2 && r2 > 1e-24)) continue;
-                int sj = S.types[j];
                 if (ZHOU) {
                     T r = pair_dist<T>(r2);
                     T Sw, dSw;
@@ -329,6 +344,7 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *_
             double rb = acc > 0.0 ? acc : 0.0;
             double F, dF;
             embed64(E, E.F_f[si], rb, F, dF);
+            pk[i].w = dF;
             aux[2 * (size_t)i] = dF;
             aux[2 * (size_t)i + 1] = F;
         }
@@ -337,16 +353,25 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *_
 
 // Force pass over the upper half of every row: each unordered pair once.
 // The pair force on i is accumulated here; the one on j (its negative) is
-// stored in slot (i -> j) for j's gather.  Energy phi and the virial of the
-// pair go to i, the lower index.
+// written to j's own slot (j -> i) = rev(i -> j), so j's gather reads its row
+// contiguously.  Energy phi and the virial of the pair go to i, the lower
+// index.  SlotT is float in the mixed path (a per-pair term, accumulated in
+// float64 by the gather) and double in the float64 path.
+template <typename T> struct SlotVec;
+template <> struct SlotVec<double> { typedef double3 type; };
+template <> struct SlotVec<float> { typedef float3 type; };
+
 template <typename T, int LPA, bool ZHOU>
 __global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__restrict__ row_off,
                                                        const int *__restrict__ upper,
-                                                       const int *__restrict__ nbr, EamDev E,
+                                                       const int *__restrict__ nbr,
+                                                       const int *__restrict__ rev, EamDev E,
+                                                       const double4 *__restrict__ pk,
                                                        const double *__restrict__ aux,
-                                                       double *__restrict__ slot_f,
+                                                       typename SlotVec<T>::type *__restrict__ slot_f,
                                                        double *__restrict__ f_local,
                                                        double *__restrict__ per_atom) {
+    typedef typename SlotVec<T>::type V3;
     __shared__ ZTab<T> Z;
     if (ZHOU) load_ztab<T>(E, Z);
     const int sub = threadIdx.x & (LPA - 1);
@@ -358,19 +383,20 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__r
         double vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
         if (i < S.n_atoms) {
             int si = S.types[i];
-            double Fp_i = aux[2 * (size_t)i];
+            double4 pi = ld_pack(pk, i);
+            T Fp_i = (T)pi.w;
             const double *cell = cell_of(S, i);
-            double xi = S.pos[3 * (size_t)i], yi = S.pos[3 * (size_t)i + 1], zi = S.pos[3 * (size_t)i + 2];
             int end = row_off[i + 1];
             for (int s = upper[i] + sub; s < end; s += LPA) {
                 int j = nbr[s];
+                int rs = rev[s];
+                double4 pj = ld_pack(pk, j);
+                int sj = __ldg(S.types + j);
                 double dx, dy, dz;
-                mic_fast(cell, S.pos[3 * (size_t)j] - xi, S.pos[3 * (size_t)j + 1] - yi,
-                         S.pos[3 * (size_t)j + 2] - zi, dx, dy, dz);
+                mic_fast(cell, pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
                 double r2 = dx * dx + dy * dy + dz * dz;
                 double px = 0, py = 0, pz = 0;
                 if (r2 < rc2 && r2 > 1e-24) {
-                    int sj = S.types[j];
                     npair += 1.0;
                     T r = pair_dist<T>(r2);
                     T phi, dphi, drho_j, drho_i;
@@ -383,8 +409,7 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__r
                         feval<T>(E, E.rho_f[sj], rr, rj, drho_j);
                         feval<T>(E, E.rho_f[si], rr, ri, drho_i);
                     }
-                    double Fp_j = aux[2 * (size_t)j];
-                    T c = dphi + (T)Fp_i * drho_j + (T)Fp_j * drho_i;
+                    T c = dphi + Fp_i * drho_j + (T)pj.w * drho_i;
                     double sc = (double)fdiv<T>(c, r);
                     px = sc * dx;
                     py = sc * dy;
@@ -400,10 +425,11 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__r
                     vxz -= px * dz;
                     vyz -= py * dz;
                 }
-                size_t o = 3 * (size_t)s;
-                slot_f[o] = px;
-                slot_f[o + 1] = py;
-                slot_f[o + 2] = pz;
+                V3 w;
+                w.x = (T)(-px);
+                w.y = (T)(-py);
+                w.z = (T)(-pz);
+                slot_f[rs] = w;
             }
         }
         fx = group_sum<LPA>(fx);
@@ -431,57 +457,71 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__r
     }
 }
 
-// F_a = (pairs above a) - sum of the forces stored by the lower neighbours.
+// F_a = (pairs above a) + the forces its lower neighbours left in a's own
+// lower slots; lane group per atom, contiguous reads.
+template <typename V3, int LPA>
 __global__ void eam_gather(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ upper,
-                           const int *__restrict__ rev, const double *__restrict__ slot_f,
-                           const double *__restrict__ f_local, double *__restrict__ forces) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= n_atoms) return;
-    double fx = f_local[3 * (size_t)a], fy = f_local[3 * (size_t)a + 1], fz = f_local[3 * (size_t)a + 2];
-    for (int s = row_off[a]; s < upper[a]; ++s) {
-        size_t o = 3 * (size_t)rev[s];
-        fx -= slot_f[o];
-        fy -= slot_f[o + 1];
-        fz -= slot_f[o + 2];
+                           const V3 *__restrict__ slot_f, const double *__restrict__ f_local,
+                           double *__restrict__ forces) {
+    const int sub = threadIdx.x & (LPA - 1);
+    const int gpb = blockDim.x / LPA;
+    int a = blockIdx.x * gpb + threadIdx.x / LPA;
+    double fx = 0, fy = 0, fz = 0;
+    if (a < n_atoms) {
+        for (int s = row_off[a] + sub; s < upper[a]; s += LPA) {
+            V3 w = slot_f[s];
+            fx += (double)w.x;
+            fy += (double)w.y;
+            fz += (double)w.z;
+        }
     }
-    forces[3 * (size_t)a] = fx;
-    forces[3 * (size_t)a + 1] = fy;
-    forces[3 * (size_t)a + 2] = fz;
+    fx = group_sum<LPA>(fx);
+    fy = group_sum<LPA>(fy);
+    fz = group_sum<LPA>(fz);
+    if (sub == 0 && a < n_atoms) {
+        forces[3 * (size_t)a] = f_local[3 * (size_t)a] + fx;
+        forces[3 * (size_t)a + 1] = f_local[3 * (size_t)a + 1] + fy;
+        forces[3 * (size_t)a + 2] = f_local[3 * (size_t)a + 2] + fz;
+    }
 }
 
 template <typename T, int LPA, bool ZHOU>
-static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, double *aux, double *slot_f,
-                      double *f_local, double *forces, double *per_atom, cudaStream_t st) {
+static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, double4 *pk, double *aux,
+                      void *slot, double *f_local, double *forces, double *per_atom, cudaStream_t st) {
+    typedef typename SlotVec<T>::type V3;
     int gpb = EAM_BLOCK / LPA;
     int blocks = (S.n_atoms + gpb - 1) / gpb;
+    PROF_BEGIN("eam_pack", st);
+    eam_pack<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S, pk);
+    PROF_END("eam_pack", st);
     int g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_density<T, LPA, ZHOU>);
     PROF_BEGIN("eam_density", st);
-    eam_density<T, LPA, ZHOU><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, E, aux);
+    eam_density<T, LPA, ZHOU><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, E, pk, aux);
     PROF_END("eam_density", st);
     MBF_CHECK_LAUNCH();
     g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_force<T, LPA, ZHOU>);
     PROF_BEGIN("eam_force", st);
-    eam_force<T, LPA, ZHOU><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, E, aux, slot_f,
-                                                     f_local, per_atom);
+    eam_force<T, LPA, ZHOU><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, E, pk,
+                                                     aux, (V3 *)slot, f_local, per_atom);
     PROF_END("eam_force", st);
     MBF_CHECK_LAUNCH();
     PROF_BEGIN("eam_gather", st);
-    eam_gather<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S.n_atoms, nl->row_off, nl->upper, nl->rev, slot_f,
-                                                         f_local, forces);
+    eam_gather<V3, 8><<<(S.n_atoms + 15) / 16, 128, 0, st>>>(S.n_atoms, nl->row_off, nl->upper,
+                                                             (const V3 *)slot, f_local, forces);
     PROF_END("eam_gather", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;
 }
 
 template <typename T, bool ZHOU>
-static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E, double *aux,
-                            double *slot_f, double *f_local, double *forces, double *per_atom,
+static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E, double4 *pk,
+                            double *aux, void *slot, double *f_local, double *forces, double *per_atom,
                             cudaStream_t st) {
     switch (lpa) {
-        case 4: return eam_launch<T, 4, ZHOU>(S, nl, E, aux, slot_f, f_local, forces, per_atom, st);
-        case 8: return eam_launch<T, 8, ZHOU>(S, nl, E, aux, slot_f, f_local, forces, per_atom, st);
-        case 16: return eam_launch<T, 16, ZHOU>(S, nl, E, aux, slot_f, f_local, forces, per_atom, st);
-        case 32: return eam_launch<T, 32, ZHOU>(S, nl, E, aux, slot_f, f_local, forces, per_atom, st);
+        case 4: return eam_launch<T, 4, ZHOU>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
+        case 8: return eam_launch<T, 8, ZHOU>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
+        case 16: return eam_launch<T, 16, ZHOU>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
+        case 32: return eam_launch<T, 32, ZHOU>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
         default: return MBF_ERR_ARGUMENT;
     }
 }
@@ -516,17 +556,18 @@ extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mb
     double *aux = ws_at<double>(workspace, L.atom_aux);
     double *per_atom = ws_at<double>(workspace, L.per_atom);
     double *partial = ws_at<double>(workspace, L.partial);
-    double *slot_f = ws_at<double>(workspace, L.slot);
+    void *slot_f = ws_at<char>(workspace, L.slot);
     double *f_local = ws_at<double>(workspace, L.f_local);
+    double4 *pk = ws_at<double4>(workspace, L.pack);
     int lpa = lanes_per_atom > 0 ? lanes_per_atom : 8;
     bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
     int rc;
     if (precision == MBF_FP64)
-        rc = zhou ? eam_dispatch_lpa<double, true>(lpa, S, nl, E, aux, slot_f, f_local, forces, per_atom, st)
-                  : eam_dispatch_lpa<double, false>(lpa, S, nl, E, aux, slot_f, f_local, forces, per_atom, st);
+        rc = zhou ? eam_dispatch_lpa<double, true>(lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, st)
+                  : eam_dispatch_lpa<double, false>(lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, st);
     else
-        rc = zhou ? eam_dispatch_lpa<float, true>(lpa, S, nl, E, aux, slot_f, f_local, forces, per_atom, st)
-                  : eam_dispatch_lpa<float, false>(lpa, S, nl, E, aux, slot_f, f_local, forces, per_atom, st);
+        rc = zhou ? eam_dispatch_lpa<float, true>(lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, st)
+                  : eam_dispatch_lpa<float, false>(lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
 }

@@ -66,8 +66,8 @@ struct SwRow {
 // SYM: every (i, j, k) record equals its (i, k, j) twin (one species), so a
 // slot needs one h evaluation per partner with the full lambda.
 template <typename T, int MAXN, bool SYM>
-__global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr, SwDev P,
-                         double *__restrict__ slot_G, double *__restrict__ f_local,
+__global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr,
+                         const int *__restrict__ rev, SwDev P, double *__restrict__ slot_G, double *__restrict__ f_local,
                          double *__restrict__ per_atom, int *__restrict__ err) {
     constexpr int GPB = SwGeom<MAXN>::GPB;
     __shared__ SwRow<T, MAXN> rows[GPB];
@@ -185,7 +185,8 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
                 v[7] += -hz * dy + Gz * dy;
                 v[8] += -hz * dz + Gz * dz;
                 npair += R.ok[s] ? 1.0 : 0.0;
-                size_t o = 3 * (size_t)(beg + s);
+                // the force on neighbour x goes to x's own slot (x -> i)
+                size_t o = 3 * (size_t)rev[beg + s];
                 slot_G[o] = Gx;
                 slot_G[o + 1] = Gy;
                 slot_G[o + 2] = Gz;
@@ -219,10 +220,10 @@ static int sw_launch(const SysView &S, const mbf_nlist *nl, const SwDev &P, doub
     int blocks = (S.n_atoms + GPB - 1) / GPB;
     int g = persistent_grid(blocks, BLOCK, (const void *)sw_force<T, MAXN, SYM>);
     PROF_BEGIN("sw_force", st);
-    sw_force<T, MAXN, SYM><<<g, BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, slot_G, f_local, per_atom, err);
+    sw_force<T, MAXN, SYM><<<g, BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, nl->rev, P, slot_G, f_local, per_atom, err);
     PROF_END("sw_force", st);
     MBF_CHECK_LAUNCH();
-    return gather_forces(S.n_atoms, nl->row_off, nl->rev, slot_G, f_local, forces, st);
+    return gather_forces(S.n_atoms, nl->row_off, slot_G, f_local, forces, st);
 }
 
 template <typename T, bool SYM>

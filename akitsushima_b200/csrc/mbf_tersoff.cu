@@ -8,8 +8,8 @@
 //
 // Owner computes, no atomics: the lane group of centre i evaluates every
 // zeta-term gradient of its angles, keeps the force on i and writes the force
-// each angle puts on neighbour x into the slot (i -> x); atom a later adds
-// the slots (x -> a) of all its neighbours x (gather_forces).
+// its angles put on neighbour x into x's own slot (x -> i); atom a later sums
+// its own row of slots (gather_forces).
 #include "mbf_util.cuh"
 
 namespace mbf {
@@ -325,7 +325,8 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
                 v[7] += -hz * dy + Gz * dy;
                 v[8] += -hz * dz + Gz * dz;
                 npair += R.ok[s] ? 1.0 : 0.0;
-                size_t o = 3 * (size_t)(beg + s);
+                // the force on neighbour x goes to x's own slot (x -> i)
+                size_t o = 3 * (size_t)rev[beg + s];
                 slot_G[o] = Gx;
                 slot_G[o + 1] = Gy;
                 slot_G[o + 2] = Gz;
@@ -368,7 +369,7 @@ static int te_launch(const SysView &S, const mbf_nlist *nl, const TeDev &P, doub
                                          per_atom, err);
     PROF_END("te_force", st);
     MBF_CHECK_LAUNCH();
-    return gather_forces(S.n_atoms, nl->row_off, nl->rev, slot_G, f_local, forces, st);
+    return gather_forces(S.n_atoms, nl->row_off, slot_G, f_local, forces, st);
 }
 
 }  // namespace mbf

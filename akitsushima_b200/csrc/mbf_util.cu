@@ -166,29 +166,36 @@ int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, in
     return MBF_OK;
 }
 
-// Gather the three-body forces a centre left on its neighbours: F_a +=
-// sum over slots (a -> x) of G[rev(a -> x)], the force on a from centre x.
-__global__ void gather_slot_forces(int n_atoms, const int *__restrict__ row_off,
-                                   const int *__restrict__ rev, const double *__restrict__ G,
+// Gather the three-body forces the centres left on atom a: every centre x
+// wrote the force its angles put on a into a's own slot (a -> x), so the
+// row is read contiguously, lane group per atom.
+__global__ void gather_slot_forces(int n_atoms, const int *__restrict__ row_off, const double *__restrict__ G,
                                    const double *__restrict__ f_local, double *__restrict__ forces) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= n_atoms) return;
-    double fx = f_local[3 * (size_t)a], fy = f_local[3 * (size_t)a + 1], fz = f_local[3 * (size_t)a + 2];
-    for (int s = row_off[a]; s < row_off[a + 1]; ++s) {
-        int r = rev[s];
-        fx += G[3 * (size_t)r];
-        fy += G[3 * (size_t)r + 1];
-        fz += G[3 * (size_t)r + 2];
+    constexpr int LPA = 8;
+    const int sub = threadIdx.x & (LPA - 1);
+    int a = blockIdx.x * (blockDim.x / LPA) + threadIdx.x / LPA;
+    double fx = 0, fy = 0, fz = 0;
+    if (a < n_atoms) {
+        for (int s = row_off[a] + sub; s < row_off[a + 1]; s += LPA) {
+            fx += G[3 * (size_t)s];
+            fy += G[3 * (size_t)s + 1];
+            fz += G[3 * (size_t)s + 2];
+        }
     }
-    forces[3 * (size_t)a] = fx;
-    forces[3 * (size_t)a + 1] = fy;
-    forces[3 * (size_t)a + 2] = fz;
+    fx = group_sum<LPA>(fx);
+    fy = group_sum<LPA>(fy);
+    fz = group_sum<LPA>(fz);
+    if (sub == 0 && a < n_atoms) {
+        forces[3 * (size_t)a] = f_local[3 * (size_t)a] + fx;
+        forces[3 * (size_t)a + 1] = f_local[3 * (size_t)a + 1] + fy;
+        forces[3 * (size_t)a + 2] = f_local[3 * (size_t)a + 2] + fz;
+    }
 }
 
-int gather_forces(int n_atoms, const int *row_off, const int *rev, const double *G,
-                  const double *f_local, double *forces, cudaStream_t st) {
+int gather_forces(int n_atoms, const int *row_off, const double *G, const double *f_local, double *forces,
+                  cudaStream_t st) {
     PROF_BEGIN("gather_forces", st);
-    gather_slot_forces<<<(n_atoms + 255) / 256, 256, 0, st>>>(n_atoms, row_off, rev, G, f_local, forces);
+    gather_slot_forces<<<(n_atoms + 15) / 16, 128, 0, st>>>(n_atoms, row_off, G, f_local, forces);
     PROF_END("gather_forces", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;

@@ -19,19 +19,20 @@ int exclusive_scan(const int *in, int *out, int n, int *ws, cudaStream_t st);
 int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, int n_struct,
                          double *partial, double *energy, double *virial, cudaStream_t st);
 
-int gather_forces(int n_atoms, const int *row_off, const int *rev, const double *G,
-                  const double *f_local, double *forces, cudaStream_t st);
+int gather_forces(int n_atoms, const int *row_off, const double *G, const double *f_local, double *forces,
+                  cudaStream_t st);
 
 // Layout of the evaluation workspace (all offsets 256-byte aligned):
 //   err      device error word (int)
 //   per_atom (n_atoms, ATOM_ACC) doubles
 //   f_local  (n_atoms, 3) doubles (three-body potentials: centre-local force)
 //   atom_aux (n_atoms, 2) doubles (EAM F'(rho), F(rho))
+//   pack     (n_atoms, 4) doubles (position + F'(rho), one record per atom)
 //   slot     (n_slots, 3) doubles (three-body force left on each neighbour)
 //   slot_b   (n_slots, 2) doubles (Tersoff bond order and its derivative)
 //   partial  (n_chunks, ATOM_ACC) doubles
 struct EvalLayout {
-    size_t err, per_atom, f_local, atom_aux, slot, slot_b, partial, total;
+    size_t err, per_atom, f_local, atom_aux, pack, slot, slot_b, partial, total;
 };
 
 static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -47,6 +48,8 @@ static inline EvalLayout eval_layout(int n_atoms, long long n_slots, int n_chunk
     o = align256(o + sizeof(double) * (size_t)n_atoms * 3);
     L.atom_aux = o;
     o = align256(o + sizeof(double) * (size_t)n_atoms * 2);
+    L.pack = o;
+    o = align256(o + sizeof(double) * (size_t)n_atoms * 4);
     L.slot = o;
     o = align256(o + sizeof(double) * (size_t)n_slots * 3);
     L.slot_b = o;

@@ -144,10 +144,10 @@ class DevicePotential:
         nl, batch, dl = self._resolve_list(lattice, pos, neigh_list, dev)
         batch.set_lattice(0, lattice)
         batch.set_positions(pos)
-        batch.set_types(torch.from_numpy(np.ascontiguousarray(ids)).to(dev, non_blocking=True))
+        batch.set_types(ids)
         res = self.evaluate(batch, dl)
+        f = batch.forces_to_host(res.forces)
         e = float(res.energy[0].item())
-        f = res.forces.cpu().numpy()
         if not need_stress:
             return e, f, None
         vol = abs(float(np.linalg.det(lattice)))

@@ -120,6 +120,9 @@ class Batch:
             np.repeat(np.arange(self.n_struct, dtype=np.int32), counts), device=dev)
         self.pos = torch.empty((self.n_atoms, 3), dtype=torch.float64, device=dev)
         self.types = torch.empty(self.n_atoms, dtype=torch.int32, device=dev)
+        self._pins = {}
+        self._pin_busy = {}
+        self._types_host = None
         self.set_positions(positions)
         self.set_types(type_ids)
         # reduction plan: chunks of REDUCE_CHUNK atoms inside one structure
@@ -140,35 +143,74 @@ class Batch:
 
     def set_positions(self, positions):
         """Copy new positions in place: one (N, 3) array or tensor for the
-        whole batch, or a sequence of (N_s, 3) arrays, one per structure."""
+        whole batch, or a sequence of (N_s, 3) arrays, one per structure.
+        Host arrays go through a pinned staging buffer (asynchronous copy)."""
         if isinstance(positions, torch.Tensor):
             src = positions.reshape(-1, 3)
-        elif isinstance(positions, np.ndarray) and positions.ndim == 2:
-            arr = np.ascontiguousarray(positions, dtype=np.float64)
-            if not np.isfinite(arr).all():
-                raise ValueError("positions contain NaN or inf")
-            src = torch.from_numpy(arr)
+            if tuple(src.shape) != (self.n_atoms, 3):
+                raise ValueError(f"positions have shape {tuple(src.shape)}, expected ({self.n_atoms}, 3)")
+            self.pos.copy_(src.to(torch.float64), non_blocking=src.device.type != "cpu")
+            return
+        if isinstance(positions, np.ndarray) and positions.ndim == 2:
+            arr = positions
         else:
-            parts = [torch.as_tensor(np.asarray(p, np.float64)).reshape(-1, 3)
-                     if not isinstance(p, torch.Tensor) else p.reshape(-1, 3).to("cpu", torch.float64)
-                     for p in positions]
-            src = torch.cat(parts) if parts else torch.zeros((0, 3), dtype=torch.float64)
-        if tuple(src.shape) != (self.n_atoms, 3):
-            raise ValueError(f"positions have shape {tuple(src.shape)}, expected ({self.n_atoms}, 3)")
-        self.pos.copy_(src.to(torch.float64), non_blocking=src.device.type != "cpu")
+            arr = np.concatenate([np.asarray(p, np.float64).reshape(-1, 3) for p in positions]) \
+                if len(positions) else np.zeros((0, 3))
+        if arr.shape != (self.n_atoms, 3):
+            raise ValueError(f"positions have shape {arr.shape}, expected ({self.n_atoms}, 3)")
+        if not np.isfinite(arr).all():
+            raise ValueError("positions contain NaN or inf")
+        if self.device.type != "cuda":
+            self.pos.copy_(torch.from_numpy(np.ascontiguousarray(arr, np.float64)))
+            return
+        pin = self._pinned("pos", (self.n_atoms, 3), torch.float64)
+        if self._pin_busy.get("pos"):
+            # the previous asynchronous copy out of this buffer must finish first
+            torch.cuda.current_stream(self.device).synchronize()
+        np.copyto(pin.numpy(), arr, casting="same_kind")
+        self.pos.copy_(pin, non_blocking=True)
+        self._pin_busy["pos"] = True
+
+    def _pinned(self, key, shape, dtype):
+        buf = self._pins.get(key)
+        if buf is None or tuple(buf.shape) != tuple(shape):
+            buf = torch.empty(shape, dtype=dtype, pin_memory=True)
+            self._pins[key] = buf
+        return buf
+
+    def forces_to_host(self, forces):
+        """Device (N, 3) forces to a host numpy array through a pinned buffer."""
+        if self.device.type != "cuda":
+            return forces.cpu().numpy()
+        pin = self._pinned("forces", (self.n_atoms, 3), torch.float64)
+        pin.copy_(forces, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        self._pin_busy["pos"] = False
+        return pin.numpy().copy()
 
     def set_types(self, type_ids):
+        """Species ids (torch tensor, or host arrays; an unchanged host array
+        is not uploaded again)."""
         if isinstance(type_ids, torch.Tensor):
-            self.types.copy_(type_ids.to(torch.int32))
+            self.types.copy_(type_ids.to(torch.int32), non_blocking=type_ids.device.type != "cpu")
+            self._types_host = None
             return
-        arr = np.concatenate([np.asarray(t, np.int32).reshape(-1) for t in type_ids]) \
-            if len(type_ids) else np.zeros(0, np.int32)
+        if isinstance(type_ids, np.ndarray) and type_ids.ndim == 1:
+            arr = type_ids.astype(np.int32, copy=False)
+        else:
+            arr = np.concatenate([np.asarray(t, np.int32).reshape(-1) for t in type_ids]) \
+                if len(type_ids) else np.zeros(0, np.int32)
         if arr.shape != (self.n_atoms,):
             raise ValueError("type_ids do not match the atom count")
-        self.types.copy_(torch.from_numpy(arr))
+        if self._types_host is not None and np.array_equal(arr, self._types_host):
+            return
+        self.types.copy_(torch.from_numpy(np.ascontiguousarray(arr)))
+        self._types_host = arr.copy()
 
     def set_lattice(self, s, lattice):
         lat = np.asarray(lattice, np.float64).reshape(3, 3)
+        if np.array_equal(lat, self.lattices[s]):
+            return
         cell_metrics(lat)
         self.lattices[s] = lat
         self.volumes[s] = abs(np.linalg.det(lat))

@@ -23,7 +23,6 @@ max over ranks.
 import argparse
 import json
 import os
-import subprocess
 import sys
 import time
 
@@ -53,45 +52,62 @@ def cpu_count():
         return os.cpu_count() or 1
 
 
-def clocks_start(path):
-    cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
-           "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-           "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-           "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"]
-    try:
-        fh = open(path, "w")
-        return subprocess.Popen(cmd, stdout=fh, stderr=subprocess.DEVNULL), fh
-    except (OSError, FileNotFoundError):
-        return None, None
+class ClockSampler:
+    """SM clock and clock-event reasons sampled through NVML every few
+    milliseconds on a background thread while the timed region runs (read
+    only; no setting of the GPU is touched)."""
 
+    NAMES = {"applications_clocks_setting": 0x2, "sw_power_cap": 0x4, "hw_slowdown": 0x8,
+             "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+             "hw_power_brake_slowdown": 0x80}
 
-def clocks_stop(proc_fh, path, gpu_index):
-    proc, fh = proc_fh
-    if proc is None:
-        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-    proc.terminate()
-    try:
-        proc.wait(timeout=5)
-    except subprocess.TimeoutExpired:
-        proc.kill()
-    fh.close()
-    sm, mx, reasons = [], None, set()
-    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-    with open(path) as f:
-        for line in f:
-            p = [x.strip() for x in line.split(",")]
-            if len(p) < 9 or p[0] != str(gpu_index):
-                continue
+    def __init__(self, gpu_index, period_s=0.002):
+        import threading
+        self.samples, self.reasons, self.max_mhz, self.err = [], set(), None, None
+        self._stop = threading.Event()
+        self._period = period_s
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(gpu_index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM))
+        except Exception as exc:  # no NVML: report it instead of a number
+            self._nv = None
+            self.err = f"nvml unavailable: {exc}"
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
             try:
-                sm.append(float(p[1]))
-                mx = float(p[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, p[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-    return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
-            "reasons": sorted(reasons), "samples": len(sm)}
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for name, b in self.NAMES.items():
+                    if bits & b:
+                        self.reasons.add(name)
+            except Exception as exc:
+                self.err = str(exc)
+                return
+            self._stop.wait(self._period)
+
+    def __enter__(self):
+        if self._nv is not None:
+            self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._nv is not None:
+            self._t.join(timeout=2)
+
+    def summary(self):
+        out = {"sm_mhz": float(np.median(self.samples)) if self.samples else None,
+               "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+               "samples": len(self.samples), "source": "NVML, 2 ms period, during the timed steps"}
+        if self.err:
+            out["note"] = self.err
+        return out
 
 
 def time_reference(lat, pos, ids, steps, warmup):
@@ -183,23 +199,21 @@ def main():
     torch.cuda.synchronize()
 
     # timed region
-    clk_path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
-    os.makedirs(os.path.dirname(clk_path), exist_ok=True)
-    clk = clocks_start(clk_path)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    for k in range(args.steps):
-        flush.zero_()
-        ev[k][0].record()
-        pot.evaluate(batch, dnl, out=out)
-        ev[k][1].record()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    clocks = clocks_stop(clk, clk_path, local)
+    with ClockSampler(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            pot.evaluate(batch, dnl, out=out)
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    clocks = clk.summary()
     ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
     if dist:
         t = torch.tensor([ms], device=dev, dtype=torch.float64)
