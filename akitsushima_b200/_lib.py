@@ -26,7 +26,7 @@ _sz = ctypes.c_size_t
 
 class MbfSystem(ctypes.Structure):
     _fields_ = [("n_atoms", _i), ("n_struct", _i), ("positions", _vp), ("types", _vp),
-                ("atom_struct", _vp), ("struct_off", _vp), ("cells", _vp)]
+                ("atom_struct", _vp), ("struct_off", _vp), ("cells", _vp), ("orthorhombic", _i)]
 
 
 class MbfNlist(ctypes.Structure):

@@ -29,6 +29,7 @@ struct SysView {
     const int *atom_struct;
     const int *struct_off;
     const double *cells;
+    int ortho;
 };
 
 static inline SysView make_view(const mbf_system *s) {
@@ -40,6 +41,7 @@ static inline SysView make_view(const mbf_system *s) {
     v.atom_struct = s->atom_struct;
     v.struct_off = s->struct_off;
     v.cells = s->cells;
+    v.ortho = s->orthorhombic;
     return v;
 }
 

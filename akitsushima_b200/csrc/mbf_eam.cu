@@ -276,6 +276,31 @@ __device__ __forceinline__ void mic_fast(const double *__restrict__ c, double rx
     dz = sx * c[2] + sy * c[5] + sz * c[8];
 }
 
+// The cell of one atom as the force kernels need it: a diagonal cell keeps
+// six scalars (lengths and inverse lengths) instead of the 3x3 pair.
+template <bool ORTHO>
+struct CellView {
+    const double *c;
+    double L0, L1, L2, i0, i1, i2;
+    __device__ __forceinline__ void load(const SysView &S, int atom) {
+        c = cell_of(S, atom);
+        if (ORTHO) {
+            L0 = c[0]; L1 = c[4]; L2 = c[8];
+            i0 = c[9]; i1 = c[13]; i2 = c[17];
+        }
+    }
+    __device__ __forceinline__ void mic(double rx, double ry, double rz, double &dx, double &dy,
+                                        double &dz) const {
+        if (ORTHO) {
+            dx = rx - L0 * rint_shift(rx * i0);
+            dy = ry - L1 * rint_shift(ry * i1);
+            dz = rz - L2 * rint_shift(rz * i2);
+        } else {
+            mic_fast(c, rx, ry, rz, dx, dy, dz);
+        }
+    }
+};
+
 // Distance of a minimum-imaged displacement in the working precision: the
 // wrap and the square stay float64; the root is taken in T.
 template <typename T>
@@ -300,7 +325,9 @@ __device__ __forceinline__ double4 ld_pack(const double4 *__restrict__ pk, int j
 }
 
 // rho-bar_i over the full row, F(rho-bar_i) and F'(rho-bar_i) in float64.
-template <typename T, int LPA, bool ZHOU>
+// The next neighbour's index, record and species are loaded one iteration
+// ahead of their use.
+template <typename T, int LPA, bool ZHOU, bool ORTHO>
 __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *__restrict__ row_off,
                                                          const int *__restrict__ nbr, EamDev E,
                                                          double4 *__restrict__ pk,
@@ -313,18 +340,25 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *_
     for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
         int i = base + threadIdx.x / LPA;
         double acc = 0.0;
-        int si = 0;
         if (i < S.n_atoms) {
-            si = S.types[i];
-            const double *cell = cell_of(S, i);
+            CellView<ORTHO> cv;
+            cv.load(S, i);
             double4 pi = ld_pack(pk, i);
             int end = row_off[i + 1];
-            for (int s = row_off[i] + sub; s < end; s += LPA) {
-                int j = nbr[s];
-                double4 pj = ld_pack(pk, j);
-                int sj = __ldg(S.types + j);
+            int s = row_off[i] + sub;
+            int jn = s < end ? nbr[s] : i;
+            double4 pn = ld_pack(pk, jn);
+            int tn = __ldg(S.types + jn);
+            for (; s < end; s += LPA) {
+                double4 pj = pn;
+                int sj = tn;
+                if (s + LPA < end) {
+                    jn = nbr[s + LPA];
+                    pn = ld_pack(pk, jn);
+                    tn = __ldg(S.types + jn);
+                }
                 double dx, dy, dz;
-                mic_fast(cell, pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
+                cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
                 double r2 = dx * dx + dy * dy + dz * dz;
                 if (!(r2 < rc2 && r2 > 1e-24)) continue;
                 if (ZHOU) {
@@ -340,15 +374,24 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *_
             }
         }
         acc = group_sum<LPA>(acc);
-        if (sub == 0 && i < S.n_atoms) {
-            double rb = acc > 0.0 ? acc : 0.0;
-            double F, dF;
-            embed64(E, E.F_f[si], rb, F, dF);
-            pk[i].w = dF;
-            aux[2 * (size_t)i] = dF;
-            aux[2 * (size_t)i + 1] = F;
-        }
+        if (sub == 0 && i < S.n_atoms) aux[2 * (size_t)i] = acc;
     }
+}
+
+// F(rho-bar) and F'(rho-bar) in float64, rho-bar clamped at 0
+// (engine/_eam_kernels.py:268-274); kept out of the density loop so the
+// float64 pow/log of the embedding does not set that kernel's register count.
+__global__ void eam_embed(int n_atoms, const int *__restrict__ types, EamDev E, double4 *__restrict__ pk,
+                          double *__restrict__ aux) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_atoms) return;
+    double acc = aux[2 * (size_t)i];
+    double rb = acc > 0.0 ? acc : 0.0;
+    double F, dF;
+    embed64(E, E.F_f[types[i]], rb, F, dF);
+    pk[i].w = dF;
+    aux[2 * (size_t)i] = dF;
+    aux[2 * (size_t)i + 1] = F;
 }
 
 // Force pass over the upper half of every row: each unordered pair once.
@@ -361,8 +404,8 @@ template <typename T> struct SlotVec;
 template <> struct SlotVec<double> { typedef double3 type; };
 template <> struct SlotVec<float> { typedef float3 type; };
 
-template <typename T, int LPA, bool ZHOU>
-__global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__restrict__ row_off,
+template <typename T, int LPA, bool ZHOU, bool ORTHO>
+__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? 6 : 4) eam_force(SysView S, const int *__restrict__ row_off,
                                                        const int *__restrict__ upper,
                                                        const int *__restrict__ nbr,
                                                        const int *__restrict__ rev, EamDev E,
@@ -379,25 +422,36 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__r
     const double rc = E.r_cut, rc2 = rc * rc;
     for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
         int i = base + threadIdx.x / LPA;
-        double fx = 0, fy = 0, fz = 0, e = 0, npair = 0;
+        double fx = 0, fy = 0, fz = 0, e = 0;
+        int npair = 0;
         double vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
         if (i < S.n_atoms) {
             int si = S.types[i];
             double4 pi = ld_pack(pk, i);
             T Fp_i = (T)pi.w;
-            const double *cell = cell_of(S, i);
+            CellView<ORTHO> cv;
+            cv.load(S, i);
             int end = row_off[i + 1];
-            for (int s = upper[i] + sub; s < end; s += LPA) {
-                int j = nbr[s];
-                int rs = rev[s];
-                double4 pj = ld_pack(pk, j);
-                int sj = __ldg(S.types + j);
+            int s = upper[i] + sub;
+            int jn = s < end ? nbr[s] : i;
+            int rn = s < end ? rev[s] : 0;
+            double4 pn = ld_pack(pk, jn);
+            int tn = __ldg(S.types + jn);
+            for (; s < end; s += LPA) {
+                double4 pj = pn;
+                int sj = tn, rs = rn;
+                if (s + LPA < end) {
+                    jn = nbr[s + LPA];
+                    rn = rev[s + LPA];
+                    pn = ld_pack(pk, jn);
+                    tn = __ldg(S.types + jn);
+                }
                 double dx, dy, dz;
-                mic_fast(cell, pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
+                cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
                 double r2 = dx * dx + dy * dy + dz * dz;
                 double px = 0, py = 0, pz = 0;
                 if (r2 < rc2 && r2 > 1e-24) {
-                    npair += 1.0;
+                    npair += 1;
                     T r = pair_dist<T>(r2);
                     T phi, dphi, drho_j, drho_i;
                     if (ZHOU) {
@@ -452,7 +506,7 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_force(SysView S, const int *__r
             pa[1] = vxx; pa[2] = vxy; pa[3] = vxz;
             pa[4] = vxy; pa[5] = vyy; pa[6] = vyz;
             pa[7] = vxz; pa[8] = vyz; pa[9] = vzz;
-            pa[10] = npair;
+            pa[10] = (double)npair;
         }
     }
 }
@@ -485,7 +539,7 @@ __global__ void eam_gather(int n_atoms, const int *__restrict__ row_off, const i
     }
 }
 
-template <typename T, int LPA, bool ZHOU>
+template <typename T, int LPA, bool ZHOU, bool ORTHO>
 static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, double4 *pk, double *aux,
                       void *slot, double *f_local, double *forces, double *per_atom, cudaStream_t st) {
     typedef typename SlotVec<T>::type V3;
@@ -494,14 +548,18 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, do
     PROF_BEGIN("eam_pack", st);
     eam_pack<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S, pk);
     PROF_END("eam_pack", st);
-    int g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_density<T, LPA, ZHOU>);
+    int g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_density<T, LPA, ZHOU, ORTHO>);
     PROF_BEGIN("eam_density", st);
-    eam_density<T, LPA, ZHOU><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, E, pk, aux);
+    eam_density<T, LPA, ZHOU, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, E, pk, aux);
     PROF_END("eam_density", st);
     MBF_CHECK_LAUNCH();
-    g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_force<T, LPA, ZHOU>);
+    PROF_BEGIN("eam_embed", st);
+    eam_embed<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S.n_atoms, S.types, E, pk, aux);
+    PROF_END("eam_embed", st);
+    MBF_CHECK_LAUNCH();
+    g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_force<T, LPA, ZHOU, ORTHO>);
     PROF_BEGIN("eam_force", st);
-    eam_force<T, LPA, ZHOU><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, E, pk,
+    eam_force<T, LPA, ZHOU, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, E, pk,
                                                      aux, (V3 *)slot, f_local, per_atom);
     PROF_END("eam_force", st);
     MBF_CHECK_LAUNCH();
@@ -513,17 +571,28 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, do
     return MBF_OK;
 }
 
-template <typename T, bool ZHOU>
+template <typename T, bool ZHOU, bool ORTHO>
 static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E, double4 *pk,
                             double *aux, void *slot, double *f_local, double *forces, double *per_atom,
                             cudaStream_t st) {
     switch (lpa) {
-        case 4: return eam_launch<T, 4, ZHOU>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
-        case 8: return eam_launch<T, 8, ZHOU>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
-        case 16: return eam_launch<T, 16, ZHOU>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
-        case 32: return eam_launch<T, 32, ZHOU>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
+        case 4: return eam_launch<T, 4, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
+        case 8: return eam_launch<T, 8, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
+        case 16: return eam_launch<T, 16, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
+        case 32: return eam_launch<T, 32, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
         default: return MBF_ERR_ARGUMENT;
     }
+}
+
+template <typename T>
+static int eam_dispatch(bool zhou, int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E,
+                        double4 *pk, double *aux, void *slot, double *f_local, double *forces,
+                        double *per_atom, cudaStream_t st) {
+    if (zhou)
+        return S.ortho ? eam_dispatch_lpa<T, true, true>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, st)
+                       : eam_dispatch_lpa<T, true, false>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
+    return S.ortho ? eam_dispatch_lpa<T, false, true>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, st)
+                   : eam_dispatch_lpa<T, false, false>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
 }
 
 }  // namespace mbf
@@ -563,11 +632,9 @@ extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mb
     bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
     int rc;
     if (precision == MBF_FP64)
-        rc = zhou ? eam_dispatch_lpa<double, true>(lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, st)
-                  : eam_dispatch_lpa<double, false>(lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, st);
+        rc = eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, st);
     else
-        rc = zhou ? eam_dispatch_lpa<float, true>(lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, st)
-                  : eam_dispatch_lpa<float, false>(lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, st);
+        rc = eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
 }

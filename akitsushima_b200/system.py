@@ -218,10 +218,11 @@ class Batch:
         self.cells[s].copy_(torch.from_numpy(row))
 
     def mbf_system(self):
-        s = _lib.MbfSystem(self.n_atoms, self.n_struct, _lib.ptr(self.pos), _lib.ptr(self.types),
-                           _lib.ptr(self.atom_struct), _lib.ptr(self.struct_off),
-                           _lib.ptr(self.cells))
-        return s
+        off = self.lattices - np.einsum("sij,ij->sij", self.lattices, np.eye(3))
+        ortho = 1 if not np.any(off) else 0
+        return _lib.MbfSystem(self.n_atoms, self.n_struct, _lib.ptr(self.pos), _lib.ptr(self.types),
+                              _lib.ptr(self.atom_struct), _lib.ptr(self.struct_off),
+                              _lib.ptr(self.cells), ortho)
 
     def reduce_plan(self):
         return _lib.MbfReducePlan(int(self.chunk.shape[0]), _lib.ptr(self.chunk),

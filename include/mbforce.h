@@ -58,6 +58,9 @@ typedef struct mbf_system {
     const int *atom_struct;    /* (n_atoms,) */
     const int *struct_off;     /* (n_struct + 1) */
     const double *cells;       /* (n_struct, 18) */
+    int orthorhombic;          /* 1 if every lattice is diagonal (off-diagonal
+                                  entries exactly 0): kernels use a 3-axis
+                                  minimum image; 0 for general cells */
 } mbf_system;
 
 typedef struct mbf_nlist {
