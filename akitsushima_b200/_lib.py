@@ -9,7 +9,7 @@ import os
 import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libmbforce.so")
+LIB_PATH = os.environ.get("MBF_LIB_PATH") or os.path.join(_HERE, "libmbforce.so")
 
 MBF_OK = 0
 MBF_ERR_CAPACITY = -3
@@ -73,6 +73,7 @@ _SIGS = {
     "mbf_nl_half_workspace_bytes": (_sz, [_i]),
     "mbf_nl_half_pairs": (_i, [ctypes.POINTER(MbfNlist), _vp, _vp, _vp, _sz, _vp]),
     "mbf_eval_workspace_bytes": (_sz, [_i, _ll, _i]),
+    "mbf_eval_status": (_i, [_vp, ctypes.POINTER(_i), _vp]),
     "mbf_eam_eval": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                           ctypes.POINTER(MbfEamTables), ctypes.POINTER(MbfReducePlan), _i, _i,
                           _vp, _sz, _vp, _vp, _vp, _vp]),

@@ -40,12 +40,15 @@ def up_to_date():
     return all(os.path.getmtime(p) <= t for p in _deps())
 
 
-def build(force=False, verbose=False, extra=()):
-    """Compile every .cu of csrc/ into one shared library (parallel objects)."""
-    if not force and up_to_date():
+def build(force=False, verbose=False, extra=(), out=None):
+    """Compile every .cu of csrc/ into one shared library (parallel objects).
+    ``extra`` adds nvcc flags (e.g. -DMBF_CHECKS for the bounds-checked
+    debugging build); ``out`` writes the library elsewhere."""
+    lib_path = out or LIB
+    if not force and out is None and up_to_date():
         return LIB
     nvcc = nvcc_path()
-    objdir = os.path.join(PKG, "_build")
+    objdir = os.path.join(PKG, "_build" if out is None else "_build_alt")
     os.makedirs(objdir, exist_ok=True)
     flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                     "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
@@ -68,15 +71,18 @@ def build(force=False, verbose=False, extra=()):
             failed.append(src)
     if failed:
         raise RuntimeError("nvcc failed on " + ", ".join(os.path.basename(f) for f in failed))
-    tmp = LIB + ".tmp"
+    tmp = lib_path + ".tmp"
     subprocess.run([nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib_path)
+    return lib_path
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("-v", "--verbose", action="store_true")
+    ap.add_argument("--checks", action="store_true", help="bounds-checked debugging build")
+    ap.add_argument("--out", default=None, help="library path (default: in the package)")
     a = ap.parse_args()
-    print(build(force=a.force, verbose=a.verbose))
+    print(build(force=a.force, verbose=a.verbose, extra=["-DMBF_CHECKS"] if a.checks else (),
+                out=a.out))

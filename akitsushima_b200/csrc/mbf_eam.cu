@@ -28,6 +28,23 @@ struct EamDev {
     double r_cut;
 };
 
+// Bounds checks on every neighbour-list index the kernels dereference: a
+// failed check records (site, index) in the workspace error words and skips
+// the access; mbf_eval_status() returns them to the host.  They are always
+// compiled in: the float64 build of these kernels without them raised an
+// illegal-address fault on B200 whose cause was not found, while the checked
+// build, with the same indices, runs clean.
+struct Chk {
+    int *err;
+    int n_atoms;
+    long long n_slots;
+    int ns;
+};
+#define MBF_OK_IDX(ck, site, idx, lo, hi)                                          \
+    (((long long)(idx) >= (long long)(lo) && (long long)(idx) < (long long)(hi))    \
+         ? true                                                                    \
+         : (atomicCAS((ck).err + 1, 0, (site)) == 0 ? ((ck).err[2] = (int)(idx), false) : false))
+
 // ---- generic function evaluation (engine/_eam_kernels.py:129-228) -------
 
 template <typename T>
@@ -331,7 +348,7 @@ template <typename T, int LPA, bool ZHOU, bool ORTHO>
 __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *__restrict__ row_off,
                                                          const int *__restrict__ nbr, EamDev E,
                                                          double4 *__restrict__ pk,
-                                                         double *__restrict__ aux) {
+                                                         double *__restrict__ aux, Chk ck) {
     __shared__ ZTab<T> Z;
     if (ZHOU) load_ztab<T>(E, Z);
     const int sub = threadIdx.x & (LPA - 1);
@@ -346,14 +363,19 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *_
             double4 pi = ld_pack(pk, i);
             int end = row_off[i + 1];
             int s = row_off[i] + sub;
-            int jn = s < end ? nbr[s] : i;
+            if (!MBF_OK_IDX(ck, 11, end, 0, ck.n_slots + 1)) end = s;
+            int jn = i;
+            if (s < end && MBF_OK_IDX(ck, 12, s, 0, ck.n_slots)) jn = nbr[s];
+            if (!MBF_OK_IDX(ck, 13, jn, 0, ck.n_atoms)) jn = i;
             double4 pn = ld_pack(pk, jn);
             int tn = __ldg(S.types + jn);
             for (; s < end; s += LPA) {
                 double4 pj = pn;
                 int sj = tn;
+                if (!MBF_OK_IDX(ck, 14, sj, 0, ck.ns)) sj = 0;
                 if (s + LPA < end) {
-                    jn = nbr[s + LPA];
+                    jn = MBF_OK_IDX(ck, 15, s + LPA, 0, ck.n_slots) ? nbr[s + LPA] : i;
+                    if (!MBF_OK_IDX(ck, 16, jn, 0, ck.n_atoms)) jn = i;
                     pn = ld_pack(pk, jn);
                     tn = __ldg(S.types + jn);
                 }
@@ -382,9 +404,10 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *_
 // (engine/_eam_kernels.py:268-274); kept out of the density loop so the
 // float64 pow/log of the embedding does not set that kernel's register count.
 __global__ void eam_embed(int n_atoms, const int *__restrict__ types, EamDev E, double4 *__restrict__ pk,
-                          double *__restrict__ aux) {
+                          double *__restrict__ aux, Chk ck) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_atoms) return;
+    if (!MBF_OK_IDX(ck, 41, types[i], 0, ck.ns)) return;
     double acc = aux[2 * (size_t)i];
     double rb = acc > 0.0 ? acc : 0.0;
     double F, dF;
@@ -405,7 +428,7 @@ template <> struct SlotVec<double> { typedef double3 type; };
 template <> struct SlotVec<float> { typedef float3 type; };
 
 template <typename T, int LPA, bool ZHOU, bool ORTHO>
-__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? 6 : 4) eam_force(SysView S, const int *__restrict__ row_off,
+__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? 6 : 1) eam_force(SysView S, const int *__restrict__ row_off,
                                                        const int *__restrict__ upper,
                                                        const int *__restrict__ nbr,
                                                        const int *__restrict__ rev, EamDev E,
@@ -413,7 +436,7 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? 6 : 4) eam_force(S
                                                        const double *__restrict__ aux,
                                                        typename SlotVec<T>::type *__restrict__ slot_f,
                                                        double *__restrict__ f_local,
-                                                       double *__restrict__ per_atom) {
+                                                       double *__restrict__ per_atom, Chk ck) {
     typedef typename SlotVec<T>::type V3;
     __shared__ ZTab<T> Z;
     if (ZHOU) load_ztab<T>(E, Z);
@@ -432,17 +455,27 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? 6 : 4) eam_force(S
             CellView<ORTHO> cv;
             cv.load(S, i);
             int end = row_off[i + 1];
-            int s = upper[i] + sub;
-            int jn = s < end ? nbr[s] : i;
-            int rn = s < end ? rev[s] : 0;
+            int up = upper[i];
+            if (!MBF_OK_IDX(ck, 21, up, row_off[i], end + 1)) up = end;
+            int s = up + sub;
+            int jn = i, rn = 0;
+            if (s < end && MBF_OK_IDX(ck, 22, s, 0, ck.n_slots)) {
+                jn = nbr[s];
+                rn = rev[s];
+            }
+            if (!MBF_OK_IDX(ck, 23, jn, 0, ck.n_atoms)) jn = i;
             double4 pn = ld_pack(pk, jn);
             int tn = __ldg(S.types + jn);
             for (; s < end; s += LPA) {
                 double4 pj = pn;
                 int sj = tn, rs = rn;
+                if (!MBF_OK_IDX(ck, 24, sj, 0, ck.ns)) sj = 0;
                 if (s + LPA < end) {
-                    jn = nbr[s + LPA];
-                    rn = rev[s + LPA];
+                    if (MBF_OK_IDX(ck, 25, s + LPA, 0, ck.n_slots)) {
+                        jn = nbr[s + LPA];
+                        rn = rev[s + LPA];
+                    }
+                    if (!MBF_OK_IDX(ck, 26, jn, 0, ck.n_atoms)) jn = i;
                     pn = ld_pack(pk, jn);
                     tn = __ldg(S.types + jn);
                 }
@@ -483,7 +516,7 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? 6 : 4) eam_force(S
                 w.x = (T)(-px);
                 w.y = (T)(-py);
                 w.z = (T)(-pz);
-                slot_f[rs] = w;
+                if (MBF_OK_IDX(ck, 27, rs, 0, ck.n_slots)) slot_f[rs] = w;
             }
         }
         fx = group_sum<LPA>(fx);
@@ -516,13 +549,16 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? 6 : 4) eam_force(S
 template <typename V3, int LPA>
 __global__ void eam_gather(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ upper,
                            const V3 *__restrict__ slot_f, const double *__restrict__ f_local,
-                           double *__restrict__ forces) {
+                           double *__restrict__ forces, Chk ck) {
     const int sub = threadIdx.x & (LPA - 1);
     const int gpb = blockDim.x / LPA;
     int a = blockIdx.x * gpb + threadIdx.x / LPA;
     double fx = 0, fy = 0, fz = 0;
     if (a < n_atoms) {
-        for (int s = row_off[a] + sub; s < upper[a]; s += LPA) {
+        int up = upper[a];
+        if (!MBF_OK_IDX(ck, 31, up, row_off[a], row_off[a + 1] + 1)) up = row_off[a];
+        for (int s = row_off[a] + sub; s < up; s += LPA) {
+            if (!MBF_OK_IDX(ck, 32, s, 0, ck.n_slots)) break;
             V3 w = slot_f[s];
             fx += (double)w.x;
             fy += (double)w.y;
@@ -541,7 +577,7 @@ __global__ void eam_gather(int n_atoms, const int *__restrict__ row_off, const i
 
 template <typename T, int LPA, bool ZHOU, bool ORTHO>
 static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, double4 *pk, double *aux,
-                      void *slot, double *f_local, double *forces, double *per_atom, cudaStream_t st) {
+                      void *slot, double *f_local, double *forces, double *per_atom, Chk ck, cudaStream_t st) {
     typedef typename SlotVec<T>::type V3;
     int gpb = EAM_BLOCK / LPA;
     int blocks = (S.n_atoms + gpb - 1) / gpb;
@@ -550,22 +586,22 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, do
     PROF_END("eam_pack", st);
     int g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_density<T, LPA, ZHOU, ORTHO>);
     PROF_BEGIN("eam_density", st);
-    eam_density<T, LPA, ZHOU, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, E, pk, aux);
+    eam_density<T, LPA, ZHOU, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, E, pk, aux, ck);
     PROF_END("eam_density", st);
     MBF_CHECK_LAUNCH();
     PROF_BEGIN("eam_embed", st);
-    eam_embed<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S.n_atoms, S.types, E, pk, aux);
+    eam_embed<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S.n_atoms, S.types, E, pk, aux, ck);
     PROF_END("eam_embed", st);
     MBF_CHECK_LAUNCH();
     g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_force<T, LPA, ZHOU, ORTHO>);
     PROF_BEGIN("eam_force", st);
     eam_force<T, LPA, ZHOU, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, E, pk,
-                                                     aux, (V3 *)slot, f_local, per_atom);
+                                                     aux, (V3 *)slot, f_local, per_atom, ck);
     PROF_END("eam_force", st);
     MBF_CHECK_LAUNCH();
     PROF_BEGIN("eam_gather", st);
     eam_gather<V3, 8><<<(S.n_atoms + 15) / 16, 128, 0, st>>>(S.n_atoms, nl->row_off, nl->upper,
-                                                             (const V3 *)slot, f_local, forces);
+                                                             (const V3 *)slot, f_local, forces, ck);
     PROF_END("eam_gather", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;
@@ -574,12 +610,12 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, do
 template <typename T, bool ZHOU, bool ORTHO>
 static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E, double4 *pk,
                             double *aux, void *slot, double *f_local, double *forces, double *per_atom,
-                            cudaStream_t st) {
+                            Chk ck, cudaStream_t st) {
     switch (lpa) {
-        case 4: return eam_launch<T, 4, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
-        case 8: return eam_launch<T, 8, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
-        case 16: return eam_launch<T, 16, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
-        case 32: return eam_launch<T, 32, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
+        case 4: return eam_launch<T, 4, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
+        case 8: return eam_launch<T, 8, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
+        case 16: return eam_launch<T, 16, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
+        case 32: return eam_launch<T, 32, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
         default: return MBF_ERR_ARGUMENT;
     }
 }
@@ -587,12 +623,12 @@ static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, cons
 template <typename T>
 static int eam_dispatch(bool zhou, int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E,
                         double4 *pk, double *aux, void *slot, double *f_local, double *forces,
-                        double *per_atom, cudaStream_t st) {
+                        double *per_atom, Chk ck, cudaStream_t st) {
     if (zhou)
-        return S.ortho ? eam_dispatch_lpa<T, true, true>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, st)
-                       : eam_dispatch_lpa<T, true, false>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
-    return S.ortho ? eam_dispatch_lpa<T, false, true>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, st)
-                   : eam_dispatch_lpa<T, false, false>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, st);
+        return S.ortho ? eam_dispatch_lpa<T, true, true>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st)
+                       : eam_dispatch_lpa<T, true, false>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
+    return S.ortho ? eam_dispatch_lpa<T, false, true>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st)
+                   : eam_dispatch_lpa<T, false, false>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
 }
 
 }  // namespace mbf
@@ -626,15 +662,21 @@ extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mb
     double *per_atom = ws_at<double>(workspace, L.per_atom);
     double *partial = ws_at<double>(workspace, L.partial);
     void *slot_f = ws_at<char>(workspace, L.slot);
+    Chk ck;
+    ck.err = ws_at<int>(workspace, L.err);
+    ck.n_atoms = sys->n_atoms;
+    ck.n_slots = nl->n_slots;
+    ck.ns = tab->ns;
+    if (cudaMemsetAsync(ck.err, 0, 16, st) != cudaSuccess) return MBF_ERR_CUDA;
     double *f_local = ws_at<double>(workspace, L.f_local);
     double4 *pk = ws_at<double4>(workspace, L.pack);
     int lpa = lanes_per_atom > 0 ? lanes_per_atom : 8;
     bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
     int rc;
     if (precision == MBF_FP64)
-        rc = eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, st);
+        rc = eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, st);
     else
-        rc = eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, st);
+        rc = eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
 }

@@ -399,7 +399,7 @@ extern "C" int mbf_tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, cons
     P.tri = tab->tri;
     P.rc = tab->r_cut;
     int *err = ws_at<int>(workspace, L.err);
-    if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return MBF_ERR_CUDA;
+    if (cudaMemsetAsync(err, 0, 16, st) != cudaSuccess) return MBF_ERR_CUDA;
     double *per_atom = ws_at<double>(workspace, L.per_atom);
     double *f_local = ws_at<double>(workspace, L.f_local);
     double *slot_G = ws_at<double>(workspace, L.slot);

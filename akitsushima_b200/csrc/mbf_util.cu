@@ -224,4 +224,13 @@ size_t mbf_eval_workspace_bytes(int n_atoms, long long n_slots, int n_chunks) {
     return mbf::eval_layout(n_atoms, n_slots, n_chunks).total;
 }
 
+int mbf_eval_status(const void *workspace, int *host_words, void *stream) {
+    if (!workspace || !host_words) return MBF_ERR_ARGUMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemcpyAsync(host_words, workspace, 4 * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return MBF_ERR_CUDA;
+    return MBF_OK;
+}
+
 }  // extern "C"

@@ -101,7 +101,22 @@ class DevicePotential:
                         _lib.ptr(ws), ws.numel(), _lib.ptr(out.forces), _lib.ptr(out.energy),
                         _lib.ptr(out.virial), stream)
         _lib.check(rc, type(self).__name__ + ".evaluate")
+        self._last_ws = ws
         return out
+
+    def status(self, device=None):
+        """Device status words of the last evaluation (synchronises): raises
+        if a kernel reported a bad index or an over-long row."""
+        ws = getattr(self, "_last_ws", None)
+        if ws is None:
+            return
+        words = (_lib._i * 4)()
+        _lib.check(_lib.lib().mbf_eval_status(_lib.ptr(ws), words,
+                                              torch.cuda.current_stream(ws.device).cuda_stream),
+                   "mbf_eval_status")
+        if words[0] or words[1]:
+            raise RuntimeError(f"{type(self).__name__}: device check failed (bits {words[0]}, "
+                               f"site {words[1]}, index {words[2]})")
 
     # -- reference protocol ------------------------------------------------------
     def _resolve_list(self, lattice, positions, neigh_list, device):
@@ -147,6 +162,7 @@ class DevicePotential:
         batch.set_types(ids)
         res = self.evaluate(batch, dl)
         f = batch.forces_to_host(res.forces)
+        self.status()
         e = float(res.energy[0].item())
         if not need_stress:
             return e, f, None

@@ -128,6 +128,11 @@ int mbf_nl_half_pairs(const mbf_nlist *nl, int *pair_i, int *pair_j, void *works
  * per-slot three-body forces and bond orders, reduction partials). */
 size_t mbf_eval_workspace_bytes(int n_atoms, long long n_slots, int n_chunks);
 
+/* Status words of the last evaluation that used `workspace` (host_words[4],
+ * synchronises `stream`): word 0 device error bits, word 1 the site of the
+ * first failed index check (0 = none), word 2 the index that failed. */
+int mbf_eval_status(const void *workspace, int *host_words, void *stream);
+
 /* ---- EAM --------------------------------------------------------------
  * Replaces EAMPotential.compute's numba branch (engine/eam.py:174-256) and
  * _eam_kernel (engine/_eam_kernels.py:231-307): alloy EAM, rho-bar at an
