@@ -77,6 +77,9 @@ _SIGS = {
     "mbf_eam_eval": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                           ctypes.POINTER(MbfEamTables), ctypes.POINTER(MbfReducePlan), _i, _i,
                           _vp, _sz, _vp, _vp, _vp, _vp]),
+    "mbf_eam_eval_static": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
+                                 ctypes.POINTER(MbfEamTables), ctypes.POINTER(MbfReducePlan), _i, _i,
+                                 _vp, _vp, _vp, _vp]),
     "mbf_tersoff_eval": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                               ctypes.POINTER(MbfTersoffTables), ctypes.POINTER(MbfReducePlan), _i,
                               _vp, _sz, _vp, _vp, _vp, _vp]),

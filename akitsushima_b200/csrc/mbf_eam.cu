@@ -7,6 +7,8 @@
 // a pair's functions are evaluated from both sides and nothing is written
 // twice.  rho-bar is accumulated and clamped in float64 and F(rho-bar) is
 // evaluated in float64 in both precisions.
+#include <mutex>
+
 #include "mbf_util.cuh"
 
 namespace mbf {
@@ -673,6 +675,91 @@ extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mb
     int lpa = lanes_per_atom > 0 ? lanes_per_atom : 8;
     bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
     int rc;
+    if (precision == MBF_FP64)
+        rc = eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, st);
+    else
+        rc = eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, st);
+    if (rc != MBF_OK) return rc;
+    return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
+}
+
+// ---- the same evaluation without any allocation -----------------------------
+//
+// Some callers cannot allocate device memory: a host program that owns the
+// whole device memory budget and hands its plug-ins only input and output
+// buffers, or a time-step loop that must not synchronise the device the way
+// cudaMalloc / cudaFree can.  mbf_eam_eval_static serves them: its scratch is
+// this file-scope device array, reserved when the library is loaded and held
+// by every GPU that loads the library until the process exits.
+
+#define MBF_STATIC_SCRATCH_BYTES MBF_EAM_STATIC_SCRATCH_BYTES
+
+static __device__ __align__(256) unsigned char g_eam_scratch[MBF_STATIC_SCRATCH_BYTES];
+
+namespace mbf {
+
+// Device address of g_eam_scratch, looked up once per device.  Host code
+// must not use the array's name as a pointer: on the host it is only a
+// stand-in symbol, not a device address.
+static std::mutex g_scratch_mu;
+static void *g_scratch_ptr[64];
+
+static int scratch_address(void **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MBF_ERR_CUDA;
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_ptr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_eam_scratch) != cudaSuccess || !p) return MBF_ERR_CUDA;
+        g_scratch_ptr[dev] = p;
+    }
+    *out = g_scratch_ptr[dev];
+    return MBF_OK;
+}
+
+}  // namespace mbf
+
+extern "C" int mbf_eam_eval_static(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                                   const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
+                                   double *forces, double *energy, double *virial, void *stream) {
+    if (!sys || !nl || !tab || !plan || !forces || !energy || !virial) return MBF_ERR_ARGUMENT;
+    if (precision != MBF_FP64 && precision != MBF_MIXED) return MBF_ERR_ARGUMENT;
+    if (nl->n_atoms != sys->n_atoms || tab->ns <= 0) return MBF_ERR_ARGUMENT;
+    EvalLayout L = eval_layout(sys->n_atoms, nl->n_slots, plan->n_chunks);
+    if (L.total > (size_t)MBF_STATIC_SCRATCH_BYTES) return MBF_ERR_SCRATCH_LIMIT;
+    void *workspace = nullptr;
+    int rc = scratch_address(&workspace);
+    if (rc != MBF_OK) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (sys->n_atoms == 0) {
+        if (cudaMemsetAsync(energy, 0, sizeof(double) * sys->n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
+        if (cudaMemsetAsync(virial, 0, sizeof(double) * 9 * sys->n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
+        return MBF_OK;
+    }
+    SysView S = make_view(sys);
+    EamDev E;
+    E.ns = tab->ns; E.nf = tab->nf; E.nX = tab->nX;
+    E.codes = tab->codes; E.P = tab->P; E.xo = tab->xo; E.nx = tab->nx;
+    E.X = tab->X; E.C = tab->C;
+    E.rho_f = tab->rho_f; E.F_f = tab->F_f; E.phi_f = tab->phi_f;
+    E.r_cut = tab->r_cut;
+    if (!nl->upper) return MBF_ERR_ARGUMENT;
+    double *aux = ws_at<double>(workspace, L.atom_aux);
+    double *per_atom = ws_at<double>(workspace, L.per_atom);
+    double *partial = ws_at<double>(workspace, L.partial);
+    void *slot_f = ws_at<char>(workspace, L.slot);
+    Chk ck;
+    ck.err = ws_at<int>(workspace, L.err);
+    ck.n_atoms = sys->n_atoms;
+    ck.n_slots = nl->n_slots;
+    ck.ns = tab->ns;
+    // the scratch keeps the previous call's contents: the error words must
+    // start at zero; every other region is fully written before it is read
+    if (cudaMemsetAsync(ck.err, 0, 16, st) != cudaSuccess) return MBF_ERR_CUDA;
+    double *f_local = ws_at<double>(workspace, L.f_local);
+    double4 *pk = ws_at<double4>(workspace, L.pack);
+    int lpa = lanes_per_atom > 0 ? lanes_per_atom : 8;
+    bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
     if (precision == MBF_FP64)
         rc = eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, st);
     else

@@ -168,6 +168,30 @@ int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_table
                  void *workspace, size_t workspace_bytes,
                  double *forces, double *energy, double *virial, void *stream);
 
+/* mbf_eam_eval without a workspace argument: no counterpart in the reference.
+ * For callers that cannot allocate device memory -- a host program that
+ * owns the whole device memory budget and gives its plug-ins only their
+ * input and output buffers, or a time-step loop that must not pay the device
+ * synchronisation cudaMalloc / cudaFree can cause.  The call allocates
+ * nothing: its scratch is a fixed device array of
+ * MBF_EAM_STATIC_SCRATCH_BYTES that the library reserves on every GPU that
+ * loads it, until the process exits.  Inputs and outputs are as for
+ * mbf_eam_eval.
+ *   - Returns MBF_ERR_SCRATCH_LIMIT, doing nothing, when the structure needs
+ *     more scratch than that (mbf_eval_workspace_bytes(n_atoms, n_slots,
+ *     n_chunks) > MBF_EAM_STATIC_SCRATCH_BYTES, e.g. beyond about 8000 atoms
+ *     of an fcc alloy with an 80-neighbour list).
+ *   - The first call on a device looks the array's device address up (once
+ *     per device); make that first call before any stream capture.
+ *   - Every call on a device uses the same array and it keeps the previous
+ *     call's contents (the call clears what must start at zero).  Calls whose
+ *     work overlaps on the GPU -- two streams, or two host threads -- race
+ *     on it: serialise them.                                              */
+#define MBF_EAM_STATIC_SCRATCH_BYTES (32u << 20)
+int mbf_eam_eval_static(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                        const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
+                        double *forces, double *energy, double *virial, void *stream);
+
 /* ---- Tersoff ----------------------------------------------------------
  * Replaces TersoffPotential.compute (engine/tersoff.py:1208-1711): both the
  * single-species flat form (m = 3, gamma = 1; :1233-1513) and the
