@@ -81,10 +81,10 @@ _SIGS = {
                                  ctypes.POINTER(MbfEamTables), ctypes.POINTER(MbfReducePlan), _i, _i,
                                  _vp, _vp, _vp, _vp]),
     "mbf_tersoff_eval": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
-                              ctypes.POINTER(MbfTersoffTables), ctypes.POINTER(MbfReducePlan), _i,
+                              ctypes.POINTER(MbfTersoffTables), ctypes.POINTER(MbfReducePlan), _i, _i,
                               _vp, _sz, _vp, _vp, _vp, _vp]),
     "mbf_sw_eval": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
-                         ctypes.POINTER(MbfSwTables), ctypes.POINTER(MbfReducePlan), _i, _vp, _sz,
+                         ctypes.POINTER(MbfSwTables), ctypes.POINTER(MbfReducePlan), _i, _i, _vp, _sz,
                          _vp, _vp, _vp, _vp]),
     "mbf_profile_begin": (None, []),
     "mbf_profile_end": (_i, [ctypes.c_char_p, _sz]),

@@ -11,10 +11,11 @@
 
 namespace mbf {
 
-constexpr int SW_LPA = 8;
-template <int MAXN> struct SwGeom {
+// Lanes per atom (LPA) is a template parameter chosen by the host (the
+// autotuner); lane groups per block keep the staged rows under 48 KB.
+template <int MAXN, int LPA> struct SwGeom {
     static constexpr int GPB = 512 / MAXN;
-    static constexpr int BLOCK = GPB * SW_LPA;
+    static constexpr int BLOCK = GPB * LPA;
 };
 
 struct SwDev {
@@ -65,17 +66,17 @@ struct SwRow {
 
 // SYM: every (i, j, k) record equals its (i, k, j) twin (one species), so a
 // slot needs one h evaluation per partner with the full lambda.
-template <typename T, int MAXN, bool SYM>
+template <typename T, int MAXN, bool SYM, int LPA>
 __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr,
                          const int *__restrict__ rev, SwDev P, double *__restrict__ slot_G, double *__restrict__ f_local,
                          double *__restrict__ per_atom, int *__restrict__ err) {
-    constexpr int GPB = SwGeom<MAXN>::GPB;
+    constexpr int GPB = SwGeom<MAXN, LPA>::GPB;
     __shared__ SwRow<T, MAXN> rows[GPB];
-    const int sub = threadIdx.x & (SW_LPA - 1);
-    SwRow<T, MAXN> &R = rows[threadIdx.x / SW_LPA];
+    const int sub = threadIdx.x & (LPA - 1);
+    SwRow<T, MAXN> &R = rows[threadIdx.x / LPA];
     const int ns = P.ns;
     for (int base = blockIdx.x * GPB; base < S.n_atoms; base += gridDim.x * GPB) {
-        int i = base + threadIdx.x / SW_LPA;
+        int i = base + threadIdx.x / LPA;
         int beg = 0, n = 0;
         bool live = i < S.n_atoms;
         if (live) {
@@ -89,7 +90,7 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
         if (live) {
             const double *cell = cell_of(S, i);
             double xi = S.pos[3 * (size_t)i], yi = S.pos[3 * (size_t)i + 1], zi = S.pos[3 * (size_t)i + 2];
-            for (int s = sub; s < n; s += SW_LPA) {
+            for (int s = sub; s < n; s += LPA) {
                 int j = nbr[beg + s];
                 double dx, dy, dz;
                 mic_exact(cell, S.pos[3 * (size_t)j] - xi, S.pos[3 * (size_t)j + 1] - yi,
@@ -108,7 +109,7 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
         double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         if (live) {
             int si = S.types[i];
-            for (int s = sub; s < n; s += SW_LPA) {
+            for (int s = sub; s < n; s += LPA) {
                 double Gx = 0, Gy = 0, Gz = 0, cx = 0;
                 double dx = (double)R.x[s], dy = (double)R.y[s], dz = (double)R.z[s];
                 if (R.ok[s]) {
@@ -192,13 +193,13 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
                 slot_G[o + 2] = Gz;
             }
         }
-        fx = group_sum<SW_LPA>(fx);
-        fy = group_sum<SW_LPA>(fy);
-        fz = group_sum<SW_LPA>(fz);
-        e = group_sum<SW_LPA>(e);
-        npair = group_sum<SW_LPA>(npair);
+        fx = group_sum<LPA>(fx);
+        fy = group_sum<LPA>(fy);
+        fz = group_sum<LPA>(fz);
+        e = group_sum<LPA>(e);
+        npair = group_sum<LPA>(npair);
 #pragma unroll
-        for (int q = 0; q < 9; ++q) v[q] = group_sum<SW_LPA>(v[q]);
+        for (int q = 0; q < 9; ++q) v[q] = group_sum<LPA>(v[q]);
         if (sub == 0 && i < S.n_atoms) {
             f_local[3 * (size_t)i] = fx;
             f_local[3 * (size_t)i + 1] = fy;
@@ -213,25 +214,37 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
     }
 }
 
-template <typename T, int MAXN, bool SYM>
+template <typename T, int MAXN, bool SYM, int LPA>
 static int sw_launch(const SysView &S, const mbf_nlist *nl, const SwDev &P, double *slot_G, double *f_local,
                      double *per_atom, double *forces, int *err, cudaStream_t st) {
-    constexpr int GPB = SwGeom<MAXN>::GPB, BLOCK = SwGeom<MAXN>::BLOCK;
+    constexpr int GPB = SwGeom<MAXN, LPA>::GPB, BLOCK = SwGeom<MAXN, LPA>::BLOCK;
     int blocks = (S.n_atoms + GPB - 1) / GPB;
-    int g = persistent_grid(blocks, BLOCK, (const void *)sw_force<T, MAXN, SYM>);
+    int g = persistent_grid(blocks, BLOCK, (const void *)sw_force<T, MAXN, SYM, LPA>);
     PROF_BEGIN("sw_force", st);
-    sw_force<T, MAXN, SYM><<<g, BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, nl->rev, P, slot_G, f_local, per_atom, err);
+    sw_force<T, MAXN, SYM, LPA><<<g, BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, nl->rev, P, slot_G, f_local, per_atom, err);
     PROF_END("sw_force", st);
     MBF_CHECK_LAUNCH();
     return gather_forces(S.n_atoms, nl->row_off, slot_G, f_local, forces, st);
 }
 
+template <typename T, int MAXN, bool SYM>
+static int sw_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const SwDev &P, double *slot_G, double *f_local,
+                  double *per_atom, double *forces, int *err, cudaStream_t st) {
+    switch (lpa) {
+        case 4: return sw_launch<T, MAXN, SYM, 4>(S, nl, P, slot_G, f_local, per_atom, forces, err, st);
+        case 8: return sw_launch<T, MAXN, SYM, 8>(S, nl, P, slot_G, f_local, per_atom, forces, err, st);
+        case 16: return sw_launch<T, MAXN, SYM, 16>(S, nl, P, slot_G, f_local, per_atom, forces, err, st);
+        default: return MBF_ERR_ARGUMENT;
+    }
+}
+
 template <typename T, bool SYM>
-static int sw_dispatch(int mr, const SysView &S, const mbf_nlist *nl, const SwDev &P, double *slot_G,
+static int sw_dispatch(int mr, int lpa, const SysView &S, const mbf_nlist *nl, const SwDev &P, double *slot_G,
                        double *f_local, double *per_atom, double *forces, int *err, cudaStream_t st) {
-    if (mr <= 32) return sw_launch<T, 32, SYM>(S, nl, P, slot_G, f_local, per_atom, forces, err, st);
-    if (mr <= 64) return sw_launch<T, 64, SYM>(S, nl, P, slot_G, f_local, per_atom, forces, err, st);
-    return sw_launch<T, 128, SYM>(S, nl, P, slot_G, f_local, per_atom, forces, err, st);
+    if (lpa <= 0) lpa = 8;
+    if (mr <= 32) return sw_lpa<T, 32, SYM>(lpa, S, nl, P, slot_G, f_local, per_atom, forces, err, st);
+    if (mr <= 64) return sw_lpa<T, 64, SYM>(lpa, S, nl, P, slot_G, f_local, per_atom, forces, err, st);
+    return sw_lpa<T, 128, SYM>(lpa, S, nl, P, slot_G, f_local, per_atom, forces, err, st);
 }
 
 }  // namespace mbf
@@ -239,7 +252,8 @@ static int sw_dispatch(int mr, const SysView &S, const mbf_nlist *nl, const SwDe
 using namespace mbf;
 
 extern "C" int mbf_sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables *tab,
-                           const mbf_reduce_plan *plan, int precision, void *workspace, size_t workspace_bytes,
+                           const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
+                           size_t workspace_bytes,
                            double *forces, double *energy, double *virial, void *stream) {
     if (!sys || !nl || !tab || !plan || !workspace || !forces || !energy || !virial) return MBF_ERR_ARGUMENT;
     if (precision != MBF_FP64 && precision != MBF_MIXED) return MBF_ERR_ARGUMENT;
@@ -270,11 +284,11 @@ extern "C" int mbf_sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf
     bool sym = tab->ns == 1;
     int rc;
     if (precision == MBF_FP64)
-        rc = sym ? sw_dispatch<double, true>(mr, S, nl, P, slot_G, f_local, per_atom, forces, err, st)
-                 : sw_dispatch<double, false>(mr, S, nl, P, slot_G, f_local, per_atom, forces, err, st);
+        rc = sym ? sw_dispatch<double, true>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, st)
+                 : sw_dispatch<double, false>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, st);
     else
-        rc = sym ? sw_dispatch<float, true>(mr, S, nl, P, slot_G, f_local, per_atom, forces, err, st)
-                 : sw_dispatch<float, false>(mr, S, nl, P, slot_G, f_local, per_atom, forces, err, st);
+        rc = sym ? sw_dispatch<float, true>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, st)
+                 : sw_dispatch<float, false>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
 }

@@ -14,11 +14,11 @@
 
 namespace mbf {
 
-constexpr int TE_LPA = 8;
-// Lane groups per block: the staged rows of a block stay under 48 KB.
-template <int MAXN> struct TeGeom {
+// Lanes per atom (LPA) is a template parameter chosen by the host (the
+// autotuner); lane groups per block keep the staged rows under 48 KB.
+template <int MAXN, int LPA> struct TeGeom {
     static constexpr int GPB = 512 / MAXN;
-    static constexpr int BLOCK = GPB * TE_LPA;
+    static constexpr int BLOCK = GPB * LPA;
 };
 
 struct TeDev {
@@ -98,12 +98,12 @@ struct TeRow {
     int ok[MAXN];
 };
 
-template <typename T, int MAXN>
+template <typename T, int MAXN, int LPA>
 __device__ __forceinline__ void te_stage(const SysView &S, const int *__restrict__ nbr, int i, int beg,
                                          int n, double rc, TeRow<T, MAXN> &R, int sub) {
     const double *cell = cell_of(S, i);
     double xi = S.pos[3 * (size_t)i], yi = S.pos[3 * (size_t)i + 1], zi = S.pos[3 * (size_t)i + 2];
-    for (int s = sub; s < n; s += TE_LPA) {
+    for (int s = sub; s < n; s += LPA) {
         int j = nbr[beg + s];
         double dx, dy, dz;
         mic_exact(cell, S.pos[3 * (size_t)j] - xi, S.pos[3 * (size_t)j + 1] - yi,
@@ -118,16 +118,16 @@ __device__ __forceinline__ void te_stage(const SysView &S, const int *__restrict
     }
 }
 
-template <typename T, int MAXN>
+template <typename T, int MAXN, int LPA>
 __global__ void te_zeta(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr, TeDev P,
                         double *__restrict__ slot_b, int *__restrict__ err) {
-    constexpr int GPB = TeGeom<MAXN>::GPB;
+    constexpr int GPB = TeGeom<MAXN, LPA>::GPB;
     __shared__ TeRow<T, MAXN> rows[GPB];
-    const int sub = threadIdx.x & (TE_LPA - 1);
-    TeRow<T, MAXN> &R = rows[threadIdx.x / TE_LPA];
+    const int sub = threadIdx.x & (LPA - 1);
+    TeRow<T, MAXN> &R = rows[threadIdx.x / LPA];
     const int ns = P.ns;
     for (int base = blockIdx.x * GPB; base < S.n_atoms; base += gridDim.x * GPB) {
-        int i = base + threadIdx.x / TE_LPA;
+        int i = base + threadIdx.x / LPA;
         int beg = 0, n = 0;
         bool live = i < S.n_atoms;
         if (live) {
@@ -138,11 +138,11 @@ __global__ void te_zeta(SysView S, const int *__restrict__ row_off, const int *_
                 live = false;
             }
         }
-        if (live) te_stage<T, MAXN>(S, nbr, i, beg, n, P.rc, R, sub);
+        if (live) te_stage<T, MAXN, LPA>(S, nbr, i, beg, n, P.rc, R, sub);
         __syncwarp();
         if (live) {
             int si = S.types[i];
-            for (int s = sub; s < n; s += TE_LPA) {
+            for (int s = sub; s < n; s += LPA) {
                 double b = 1.0, db = 0.0;
                 if (R.ok[s]) {
                     int j = nbr[beg + s];
@@ -183,18 +183,18 @@ __global__ void te_zeta(SysView S, const int *__restrict__ row_off, const int *_
     }
 }
 
-template <typename T, int MAXN>
+template <typename T, int MAXN, int LPA>
 __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr,
                          const int *__restrict__ rev, TeDev P, const double *__restrict__ slot_b,
                          double *__restrict__ slot_G, double *__restrict__ f_local,
                          double *__restrict__ per_atom, int *__restrict__ err) {
-    constexpr int GPB = TeGeom<MAXN>::GPB;
+    constexpr int GPB = TeGeom<MAXN, LPA>::GPB;
     __shared__ TeRow<T, MAXN> rows[GPB];
-    const int sub = threadIdx.x & (TE_LPA - 1);
-    TeRow<T, MAXN> &R = rows[threadIdx.x / TE_LPA];
+    const int sub = threadIdx.x & (LPA - 1);
+    TeRow<T, MAXN> &R = rows[threadIdx.x / LPA];
     const int ns = P.ns;
     for (int base = blockIdx.x * GPB; base < S.n_atoms; base += gridDim.x * GPB) {
-        int i = base + threadIdx.x / TE_LPA;
+        int i = base + threadIdx.x / LPA;
         int beg = 0, n = 0;
         bool live = i < S.n_atoms;
         if (live) {
@@ -205,19 +205,19 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
                 live = false;
             }
         }
-        if (live) te_stage<T, MAXN>(S, nbr, i, beg, n, P.rc, R, sub);
+        if (live) te_stage<T, MAXN, LPA>(S, nbr, i, beg, n, P.rc, R, sub);
         __syncwarp();
         double fx = 0, fy = 0, fz = 0, e = 0, npair = 0;
         double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         int si = live ? S.types[i] : 0;
         // pass 1: pair terms and the zeta-gradient coefficients
-        double cxs[(MAXN + TE_LPA - 1) / TE_LPA];
-        double pair_r[(MAXN + TE_LPA - 1) / TE_LPA];
+        double cxs[(MAXN + LPA - 1) / LPA];
+        double pair_r[(MAXN + LPA - 1) / LPA];
         if (live) {
             const double *cell = cell_of(S, i);
             double xi = S.pos[3 * (size_t)i], yi = S.pos[3 * (size_t)i + 1], zi = S.pos[3 * (size_t)i + 2];
             int q = 0;
-            for (int s = sub; s < n; s += TE_LPA, ++q) {
+            for (int s = sub; s < n; s += LPA, ++q) {
                 {
                     int j = nbr[beg + s];
                     double dx, dy, dz;
@@ -261,7 +261,7 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
         // pass 2: three-body forces per slot
         if (live) {
             int q = 0;
-            for (int s = sub; s < n; s += TE_LPA, ++q) {
+            for (int s = sub; s < n; s += LPA, ++q) {
                 double Gx = 0, Gy = 0, Gz = 0;
                 double dx = (double)R.x[s], dy = (double)R.y[s], dz = (double)R.z[s];
                 if (R.ok[s]) {
@@ -332,13 +332,13 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
                 slot_G[o + 2] = Gz;
             }
         }
-        fx = group_sum<TE_LPA>(fx);
-        fy = group_sum<TE_LPA>(fy);
-        fz = group_sum<TE_LPA>(fz);
-        e = group_sum<TE_LPA>(e);
-        npair = group_sum<TE_LPA>(npair);
+        fx = group_sum<LPA>(fx);
+        fy = group_sum<LPA>(fy);
+        fz = group_sum<LPA>(fz);
+        e = group_sum<LPA>(e);
+        npair = group_sum<LPA>(npair);
 #pragma unroll
-        for (int q = 0; q < 9; ++q) v[q] = group_sum<TE_LPA>(v[q]);
+        for (int q = 0; q < 9; ++q) v[q] = group_sum<LPA>(v[q]);
         if (sub == 0 && i < S.n_atoms) {
             f_local[3 * (size_t)i] = fx;
             f_local[3 * (size_t)i + 1] = fy;
@@ -353,23 +353,51 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
     }
 }
 
-template <typename T, int MAXN>
+template <typename T, int MAXN, int LPA>
 static int te_launch(const SysView &S, const mbf_nlist *nl, const TeDev &P, double *slot_b, double *slot_G,
                      double *f_local, double *per_atom, double *forces, int *err, cudaStream_t st) {
-    constexpr int GPB = TeGeom<MAXN>::GPB, BLOCK = TeGeom<MAXN>::BLOCK;
+    constexpr int GPB = TeGeom<MAXN, LPA>::GPB, BLOCK = TeGeom<MAXN, LPA>::BLOCK;
     int blocks = (S.n_atoms + GPB - 1) / GPB;
-    int g = persistent_grid(blocks, BLOCK, (const void *)te_zeta<T, MAXN>);
+    int g = persistent_grid(blocks, BLOCK, (const void *)te_zeta<T, MAXN, LPA>);
     PROF_BEGIN("te_zeta", st);
-    te_zeta<T, MAXN><<<g, BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, slot_b, err);
+    te_zeta<T, MAXN, LPA><<<g, BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, slot_b, err);
     PROF_END("te_zeta", st);
     MBF_CHECK_LAUNCH();
-    g = persistent_grid(blocks, BLOCK, (const void *)te_force<T, MAXN>);
+    g = persistent_grid(blocks, BLOCK, (const void *)te_force<T, MAXN, LPA>);
     PROF_BEGIN("te_force", st);
-    te_force<T, MAXN><<<g, BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, nl->rev, P, slot_b, slot_G, f_local,
+    te_force<T, MAXN, LPA><<<g, BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, nl->rev, P, slot_b, slot_G, f_local,
                                          per_atom, err);
     PROF_END("te_force", st);
     MBF_CHECK_LAUNCH();
     return gather_forces(S.n_atoms, nl->row_off, slot_G, f_local, forces, st);
+}
+
+template <typename T, int MAXN>
+static int te_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const TeDev &P, double *slot_b,
+                  double *slot_G, double *f_local, double *per_atom, double *forces, int *err, cudaStream_t st) {
+    switch (lpa) {
+        case 4: return te_launch<T, MAXN, 4>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
+        case 8: return te_launch<T, MAXN, 8>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
+        case 16: return te_launch<T, MAXN, 16>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
+        default: return MBF_ERR_ARGUMENT;
+    }
+}
+
+template <typename T>
+static int te_rows(int mr, int lpa, const SysView &S, const mbf_nlist *nl, const TeDev &P, double *slot_b,
+                   double *slot_G, double *f_local, double *per_atom, double *forces, int *err, cudaStream_t st) {
+    if (mr <= 32) return te_lpa<T, 32>(lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
+    if (mr <= 64) return te_lpa<T, 64>(lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
+    return te_lpa<T, 128>(lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
+}
+
+static int te_dispatch(int precision, int mr, int lpa, const SysView &S, const mbf_nlist *nl, const TeDev &P,
+                       double *slot_b, double *slot_G, double *f_local, double *per_atom, double *forces,
+                       int *err, cudaStream_t st) {
+    if (lpa <= 0) lpa = 8;
+    return precision == MBF_FP64
+               ? te_rows<double>(mr, lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st)
+               : te_rows<float>(mr, lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
 }
 
 }  // namespace mbf
@@ -377,7 +405,7 @@ static int te_launch(const SysView &S, const mbf_nlist *nl, const TeDev &P, doub
 using namespace mbf;
 
 extern "C" int mbf_tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_tersoff_tables *tab,
-                                const mbf_reduce_plan *plan, int precision, void *workspace,
+                                const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
                                 size_t workspace_bytes, double *forces, double *energy, double *virial,
                                 void *stream) {
     if (!sys || !nl || !tab || !plan || !workspace || !forces || !energy || !virial) return MBF_ERR_ARGUMENT;
@@ -405,17 +433,8 @@ extern "C" int mbf_tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, cons
     double *slot_G = ws_at<double>(workspace, L.slot);
     double *slot_b = ws_at<double>(workspace, L.slot_b);
     double *partial = ws_at<double>(workspace, L.partial);
-    int rc;
-    int mr = nl->max_row;
-    if (precision == MBF_FP64) {
-        rc = mr <= 32 ? te_launch<double, 32>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st)
-             : mr <= 64 ? te_launch<double, 64>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st)
-                        : te_launch<double, 128>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
-    } else {
-        rc = mr <= 32 ? te_launch<float, 32>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st)
-             : mr <= 64 ? te_launch<float, 64>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st)
-                        : te_launch<float, 128>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
-    }
+    int rc = te_dispatch(precision, nl->max_row, lanes_per_atom, S, nl, P, slot_b, slot_G, f_local, per_atom,
+                         forces, err, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
 }

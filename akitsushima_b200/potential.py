@@ -83,14 +83,19 @@ class DevicePotential:
         return t
 
     # -- device-level evaluation -----------------------------------------------
-    def evaluate(self, batch, dlist, precision=None, out=None):
+    def evaluate(self, batch, dlist, precision=None, out=None, ws=None):
         """Energy, forces and virial of every structure of ``batch`` with the
-        device list ``dlist`` (a DeviceNeighbourList).  Returns EvalResult."""
+        device list ``dlist`` (a DeviceNeighbourList).  Returns EvalResult.
+        ``ws`` is a caller-owned uint8 workspace (default: the thread's shared
+        one, which a later, larger call may replace)."""
         prec = precision_code(precision or self.precision)
         dev = batch.device
         L = _lib.lib()
         nbytes = int(L.mbf_eval_workspace_bytes(batch.n_atoms, dlist.n_slots, batch.n_chunks))
-        ws = workspace(dev, nbytes)
+        if ws is None:
+            ws = workspace(dev, nbytes)
+        elif ws.numel() < nbytes:
+            raise ValueError(f"evaluate: workspace of {ws.numel()} bytes, {nbytes} needed")
         if out is None:
             out = EvalResult(torch.empty(batch.n_struct, dtype=torch.float64, device=dev),
                              torch.empty((batch.n_atoms, 3), dtype=torch.float64, device=dev),

@@ -124,6 +124,8 @@ class StillingerWeberPotential(DevicePotential):
         st = _lib.MbfSwTables(len(self.species), _lib.ptr(t[0]), _lib.ptr(t[1]), _lib.ptr(t[2]), rc)
         return (st, *t)
 
+    lanes_per_atom = 8
+
     def _call(self, L, sysd, nld, tabs, plan, prec, ws, nbytes, forces, energy, virial, stream):
-        return L.mbf_sw_eval(sysd, nld, tabs[0], plan, prec, ws, nbytes, forces, energy, virial,
+        return L.mbf_sw_eval(sysd, nld, tabs[0], plan, prec, int(self.lanes_per_atom), ws, nbytes, forces, energy, virial,
                              stream)

@@ -102,8 +102,10 @@ class TersoffPotential(DevicePotential):
         st = _lib.MbfTersoffTables(len(self.species), _lib.ptr(tb_t), _lib.ptr(tri_t), self.r_cut)
         return (st, tb_t, tri_t)
 
+    lanes_per_atom = 8
+
     def _call(self, L, sysd, nld, tabs, plan, prec, ws, nbytes, forces, energy, virial, stream):
-        return L.mbf_tersoff_eval(sysd, nld, tabs[0], plan, prec, ws, nbytes, forces, energy,
+        return L.mbf_tersoff_eval(sysd, nld, tabs[0], plan, prec, int(self.lanes_per_atom), ws, nbytes, forces, energy,
                                   virial, stream)
 
 

@@ -19,6 +19,16 @@ the timed region).
 With --gpus N > 1 (torchrun), every rank evaluates its own replica of the
 structure ("replicas only": one structure does not shard) and the time is the
 max over ranks.
+
+--workload batched_si512: 512 independent periodic Si structures (diamond
+supercells of {1..4}^3 cell multiples, symmetric strain entries uniform
++-3 %, Gaussian displacements 0.1 A); one step evaluates every structure
+with Tersoff (1988 Si(C)) and with Stillinger-Weber, replayed as one CUDA
+graph with the autotuned lanes-per-atom.  value counts atoms of the original
+structures (thin cells are evaluated as replicated supercells; the replicas
+are overhead, not counted).  With N ranks every rank takes 512 / N
+structures ("weak": a fixed share per rank would be 512 each; here the set is
+split, "strong").
 """
 import argparse
 import json
@@ -43,6 +53,30 @@ def make_cuni(n_cells=40, a=3.58, sigma=0.08, seed=0):
     pos = frac * a + rng.normal(0.0, sigma, frac.shape)
     ids = np.random.default_rng(seed + 1).integers(0, 2, len(pos)).astype(np.int32)
     return np.eye(3) * a * n_cells, pos, ids
+
+
+DIAMOND = np.array([[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0],
+                    [0.25, 0.25, 0.25], [0.25, 0.75, 0.75], [0.75, 0.25, 0.75],
+                    [0.75, 0.75, 0.25]], float)
+
+
+def make_si_set(n=512, a=5.431, strain=0.03, sigma=0.1, seed=0):
+    """Uneven strained Si diamond supercells: (lattice, positions, types)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        reps = rng.integers(1, 5, size=3)
+        g = [np.arange(r) for r in reps]
+        cells = np.stack(np.meshgrid(*g, indexing="ij"), -1).reshape(-1, 3)
+        frac = (DIAMOND[None] + cells[:, None]).reshape(-1, 3)
+        lat = np.diag(reps.astype(float)) * a
+        pos = frac * a
+        e = rng.uniform(-strain, strain, (3, 3))
+        m = np.eye(3) + 0.5 * (e + e.T)
+        lat, pos = lat @ m, pos @ m
+        pos = pos + rng.normal(0.0, sigma, pos.shape)
+        out.append((lat, pos, ["Si"] * len(pos)))
+    return out
 
 
 def cpu_count():
@@ -129,6 +163,211 @@ def time_reference(lat, pos, ids, steps, warmup):
         ts.append(time.perf_counter() - t0)
     return float(np.mean(ts)), threads
 
+def time_reference_batched(structs, n_sample):
+    """The oracle port of the reference's Tersoff and SW numba paths over the
+    first n_sample structures (thin cells as the same replicated
+    supercells), every host thread, prebuilt pair lists; seconds per
+    structure-pair-of-evaluations and the atoms counted."""
+    import oracle
+    from akitsushima_b200.published_parameters import SW_SI_1985, TERSOFF_SI_1988
+    from akitsushima_b200.system import replicate_thin
+    threads = cpu_count()
+    oracle.set_threads(threads)
+    rc_t = TERSOFF_SI_1988["R"] + TERSOFF_SI_1988["D"]
+    rc_s = SW_SI_1985["a"] * SW_SI_1985["sigma"]
+    work = []
+    for lat, pos, _ in structs[:n_sample]:
+        z = np.zeros(len(pos), np.int32)
+        lt, pt, _, _ = replicate_thin(lat, pos, z, rc_t + 0.3)
+        ls, ps, _, _ = replicate_thin(lat, pos, z, rc_s + 0.3)
+        work.append((len(pos), lt, pt, oracle.nl_build(lt, pt, rc_t, 0.3)[:2],
+                     ls, ps, oracle.nl_build(ls, ps, rc_s, 0.3)[:2]))
+    t0 = time.perf_counter()
+    atoms = 0
+    for n, lt, pt, pr_t, ls, ps, pr_s in work:
+        oracle.tersoff_single(TERSOFF_SI_1988, lt, pt, pr_t)
+        oracle.sw_single(SW_SI_1985, ls, ps, pr_s)
+        atoms += 2 * n
+    return time.perf_counter() - t0, atoms, threads
+
+
+def run_batched(args, world, rank, local):
+    n_struct = 512
+    structs = make_si_set(n_struct)
+    cfg = {"workload": "batched_si512_tersoff_sw", "n_structures": n_struct,
+           "sizes": "diamond {1..4}^3 cell multiples, 8-512 atoms", "strain": 0.03,
+           "sigma": 0.1, "skin": 0.3, "precision": args.precision,
+           "potentials": ["Tersoff 1988 Si(C)", "Stillinger-Weber 1985 Si"],
+           "l2": "256 MB scratch write between steps, outside the timed events",
+           "parallelism": f"split{world}"}
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        import oracle  # noqa: F401  (built by __graft_entry__.build)
+        per = []
+        for _ in range(max(1, args.warmup) if args.steps > 0 else 0):
+            time_reference_batched(structs, 8)
+        for _ in range(args.steps):
+            t, atoms, threads = time_reference_batched(structs, 128)
+            per.append(atoms / t)
+        v = float(np.mean(per))
+        line = {"metric": METRIC, "value": v, "unit": "atoms/s", "impl": "reference",
+                "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": None, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(cfg, precision="fp64"),
+                "cpu_baseline": {"value": v, "unit": "atoms/s", "cores": threads, "kind": "port",
+                                 "sample": "per step: Tersoff + SW force calls of the first 128 "
+                                           "of the 512 structures, prebuilt pair lists"},
+                "e2e": {"value": v, "unit": "atoms/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    import akitsushima_b200 as ak
+    from akitsushima_b200 import _lib
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    mine = structs[rank::world]
+    n_atoms = sum(len(p) for _, p, _ in mine)
+    pots = [ak.TersoffPotential(ak.TERSOFF_SI_1988, species=["Si"], precision=args.precision),
+            ak.StillingerWeberPotential(ak.SW_SI_1985, species=["Si"], precision=args.precision)]
+    evs = [ak.BatchedEvaluator(p, mine, skin=0.3, device=dev) for p in pots]
+    tuned = [ev.autotune(candidates=(4, 8, 16), reps=5) for ev in evs]
+    for ev in evs:
+        ev.run()
+    torch.cuda.synchronize()
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        for ev in evs:
+            ev._eval()
+    torch.cuda.current_stream(dev).wait_stream(side)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        for ev in evs:
+            ev._eval()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize()
+
+    ev_t = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            ev_t[k][0].record()
+            graph.replay()
+            ev_t[k][1].record()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    ms = sum(a.elapsed_time(b) for a, b in ev_t) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_atoms = sum(len(p) for _, p, _ in structs)
+    value = 2 * total_atoms / (ms * 1e-3)
+
+    # per-kernel breakdown (eager, same launches as the graph)
+    _lib.profile_begin()
+    for _ in range(args.steps):
+        for ev in evs:
+            ev._eval()
+    prof = _lib.profile_end()
+    launches = sum(c for c, _ in prof.values()) / args.steps
+
+    # the same work as per-structure launches (one list + one call each)
+    singles = []
+    for lat, pos, types in mine:
+        row = []
+        for p in pots:
+            b = ak.Batch.single(*_replicated(lat, pos, p.r_cut + 0.3), device=dev)
+            dl = ak.DeviceNeighbourList(p.r_cut + 0.3).build(b)
+            row.append((p, b, dl))
+        singles.append(row)
+    for row in singles:
+        for p, b, dl in row:
+            p.evaluate(b, dl)
+    torch.cuda.synchronize()
+    a, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for row in singles:
+        for p, b, dl in row:
+            p.evaluate(b, dl)
+    b_.record()
+    torch.cuda.synchronize()
+    ms_single = a.elapsed_time(b_)
+
+    # end to end: host positions in (pinned staging), per-structure forces,
+    # energies and stresses out, through the evaluator's public calls
+    host_pos = [np.ascontiguousarray(ev.batch.pos.cpu().numpy()) for ev in evs]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        res = []
+        for ev, hp in zip(evs, host_pos):
+            ev.batch.set_positions(hp)
+            res.append(ev.results())
+    t_e2e = (time.perf_counter() - t0) / args.e2e_steps
+    if dist:
+        t = torch.tensor([t_e2e, ms_single], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e, ms_single = float(t[0].item()), float(t[1].item())
+    h2d = sum(ev.batch.n_atoms * 24 for ev in evs)
+    d2h = sum(ev.n_atoms * 24 + ev.n_structures * (8 + 72) for ev in evs)
+    e2e = {"value": 2 * total_atoms / t_e2e, "unit": "atoms/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "ms_per_step": t_e2e * 1e3,
+           "path": "BatchedEvaluator: batch.set_positions(numpy) + results() -> numpy, "
+                   "Tersoff and SW"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t_cpu, atoms, threads = time_reference_batched(structs, 32)
+        cpu = {"value": atoms / t_cpu, "unit": "atoms/s", "cores": threads, "kind": "port",
+               "sample": "Tersoff + SW force calls of the first 32 of the 512 structures, "
+                         "oracle port of the reference's numba paths, prebuilt pair lists"}
+    clocks = clk.summary()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+            "config": cfg, "structures_per_s": 2 * n_struct / (ms * 1e-3),
+            "gpu_launches": int(round(launches * args.steps)), "gpu_launches_per_step": launches,
+            "clocks": clocks, "autotune": tuned,
+            "per_structure_launches": {"ms_per_step": ms_single,
+                                       "value": 2 * total_atoms / (ms_single * 1e-3),
+                                       "speedup_of_batched": ms_single / ms},
+            "kernels": {k: {"launches": c, "ms_per_launch": t / c} for k, (c, t) in prof.items()},
+            "e2e": e2e, "cpu_baseline": cpu, "roofline": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _replicated(lat, pos, r_list):
+    from akitsushima_b200.system import replicate_thin
+    L2, P2, T2, _ = replicate_thin(lat, pos, np.zeros(len(pos), np.int32), r_list)
+    return L2, P2, T2
+
 
 def main():
     ap = argparse.ArgumentParser()
@@ -141,12 +380,15 @@ def main():
     ap.add_argument("--lanes", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--workload", default="eam_cuni_256k", choices=["eam_cuni_256k", "batched_si512"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "batched_si512":
+        return run_batched(args, world, rank, local)
     lat, pos, ids = make_cuni(args.cells)
     n_atoms = len(pos)
     workload = f"eam_zhou_cuni_fcc{args.cells}^3_{n_atoms}_atoms"

@@ -199,6 +199,8 @@ int mbf_eam_eval_static(const mbf_system *sys, const mbf_nlist *nl, const mbf_ea
  * (:1606-1653).  tb (ns*ns, 10) float64 rows [valid, A, B, lambda1, lambda2,
  * R, D, beta, n, unused]; tri (ns*ns*ns, 8) rows [valid, c, d, h, lambda3,
  * m, gamma, unused]. r_cut = the largest R + D.                           */
+/* lanes_per_atom (Tersoff, SW): lanes of one atom's group, 4, 8 or 16 (0 =
+ * 8); a tile shape the autotuner picks per workload. */
 typedef struct mbf_tersoff_tables {
     int ns;
     const double *tb;
@@ -208,7 +210,7 @@ typedef struct mbf_tersoff_tables {
 
 int mbf_tersoff_eval(const mbf_system *sys, const mbf_nlist *nl,
                      const mbf_tersoff_tables *tab, const mbf_reduce_plan *plan,
-                     int precision, void *workspace, size_t workspace_bytes,
+                     int precision, int lanes_per_atom, void *workspace, size_t workspace_bytes,
                      double *forces, double *energy, double *virial, void *stream);
 
 /* ---- Stillinger-Weber -------------------------------------------------
@@ -227,7 +229,7 @@ typedef struct mbf_sw_tables {
 } mbf_sw_tables;
 
 int mbf_sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables *tab,
-                const mbf_reduce_plan *plan, int precision, void *workspace,
+                const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
                 size_t workspace_bytes, double *forces, double *energy,
                 double *virial, void *stream);
 
