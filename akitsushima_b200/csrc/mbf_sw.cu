@@ -26,46 +26,46 @@ struct SwDev {
     double rc;
 };
 
-// Three-body term h and its gradient w.r.t. r_ij and r_ik
-// (engine/stillinger_weber.py:96-154).
+// Per-leg factors of the three-body term (engine/stillinger_weber.py:96-154):
+// h(i, j, k) = c3 E_j E_k (cos theta_jik - cos0)^2 with E_x = exp(gamma_x /
+// (r_ix / sigma_x - a_x)) and dE_x/dr_ix = E_x D_x, D_x = -gamma_x /
+// (sigma_x (r_ix / sigma_x - a_x)^2).  A leg at or beyond a_x sigma_x has
+// E = D = 0, which zeroes every angle it takes part in (the reference's
+// early return).  The legs depend only on (centre, neighbour), so they are
+// evaluated once per slot, not once per angle.
 template <typename T>
-__device__ __forceinline__ T sw_h3(T rijx, T rijy, T rijz, T r_ij, T rikx, T riky, T rikz, T r_ik, T sig_j,
-                                   T a_j, T gam_j, T sig_k, T a_k, T gam_k, T c3, T costh0, T gj[3], T gk[3]) {
-    T xij = r_ij / sig_j, xik = r_ik / sig_k;
-    if (xij >= a_j || xik >= a_k) {
-        gj[0] = gj[1] = gj[2] = gk[0] = gk[1] = gk[2] = T(0);
-        return T(0);
+__device__ __forceinline__ void sw_leg(T r, T sig, T a, T gam, T &E, T &D) {
+    T x = r / sig;
+    if (!(x < a)) {
+        E = T(0);
+        D = T(0);
+        return;
     }
-    T dj = xij - a_j, dk = xik - a_k;
-    T e_ij = clamped_exp<T>(gam_j / dj), e_ik = clamped_exp<T>(gam_k / dk);
-    T cos_th = (rijx * rikx + rijy * riky + rijz * rikz) / (r_ij * r_ik);
-    T dcos = cos_th - costh0;
-    T h = c3 * e_ij * e_ik * dcos * dcos;
-    T pre = c3 * e_ij * e_ik * dcos;
-    T inv_ij = T(1) / r_ij, inv_ik = T(1) / r_ik;
-    T ujx = rijx * inv_ij, ujy = rijy * inv_ij, ujz = rijz * inv_ij;
-    T ukx = rikx * inv_ik, uky = riky * inv_ik, ukz = rikz * inv_ik;
-    T rad_j = pre * dcos * (-gam_j / (sig_j * dj * dj));
-    T rad_k = pre * dcos * (-gam_k / (sig_k * dk * dk));
-    T ang_j = T(2) * pre * inv_ij, ang_k = T(2) * pre * inv_ik;
-    gj[0] = rad_j * ujx + ang_j * (ukx - cos_th * ujx);
-    gj[1] = rad_j * ujy + ang_j * (uky - cos_th * ujy);
-    gj[2] = rad_j * ujz + ang_j * (ukz - cos_th * ujz);
-    gk[0] = rad_k * ukx + ang_k * (ujx - cos_th * ukx);
-    gk[1] = rad_k * uky + ang_k * (ujy - cos_th * uky);
-    gk[2] = rad_k * ukz + ang_k * (ujz - cos_th * ukz);
-    return h;
+    T d = x - a;
+    E = clamped_exp<T>(gam / d);
+    D = -gam / (sig * d * d);
 }
 
+// One centre's row staged in shared memory: displacements, 1/r, leg
+// factors, species, and the slots inside the cutoff compacted into `list`.
 template <typename T, int MAXN>
 struct SwRow {
-    T x[MAXN], y[MAXN], z[MAXN], r[MAXN];
+    T x[MAXN], y[MAXN], z[MAXN], r[MAXN], ir[MAXN], E[MAXN], D[MAXN];
     int sp[MAXN];
-    int ok[MAXN];
+    int list[MAXN];
 };
 
-// SYM: every (i, j, k) record equals its (i, k, j) twin (one species), so a
-// slot needs one h evaluation per partner with the full lambda.
+// SYM: every (i, j, k) record equals its (i, k, j) twin (one species): one
+// coefficient and cos0 for every angle.  Otherwise both orders, each with
+// its own record (lambda/2 of (i, j, k) and of (i, k, j)).
+//
+// For slot s and partner k (both inside the cutoff, k != s) with
+// P = E_s E_k, cos = u_s . u_k, dc_o = cos - cos0_o over the orders o:
+//   energy booked on slot s:  c_1 P dc_1^2        (order (i, s, k))
+//   dh/dr_s = P [D_s A u_s + (B / r_s)(u_k - cos u_s)],
+//   A = sum_o c_o dc_o^2,  B = 2 sum_o c_o dc_o,
+// so each ordered triple's energy is booked once and each slot collects the
+// whole gradient of every angle on its own leg.
 template <typename T, int MAXN, bool SYM, int LPA>
 __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr,
                          const int *__restrict__ rev, SwDev P, double *__restrict__ slot_G, double *__restrict__ f_local,
@@ -73,11 +73,13 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
     constexpr int GPB = SwGeom<MAXN, LPA>::GPB;
     __shared__ SwRow<T, MAXN> rows[GPB];
     const int sub = threadIdx.x & (LPA - 1);
+    const int lane = threadIdx.x & 31;
+    const unsigned gmask = (LPA == 32) ? 0xffffffffu : (((1u << LPA) - 1u) << (lane & ~(LPA - 1)));
     SwRow<T, MAXN> &R = rows[threadIdx.x / LPA];
     const int ns = P.ns;
     for (int base = blockIdx.x * GPB; base < S.n_atoms; base += gridDim.x * GPB) {
         int i = base + threadIdx.x / LPA;
-        int beg = 0, n = 0;
+        int beg = 0, n = 0, nok = 0, si = 0;
         bool live = i < S.n_atoms;
         if (live) {
             beg = row_off[i];
@@ -88,90 +90,124 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
             }
         }
         if (live) {
+            si = S.types[i];
             const double *cell = cell_of(S, i);
             double xi = S.pos[3 * (size_t)i], yi = S.pos[3 * (size_t)i + 1], zi = S.pos[3 * (size_t)i + 2];
-            for (int s = sub; s < n; s += LPA) {
-                int j = nbr[beg + s];
-                double dx, dy, dz;
-                mic_exact(cell, S.pos[3 * (size_t)j] - xi, S.pos[3 * (size_t)j + 1] - yi,
-                          S.pos[3 * (size_t)j + 2] - zi, dx, dy, dz);
-                double r = sqrt(dx * dx + dy * dy + dz * dz);
-                R.x[s] = (T)dx;
-                R.y[s] = (T)dy;
-                R.z[s] = (T)dz;
-                R.r[s] = (T)r;
-                R.sp[s] = S.types[j];
-                R.ok[s] = (r < P.rc && r > 1e-12) ? 1 : 0;
+            // n is uniform over the lane group, so every lane of the group
+            // takes the same number of trips and the ballot is complete
+            for (int s0 = 0; s0 < n; s0 += LPA) {
+                int s = s0 + sub;
+                bool ok = false;
+                if (s < n) {
+                    int j = nbr[beg + s];
+                    double dx, dy, dz;
+                    mic_exact(cell, S.pos[3 * (size_t)j] - xi, S.pos[3 * (size_t)j + 1] - yi,
+                              S.pos[3 * (size_t)j + 2] - zi, dx, dy, dz);
+                    double r = sqrt(dx * dx + dy * dy + dz * dz);
+                    ok = r < P.rc && r > 1e-12;
+                    if (ok) {
+                        int sj = S.types[j];
+                        const double *ls = P.leg + 4 * (si * ns + sj);
+                        T E, D;
+                        sw_leg<T>((T)r, (T)ls[0], (T)ls[1], (T)ls[2], E, D);
+                        R.x[s] = (T)dx;
+                        R.y[s] = (T)dy;
+                        R.z[s] = (T)dz;
+                        R.r[s] = (T)r;
+                        R.ir[s] = T(1) / (T)r;
+                        R.E[s] = E;
+                        R.D[s] = D;
+                        R.sp[s] = sj;
+                    } else {
+                        size_t o = 3 * (size_t)rev[beg + s];
+                        slot_G[o] = 0.0;
+                        slot_G[o + 1] = 0.0;
+                        slot_G[o + 2] = 0.0;
+                    }
+                }
+                unsigned b = __ballot_sync(gmask, ok) >> (lane & ~(LPA - 1));
+                if (LPA < 32) b &= (1u << LPA) - 1u;
+                if (ok) R.list[nok + __popc(b & ((1u << sub) - 1u))] = s;
+                nok += __popc(b);
             }
         }
         __syncwarp();
-        double fx = 0, fy = 0, fz = 0, e = 0, npair = 0;
+        double fx = 0, fy = 0, fz = 0, e = 0;
         double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         if (live) {
-            int si = S.types[i];
-            for (int s = sub; s < n; s += LPA) {
-                double Gx = 0, Gy = 0, Gz = 0, cx = 0;
-                double dx = (double)R.x[s], dy = (double)R.y[s], dz = (double)R.z[s];
-                if (R.ok[s]) {
-                    int j = nbr[beg + s];
-                    int sj = R.sp[s];
-                    int lo = i < j ? si : sj, hi = i < j ? sj : si;
-                    // two-body (engine/stillinger_weber.py:23-52)
-                    const double *t2 = P.tb + 8 * (lo * ns + hi);
-                    T r = R.r[s];
-                    if (t2[0] != 0.0) {
-                        T sig = (T)t2[2], a = (T)t2[3];
-                        T xi_ = r / sig;
-                        if (xi_ < a) {
-                            T eps = (T)t2[1], A = (T)t2[4], B = (T)t2[5], pp = (T)t2[6], qq = (T)t2[7];
-                            T t = T(1) / (xi_ - a);
-                            T ex = clamped_exp<T>(t);
-                            T xp = RT<T>::pw(xi_, -pp), xq = RT<T>::pw(xi_, -qq);
-                            T V2 = eps * A * (B * xp - xq) * ex;
-                            T dV2 = eps * A * ex * ((-pp * B * xp / xi_ + qq * xq / xi_) + (B * xp - xq) * (-t * t));
-                            e += 0.5 * (double)V2;
-                            cx = (double)(dV2 / sig / r);
-                        }
+            T c_sym = T(0), cos0_sym = T(0);
+            if (SYM) {
+                c_sym = (T)P.tri[1];
+                cos0_sym = (T)P.tri[2];
+                if (P.tri[0] == 0.0) c_sym = T(0);
+            }
+            for (int t = sub; t < nok; t += LPA) {
+                int s = R.list[t];
+                int j = nbr[beg + s];
+                int sj = R.sp[s];
+                T xs = R.x[s], ys = R.y[s], zs = R.z[s], r = R.r[s], irs = R.ir[s];
+                T Es = R.E[s], Ds = R.D[s];
+                double dx = (double)xs, dy = (double)ys, dz = (double)zs;
+                double cx = 0.0;
+                // two-body (engine/stillinger_weber.py:23-52), record of the
+                // lower-indexed atom's species order
+                int lo = i < j ? si : sj, hi = i < j ? sj : si;
+                const double *t2 = P.tb + 8 * (lo * ns + hi);
+                if (t2[0] != 0.0) {
+                    T sig = (T)t2[2], a = (T)t2[3];
+                    T xi_ = r / sig;
+                    if (xi_ < a) {
+                        T eps = (T)t2[1], A = (T)t2[4], B = (T)t2[5], pp = (T)t2[6], qq = (T)t2[7];
+                        T tt = T(1) / (xi_ - a);
+                        T ex = clamped_exp<T>(tt);
+                        T xp = RT<T>::pw(xi_, -pp), xq = RT<T>::pw(xi_, -qq);
+                        T V2 = eps * A * (B * xp - xq) * ex;
+                        T dV2 = eps * A * ex * ((-pp * B * xp / xi_ + qq * xq / xi_) + (B * xp - xq) * (-tt * tt));
+                        e += 0.5 * (double)V2;
+                        cx = (double)(dV2 / sig / r);
                     }
-                    // three-body, slot s as one leg of every angle at i
-                    const double *ls = P.leg + 4 * (si * ns + sj);
-                    T sig_s = (T)ls[0], a_s = (T)ls[1], g_s = (T)ls[2];
-                    T gj[3], gk[3];
-                    double e3 = 0.0;
-                    for (int k = 0; k < n; ++k) {
-                        if (k == s || !R.ok[k]) continue;
-                        int sk = R.sp[k];
-                        const double *lk = P.leg + 4 * (si * ns + sk);
-                        const double *t3 = P.tri + 4 * ((si * ns + sj) * ns + sk);
-                        if (SYM) {
-                            if (t3[0] == 0.0) continue;
-                            T h = sw_h3<T>(R.x[s], R.y[s], R.z[s], r, R.x[k], R.y[k], R.z[k], R.r[k], sig_s, a_s,
-                                           g_s, (T)lk[0], (T)lk[1], (T)lk[2], T(2) * (T)t3[1], (T)t3[2], gj, gk);
-                            e3 += 0.5 * (double)h;
-                            Gx -= (double)gj[0];
-                            Gy -= (double)gj[1];
-                            Gz -= (double)gj[2];
-                        } else {
-                            if (t3[0] != 0.0) {
-                                T h = sw_h3<T>(R.x[s], R.y[s], R.z[s], r, R.x[k], R.y[k], R.z[k], R.r[k], sig_s,
-                                               a_s, g_s, (T)lk[0], (T)lk[1], (T)lk[2], (T)t3[1], (T)t3[2], gj, gk);
-                                e3 += (double)h;
-                                Gx -= (double)gj[0];
-                                Gy -= (double)gj[1];
-                                Gz -= (double)gj[2];
-                            }
-                            const double *t3r = P.tri + 4 * ((si * ns + sk) * ns + sj);
-                            if (t3r[0] != 0.0) {
-                                sw_h3<T>(R.x[k], R.y[k], R.z[k], R.r[k], R.x[s], R.y[s], R.z[s], r, (T)lk[0],
-                                         (T)lk[1], (T)lk[2], sig_s, a_s, g_s, (T)t3r[1], (T)t3r[2], gj, gk);
-                                Gx -= (double)gk[0];
-                                Gy -= (double)gk[1];
-                                Gz -= (double)gk[2];
-                            }
-                        }
-                    }
-                    e += e3;
                 }
+                // three-body angles with slot s as one leg
+                T gx = T(0), gy = T(0), gz = T(0);
+                double e3 = 0.0;
+                if (Es != T(0)) {
+                    for (int u = 0; u < nok; ++u) {
+                        if (u == t) continue;
+                        int k = R.list[u];
+                        T Ek = R.E[k];
+                        if (Ek == T(0)) continue;
+                        T xk = R.x[k], yk = R.y[k], zk = R.z[k], irk = R.ir[k];
+                        T cs = (xs * xk + ys * yk + zs * zk) * (irs * irk);
+                        T Pp = Es * Ek;
+                        T A, B, eh;
+                        if (SYM) {
+                            T dc = cs - cos0_sym;
+                            eh = c_sym * dc * dc;
+                            A = T(2) * eh;
+                            B = T(4) * c_sym * dc;
+                        } else {
+                            int sk = R.sp[k];
+                            const double *t3 = P.tri + 4 * ((si * ns + sj) * ns + sk);
+                            const double *t3r = P.tri + 4 * ((si * ns + sk) * ns + sj);
+                            T c1 = t3[0] != 0.0 ? (T)t3[1] : T(0);
+                            T c2 = t3r[0] != 0.0 ? (T)t3r[1] : T(0);
+                            T dc1 = cs - (T)t3[2], dc2 = cs - (T)t3r[2];
+                            eh = c1 * dc1 * dc1;
+                            A = eh + c2 * dc2 * dc2;
+                            B = T(2) * (c1 * dc1 + c2 * dc2);
+                        }
+                        e3 += (double)(Pp * eh);
+                        // dh/dr_s = P [(D_s A - B cos / r_s) u_s + (B / r_k) ... ] in
+                        // displacement form: u_s = d_s / r_s, u_k = d_k / r_k
+                        T as = Pp * (Ds * A - B * cs * irs) * irs;
+                        T ak = Pp * B * irs * irk;
+                        gx += as * xs + ak * xk;
+                        gy += as * ys + ak * yk;
+                        gz += as * zs + ak * zk;
+                    }
+                }
+                e += e3;
+                double Gx = -(double)gx, Gy = -(double)gy, Gz = -(double)gz;
                 fx += cx * dx - Gx;
                 fy += cx * dy - Gy;
                 fz += cx * dz - Gz;
@@ -185,8 +221,7 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
                 v[6] += -hz * dx + Gz * dx;
                 v[7] += -hz * dy + Gz * dy;
                 v[8] += -hz * dz + Gz * dz;
-                npair += R.ok[s] ? 1.0 : 0.0;
-                // the force on neighbour x goes to x's own slot (x -> i)
+                // the force on neighbour j goes to j's own slot (j -> i)
                 size_t o = 3 * (size_t)rev[beg + s];
                 slot_G[o] = Gx;
                 slot_G[o + 1] = Gy;
@@ -197,7 +232,6 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
         fy = group_sum<LPA>(fy);
         fz = group_sum<LPA>(fz);
         e = group_sum<LPA>(e);
-        npair = group_sum<LPA>(npair);
 #pragma unroll
         for (int q = 0; q < 9; ++q) v[q] = group_sum<LPA>(v[q]);
         if (sub == 0 && i < S.n_atoms) {
@@ -208,7 +242,7 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
             pa[0] = e;
 #pragma unroll
             for (int q = 0; q < 9; ++q) pa[1 + q] = v[q];
-            pa[10] = npair;
+            pa[10] = (double)nok;
         }
         __syncwarp();
     }
