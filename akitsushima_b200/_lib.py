@@ -69,7 +69,18 @@ _SIGS = {
     "mbf_nl_workspace_bytes": (_sz, [_i, _i]),
     "mbf_nl_build": (_i, [ctypes.POINTER(MbfSystem), _vp, _i, _d, _vp, _sz, _vp, _vp, _vp, _vp, _ll,
                           ctypes.POINTER(_ll), ctypes.POINTER(_i), _vp]),
+    "mbf_nl_rebuild_async": (_i, [ctypes.POINTER(MbfSystem), _vp, _i, _d, _vp, _sz, _vp, _vp, _vp, _vp,
+                                  _ll, _i, _vp, _vp]),
     "mbf_nl_max_displacement": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _vp]),
+    "mbf_md_kick_drift": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _vp, _d, _vp]),
+    "mbf_md_partial_count": (_i, [_i]),
+    "mbf_md_kick": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _d, _vp, _vp, _vp, _i, _vp, _vp]),
+    "mbf_md_skin_check": (_i, [ctypes.POINTER(MbfSystem), _vp, _d, _d, _vp, _vp, _i, _vp, _vp, _vp,
+                               ctypes.c_ulonglong, _vp]),
+    "mbf_md_rebuild_done": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp]),
+    "mbf_capture_cond_create": (_i, [_vp, ctypes.POINTER(ctypes.c_ulonglong)]),
+    "mbf_capture_if_begin": (_i, [_vp, _vp, ctypes.c_ulonglong]),
+    "mbf_capture_if_end": (_i, [_vp]),
     "mbf_nl_half_workspace_bytes": (_sz, [_i]),
     "mbf_nl_half_pairs": (_i, [ctypes.POINTER(MbfNlist), _vp, _vp, _vp, _sz, _vp]),
     "mbf_eval_workspace_bytes": (_sz, [_i, _ll, _i]),
@@ -90,6 +101,11 @@ _SIGS = {
     "mbf_profile_end": (_i, [ctypes.c_char_p, _sz]),
     "mbf_peak_probe": (_i, [_i, _vp, _sz, ctypes.POINTER(_d), _vp]),
 }
+
+MBF_STATUS_ROW_TOO_LONG = 1
+MBF_STATUS_BAD_INDEX = 2
+MBF_STATUS_CAPACITY = 4
+MBF_STATUS_SKIN = 8
 
 # Entry points declared in include/mbforce.h (checked by the CPU tests).
 EXPORTED = tuple(_SIGS)

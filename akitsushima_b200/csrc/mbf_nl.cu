@@ -267,11 +267,14 @@ __global__ void nl_max_disp(SysView S, const double *__restrict__ ref, const dou
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= S.n_atoms) return;
     int s = S.n_struct > 1 ? S.atom_struct[a] : 0;
-    const double *M = maps + 9 * (size_t)s;
     const double *r0 = ref + 3 * (size_t)a;
-    double ax = r0[0] * M[0] + r0[1] * M[3] + r0[2] * M[6];
-    double ay = r0[0] * M[1] + r0[1] * M[4] + r0[2] * M[7];
-    double az = r0[0] * M[2] + r0[1] * M[5] + r0[2] * M[8];
+    double ax = r0[0], ay = r0[1], az = r0[2];
+    if (maps) {  // null: lattice unchanged, M = I
+        const double *M = maps + 9 * (size_t)s;
+        ax = r0[0] * M[0] + r0[1] * M[3] + r0[2] * M[6];
+        ay = r0[0] * M[1] + r0[1] * M[4] + r0[2] * M[7];
+        az = r0[0] * M[2] + r0[1] * M[5] + r0[2] * M[8];
+    }
     double dx, dy, dz;
     mic_exact(S.cells + 18 * (size_t)s, S.pos[3 * (size_t)a] - ax, S.pos[3 * (size_t)a + 1] - ay,
               S.pos[3 * (size_t)a + 2] - az, dx, dy, dz);
@@ -303,6 +306,62 @@ __global__ void nl_upper_write(int n_atoms, const int *__restrict__ row_off, con
     }
 }
 
+// Device-side checks of the graph-capturable rebuild: a list that would not
+// fit its buffers or a row beyond the caller's staging limit sets a status
+// bit and leaves every row empty (no slot is written), so later kernels of a
+// captured sequence read nothing out of bounds.
+__global__ void nl_guard(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ mrow,
+                         long long cap, int limit, int *__restrict__ status, int *__restrict__ skip) {
+    if (threadIdx.x != 0) return;
+    int bad = 0;
+    if ((long long)row_off[n_atoms] > cap) bad |= MBF_STATUS_CAPACITY;
+    if (*mrow > limit) bad |= MBF_STATUS_ROW_TOO_LONG;
+    *skip = bad;
+    if (bad) atomicOr(status, bad);
+}
+
+__global__ void nl_clear_if(int n_atoms, const int *__restrict__ skip, int *__restrict__ row_off,
+                            int *__restrict__ upper) {
+    if (*skip == 0) return;
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a <= n_atoms) row_off[a] = 0;
+    if (a < n_atoms) upper[a] = 0;
+}
+
+// Records d (this step's largest displacement since the last rebuild) and
+// the reference's rebuild decision r_list - 2 d <= r_cut (any structure,
+// engine/neighborlist.py:653-673 with the lattice unchanged); sets the
+// graph conditional that gates the rebuild branch when one is given, and
+// flags MBF_STATUS_SKIN when a status word is given (fixed-interval runs,
+// where the decision is an assertion).
+__global__ void nl_skin_record(int n_struct, const double *__restrict__ d, double r_list, double r_cut,
+                               double *__restrict__ d_log,
+                               int rows, int *__restrict__ counter, int *__restrict__ gate, int *__restrict__ status,
+                               unsigned long long cond) {
+    if (threadIdx.x != 0) return;
+    int row = *counter % rows;
+    int need = 0;
+    for (int s = 0; s < n_struct; ++s) {
+        d_log[(size_t)row * n_struct + s] = d[s];
+        if (r_list - 2.0 * d[s] <= r_cut) need = 1;
+    }
+    *gate = need;
+    if (need && status) atomicOr(status, MBF_STATUS_SKIN);
+    if (cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, need ? 1u : 0u);
+    *counter += 1;
+}
+
+__global__ void nl_count_rebuild(int *__restrict__ n) {
+    if (threadIdx.x == 0) *n += 1;
+}
+
+__global__ void nl_status_merge(const int *__restrict__ err, int *__restrict__ status) {
+    if (threadIdx.x != 0) return;
+    int e = err[0];
+    if (e & MBF_DEV_ROW_TOO_LONG) atomicOr(status, MBF_STATUS_ROW_TOO_LONG);
+    if (e & ~MBF_DEV_ROW_TOO_LONG) atomicOr(status, MBF_STATUS_BAD_INDEX);
+}
+
 }  // namespace mbf
 
 using namespace mbf;
@@ -313,17 +372,9 @@ size_t mbf_nl_workspace_bytes(int n_atoms, int n_cells_total) {
     return nl_layout(n_atoms, n_cells_total).total;
 }
 
-int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total, double r_list,
-                 void *workspace, size_t workspace_bytes, int *row_off, int *nbr, int *rev, int *upper,
-                 long long nbr_capacity, long long *n_slots, int *max_row, void *stream) {
-    if (!sys || !grids || !workspace || !row_off || !n_slots || !max_row || sys->n_atoms < 0 ||
-        n_cells_total <= 0 || !(r_list > 0.0))
-        return MBF_ERR_ARGUMENT;
-    cudaStream_t st = (cudaStream_t)stream;
-    int N = sys->n_atoms;
-    NlLayout L = nl_layout(N, n_cells_total);
-    if (workspace_bytes < L.total) return MBF_ERR_WORKSPACE;
-    SysView S = make_view(sys);
+static int nl_prepare(const SysView &S, const int *grids, int n_cells_total, double rl2, void *workspace,
+                      const NlLayout &L, int *row_off, cudaStream_t st) {
+    int N = S.n_atoms;
     int *err = ws_at<int>(workspace, L.err);
     int *atom_cell = ws_at<int>(workspace, L.atom_cell);
     int *cell_count = ws_at<int>(workspace, L.cell_count);
@@ -337,12 +388,6 @@ int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total, dou
     if (cudaMemsetAsync(mrow, 0, sizeof(int), st) != cudaSuccess) return MBF_ERR_CUDA;
     if (cudaMemsetAsync(cell_count, 0, sizeof(int) * (size_t)n_cells_total, st) != cudaSuccess)
         return MBF_ERR_CUDA;
-    if (N == 0) {
-        if (cudaMemsetAsync(row_off, 0, sizeof(int), st) != cudaSuccess) return MBF_ERR_CUDA;
-        *n_slots = 0;
-        *max_row = 0;
-        return MBF_OK;
-    }
     PROF_BEGIN("nl_assign", st);
     nl_assign<<<(N + 255) / 256, 256, 0, st>>>(S, grids, atom_cell, cell_count);
     PROF_END("nl_assign", st);
@@ -355,28 +400,25 @@ int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total, dou
     nl_fill_cells<<<(N + 255) / 256, 256, 0, st>>>(N, atom_cell, cursor, cell_atoms);
     nl_sort_cells<<<(n_cells_total + 127) / 128, 128, 0, st>>>(n_cells_total, cell_start, cell_atoms);
     MBF_CHECK_LAUNCH();
-    double rl2 = r_list * r_list;
     int blocks = (N + NL_WARPS - 1) / NL_WARPS;
     int g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_count);
     PROF_BEGIN("nl_count", st);
     nl_count<<<g, 32 * NL_WARPS, 0, st>>>(S, grids, cell_start, cell_atoms, atom_cell, rl2, row_cnt, mrow);
     PROF_END("nl_count", st);
     MBF_CHECK_LAUNCH();
-    rc = exclusive_scan(row_cnt, row_off, N, scan_ws, st);
-    if (rc != MBF_OK) return rc;
-    int host[2];
-    if (cudaMemcpyAsync(&host[0], row_off + N, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaMemcpyAsync(&host[1], mrow, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-        return MBF_ERR_CUDA;
-    *n_slots = host[0];
-    *max_row = host[1];
-    if ((long long)host[0] > nbr_capacity || !nbr || !rev) return MBF_ERR_CAPACITY;
-    if (!upper) return MBF_ERR_ARGUMENT;
-    if (host[1] > NL_MAXROW) return MBF_ERR_ROW_TOO_LONG;
-    g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_fill);
+    return exclusive_scan(row_cnt, row_off, N, scan_ws, st);
+}
+
+static int nl_finish(const SysView &S, const int *grids, double rl2, void *workspace, const NlLayout &L,
+                     const int *row_off, int *nbr, int *rev, int *upper, cudaStream_t st) {
+    int N = S.n_atoms;
+    int *err = ws_at<int>(workspace, L.err);
+    int blocks = (N + NL_WARPS - 1) / NL_WARPS;
+    int g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_fill);
     PROF_BEGIN("nl_fill", st);
-    nl_fill<<<g, 32 * NL_WARPS, 0, st>>>(S, grids, cell_start, cell_atoms, atom_cell, rl2, row_off, nbr, upper, err);
+    nl_fill<<<g, 32 * NL_WARPS, 0, st>>>(S, grids, ws_at<int>(workspace, L.cell_start),
+                                         ws_at<int>(workspace, L.cell_atoms), ws_at<int>(workspace, L.atom_cell),
+                                         rl2, row_off, nbr, upper, err);
     PROF_END("nl_fill", st);
     MBF_CHECK_LAUNCH();
     g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_reverse);
@@ -384,12 +426,76 @@ int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total, dou
     nl_reverse<<<g, 32 * NL_WARPS, 0, st>>>(N, row_off, nbr, rev, err);
     PROF_END("nl_reverse", st);
     MBF_CHECK_LAUNCH();
+    return MBF_OK;
+}
+
+int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total, double r_list,
+                 void *workspace, size_t workspace_bytes, int *row_off, int *nbr, int *rev, int *upper,
+                 long long nbr_capacity, long long *n_slots, int *max_row, void *stream) {
+    if (!sys || !grids || !workspace || !row_off || !n_slots || !max_row || sys->n_atoms < 0 ||
+        n_cells_total <= 0 || !(r_list > 0.0))
+        return MBF_ERR_ARGUMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    int N = sys->n_atoms;
+    NlLayout L = nl_layout(N, n_cells_total);
+    if (workspace_bytes < L.total) return MBF_ERR_WORKSPACE;
+    SysView S = make_view(sys);
+    if (N == 0) {
+        if (cudaMemsetAsync(row_off, 0, sizeof(int), st) != cudaSuccess) return MBF_ERR_CUDA;
+        *n_slots = 0;
+        *max_row = 0;
+        return MBF_OK;
+    }
+    double rl2 = r_list * r_list;
+    int rc = nl_prepare(S, grids, n_cells_total, rl2, workspace, L, row_off, st);
+    if (rc != MBF_OK) return rc;
+    int host[2];
+    if (cudaMemcpyAsync(&host[0], row_off + N, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(&host[1], ws_at<int>(workspace, L.maxrow), sizeof(int), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return MBF_ERR_CUDA;
+    *n_slots = host[0];
+    *max_row = host[1];
+    if ((long long)host[0] > nbr_capacity || !nbr || !rev) return MBF_ERR_CAPACITY;
+    if (!upper) return MBF_ERR_ARGUMENT;
+    if (host[1] > NL_MAXROW) return MBF_ERR_ROW_TOO_LONG;
+    rc = nl_finish(S, grids, rl2, workspace, L, row_off, nbr, rev, upper, st);
+    if (rc != MBF_OK) return rc;
     int herr = 0;
-    if (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    if (cudaMemcpyAsync(&herr, ws_at<int>(workspace, L.err), sizeof(int), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return MBF_ERR_CUDA;
     if (herr & MBF_DEV_ROW_TOO_LONG) return MBF_ERR_ROW_TOO_LONG;
     if (herr) return MBF_ERR_ARGUMENT;
+    return MBF_OK;
+}
+
+int mbf_nl_rebuild_async(const mbf_system *sys, const int *grids, int n_cells_total, double r_list,
+                         void *workspace, size_t workspace_bytes, int *row_off, int *nbr, int *rev, int *upper,
+                         long long nbr_capacity, int max_row_limit, int *status, void *stream) {
+    if (!sys || !grids || !workspace || !row_off || !nbr || !rev || !upper || !status || sys->n_atoms <= 0 ||
+        n_cells_total <= 0 || !(r_list > 0.0) || nbr_capacity < 0 || max_row_limit <= 0 ||
+        max_row_limit > NL_MAXROW)
+        return MBF_ERR_ARGUMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    int N = sys->n_atoms;
+    NlLayout L = nl_layout(N, n_cells_total);
+    if (workspace_bytes < L.total) return MBF_ERR_WORKSPACE;
+    SysView S = make_view(sys);
+    double rl2 = r_list * r_list;
+    int rc = nl_prepare(S, grids, n_cells_total, rl2, workspace, L, row_off, st);
+    if (rc != MBF_OK) return rc;
+    int *err = ws_at<int>(workspace, L.err);
+    nl_guard<<<1, 32, 0, st>>>(N, row_off, ws_at<int>(workspace, L.maxrow), nbr_capacity, max_row_limit, status,
+                               err + 4);
+    nl_clear_if<<<(N + 256) / 256, 256, 0, st>>>(N, err + 4, row_off, upper);
+    MBF_CHECK_LAUNCH();
+    rc = nl_finish(S, grids, rl2, workspace, L, row_off, nbr, rev, upper, st);
+    if (rc != MBF_OK) return rc;
+    nl_status_merge<<<1, 32, 0, st>>>(err, status);
+    MBF_CHECK_LAUNCH();
     return MBF_OK;
 }
 
@@ -403,6 +509,39 @@ int mbf_nl_max_displacement(const mbf_system *sys, const double *ref_positions, 
     if (sys->n_atoms == 0) return MBF_OK;
     nl_max_disp<<<(sys->n_atoms + 255) / 256, 256, 0, st>>>(S, ref_positions, maps,
                                                             (unsigned long long *)d_max);
+    MBF_CHECK_LAUNCH();
+    return MBF_OK;
+}
+
+int mbf_md_skin_check(const mbf_system *sys, const double *ref_positions, double r_list, double r_cut,
+                      double *d_scratch, double *d_log, int rows, int *counter, int *gate, int *status,
+                      unsigned long long cond_handle, void *stream) {
+    if (!sys || !ref_positions || !d_scratch || !d_log || !counter || !gate || rows <= 0 || !(r_list > r_cut) ||
+        !(r_cut > 0.0) || sys->n_struct <= 0)
+        return MBF_ERR_ARGUMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    SysView S = make_view(sys);
+    if (cudaMemsetAsync(d_scratch, 0, sizeof(double) * (size_t)sys->n_struct, st) != cudaSuccess)
+        return MBF_ERR_CUDA;
+    if (sys->n_atoms > 0) {
+        nl_max_disp<<<(sys->n_atoms + 255) / 256, 256, 0, st>>>(S, ref_positions, nullptr,
+                                                                (unsigned long long *)d_scratch);
+        MBF_CHECK_LAUNCH();
+    }
+    nl_skin_record<<<1, 32, 0, st>>>(sys->n_struct, d_scratch, r_list, r_cut, d_log, rows, counter, gate,
+                                     status, cond_handle);
+    MBF_CHECK_LAUNCH();
+    return MBF_OK;
+}
+
+int mbf_md_rebuild_done(const mbf_system *sys, double *ref_positions, int *rebuild_count, void *stream) {
+    if (!sys || !ref_positions || !rebuild_count) return MBF_ERR_ARGUMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (sys->n_atoms > 0 &&
+        cudaMemcpyAsync(ref_positions, sys->positions, sizeof(double) * 3 * (size_t)sys->n_atoms,
+                        cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return MBF_ERR_CUDA;
+    nl_count_rebuild<<<1, 32, 0, st>>>(rebuild_count);
     MBF_CHECK_LAUNCH();
     return MBF_OK;
 }

@@ -120,38 +120,72 @@ int exclusive_scan(const int *in, int *out, int n, int *ws, cudaStream_t st) {
 
 // ---- per-structure reduction of per-atom (energy, virial[9]) -------------
 
-constexpr int RED_BLOCK = 256;
+constexpr int RED_BLOCK = 128;
 
-__global__ void reduce_chunks(const double *__restrict__ per_atom, const int *__restrict__ chunk,
-                              int n_chunks, double *__restrict__ partial) {
-    __shared__ double sh[RED_BLOCK];
+// Per-structure sums of the per-atom accumulators in a fixed order, so every
+// evaluation of the same input gives the same bits.  Stage 1: one block per
+// chunk of atoms (chunks never straddle structures); each thread sums its
+// atoms' ATOM_ACC values in registers, then a shuffle tree per warp and the
+// warps in order.  Stage 2: one warp per structure sums its chunks the same
+// way.
+template <int NW>
+__device__ __forceinline__ void warp_sum_acc(double (&v)[ATOM_ACC]) {
+#pragma unroll
+    for (int q = 0; q < ATOM_ACC; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(MBF_FULL, v[q], o);
+}
+
+__global__ void __launch_bounds__(RED_BLOCK) reduce_chunks(const double *__restrict__ per_atom,
+                                                           const int *__restrict__ chunk, int n_chunks,
+                                                           double *__restrict__ partial) {
+    constexpr int NW = RED_BLOCK / 32;
+    __shared__ double sh[NW][ATOM_ACC];
     int c = blockIdx.x;
     if (c >= n_chunks) return;
     int a0 = chunk[3 * c + 1], a1 = chunk[3 * c + 2];
-    for (int q = 0; q < ATOM_ACC; ++q) {
-        double s = 0.0;
-        for (int a = a0 + threadIdx.x; a < a1; a += RED_BLOCK) s += per_atom[(size_t)a * ATOM_ACC + q];
-        sh[threadIdx.x] = s;
-        __syncthreads();
-        for (int w = RED_BLOCK / 2; w > 0; w >>= 1) {
-            if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) partial[(size_t)c * ATOM_ACC + q] = sh[0];
-        __syncthreads();
+    double v[ATOM_ACC];
+#pragma unroll
+    for (int q = 0; q < ATOM_ACC; ++q) v[q] = 0.0;
+    for (int a = a0 + threadIdx.x; a < a1; a += RED_BLOCK) {
+        const double *p = per_atom + (size_t)a * ATOM_ACC;
+#pragma unroll
+        for (int q = 0; q < ATOM_ACC; ++q) v[q] += p[q];
+    }
+    warp_sum_acc<NW>(v);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+#pragma unroll
+        for (int q = 0; q < ATOM_ACC; ++q) sh[w][q] = v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < ATOM_ACC) {
+        double t = 0.0;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) t += sh[k][threadIdx.x];
+        partial[(size_t)c * ATOM_ACC + threadIdx.x] = t;
     }
 }
 
 __global__ void reduce_structs(const double *__restrict__ partial, const int *__restrict__ chunk_first,
                                int n_struct, double *__restrict__ energy, double *__restrict__ virial) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n_struct) return;
-    double acc[ATOM_ACC];
-    for (int q = 0; q < ATOM_ACC; ++q) acc[q] = 0.0;
-    for (int c = chunk_first[s]; c < chunk_first[s + 1]; ++c)
-        for (int q = 0; q < ATOM_ACC; ++q) acc[q] += partial[(size_t)c * ATOM_ACC + q];
-    energy[s] = acc[10] > 0.0 ? acc[0] : 0.0;
-    for (int q = 0; q < 9; ++q) virial[9 * s + q] = acc[1 + q];
+    int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int l = threadIdx.x & 31;
+    if (s >= n_struct) return;  // whole warps leave together
+    double v[ATOM_ACC];
+#pragma unroll
+    for (int q = 0; q < ATOM_ACC; ++q) v[q] = 0.0;
+    for (int c = chunk_first[s] + l; c < chunk_first[s + 1]; c += 32) {
+        const double *p = partial + (size_t)c * ATOM_ACC;
+#pragma unroll
+        for (int q = 0; q < ATOM_ACC; ++q) v[q] += p[q];
+    }
+    warp_sum_acc<1>(v);
+    if (l == 0) {
+        energy[s] = v[10] > 0.0 ? v[0] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) virial[9 * s + q] = v[1 + q];
+    }
 }
 
 int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, int n_struct,
@@ -160,8 +194,7 @@ int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, in
     PROF_BEGIN("reduce_chunks", st);
     reduce_chunks<<<plan->n_chunks, RED_BLOCK, 0, st>>>(per_atom, plan->chunk, plan->n_chunks, partial);
     PROF_END("reduce_chunks", st);
-    reduce_structs<<<(n_struct + 127) / 128, 128, 0, st>>>(partial, plan->chunk_first, n_struct,
-                                                           energy, virial);
+    reduce_structs<<<(n_struct + 3) / 4, 128, 0, st>>>(partial, plan->chunk_first, n_struct, energy, virial);
     MBF_CHECK_LAUNCH();
     return MBF_OK;
 }

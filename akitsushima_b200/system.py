@@ -12,7 +12,7 @@ import torch
 from . import _lib
 
 # Atoms per reduction chunk (the per-structure energy/virial sums).
-REDUCE_CHUNK = 4096
+REDUCE_CHUNK = 512
 
 
 def cell_metrics(lattice):

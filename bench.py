@@ -362,6 +362,183 @@ def run_batched(args, world, rank, local):
     print(json.dumps(line), flush=True)
     return 0
 
+def make_si(n_cells, a=5.431, sigma=0.05, seed=0):
+    rng = np.random.default_rng(seed)
+    g = np.arange(n_cells)
+    cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    frac = (DIAMOND[None] + cells[:, None]).reshape(-1, 3)
+    pos = frac * a + rng.normal(0.0, sigma, frac.shape)
+    return np.eye(3) * a * n_cells, pos, ["Si"] * len(pos)
+
+
+MD_WORKLOADS = {
+    # name: (potential, cells, sigma, precision, MD steps per bench step)
+    "md_tersoff_si4096": ("tersoff", 8, 0.05, "fp64", 10),
+    "md_sw_si64k": ("sw", 20, 0.1, "mixed", 10),
+}
+
+
+def _md_potential(kind, precision):
+    import akitsushima_b200 as ak
+    if kind == "tersoff":
+        return ak.TersoffPotential(ak.TERSOFF_SI_1988, species=["Si"], precision=precision)
+    return ak.StillingerWeberPotential(ak.SW_SI_1985, species=["Si"], precision=precision)
+
+
+def time_reference_md(kind, lat, pos, types, n_steps):
+    """The oracle port of the reference's NVE loop and force call
+    (solvers/molecular_dynamics.py:1969-2000), every host thread, the pair
+    list rebuilt every 10 steps; seconds per MD step."""
+    import oracle
+    from akitsushima_b200.published_parameters import SW_SI_1985, TERSOFF_SI_1988
+    threads = cpu_count()
+    oracle.set_threads(threads)
+    m = np.full(len(pos), 28.086)
+    v0 = oracle.init_velocities_mb(300.0, m, np.random.default_rng(0))
+    rc = TERSOFF_SI_1988["R"] + TERSOFF_SI_1988["D"] if kind == "tersoff" else \
+        SW_SI_1985["a"] * SW_SI_1985["sigma"]
+    state = {"k": 0, "pairs": None}
+
+    def force(r):
+        if state["k"] % 10 == 0:
+            state["pairs"] = oracle.nl_build(lat, r, rc, 0.3)[:2]
+        state["k"] += 1
+        if kind == "tersoff":
+            e, f, _ = oracle.tersoff_single(TERSOFF_SI_1988, lat, r, state["pairs"])
+        else:
+            e, f, _ = oracle.sw_single(SW_SI_1985, lat, r, state["pairs"])
+        return e, f
+
+    force(pos)
+    t0 = time.perf_counter()
+    oracle.nve(force, lat, pos, m, v0, 1.0, n_steps)
+    return (time.perf_counter() - t0) / n_steps, threads
+
+
+def run_md(args, world, rank, local):
+    kind, n_cells, sigma, precision, per_step = MD_WORKLOADS[args.workload]
+    if args.precision_given:
+        precision = args.precision
+    lat, pos, types = make_si(n_cells, sigma=sigma)
+    n_atoms = len(pos)
+    cfg = {"workload": args.workload, "potential": "Tersoff 1988 Si(C)" if kind == "tersoff"
+           else "Stillinger-Weber 1985 Si", "n_atoms": n_atoms, "a": 5.431, "sigma": sigma,
+           "ensemble": "NVE velocity Verlet, dt 1 fs, Maxwell-Boltzmann 300 K (seed 0)",
+           "skin": 0.3, "rebuild": "the reference's displacement criterion (2 max|dr| >= skin), "
+                                   "checked on the device every step; the rebuild is a CUDA-graph "
+                                   "IF branch", "md_steps_per_bench_step": per_step,
+           "precision": precision, "l2": "256 MB scratch write between bench steps (each a "
+                                         "10-MD-step graph replay), outside the timed events",
+           "parallelism": f"replicas{world}"}
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        n = 3 if n_atoms > 10000 else 10
+        t, threads = time_reference_md(kind, lat, pos, types, n)
+        v = n_atoms / t
+        line = {"metric": METRIC, "value": v, "unit": "atoms/s", "impl": "reference", "n_gpus": 0,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3 * per_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": dict(cfg, precision="fp64"),
+                "cpu_baseline": {"value": v, "unit": "atoms/s", "cores": threads, "kind": "port",
+                                 "sample": f"{n} NVE steps of the {n_atoms}-atom structure (oracle port "
+                                           "of the reference loop and force call)"},
+                "e2e": {"value": v, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    from akitsushima_b200 import _lib, md
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    pot = _md_potential(kind, precision)
+    sim = md.NVE(pot, lat, pos, types, temperature=300.0, seed=0, steps_per_graph=per_step, device=dev)
+    sim.capture()
+    for _ in range(args.warmup):
+        sim.run(per_step)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            sim.run(per_step)
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    res = sim.results()
+    value = world * n_atoms * per_step / (ms * 1e-3)
+
+    # per-kernel breakdown: one interval of eager launches under the profiler
+    _lib.profile_begin()
+    sim.run(per_step, graph=False)
+    prof = _lib.profile_end()
+    launches = sum(c for c, _ in prof.values())
+
+    # end to end through the public API: host arrays in, NVE built (list,
+    # MB start, first forces), 10 x per_step steps, positions and thermo out
+    torch.cuda.synchronize()
+    n_e2e = 10 * per_step
+    t0 = time.perf_counter()
+    s2 = md.NVE(pot, lat, pos, types, temperature=300.0, seed=0, steps_per_graph=per_step, device=dev)
+    s2.run(n_e2e)
+    r2 = s2.results()
+    p2 = s2.positions
+    t_e2e = (time.perf_counter() - t0) / n_e2e
+    e2e = {"value": world * n_atoms / t_e2e, "unit": "atoms/s",
+           "h2d_bytes_per_step": (n_atoms * (24 + 24 + 4 + 8)) / n_e2e,
+           "d2h_bytes_per_step": (n_atoms * 24 + len(r2["e_pot"]) * 16) / n_e2e,
+           "ms_per_step": t_e2e * 1e3,
+           "path": f"md.NVE(numpy in) + run({n_e2e}) + results() + positions (graph captured inside)"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        n = 3 if n_atoms > 10000 else 10
+        t_cpu, threads = time_reference_md(kind, lat, pos, types, n)
+        cpu = {"value": n_atoms / t_cpu, "unit": "atoms/s", "cores": threads, "kind": "port",
+               "sample": f"{n} NVE steps of the same structure, oracle port of the reference's "
+                         "loop and numba force call"}
+    clocks = clk.summary()
+    drift = res["drift"]
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "ms_per_md_step": ms / per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64" if precision == "mixed" else "f64",
+            "data": "synthetic", "config": cfg, "gpu_launches": int(launches * args.steps),
+            "gpu_launches_per_step": launches, "clocks": clocks,
+            "kernels": {k: {"launches": c, "ms_per_launch": t / c} for k, (c, t) in prof.items()},
+            "energy": {"md_steps": int(len(drift)), "max_abs_drift_ev_per_atom":
+                       float(np.abs(drift).max() / n_atoms),
+                       "final_drift_ev_per_atom": float(drift[-1] / n_atoms),
+                       "max_skin_displacement": float(res["skin_displacement"].max()),
+                       "rebuilds": int(res["rebuilds"])},
+            "e2e": e2e, "cpu_baseline": cpu, "roofline": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
 
 def _replicated(lat, pos, r_list):
     from akitsushima_b200.system import replicate_thin
@@ -380,8 +557,10 @@ def main():
     ap.add_argument("--lanes", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--workload", default="eam_cuni_256k", choices=["eam_cuni_256k", "batched_si512"])
+    ap.add_argument("--workload", default="eam_cuni_256k",
+                    choices=["eam_cuni_256k", "batched_si512"] + sorted(MD_WORKLOADS))
     args = ap.parse_args()
+    args.precision_given = "--precision" in sys.argv
     args.warmup = max(3, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -389,6 +568,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "batched_si512":
         return run_batched(args, world, rank, local)
+    if args.workload in MD_WORKLOADS:
+        return run_md(args, world, rank, local)
     lat, pos, ids = make_cuni(args.cells)
     n_atoms = len(pos)
     workload = f"eam_zhou_cuni_fcc{args.cells}^3_{n_atoms}_atoms"

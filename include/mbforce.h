@@ -107,6 +107,27 @@ int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total,
                  int *row_off, int *nbr, int *rev, int *upper, long long nbr_capacity,
                  long long *n_slots, int *max_row, void *stream);
 
+/* Device status bits written by the graph-capturable entries below (OR-ed
+ * into a caller-owned device int that the caller clears and reads). */
+#define MBF_STATUS_ROW_TOO_LONG 1  /* a row beyond max_row_limit / staging */
+#define MBF_STATUS_BAD_INDEX 2     /* an index check failed */
+#define MBF_STATUS_CAPACITY 4      /* the list did not fit nbr_capacity */
+#define MBF_STATUS_SKIN 8          /* a rebuild found the skin criterion broken */
+
+/* The same list as mbf_nl_build rebuilt in place with no host
+ * synchronisation, so it can be captured in a CUDA graph (the neighbour
+ * list of a device MD loop, rebuilt at a fixed step interval).  The buffers
+ * keep their addresses; the slot count stays on the device (row_off[n]).
+ * A list that would need more than nbr_capacity slots, or a row longer than
+ * max_row_limit (<= 1024), sets MBF_STATUS_CAPACITY / MBF_STATUS_ROW_TOO_LONG
+ * in *status and leaves every row empty, so nothing is written out of
+ * bounds.  No counterpart in the reference, whose lists are host arrays. */
+int mbf_nl_rebuild_async(const mbf_system *sys, const int *grids, int n_cells_total,
+                         double r_list, void *workspace, size_t workspace_bytes,
+                         int *row_off, int *nbr, int *rev, int *upper,
+                         long long nbr_capacity, int max_row_limit, int *status,
+                         void *stream);
+
 /* Largest minimum-image displacement of any atom from its reference
  * position mapped by the lattice change (engine/neighborlist.py:653-668):
  * writes max_i |MIC(r_i - r_ref_i @ M_s)| per structure to d_max (n_struct),
@@ -239,6 +260,60 @@ int mbf_sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables 
  * and writes "name launches total_ms" lines to buf.  Returns the number of
  * kernels listed.  No counterpart in the reference (its timing is
  * benchmarks/bench_force.py's wall clock).                                */
+/* ---- velocity-Verlet NVE on the device ---------------------------------
+ * The integrator of NVESimulation.run (solvers/molecular_dynamics.py:
+ * 1969-2000) split around the force call: velocities in A/fs, masses in
+ * amu, forces in eV/A, inv_mass[a] = EV_ANG_TO_AMU_ANG_FS2 / m_a.
+ *
+ * mbf_md_kick_drift: v += dt/2 * F * inv_mass; r += dt * v; then the wrap
+ * of every position into its cell, frac = r @ inv(L), frac -= floor(frac),
+ * frac >= 1 -> 0, r = frac @ L (positions updated in place: `positions`
+ * is the mbf_system's array).                                            */
+int mbf_md_kick_drift(const mbf_system *sys, double *positions, double *velocities,
+                      const double *forces, const double *inv_mass, double dt, void *stream);
+
+/* v += dt/2 * F * inv_mass, and the kinetic energy of every structure,
+ * 1/2 sum m v^2 / EV_ANG_TO_AMU_ANG_FS2 in eV (_kinetic_energy,
+ * solvers/molecular_dynamics.py:239-244; m v^2 / conv = v^2 / inv_mass),
+ * summed in a fixed order: partial (mbf_md_partial_count(n_atoms) doubles
+ * per structure) is scratch, and the pair (potential energy energy[s],
+ * kinetic energy) is written to thermo at row (*counter) mod thermo_rows
+ * (thermo: (thermo_rows, n_struct, 2)); *counter (device) then advances
+ * by one.                                                               */
+int mbf_md_partial_count(int n_atoms);
+int mbf_md_kick(const mbf_system *sys, double *velocities, const double *forces,
+                const double *inv_mass, double dt, const double *energy,
+                double *partial, double *thermo, int thermo_rows, int *counter, void *stream);
+
+/* The reference's rebuild decision (engine/neighborlist.py:613-673 with
+ * the lattice fixed: rebuild iff r_list - 2 d <= r_cut, d = max_a |MIC(r_a -
+ * r_ref_a)| since the last rebuild) evaluated on the device every step:
+ * records d at row (*counter) mod rows of d_log (rows, n_struct), advances
+ * *counter, and writes the decision (1 = rebuild) to *gate (device int).
+ * cond_handle (from mbf_capture_cond_create, or 0) is set to the decision,
+ * gating an IF branch that holds mbf_nl_rebuild_async and
+ * mbf_md_rebuild_done.  A non-null status gets MBF_STATUS_SKIN when the
+ * decision is 1 (fixed-interval runs, where it is an assertion).        */
+int mbf_md_skin_check(const mbf_system *sys, const double *ref_positions, double r_list,
+                      double r_cut, double *d_scratch, double *d_log, int rows, int *counter,
+                      int *gate, int *status, unsigned long long cond_handle, void *stream);
+
+/* After a rebuild: ref_positions = positions, ++*rebuild_count (device). */
+int mbf_md_rebuild_done(const mbf_system *sys, double *ref_positions, int *rebuild_count,
+                        void *stream);
+
+/* Conditional branches inside a stream capture (CUDA graph IF nodes), so a
+ * captured MD step rebuilds its list only when the device decides to.
+ * mbf_capture_cond_create: a handle on the graph `stream` is capturing
+ * (value 0 at each launch).  mbf_capture_if_begin: adds an IF node on that
+ * handle after the stream's current work, makes it the stream's only
+ * dependency, and starts capturing `body_stream` (another stream) into the
+ * branch; mbf_capture_if_end ends the branch. No counterpart in the
+ * reference. */
+int mbf_capture_cond_create(void *stream, unsigned long long *cond_handle);
+int mbf_capture_if_begin(void *stream, void *body_stream, unsigned long long cond_handle);
+int mbf_capture_if_end(void *body_stream);
+
 void mbf_profile_begin(void);
 int mbf_profile_end(char *buf, size_t cap);
 

@@ -706,3 +706,49 @@ def eam(spec, lattice, positions, atom_types, pairs=None):
                              _l(spec.rho_fid), _l(spec.F_fid), _l(spec.phi_fid),
                              _L(len(spec.species)), ctypes.byref(st), _d(forces), _d(vir))
     return float(e), forces, vir / _volume(lattice)
+
+
+# ---- molecular dynamics ------------------------------------------------------
+EV_ANG_TO_AMU_ANG_FS2 = (1.60217663e-19 / 1.0e-10) / (1.66053906660e-27) * 1.0e-20
+K_B = 1.380649e-23 * 6.241509074e18
+
+
+def init_velocities_mb(T, masses, rng):
+    """solvers/molecular_dynamics.py:195-221 (_init_velocities_mb)."""
+    masses = np.asarray(masses, float)
+    N = len(masses)
+    sigma = np.sqrt(K_B * T * EV_ANG_TO_AMU_ANG_FS2 / masses)
+    v = rng.standard_normal((N, 3)) * sigma[:, None]
+    v -= np.sum(masses[:, None] * v, axis=0) / masses.sum()
+    e_kin = 0.5 * float(np.sum(masses[:, None] * v ** 2)) / EV_ANG_TO_AMU_ANG_FS2
+    n_dof = max(3 * N - 3, 1)
+    T_act = 2.0 * e_kin / (n_dof * K_B)
+    if T_act > 1e-12:
+        v *= np.sqrt(T / T_act)
+    return v
+
+
+def nve(force, lattice, positions, masses, velocities, dt, n_steps):
+    """Velocity Verlet with the wrap of NVESimulation.run
+    (solvers/molecular_dynamics.py:1969-2000); force(positions) -> (E, F).
+    Returns per-step (positions, velocities, e_pot, e_kin) lists."""
+    lattice = np.asarray(lattice, float)
+    r = np.array(positions, float)
+    v = np.array(velocities, float)
+    m = np.asarray(masses, float)
+    e, F = force(r)
+    acc = F * EV_ANG_TO_AMU_ANG_FS2 / m[:, None]
+    out = []
+    for _ in range(n_steps):
+        v += 0.5 * dt * acc
+        r += dt * v
+        frac = r @ np.linalg.inv(lattice)
+        frac -= np.floor(frac)
+        frac[frac >= 1.0] = 0.0
+        r = frac @ lattice
+        e, F = force(r)
+        acc = F * EV_ANG_TO_AMU_ANG_FS2 / m[:, None]
+        v += 0.5 * dt * acc
+        e_kin = 0.5 * float(np.sum(m[:, None] * v ** 2)) / EV_ANG_TO_AMU_ANG_FS2
+        out.append((r.copy(), v.copy(), e, e_kin))
+    return out

@@ -192,6 +192,22 @@ def main():
          r_cut=float(spot.r_cut), skin=0.3, pair_i=i, pair_j=j, energy=float(e),
          forces=np.asarray(f), stress=np.asarray(s), **tabs)
 
+    # ---- NVE molecular dynamics: the reference's own NVESimulation ----------
+    import tempfile
+    from akitsushima.solvers.molecular_dynamics import NVESimulation
+    latm, posm, tm = cubic(DIAMOND, 5.431, 2, ["Si"] * 8, rattle=0.05, seed=0)
+    fn = ak.force_fn_from_config({"type": "Tersoff", "species": ["Si"], "params": TERSOFF_SI})
+    with tempfile.TemporaryDirectory() as out_dir:
+        sim = NVESimulation(latm, posm, tm, force_fn=fn, r_cut=float(fn.r_cut), timestep=1.0,
+                            n_steps=20, temperature=300.0, thermo_every=1, traj_every=1000,
+                            output_dir=out_dir, skin_width=0.3, seed=7, verbose=False)
+        v0 = sim.velocities.copy()
+        sim.run()
+        thermo = np.loadtxt(os.path.join(out_dir, "thermo.log"), skiprows=1)
+    save("md_nve_si64_tersoff", lattice=latm, positions=posm, atom_types=np.array(tm), seed=7,
+         temperature=300.0, dt=1.0, n_steps=20, velocities0=v0, positions_final=sim.positions,
+         velocities_final=sim.velocities, thermo=thermo)
+
 
 if __name__ == "__main__":
     main()
