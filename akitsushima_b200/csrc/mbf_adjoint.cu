@@ -1,0 +1,455 @@
+// Tersoff adjoint: the vector-Jacobian product of (E, F, virial) with
+// respect to the dense parameter tables, for fitting.
+//
+// With upstream gradients gE (per structure), gF (per atom) and gW (per
+// structure, 3x3), the pull-back onto a parameter theta is
+//
+//   sum_s gE_s dE_s/dtheta + sum_a gF_a . dF_a/dtheta + sum_s gW_s : dW_s/dtheta
+//     = d/dtheta [ sum_s gE_s E_s + D_t E ],
+//
+// because F_a = -dE/dr_a and W_ab = -dE/deps_ab (the virial of a homogeneous
+// strain r -> (I + eps) r, compressive-positive stress times volume).  D_t E
+// is the derivative of the energy along the tangent field that moves every
+// pair vector d_ij (minimum image, j - i) by t_ij = gF_i - gF_j - gW d_ij.
+//
+// The energy is a sum of directed bond terms, each evaluated from centre i:
+//   V_ij = 1/2 fc(r_ij) [fR(r_ij) + b_ij(zeta_ij) fA(r_ij)],
+// summing to sum_{i<j} fc (fR + (b_ij + b_ji)/2 fA) (engine/tersoff.py:6-19,
+// :1399-1414, with the multi-species gating and table reads of
+// :1518-1711).  Every directed bond is re-evaluated here -- zeta included,
+// no per-triplet intermediate is stored -- in hyper-dual arithmetic: one
+// infinitesimal along the tangent t and K along parameter "sites" (the
+// places a bond reads a table entry).  The cross term of (tangent, site p)
+// is d(D_t V)/dtheta_p, the site part dV/dtheta_p.  Sites are reduced onto
+// the table entries they read in a fixed order (deterministic).
+//
+// Sites of a bond (i, j) (W = 8 + 7 ns of them):
+//   0..5   A, B, lambda1, lambda2, R, D of the pair record tb[lo, hi]
+//   6, 7   beta, n of the centre's record tb[s_i, s_j]
+//   8 + 7 s_k + 0..4  c, d, h, lambda3, gamma of tri[s_i, s_j, s_k]
+//   8 + 7 s_k + 5, 6  R, D of tb[s_i, s_k] (the cutoff of leg i-k)
+#include "mbf_util.cuh"
+
+namespace mbf {
+
+constexpr int ADJ_K = 8;        // parameter directions per pass
+constexpr int ADJ_BLOCK = 128;
+constexpr int ADJ_CHUNK = 1024; // slots per reduction block
+
+// v + t e + sum_p (p_p f_p + q_p e f_p): value, tangent, parameter
+// derivatives and their tangent cross terms.
+template <int K>
+struct HD {
+    double v, t, p[K], q[K];
+};
+
+template <int K>
+__device__ __forceinline__ HD<K> hd_const(double v) {
+    HD<K> r;
+    r.v = v;
+    r.t = 0.0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.p[k] = r.q[k] = 0.0;
+    return r;
+}
+
+// A parameter read at `site`: seeded if the site is one of this pass's.
+template <int K>
+__device__ __forceinline__ HD<K> hd_param(double v, int site, int first) {
+    HD<K> r = hd_const<K>(v);
+    int k = site - first;
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+        if (q == k) r.p[q] = 1.0;
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ HD<K> operator+(const HD<K> &a, const HD<K> &b) {
+    HD<K> r;
+    r.v = a.v + b.v;
+    r.t = a.t + b.t;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        r.p[k] = a.p[k] + b.p[k];
+        r.q[k] = a.q[k] + b.q[k];
+    }
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ HD<K> operator-(const HD<K> &a, const HD<K> &b) {
+    HD<K> r;
+    r.v = a.v - b.v;
+    r.t = a.t - b.t;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        r.p[k] = a.p[k] - b.p[k];
+        r.q[k] = a.q[k] - b.q[k];
+    }
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ HD<K> operator*(const HD<K> &a, const HD<K> &b) {
+    HD<K> r;
+    r.v = a.v * b.v;
+    r.t = a.t * b.v + a.v * b.t;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        r.p[k] = a.p[k] * b.v + a.v * b.p[k];
+        r.q[k] = a.q[k] * b.v + a.p[k] * b.t + a.t * b.p[k] + a.v * b.q[k];
+    }
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ HD<K> operator*(double s, const HD<K> &a) {
+    HD<K> r;
+    r.v = s * a.v;
+    r.t = s * a.t;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        r.p[k] = s * a.p[k];
+        r.q[k] = s * a.q[k];
+    }
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ HD<K> operator+(double s, const HD<K> &a) {
+    HD<K> r = a;
+    r.v += s;
+    return r;
+}
+
+// f(a) from f, f', f'' at a.v (the chain rule to second, mixed order).
+template <int K>
+__device__ __forceinline__ HD<K> hd_apply(const HD<K> &a, double f, double f1, double f2) {
+    HD<K> r;
+    r.v = f;
+    r.t = f1 * a.t;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        r.p[k] = f1 * a.p[k];
+        r.q[k] = f1 * a.q[k] + f2 * a.t * a.p[k];
+    }
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ HD<K> hd_inv(const HD<K> &a) {
+    double i = 1.0 / a.v;
+    return hd_apply<K>(a, i, -i * i, 2.0 * i * i * i);
+}
+
+template <int K>
+__device__ __forceinline__ HD<K> operator/(const HD<K> &a, const HD<K> &b) {
+    return a * hd_inv<K>(b);
+}
+
+template <int K>
+__device__ __forceinline__ HD<K> hd_exp(const HD<K> &a) {
+    double e = exp(a.v);
+    return hd_apply<K>(a, e, e, e);
+}
+
+template <int K>
+__device__ __forceinline__ HD<K> hd_log(const HD<K> &a) {
+    double i = 1.0 / a.v;
+    return hd_apply<K>(a, log(a.v), i, -i * i);
+}
+
+template <int K>
+__device__ __forceinline__ HD<K> hd_sin(const HD<K> &a) {
+    double s = sin(a.v), c = cos(a.v);
+    return hd_apply<K>(a, s, c, -s);
+}
+
+// exp clamped as the reference's _nb_exp (engine/_numba_common.py:12-33):
+// constant outside [-500, 500].
+template <int K>
+__device__ __forceinline__ HD<K> hd_cexp(const HD<K> &a) {
+    if (a.v > 500.0) return hd_const<K>(exp(500.0));
+    if (a.v < -500.0) return hd_const<K>(0.0);
+    return hd_exp<K>(a);
+}
+
+template <int K>
+__device__ __forceinline__ HD<K> hd_pow(const HD<K> &x, const HD<K> &y) {
+    return hd_exp<K>(y * hd_log<K>(x));
+}
+
+// fc(r) = 1/2 - 1/2 sin(pi/2 (r - R)/D) on [R - D, R + D] (engine/tersoff.py:48-54).
+template <int K>
+__device__ __forceinline__ HD<K> hd_fc(const HD<K> &r, const HD<K> &R, const HD<K> &D) {
+    if (r.v < R.v - D.v) return hd_const<K>(1.0);
+    if (r.v > R.v + D.v) return hd_const<K>(0.0);
+    HD<K> a = (0.5 * 3.14159265358979323846) * ((r - R) / D);
+    return 0.5 + (-0.5) * hd_sin<K>(a);
+}
+
+// (lambda3 u)^m for m = 1 or 3; pow otherwise (m is not a fitted value).
+template <int K>
+__device__ __forceinline__ HD<K> hd_arg(const HD<K> &l3, const HD<K> &u, double m) {
+    if (m == 3.0) return (l3 * l3 * l3) * (u * u * u);
+    if (m == 1.0) return l3 * u;
+    HD<K> mm = hd_const<K>(m);
+    return hd_pow<K>(l3, mm) * hd_pow<K>(u, mm);
+}
+
+// The slot's owning atom: rows are sorted, so a binary search in row_off.
+__device__ __forceinline__ int slot_owner(const int *__restrict__ row_off, int n_atoms, int s) {
+    int lo = 0, hi = n_atoms - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (row_off[mid] <= s) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+struct AdjTab {
+    int ns;
+    const double *tb;   // (ns*ns, 10): valid A B l1 l2 R D beta n -
+    const double *tri;  // (ns^3, 8):   valid c d h l3 m gam -
+    double rc;
+};
+
+struct AdjIn {
+    const double *gE, *gF, *gW;  // (S,), (N, 3), (S, 9); null = 0
+};
+
+// Pair vector, its length and its tangent t = gF_i - gF_j - gW d.
+__device__ __forceinline__ void adj_leg(const SysView &S, const AdjIn &G, const double *cell, int i, int j,
+                                        int s_struct, double d[3], double &r, double tg[3]) {
+    mic_exact(cell, S.pos[3 * (size_t)j] - S.pos[3 * (size_t)i], S.pos[3 * (size_t)j + 1] - S.pos[3 * (size_t)i + 1],
+              S.pos[3 * (size_t)j + 2] - S.pos[3 * (size_t)i + 2], d[0], d[1], d[2]);
+    r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    for (int a = 0; a < 3; ++a) {
+        double t = 0.0;
+        if (G.gF) t = G.gF[3 * (size_t)i + a] - G.gF[3 * (size_t)j + a];
+        if (G.gW) {
+            const double *w = G.gW + 9 * (size_t)s_struct + 3 * a;
+            t -= w[0] * d[0] + w[1] * d[1] + w[2] * d[2];
+        }
+        tg[a] = t;
+    }
+}
+
+// One pass (sites first .. first + K - 1) over every directed bond slot.
+// site_out (n_slots, W); code[s] = (s_i * ns + s_j) * 2 + (i < j) for a
+// contributing bond, -1 otherwise (written by pass 0).
+template <int K>
+__global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_sites(SysView S, const int *__restrict__ row_off,
+                                                              const int *__restrict__ nbr, AdjTab P, AdjIn G,
+                                                              int n_slots, int W, int first,
+                                                              double *__restrict__ site_out, int *__restrict__ code) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_slots) return;
+    const int ns = P.ns;
+    double *out = site_out + (size_t)s * W;
+    int last = first + K < W ? first + K : W;
+    if (s >= row_off[S.n_atoms]) {  // capacity beyond the list's slots
+        if (first == 0) code[s] = -1;
+        for (int w = first; w < last; ++w) out[w] = 0.0;
+        return;
+    }
+    int i = slot_owner(row_off, S.n_atoms, s);
+    int j = nbr[s];
+    int sst = S.n_struct > 1 ? S.atom_struct[i] : 0;
+    const double *cell = cell_of(S, i);
+    int si = S.types[i], sj = S.types[j];
+    int lo = i < j ? si : sj, hi = i < j ? sj : si;
+    const double *tp = P.tb + 10 * (lo * ns + hi);
+    double dij[3], rij, tij[3];
+    adj_leg(S, G, cell, i, j, sst, dij, rij, tij);
+    bool live = rij < P.rc && rij > 1e-12 && tp[0] != 0.0;
+    if (first == 0) code[s] = live ? ((si * ns + sj) * 2 + (i < j ? 1 : 0)) : -1;
+    if (!live) {
+        for (int w = first; w < last; ++w) out[w] = 0.0;
+        return;
+    }
+    HD<K> r = hd_const<K>(rij);
+    r.t = (dij[0] * tij[0] + dij[1] * tij[1] + dij[2] * tij[2]) / rij;
+    HD<K> A = hd_param<K>(tp[1], 0, first), B = hd_param<K>(tp[2], 1, first);
+    HD<K> l1 = hd_param<K>(tp[3], 2, first), l2 = hd_param<K>(tp[4], 3, first);
+    HD<K> Rp = hd_param<K>(tp[5], 4, first), Dp = hd_param<K>(tp[6], 5, first);
+    HD<K> fc = hd_fc<K>(r, Rp, Dp);
+    HD<K> fr = A * hd_cexp<K>((-1.0) * (l1 * r));
+    HD<K> fa = (-1.0) * (B * hd_cexp<K>((-1.0) * (l2 * r)));
+    // zeta_ij over the other neighbours k of i (engine/tersoff.py:528-540)
+    HD<K> zeta = hd_const<K>(0.0);
+    int beg = row_off[i], end = row_off[i + 1];
+    for (int sk_slot = beg; sk_slot < end; ++sk_slot) {
+        if (sk_slot == s) continue;
+        int k = nbr[sk_slot];
+        double dik[3], rik, tik[3];
+        adj_leg(S, G, cell, i, k, sst, dik, rik, tik);
+        if (!(rik < P.rc && rik > 1e-12)) continue;
+        int sk = S.types[k];
+        const double *tk = P.tb + 10 * (si * ns + sk);
+        const double *t3 = P.tri + 8 * ((si * ns + sj) * ns + sk);
+        if (tk[0] == 0.0 || t3[0] == 0.0) continue;
+        int base = 8 + 7 * sk;
+        HD<K> rk = hd_const<K>(rik);
+        rk.t = (dik[0] * tik[0] + dik[1] * tik[1] + dik[2] * tik[2]) / rik;
+        HD<K> Rk = hd_param<K>(tk[5], base + 5, first), Dk = hd_param<K>(tk[6], base + 6, first);
+        HD<K> fck = hd_fc<K>(rk, Rk, Dk);
+        if (fck.v == 0.0) continue;
+        HD<K> dot = hd_const<K>(dij[0] * dik[0] + dij[1] * dik[1] + dij[2] * dik[2]);
+        dot.t = tij[0] * dik[0] + tij[1] * dik[1] + tij[2] * dik[2] + dij[0] * tik[0] + dij[1] * tik[1] +
+                dij[2] * tik[2];
+        HD<K> cs = dot / (r * rk);
+        HD<K> c = hd_param<K>(t3[1], base + 0, first), d = hd_param<K>(t3[2], base + 1, first);
+        HD<K> h = hd_param<K>(t3[3], base + 2, first), l3 = hd_param<K>(t3[4], base + 3, first);
+        HD<K> gam = hd_param<K>(t3[6], base + 4, first);
+        HD<K> hc = h - cs;
+        HD<K> d2 = d * d, hc2 = hc * hc;
+        HD<K> g = 1.0 + ((c * c) * hc2) / (d2 * (d2 + hc2));
+        HD<K> ex = hd_cexp<K>(hd_arg<K>(l3, r - rk, t3[5]));
+        zeta = zeta + gam * fck * g * ex;
+    }
+    // b_ij with beta, n of the centre's record (engine/tersoff.py:1380-1391,
+    // :1693-1702): 1 unless zeta > 0 and beta != 0
+    const double *tij_rec = P.tb + 10 * (si * ns + sj);
+    HD<K> b = hd_const<K>(1.0);
+    if (zeta.v > 0.0 && tij_rec[7] != 0.0) {
+        HD<K> beta = hd_param<K>(tij_rec[7], 6, first), nn = hd_param<K>(tij_rec[8], 7, first);
+        HD<K> bz = hd_pow<K>(beta * zeta, nn);
+        b = hd_exp<K>(hd_log<K>(1.0 + bz) * ((-0.5) * hd_inv<K>(nn)));
+    }
+    HD<K> V = 0.5 * (fc * (fr + b * fa));
+    double ge = G.gE ? G.gE[sst] : 0.0;
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+        if (first + q < W) out[first + q] = ge * V.p[q] + V.q[q];
+}
+
+// Site values onto table entries: block b sums its chunk of slots for every
+// entry e (one thread each), in slot order.  Entries: tb (ns*ns, 10) then
+// tri (ns^3, 8), the layout of the tables themselves.
+__global__ void te_adjoint_entries(int n_slots, int ns, int W, const double *__restrict__ site_out,
+                                   const int *__restrict__ code, double *__restrict__ partial) {
+    int ne = 10 * ns * ns + 8 * ns * ns * ns;
+    int s0 = blockIdx.x * ADJ_CHUNK, s1 = min(n_slots, s0 + ADJ_CHUNK);
+    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        double acc = 0.0;
+        if (e < 10 * ns * ns) {
+            int row = e / 10, col = e % 10, a = row / ns, b = row % ns;
+            for (int s = s0; s < s1; ++s) {
+                int c = code[s];
+                if (c < 0) continue;
+                int lower = c & 1, pij = c >> 1, si = pij / ns, sj = pij % ns;
+                int lo = lower ? si : sj, hi = lower ? sj : si;
+                const double *o = site_out + (size_t)s * W;
+                if (col >= 1 && col <= 6 && lo == a && hi == b) acc += o[col - 1];
+                if ((col == 7 || col == 8) && si == a && sj == b) acc += o[6 + col - 7];
+                if ((col == 5 || col == 6) && si == a) acc += o[8 + 7 * b + 5 + (col - 5)];
+            }
+        } else {
+            int e3 = e - 10 * ns * ns;
+            int row = e3 / 8, col = e3 % 8;
+            int a = row / (ns * ns), b = (row / ns) % ns, k = row % ns;
+            int site = (col >= 1 && col <= 4) ? col - 1 : (col == 6 ? 4 : -1);
+            if (site >= 0) {
+                for (int s = s0; s < s1; ++s) {
+                    int c = code[s];
+                    if (c < 0) continue;
+                    int pij = c >> 1, si = pij / ns, sj = pij % ns;
+                    if (si == a && sj == b) acc += site_out[(size_t)s * W + 8 + 7 * k + site];
+                }
+            }
+        }
+        partial[(size_t)blockIdx.x * ne + e] = acc;
+    }
+}
+
+__global__ void te_adjoint_final(int n_blocks, int ns, const double *__restrict__ partial,
+                                 double *__restrict__ d_tb, double *__restrict__ d_tri) {
+    int ne = 10 * ns * ns + 8 * ns * ns * ns;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int b = 0; b < n_blocks; ++b) acc += partial[(size_t)b * ne + e];
+        if (e < 10 * ns * ns) d_tb[e] = acc;
+        else d_tri[e - 10 * ns * ns] = acc;
+    }
+}
+
+struct AdjLayout {
+    size_t site, code, partial, total;
+    int W, ne, n_blocks;
+};
+
+static AdjLayout adj_layout(long long n_slots, int ns) {
+    AdjLayout L;
+    L.W = 8 + 7 * ns;
+    L.ne = 10 * ns * ns + 8 * ns * ns * ns;
+    L.n_blocks = (int)((n_slots + ADJ_CHUNK - 1) / ADJ_CHUNK);
+    if (L.n_blocks < 1) L.n_blocks = 1;
+    size_t o = 0;
+    L.site = o;
+    o = align256(o + sizeof(double) * (size_t)(n_slots > 0 ? n_slots : 1) * L.W);
+    L.code = o;
+    o = align256(o + sizeof(int) * (size_t)(n_slots > 0 ? n_slots : 1));
+    L.partial = o;
+    o = align256(o + sizeof(double) * (size_t)L.n_blocks * L.ne);
+    L.total = o;
+    return L;
+}
+
+}  // namespace mbf
+
+using namespace mbf;
+
+extern "C" {
+
+size_t mbf_tersoff_adjoint_workspace_bytes(long long n_slots, int ns) {
+    if (ns <= 0 || n_slots < 0) return 0;
+    return adj_layout(n_slots, ns).total;
+}
+
+int mbf_tersoff_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_tersoff_tables *tab,
+                        const double *g_energy, const double *g_forces, const double *g_virial, void *workspace,
+                        size_t workspace_bytes, double *d_tb, double *d_tri, void *stream) {
+    if (!sys || !nl || !tab || !workspace || !d_tb || !d_tri || tab->ns <= 0 || tab->ns > 8)
+        return MBF_ERR_ARGUMENT;
+    if (nl->n_atoms != sys->n_atoms) return MBF_ERR_ARGUMENT;
+    AdjLayout L = adj_layout(nl->n_slots, tab->ns);
+    if (workspace_bytes < L.total) return MBF_ERR_WORKSPACE;
+    cudaStream_t st = (cudaStream_t)stream;
+    int ns = tab->ns;
+    if (sys->n_atoms == 0 || nl->n_slots == 0) {
+        if (cudaMemsetAsync(d_tb, 0, sizeof(double) * 10 * ns * ns, st) != cudaSuccess ||
+            cudaMemsetAsync(d_tri, 0, sizeof(double) * 8 * ns * ns * ns, st) != cudaSuccess)
+            return MBF_ERR_CUDA;
+        return MBF_OK;
+    }
+    SysView S = make_view(sys);
+    AdjTab P;
+    P.ns = ns;
+    P.tb = tab->tb;
+    P.tri = tab->tri;
+    P.rc = tab->r_cut;
+    AdjIn G;
+    G.gE = g_energy;
+    G.gF = g_forces;
+    G.gW = g_virial;
+    double *site = ws_at<double>(workspace, L.site);
+    int *code = ws_at<int>(workspace, L.code);
+    double *partial = ws_at<double>(workspace, L.partial);
+    int n_slots = (int)nl->n_slots;
+    int grid = (n_slots + ADJ_BLOCK - 1) / ADJ_BLOCK;
+    PROF_BEGIN("te_adjoint_sites", st);
+    for (int first = 0; first < L.W; first += ADJ_K)
+        te_adjoint_sites<ADJ_K><<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, n_slots, L.W, first,
+                                                              site, code);
+    PROF_END("te_adjoint_sites", st);
+    MBF_CHECK_LAUNCH();
+    int threads = L.ne < 1024 ? ((L.ne + 31) / 32) * 32 : 1024;
+    te_adjoint_entries<<<L.n_blocks, threads, 0, st>>>(n_slots, ns, L.W, site, code, partial);
+    te_adjoint_final<<<(L.ne + 127) / 128, 128, 0, st>>>(L.n_blocks, ns, partial, d_tb, d_tri);
+    MBF_CHECK_LAUNCH();
+    return MBF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,586 @@
+"""Tersoff fitting on the GPU: the reference's weighted E/F/S loss and its
+exact gradient with respect to the parameters.
+
+The reference evaluates its fit loss structure by structure on the CPU
+(fitting/loss.py:51-260) and gets gradients by forward differences, one
+full loss evaluation per parameter (fitting/driver.py:802-816).  Here the
+whole training set is one batch: one device neighbour list, one evaluation
+launch sequence (mbf_tersoff_eval, float64), the loss in torch, and the
+gradient from one adjoint call (mbf_tersoff_adjoint) behind a
+torch.autograd.Function -- the vector-Jacobian product of (E, F, virial)
+with respect to the dense parameter tables, which torch chains back
+through the parameter decoding (log variables, Tersoff-1989 mixing rules,
+tied records) to the optimisation vector x.
+
+Parameter sets mirror the reference's (fitting/parameter_sets.py:1035-1296):
+the same variables, names, x0, bounds, log-space keys and decode(); each
+also decodes differentiably (decode_torch).
+"""
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .force_fn import PotentialEngine
+from .neighbourlist import DeviceNeighbourList
+from .system import Batch, default_device, replicate_thin, species_ids
+from .tersoff import TERSOFF1989_ELEMENT_KEYS, TersoffPotential, tersoff1989_to_triplets
+
+_TB_KEYS = (("A", 0.0), ("B", 0.0), ("lambda1", 0.0), ("lambda2", 0.0), ("R", 1.0), ("D", 1.0),
+            ("beta", 0.0), ("n", 1.0))
+
+
+def _scalar(v, like):
+    if torch.is_tensor(v):
+        return v.to(dtype=torch.float64, device=like.device).reshape(())
+    return torch.tensor(float(v), dtype=torch.float64, device=like.device)
+
+
+def tables_from_records(records, species, device):
+    """Dense tables (tb (ns*ns, 10), tri (ns^3, 8), float64 torch) of a
+    {(i, j, k): record} table, laid out as TersoffPotential.host_tables
+    builds them (engine/tersoff.py:1606-1653); entries given as 0-d tensors
+    keep their autograd history."""
+    ref = torch.zeros((), dtype=torch.float64, device=device)
+    tb_rows, tri_rows = [], []
+    for a in species:
+        for b in species:
+            rec = records.get((a, b, b))
+            if rec is None:
+                vals = [0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 1.0, 0.0, 1.0, 0.0]
+            else:
+                vals = [1.0] + [rec.get(k, d) for k, d in _TB_KEYS] + [0.0]
+            tb_rows.append(torch.stack([_scalar(v, ref) for v in vals]))
+    for a in species:
+        for b in species:
+            for c in species:
+                rec = records.get((a, b, c))
+                if rec is None:
+                    vals = [0.0, 0.0, 1.0, 0.0, 0.0, 3.0, 1.0, 0.0]
+                else:
+                    vals = [1.0, rec["c"], rec["d"], rec["h"], rec.get("lambda3", 0.0), rec.get("m", 3.0),
+                            rec.get("gamma", 1.0), 0.0]
+                tri_rows.append(torch.stack([_scalar(v, ref) for v in vals]))
+    return torch.stack(tb_rows).contiguous(), torch.stack(tri_rows).contiguous()
+
+
+def table_cutoff(tb):
+    """Largest R + D over the valid pair records (the list radius)."""
+    t = tb.detach().cpu().numpy()
+    valid = t[:, 0] != 0.0
+    return float(np.max(t[valid, 5] + t[valid, 6])) if valid.any() else 0.0
+
+
+# ---- parameter sets ------------------------------------------------------------
+
+class _Variables:
+    """x <-> named variables (fitting/parameter_sets.py:1035-1065)."""
+
+    _LOG_KEYS = frozenset()
+    _BOUNDS = {}
+
+    @property
+    def x0(self):
+        return self._x0.copy()
+
+    @property
+    def bounds(self):
+        return self._bounds
+
+    @property
+    def variable_names(self):
+        return [name for name, _, _ in self.variables]
+
+    def _setup_vector(self, initial_values, owner):
+        x0, bounds = [], []
+        for (name, key, _), v in zip(self.variables, initial_values):
+            lo, hi = self._BOUNDS[key]
+            if not lo <= v <= hi:
+                raise ValueError(f"{owner}: initial {name} = {v} lies outside its search range [{lo}, {hi}].")
+            if key in self._LOG_KEYS:
+                x0.append(math.log(v))
+                bounds.append((math.log(lo), math.log(hi)))
+            else:
+                x0.append(v)
+                bounds.append((lo, hi))
+        self._x0 = np.array(x0)
+        self._bounds = bounds
+
+    def _value(self, key, xi):
+        if torch.is_tensor(xi):
+            return torch.exp(xi) if key in self._LOG_KEYS else xi
+        return float(np.exp(xi)) if key in self._LOG_KEYS else float(xi)
+
+    def build_engine(self, params):
+        return PotentialEngine().add(TersoffPotential(params["tersoff"], species=self.species))
+
+
+def _nested(records):
+    if isinstance(records, dict) and all(isinstance(k, tuple) for k in records):
+        return {tuple(k): dict(v) for k, v in records.items()}
+    out = {}
+    for rec in records:
+        rec = dict(rec)
+        out[(rec.pop("i"), rec.pop("j"), rec.pop("k"))] = rec
+    return out
+
+
+class MultiSpeciesTersoffParameterSet(_Variables):
+    """The (i, j, k) record table as variables (reference
+    fitting/parameter_sets.py:1068-1203): pair keys A, B, lambda1, lambda2
+    (R, D) one variable per unordered pair, written to (i, j, j) and
+    (j, i, i); beta, n one per diagonal record; c, d, h (lambda3, gamma) one
+    per record, or per centre element with tie="centre".  Fixed by default:
+    R, D, m, gamma, lambda3, beta, n."""
+
+    _DEFAULT_FIX = ("R", "D", "m", "gamma", "lambda3", "beta", "n")
+    _DEFAULT_FIT = ("A", "B", "lambda1", "lambda2", "c", "d", "h")
+    _PAIR_KEYS = ("A", "B", "lambda1", "lambda2", "R", "D")
+    _BOND_KEYS = ("beta", "n")
+    _ANGLE_KEYS = ("c", "d", "h", "lambda3", "gamma")
+    _LOG_KEYS = frozenset({"A", "B", "lambda1", "lambda2", "beta", "n", "c", "d", "gamma"})
+    _BOUNDS = {"A": (1.0, 1e5), "B": (0.1, 1e4), "lambda1": (0.5, 10.0), "lambda2": (0.1, 8.0),
+               "beta": (1e-10, 10.0), "n": (0.05, 10.0), "c": (1e-3, 1e7), "d": (1e-2, 1e4),
+               "h": (-1.0, 1.0), "lambda3": (0.0, 5.0), "gamma": (1e-3, 100.0), "R": (1.0, 5.0),
+               "D": (0.02, 0.5)}
+
+    def __init__(self, initial_records, species, fix_params=None, fit_keys=None, tie="record"):
+        if tie not in ("record", "centre"):
+            raise ValueError("MultiSpeciesTersoffParameterSet: tie must be 'record' or 'centre'")
+        self.species = list(species)
+        self.records = _nested(initial_records)
+        for sp in {e for t in self.records for e in t}:
+            if sp not in self.species:
+                raise ValueError(f"Tersoff record element '{sp}' is not among the species {self.species}")
+        fixed = set(self._DEFAULT_FIX) | set(fix_params or ())
+        keys = list(fit_keys) if fit_keys else list(self._DEFAULT_FIT)
+        self.fit_keys = [k for k in keys if k not in fixed]
+        unknown = [k for k in self.fit_keys if k not in self._BOUNDS]
+        if unknown:
+            raise ValueError(f"MultiSpeciesTersoffParameterSet: unknown fit key(s) {unknown}")
+        self._check_pairs()
+        self.variables = []
+        seen_pairs, seen_centres = set(), set()
+        for (i, j, k) in self.records:
+            if j == k:
+                pair = frozenset((i, j))
+                if pair not in seen_pairs:
+                    seen_pairs.add(pair)
+                    tw = [(i, j, j)] + ([(j, i, i)] if i != j else [])
+                    for key in self.fit_keys:
+                        if key in self._PAIR_KEYS:
+                            self.variables.append((f"{i}-{j}:{key}", key, [(t, key) for t in tw]))
+                for key in self.fit_keys:
+                    if key in self._BOND_KEYS:
+                        self.variables.append((f"{i};{j}:{key}", key, [((i, j, j), key)]))
+            for key in self.fit_keys:
+                if key not in self._ANGLE_KEYS:
+                    continue
+                if tie == "centre":
+                    if (i, key) in seen_centres:
+                        continue
+                    seen_centres.add((i, key))
+                    tg = [(t, key) for t in self.records if t[0] == i]
+                    self.variables.append((f"{i};*:{key}", key, tg))
+                else:
+                    self.variables.append((f"{i};{j},{k}:{key}", key, [((i, j, k), key)]))
+        init = []
+        for name, key, targets in self.variables:
+            try:
+                init.append(float(np.mean([self.records[t][kk] for t, kk in targets])))
+            except KeyError:
+                raise ValueError(f"MultiSpeciesTersoffParameterSet: a record of {name} has no '{key}'") from None
+        self._setup_vector(init, "MultiSpeciesTersoffParameterSet")
+
+    def _check_pairs(self):
+        for (i, j, k), rec in self.records.items():
+            if j != k or i == j:
+                continue
+            twin = self.records.get((j, i, i))
+            if twin is None:
+                raise ValueError(f"Tersoff record ({i},{j},{j}) has no partner ({j},{i},{i}); the {i}-{j} pair "
+                                 "is read from whichever belongs to the lower-indexed atom, so both are required.")
+            for key in self._PAIR_KEYS:
+                a, b = rec.get(key), twin.get(key)
+                if (a is None) != (b is None) or (a is not None and not np.isclose(a, b, rtol=1e-12, atol=0.0)):
+                    raise ValueError(f"Tersoff records ({i},{j},{j}) and ({j},{i},{i}) disagree on '{key}' "
+                                     f"({a} vs {b}); the engine would read one or the other depending on atom "
+                                     "order.")
+
+    def _decode(self, x):
+        out = {t: dict(p) for t, p in self.records.items()}
+        for xi, (_, key, targets) in zip(x, self.variables):
+            v = self._value(key, xi)
+            for triple, kk in targets:
+                out[triple][kk] = v
+        return {"tersoff": out}
+
+    def decode(self, x):
+        """{'tersoff': {(i, j, k): full parameter dict}} (floats)."""
+        return self._decode(np.asarray(x, float))
+
+    def decode_torch(self, x):
+        """The same with 0-d tensor entries carrying x's autograd history."""
+        return self._decode(list(x.unbind(0)))
+
+
+def _mix_1989(el, chi, species, omega):
+    """Tersoff (1989) mixing rules (PRB 39, 5566, eqs. 1a-1e) on values that
+    may be 0-d tensors: the expansion of tersoff1989_to_triplets written
+    with torch operations so it can be differentiated."""
+    def sq(v):
+        return torch.sqrt(v) if torch.is_tensor(v) else math.sqrt(v)
+
+    def pair(table, a, b, default):
+        for k in (f"{a}-{b}", f"{b}-{a}"):
+            if k in table:
+                return table[k]
+        return default
+
+    out = {}
+    for i in species:
+        pi = el[i]
+        for j in species:
+            pj = el[j]
+            x = 1.0 if i == j else pair(chi, i, j, None)
+            r_ij = sq(pi["R"] * pj["R"])
+            s_ij = sq(pi["S"] * pj["S"])
+            for k in species:
+                rec = {"c": pi["c"], "d": pi["d"], "h": pi["h"], "lambda3": 0.0, "m": 3.0,
+                       "gamma": float(pair(omega, i, k, 1.0))}
+                if j == k:
+                    rec.update(A=sq(pi["A"] * pj["A"]), B=x * sq(pi["B"] * pj["B"]),
+                               lambda1=0.5 * (pi["lambda"] + pj["lambda"]), lambda2=0.5 * (pi["mu"] + pj["mu"]),
+                               R=0.5 * (r_ij + s_ij), D=0.5 * (s_ij - r_ij), beta=pi["beta"], n=pi["n"])
+                out[(i, j, k)] = rec
+    return out
+
+
+class Tersoff1989ParameterSet(_Variables):
+    """Per-element Tersoff (1989) parameters and one chi per pair of
+    distinct elements (reference fitting/parameter_sets.py:1206-1296).
+    Default variables: A, B, lambda, mu, c, d, h of every element and every
+    chi; R, S, beta, n fixed."""
+
+    _DEFAULT_FIX = ("R", "S", "beta", "n")
+    _DEFAULT_FIT = ("A", "B", "lambda", "mu", "c", "d", "h", "chi")
+    _LOG_KEYS = frozenset({"A", "B", "lambda", "mu", "beta", "n", "c", "d", "chi", "R", "S"})
+    _BOUNDS = {"A": (1.0, 1e5), "B": (0.1, 1e4), "lambda": (0.5, 10.0), "mu": (0.1, 8.0),
+               "beta": (1e-10, 10.0), "n": (0.05, 10.0), "c": (1e-3, 1e7), "d": (1e-2, 1e4),
+               "h": (-1.0, 1.0), "chi": (0.3, 3.0), "R": (1.0, 5.0), "S": (1.0, 5.5)}
+
+    def __init__(self, elements, chi, species, fix_params=None, fit_keys=None, omega=None):
+        self.species = list(species)
+        self.elements = {s: {k: float(v) for k, v in elements[s].items()} for s in self.species if s in elements}
+        self.omega = dict(omega or {})
+        self.chi = {}
+        for a_i, a in enumerate(self.species):
+            for b in self.species[a_i + 1:]:
+                v = chi.get(f"{a}-{b}", chi.get(f"{b}-{a}"))
+                if v is None:
+                    raise ValueError(f"Tersoff1989ParameterSet: chi for {a}-{b} is not given")
+                self.chi[f"{a}-{b}"] = float(v)
+        tersoff1989_to_triplets(self.elements, self.chi, self.species, self.omega)
+        fixed = set(self._DEFAULT_FIX) | set(fix_params or ())
+        keys = list(fit_keys) if fit_keys else list(self._DEFAULT_FIT)
+        self.fit_keys = [k for k in keys if k not in fixed]
+        unknown = [k for k in self.fit_keys if k not in TERSOFF1989_ELEMENT_KEYS and k != "chi"]
+        if unknown:
+            raise ValueError(f"Tersoff1989ParameterSet: unknown fit key(s) {unknown}")
+        self.variables, init = [], []
+        for s in self.species:
+            for key in self.fit_keys:
+                if key != "chi":
+                    self.variables.append((f"{s}:{key}", key, (s, key)))
+                    init.append(self.elements[s][key])
+        if "chi" in self.fit_keys:
+            for pair, v in self.chi.items():
+                self.variables.append((f"chi:{pair}", "chi", pair))
+                init.append(v)
+        self._setup_vector(init, "Tersoff1989ParameterSet")
+
+    def _decode(self, x, torch_mode):
+        el = {s: dict(p) for s, p in self.elements.items()}
+        chi = dict(self.chi)
+        for xi, (_, key, target) in zip(x, self.variables):
+            v = self._value(key, xi)
+            if key == "chi":
+                chi[target] = v
+            else:
+                el[target[0]][key] = v
+        table = _mix_1989(el, chi, self.species, self.omega) if torch_mode else \
+            tersoff1989_to_triplets(el, chi, self.species, self.omega)
+        return {"tersoff": table, "tersoff1989": {"elements": el, "chi": chi, "omega": dict(self.omega)}}
+
+    def decode(self, x):
+        """{'tersoff': (i, j, k) table, 'tersoff1989': {elements, chi, omega}}."""
+        return self._decode(np.asarray(x, float), False)
+
+    def decode_torch(self, x):
+        return self._decode(list(x.unbind(0)), True)
+
+
+# ---- evaluation with explicit tables and its adjoint ----------------------------
+
+class _TableEval:
+    """A batch, its device list and workspaces, evaluated with given tables."""
+
+    def __init__(self, batch, skin):
+        self.batch = batch
+        self.skin = float(skin)
+        self.dlist = None
+        self.r_list = 0.0
+        self._ws = None
+        self._adj_ws = None
+
+    def _ensure_list(self, r_cut):
+        if self.dlist is None or r_cut + 1e-12 > self.r_list - self.skin:
+            self.r_list = r_cut + self.skin
+            self.dlist = DeviceNeighbourList(self.r_list).build(self.batch)
+        return self.dlist
+
+    def _tables(self, tb, tri):
+        ns = int(round(tb.shape[0] ** 0.5))
+        r_cut = table_cutoff(tb)
+        dl = self._ensure_list(r_cut)
+        return dl, _lib.MbfTersoffTables(ns, _lib.ptr(tb), _lib.ptr(tri), r_cut), ns
+
+    def evaluate(self, tb, tri):
+        dl, tabs, _ = self._tables(tb, tri)
+        b = self.batch
+        dev = b.device
+        L = _lib.lib()
+        need = int(L.mbf_eval_workspace_bytes(b.n_atoms, dl.n_slots, b.n_chunks))
+        if self._ws is None or self._ws.numel() < need:
+            self._ws = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
+        E = torch.empty(b.n_struct, dtype=torch.float64, device=dev)
+        F = torch.empty((b.n_atoms, 3), dtype=torch.float64, device=dev)
+        W = torch.empty((b.n_struct, 9), dtype=torch.float64, device=dev)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(L.mbf_tersoff_eval(b.mbf_system(), dl.mbf_nlist(), tabs, b.reduce_plan(), _lib.MBF_FP64, 8,
+                                      _lib.ptr(self._ws), self._ws.numel(), _lib.ptr(F), _lib.ptr(E), _lib.ptr(W),
+                                      st), "mbf_tersoff_eval")
+        return E, F, W
+
+    def adjoint(self, tb, tri, gE, gF, gW):
+        dl, tabs, ns = self._tables(tb, tri)
+        b = self.batch
+        dev = b.device
+        L = _lib.lib()
+        need = int(L.mbf_tersoff_adjoint_workspace_bytes(dl.n_slots, ns))
+        if self._adj_ws is None or self._adj_ws.numel() < need:
+            self._adj_ws = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
+        d_tb = torch.empty_like(tb)
+        d_tri = torch.empty_like(tri)
+        g = [None if t is None else t.to(torch.float64).contiguous() for t in (gE, gF, gW)]
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(L.mbf_tersoff_adjoint(b.mbf_system(), dl.mbf_nlist(), tabs, _lib.ptr(g[0]), _lib.ptr(g[1]),
+                                         _lib.ptr(g[2]), _lib.ptr(self._adj_ws), self._adj_ws.numel(),
+                                         _lib.ptr(d_tb), _lib.ptr(d_tri), st), "mbf_tersoff_adjoint")
+        return d_tb, d_tri
+
+
+class TersoffEFS(torch.autograd.Function):
+    """(energy (S,), forces (N, 3), virial (S, 9)) of a batch as a function
+    of the Tersoff tables; backward is one mbf_tersoff_adjoint call."""
+
+    @staticmethod
+    def forward(ctx, tb, tri, ev):
+        tb = tb.detach().contiguous()
+        tri = tri.detach().contiguous()
+        E, F, W = ev.evaluate(tb, tri)
+        ctx.ev = ev
+        ctx.save_for_backward(tb, tri)
+        return E, F, W
+
+    @staticmethod
+    def backward(ctx, gE, gF, gW):
+        tb, tri = ctx.saved_tensors
+        d_tb, d_tri = ctx.ev.adjoint(tb, tri, gE, gF, gW)
+        return d_tb, d_tri, None
+
+
+def shard_structures(n_atoms, world):
+    """Greedy atom-count balance: largest structures first, each to the
+    rank with the fewest atoms so far (lowest rank on ties); returns one
+    sorted index list per rank."""
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for s in sorted(range(len(n_atoms)), key=lambda q: (-int(n_atoms[q]), q)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(s)
+        load[r] += int(n_atoms[s])
+    return [sorted(p) for p in parts]
+
+
+def allreduce_sum(vec, world=1, group=None):
+    """Sum a tensor over the ranks of a process group in place (the
+    reference's _mpi_allreduce_sum_scalar, fitting/loss.py:246-260); a
+    no-op for one rank.  Every rank calls it in the same order."""
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(vec, op=dist.ReduceOp.SUM, group=group)
+    return vec
+
+
+def _huber_of_squared(sq, delta):
+    """fitting/loss.py:29-48: sq if sqrt(sq) <= delta else 2 delta sqrt(sq) - delta^2."""
+    r = torch.sqrt(torch.clamp(sq, min=1e-300))
+    return torch.where(r <= delta, sq, 2.0 * delta * r - delta * delta)
+
+
+class TersoffFit:
+    """The reference's fit loss (fitting/loss.py:51-260) over a training set
+    on the GPU, and its gradient in x.
+
+    structures : dicts with lattice, positions, atom_types, natoms,
+                 ref_energy (eV/atom), optional ref_forces (N, 3),
+                 ref_stress (3, 3), volume, scale (c_s, squared) and weight
+                 (w_trust, linear) -- the reference's keys.
+    weights    : energy, forces, stress, r0, eps0 (defaults 1, 1, 0.1, 1, 1)
+                 and, for loss_type='huber', huber_delta_energy/forces/stress.
+    rank, world, group : with world > 1 this rank takes its share of the
+                 structures (shard_structures) and the loss and gradient are
+                 summed over the process group (torch.distributed), the
+                 reference's MPI split (fitting/loss.py:190-248).
+    """
+
+    def __init__(self, param_set, structures, weights=None, loss_type="squared", device=None, skin=0.3,
+                 rank=0, world=1, group=None):
+        if loss_type not in ("squared", "huber"):
+            raise ValueError(f"unknown loss_type '{loss_type}'. Choose 'squared' or 'huber'.")
+        weights = dict(weights or {})
+        if loss_type == "huber":
+            for key in ("huber_delta_energy", "huber_delta_forces", "huber_delta_stress"):
+                if key not in weights:
+                    raise ValueError(f"loss_type='huber' requires weights['{key}'] (eV)")
+        self.ps = param_set
+        self.loss_type = loss_type
+        self.w = weights
+        self.rank, self.world, self.group = int(rank), int(world), group
+        self.device = torch.device(device) if device is not None else default_device()
+        self.mine = shard_structures([s["natoms"] for s in structures], self.world)[self.rank]
+        self._setup([structures[q] for q in self.mine], skin)
+
+    def _setup(self, structs, skin):
+        dev = self.device
+        sp = self.ps.species
+        lats, poss, ids, reps, n_orig, vols = [], [], [], [], [], []
+        r_guess = table_cutoff(tables_from_records(self.ps.decode(self.ps.x0)["tersoff"], sp, "cpu")[0])
+        for s in structs:
+            t = species_ids(s["atom_types"], sp)
+            L2, P2, T2, k = replicate_thin(s["lattice"], s["positions"], t, r_guess + skin)
+            lats.append(L2)
+            poss.append(P2)
+            ids.append(T2)
+            reps.append(float(np.prod(k)))
+            n_orig.append(len(s["positions"]))
+            vols.append(float(s.get("volume", abs(np.linalg.det(np.asarray(s["lattice"], float))))))
+        self.n_struct = len(structs)
+        self.ev = _TableEval(Batch(lats, poss, ids, device=dev), skin) if structs else None
+        if not structs:
+            return
+        off = self.ev.batch.offsets
+        idx = np.concatenate([np.arange(off[q], off[q] + n) for q, n in enumerate(n_orig)])
+        self._orig = torch.as_tensor(idx, device=dev)
+        f64 = dict(dtype=torch.float64, device=dev)
+        self._n = torch.tensor(n_orig, **f64)
+        self._inv_k = torch.tensor([1.0 / k for k in reps], **f64)
+        self._vol = torch.tensor(vols, **f64)
+        self._vsup = torch.as_tensor(self.ev.batch.volumes, **f64)
+        self._atom_struct = torch.as_tensor(np.repeat(np.arange(len(structs)), n_orig), device=dev)
+        self._eref = torch.tensor([float(s["ref_energy"]) for s in structs], **f64)
+        fref, fmask, sref, smask = [], [], [], []
+        for s, n in zip(structs, n_orig):
+            f = s.get("ref_forces")
+            fref.append(np.zeros((n, 3)) if f is None else np.asarray(f, float).reshape(n, 3))
+            fmask.append(0.0 if f is None else 1.0)
+            st = s.get("ref_stress")
+            sref.append(np.zeros(9) if st is None else np.asarray(st, float).reshape(9))
+            smask.append(0.0 if st is None else 1.0)
+        self._fref = torch.as_tensor(np.concatenate(fref), **f64)
+        self._fmask = torch.tensor(fmask, **f64)
+        self._sref = torch.as_tensor(np.stack(sref), **f64)
+        self._smask = torch.tensor(smask, **f64)
+        self._cw = torch.tensor([float(s.get("weight", 1.0)) * float(s.get("scale", 1.0)) ** 2 for s in structs],
+                                **f64)
+
+    def _local_loss(self, x_t):
+        """This rank's loss as a differentiable torch scalar."""
+        if self.ev is None:
+            return x_t.sum() * 0.0
+        params = self.ps.decode_torch(x_t)
+        tb, tri = tables_from_records(params["tersoff"], self.ps.species, self.device)
+        E, F, W = TersoffEFS.apply(tb, tri, self.ev)
+        w = self.w
+        w_E, w_F, w_S = float(w.get("energy", 1.0)), float(w.get("forces", 1.0)), float(w.get("stress", 0.1))
+        r0, eps0 = float(w.get("r0", 1.0)), float(w.get("eps0", 1.0))
+        e = E * self._inv_k
+        e_sq = (e - self._n * self._eref) ** 2
+        df = F.index_select(0, self._orig) - self._fref
+        fs = torch.zeros(self.n_struct, dtype=torch.float64, device=self.device)
+        fs = fs.index_add(0, self._atom_struct, (df * df).sum(1))
+        f_sq = (r0 ** 2) * fs / (3.0 * self._n)
+        sig = W / self._vsup[:, None]
+        ds = sig - self._sref
+        s_sq = (self._vol * eps0) ** 2 * (ds * ds).mean(1)
+        if self.loss_type == "huber":
+            e_sq = _huber_of_squared(e_sq, float(w["huber_delta_energy"]))
+            f_sq = _huber_of_squared(f_sq, float(w["huber_delta_forces"]))
+            s_sq = _huber_of_squared(s_sq, float(w["huber_delta_stress"]))
+        per = w_E * e_sq + w_F * f_sq * self._fmask + w_S * s_sq * self._smask
+        return (self._cw * per).sum()
+
+    def _reduce(self, vec):
+        return allreduce_sum(vec, self.world, self.group)
+
+    def loss_and_grad(self, x):
+        """(loss, dloss/dx) at x; every rank of a group must call it."""
+        x_t = torch.tensor(np.asarray(x, float), dtype=torch.float64, device=self.device, requires_grad=True)
+        failed = 0.0
+        try:
+            loss = self._local_loss(x_t)
+            (g,) = torch.autograd.grad(loss, x_t, allow_unused=True)
+            g = torch.zeros_like(x_t) if g is None else g
+            vec = torch.cat([loss.detach().reshape(1), g.detach(), torch.zeros(1, dtype=torch.float64,
+                                                                               device=self.device)])
+        except (ValueError, RuntimeError, _lib.MbfError):
+            failed = 1.0
+            vec = torch.zeros(len(x) + 2, dtype=torch.float64, device=self.device)
+        vec[-1] = failed
+        vec = self._reduce(vec).cpu().numpy()
+        if vec[-1] > 0.0:
+            return 1e30, np.zeros(len(x))
+        return float(vec[0]), vec[1:-1]
+
+    def loss(self, x):
+        """The loss at x (1e30 if the parameters cannot be evaluated)."""
+        x_t = torch.tensor(np.asarray(x, float), dtype=torch.float64, device=self.device)
+        failed = 0.0
+        try:
+            with torch.no_grad():
+                val = self._local_loss(x_t).reshape(1)
+        except (ValueError, RuntimeError, _lib.MbfError):
+            failed, val = 1.0, torch.zeros(1, dtype=torch.float64, device=self.device)
+        vec = self._reduce(torch.cat([val, torch.tensor([failed], dtype=torch.float64, device=self.device)]))
+        vec = vec.cpu().numpy()
+        return 1e30 if vec[1] > 0.0 else float(vec[0])
+
+
+_FITS = {}
+
+
+def generic_loss_function(x, param_set, structures, weights, r_cut=None, ewald_alpha=None,
+                          coulomb_method="ewald", loss_type="squared"):
+    """fitting/loss.py:51 on the GPU for Tersoff parameter sets: the same
+    value (eV^2; 1e30 when the parameters cannot be evaluated).  r_cut,
+    ewald_alpha and coulomb_method concern charges, which Tersoff sets do
+    not carry; the list radius follows the decoded records."""
+    if loss_type not in ("squared", "huber"):
+        raise ValueError(f"generic_loss_function: unknown loss_type '{loss_type}'. Choose 'squared' or 'huber'.")
+    key = (id(param_set), id(structures), loss_type, tuple(sorted((k, float(v)) for k, v in weights.items())))
+    fit = _FITS.get(key)
+    if fit is None:
+        fit = _FITS[key] = TersoffFit(param_set, structures, weights, loss_type=loss_type)
+    return fit.loss(x)

@@ -234,6 +234,25 @@ int mbf_tersoff_eval(const mbf_system *sys, const mbf_nlist *nl,
                      int precision, int lanes_per_atom, void *workspace, size_t workspace_bytes,
                      double *forces, double *energy, double *virial, void *stream);
 
+/* Tersoff adjoint for fitting: the vector-Jacobian product of (energy,
+ * forces, virial) with respect to the tables, in float64.  Given upstream
+ * gradients g_energy (n_struct), g_forces (n_atoms, 3) and g_virial
+ * (n_struct, 9) -- any may be NULL for zero -- writes
+ *   d_tb[e]  = sum_s gE_s dE_s/dtb[e] + sum_a gF_a . dF_a/dtb[e]
+ *              + sum_s gW_s : dW_s/dtb[e]          (ns*ns, 10)
+ * and d_tri likewise (ns^3, 8), for every table entry (the valid flag, m
+ * and unused columns get 0).  Replaces the forward-difference Jacobian of
+ * the reference's fit (fitting/driver.py:802-816 over
+ * fitting/loss.py:263-319): one call instead of one loss evaluation per
+ * parameter.  Zeta is recomputed per bond, nothing per triplet is stored;
+ * the result is deterministic.  The workspace needs
+ * mbf_tersoff_adjoint_workspace_bytes(n_slots, ns).                      */
+size_t mbf_tersoff_adjoint_workspace_bytes(long long n_slots, int ns);
+int mbf_tersoff_adjoint(const mbf_system *sys, const mbf_nlist *nl,
+                        const mbf_tersoff_tables *tab, const double *g_energy,
+                        const double *g_forces, const double *g_virial, void *workspace,
+                        size_t workspace_bytes, double *d_tb, double *d_tri, void *stream);
+
 /* ---- Stillinger-Weber -------------------------------------------------
  * Replaces StillingerWeberPotential.compute (engine/stillinger_weber.py:
  * 900-1451), single- and multi-species.  tb (ns*ns, 8) rows [valid, eps,

@@ -752,3 +752,29 @@ def nve(force, lattice, positions, masses, velocities, dt, n_steps):
         e_kin = 0.5 * float(np.sum(m[:, None] * v ** 2)) / EV_ANG_TO_AMU_ANG_FS2
         out.append((r.copy(), v.copy(), e, e_kin))
     return out
+
+
+# ---- fitting -------------------------------------------------------------------
+def fit_loss(records, species, structures, weights, pairs=None):
+    """fitting/loss.py:184-260 (squared loss) with the multi-species Tersoff
+    force call: sum_s w_trust c_s^2 [w_E (E - N e_ref)^2 + w_F r0^2
+    mean|dF|^2 + w_S (V eps0)^2 mean|dsigma|^2].  pairs: optional list of
+    prebuilt (i, j) per structure."""
+    w_E = weights.get("energy", 1.0)
+    w_F = weights.get("forces", 1.0)
+    w_S = weights.get("stress", 0.1)
+    r0 = float(weights.get("r0", 1.0))
+    eps0 = float(weights.get("eps0", 1.0))
+    total = 0.0
+    for q, s in enumerate(structures):
+        N = s["natoms"]
+        vol = float(s.get("volume", abs(np.linalg.det(s["lattice"]))))
+        e, f, st = tersoff_multi(records, species, s["lattice"], s["positions"], s["atom_types"],
+                                 None if pairs is None else pairs[q])
+        tot = w_E * (N * (e / N - s["ref_energy"])) ** 2
+        if s.get("ref_forces") is not None:
+            tot += w_F * r0 ** 2 * float(np.mean((f - s["ref_forces"]) ** 2))
+        if s.get("ref_stress") is not None:
+            tot += w_S * (vol * eps0) ** 2 * float(np.mean((st - s["ref_stress"]) ** 2))
+        total += float(s.get("weight", 1.0)) * float(s.get("scale", 1.0)) ** 2 * tot
+    return total

@@ -208,6 +208,65 @@ def main():
          temperature=300.0, dt=1.0, n_steps=20, velocities0=v0, positions_final=sim.positions,
          velocities_final=sim.velocities, thermo=thermo)
 
+    # ---- fitting: SiC Tersoff-1989, the reference's loss and its gradient --
+    from akitsushima.engine.tersoff import tersoff1989_to_triplets as ref_mix
+    from akitsushima.fitting.loss import generic_loss_function, generic_residuals
+    from akitsushima.fitting.parameter_sets import (MultiSpeciesTersoffParameterSet,
+                                                    Tersoff1989ParameterSet)
+    species = ["Si", "C"]
+    el0 = {s: dict(el[s]) for s in species}
+    chi0 = {"Si-C": TERSOFF_1989["chi"]["C-Si"]}
+    rng = np.random.default_rng(31)
+    el_t = {s: {k: (v * rng.uniform(0.95, 1.05) if k in ("A", "B", "lambda", "mu", "c", "d", "h") else v)
+                for k, v in el0[s].items()} for s in species}
+    chi_t = {"Si-C": chi0["Si-C"] * rng.uniform(0.95, 1.05)}
+    target = ak.force_fn_from_config({"type": "Tersoff", "species": species,
+                                      "params": ref_mix(el_t, chi_t, species)})
+    structs, geo = [], {}
+    for q, (n, seed) in enumerate(((2, 41), (2, 42), (3, 43), (3, 44))):
+        L, P, T = cubic(DIAMOND, 4.36, n, zb, rattle=0.1, seed=seed)
+        L, P = strained(L, P, 0.02, seed + 100)
+        nl = NeighbourList(r_cut=float(target.r_cut), skin_width=0.3, backend="cll")
+        nl.build(L, P)
+        e, f, s = target(L, P, T, nl)
+        structs.append({"lattice": L, "positions": P, "atom_types": list(T), "natoms": len(P),
+                        "ref_energy": float(e) / len(P), "ref_forces": np.asarray(f),
+                        "ref_stress": np.asarray(s)})
+        geo.update({f"lattice{q}": L, f"positions{q}": P, f"atom_types{q}": np.array(T),
+                    f"ref_energy{q}": float(e) / len(P), f"ref_forces{q}": np.asarray(f),
+                    f"ref_stress{q}": np.asarray(s)})
+    weights = {"energy": 1.0, "forces": 1.0, "stress": 0.1}
+    sets = {"t1989": Tersoff1989ParameterSet(el0, chi0, species),
+            "multi": MultiSpeciesTersoffParameterSet(ref_mix(el0, chi0, species), species)}
+    out = dict(geo, n_structures=len(structs))
+    for tag, ps in sets.items():
+        x0 = ps.x0
+        lo_b = np.array([b[0] for b in ps.bounds])
+        hi_b = np.array([b[1] for b in ps.bounds])
+        r0 = generic_residuals(x0, ps, structs, weights, 3.5, None)
+        J = np.empty((len(r0), len(x0)))
+        for q in range(len(x0)):   # the fit's jacobian_fn (fitting/driver.py:802-816)
+            h = 1e-7 * max(1.0, abs(x0[q]))
+            if x0[q] + h > hi_b[q]:
+                h = -h
+            xp = np.array(x0, float)
+            xp[q] += h
+            J[:, q] = (generic_residuals(xp, ps, structs, weights, 3.5, None) - r0) / h
+        x_test = x0 + np.random.default_rng(32).uniform(-0.02, 0.02, len(x0))
+        x_test = np.clip(x_test, lo_b, hi_b)
+        tab = ps.decode(x_test)["tersoff"]
+        keys = sorted(tab)
+        out.update({f"{tag}_x0": x0, f"{tag}_names": np.array(ps.variable_names),
+                    f"{tag}_lo": lo_b, f"{tag}_hi": hi_b,
+                    f"{tag}_loss0": generic_loss_function(x0, ps, structs, weights, 3.5, None),
+                    f"{tag}_grad_fd": 2.0 * J.T @ r0, f"{tag}_x_test": x_test,
+                    f"{tag}_loss_test": generic_loss_function(x_test, ps, structs, weights, 3.5, None),
+                    f"{tag}_decoded_keys": np.array(["|".join(k) for k in keys]),
+                    f"{tag}_decoded": np.array([[float(tab[k].get(n, np.nan)) for n in
+                                                 ("A", "B", "lambda1", "lambda2", "R", "D", "beta", "n",
+                                                  "c", "d", "h", "lambda3", "m", "gamma")] for k in keys])})
+    save("fit_sic_t1989", **out)
+
 
 if __name__ == "__main__":
     main()
