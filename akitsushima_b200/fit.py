@@ -330,24 +330,25 @@ class _TableEval:
         self.batch = batch
         self.skin = float(skin)
         self.dlist = None
-        self.r_list = 0.0
+        self.list_cut = -1.0   # the largest r_cut the current list serves
         self._ws = None
         self._adj_ws = None
 
     def _ensure_list(self, r_cut):
-        if self.dlist is None or r_cut + 1e-12 > self.r_list - self.skin:
-            self.r_list = r_cut + self.skin
-            self.dlist = DeviceNeighbourList(self.r_list).build(self.batch)
+        if self.dlist is None or r_cut > self.list_cut:
+            self.dlist = DeviceNeighbourList(r_cut + self.skin).build(self.batch)
+            self.list_cut = r_cut
         return self.dlist
 
-    def _tables(self, tb, tri):
+    def _tables(self, tb, tri, r_cut=None):
         ns = int(round(tb.shape[0] ** 0.5))
-        r_cut = table_cutoff(tb)
+        if r_cut is None:
+            r_cut = table_cutoff(tb)
         dl = self._ensure_list(r_cut)
         return dl, _lib.MbfTersoffTables(ns, _lib.ptr(tb), _lib.ptr(tri), r_cut), ns
 
-    def evaluate(self, tb, tri):
-        dl, tabs, _ = self._tables(tb, tri)
+    def evaluate(self, tb, tri, r_cut=None):
+        dl, tabs, _ = self._tables(tb, tri, r_cut)
         b = self.batch
         dev = b.device
         L = _lib.lib()
@@ -363,8 +364,8 @@ class _TableEval:
                                       st), "mbf_tersoff_eval")
         return E, F, W
 
-    def adjoint(self, tb, tri, gE, gF, gW):
-        dl, tabs, ns = self._tables(tb, tri)
+    def adjoint(self, tb, tri, gE, gF, gW, r_cut=None):
+        dl, tabs, ns = self._tables(tb, tri, r_cut)
         b = self.batch
         dev = b.device
         L = _lib.lib()
@@ -383,22 +384,29 @@ class _TableEval:
 
 class TersoffEFS(torch.autograd.Function):
     """(energy (S,), forces (N, 3), virial (S, 9)) of a batch as a function
-    of the Tersoff tables; backward is one mbf_tersoff_adjoint call."""
+    of the Tersoff tables; backward is one mbf_tersoff_adjoint call.  The
+    tables may live on the host (a few dozen numbers, decoded there by
+    cheap CPU tensor operations): they are copied to the batch's device for
+    the evaluation and their gradients come back to where they live."""
 
     @staticmethod
     def forward(ctx, tb, tri, ev):
-        tb = tb.detach().contiguous()
-        tri = tri.detach().contiguous()
-        E, F, W = ev.evaluate(tb, tri)
+        dev = ev.batch.device
+        r_cut = table_cutoff(tb)
+        tb_d = tb.detach().to(dev, non_blocking=True).contiguous()
+        tri_d = tri.detach().to(dev, non_blocking=True).contiguous()
+        E, F, W = ev.evaluate(tb_d, tri_d, r_cut)
         ctx.ev = ev
-        ctx.save_for_backward(tb, tri)
+        ctx.r_cut = r_cut
+        ctx.home = tb.device
+        ctx.save_for_backward(tb_d, tri_d)
         return E, F, W
 
     @staticmethod
     def backward(ctx, gE, gF, gW):
         tb, tri = ctx.saved_tensors
-        d_tb, d_tri = ctx.ev.adjoint(tb, tri, gE, gF, gW)
-        return d_tb, d_tri, None
+        d_tb, d_tri = ctx.ev.adjoint(tb, tri, gE, gF, gW, ctx.r_cut)
+        return d_tb.to(ctx.home), d_tri.to(ctx.home), None
 
 
 def shard_structures(n_atoms, world):
@@ -509,9 +517,9 @@ class TersoffFit:
     def _local_loss(self, x_t):
         """This rank's loss as a differentiable torch scalar."""
         if self.ev is None:
-            return x_t.sum() * 0.0
+            return (x_t.sum() * 0.0).to(self.device)
         params = self.ps.decode_torch(x_t)
-        tb, tri = tables_from_records(params["tersoff"], self.ps.species, self.device)
+        tb, tri = tables_from_records(params["tersoff"], self.ps.species, x_t.device)
         E, F, W = TersoffEFS.apply(tb, tri, self.ev)
         w = self.w
         w_E, w_F, w_S = float(w.get("energy", 1.0)), float(w.get("forces", 1.0)), float(w.get("stress", 0.1))
@@ -537,14 +545,14 @@ class TersoffFit:
 
     def loss_and_grad(self, x):
         """(loss, dloss/dx) at x; every rank of a group must call it."""
-        x_t = torch.tensor(np.asarray(x, float), dtype=torch.float64, device=self.device, requires_grad=True)
+        x_t = torch.tensor(np.asarray(x, float), dtype=torch.float64, requires_grad=True)
         failed = 0.0
         try:
             loss = self._local_loss(x_t)
             (g,) = torch.autograd.grad(loss, x_t, allow_unused=True)
             g = torch.zeros_like(x_t) if g is None else g
-            vec = torch.cat([loss.detach().reshape(1), g.detach(), torch.zeros(1, dtype=torch.float64,
-                                                                               device=self.device)])
+            vec = torch.cat([loss.detach().reshape(1), g.detach().to(self.device),
+                             torch.zeros(1, dtype=torch.float64, device=self.device)])
         except (ValueError, RuntimeError, _lib.MbfError):
             failed = 1.0
             vec = torch.zeros(len(x) + 2, dtype=torch.float64, device=self.device)
@@ -556,7 +564,7 @@ class TersoffFit:
 
     def loss(self, x):
         """The loss at x (1e30 if the parameters cannot be evaluated)."""
-        x_t = torch.tensor(np.asarray(x, float), dtype=torch.float64, device=self.device)
+        x_t = torch.tensor(np.asarray(x, float), dtype=torch.float64)
         failed = 0.0
         try:
             with torch.no_grad():

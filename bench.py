@@ -540,6 +540,212 @@ def run_md(args, world, rank, local):
     return 0
 
 
+SIC_ZB = np.array([[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0],
+                   [0.25, 0.25, 0.25], [0.25, 0.75, 0.75], [0.75, 0.25, 0.75],
+                   [0.75, 0.75, 0.25]], float)
+
+
+def make_sic_set(n=256, a=4.36, strain=0.02, sigma=0.1, seed=0):
+    """Zincblende SiC, 2^3 or 3^3 conventional cells (64 or 216 atoms),
+    symmetric strain entries uniform +-2 %, Gaussian displacements."""
+    rng = np.random.default_rng(seed)
+    types8 = ["Si"] * 4 + ["C"] * 4
+    out = []
+    for _ in range(n):
+        m = int(rng.integers(2, 4))
+        g = np.arange(m)
+        cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+        frac = (SIC_ZB[None] + cells[:, None]).reshape(-1, 3)
+        lat = np.eye(3) * a * m
+        pos = frac * a
+        e = rng.uniform(-strain, strain, (3, 3))
+        M = np.eye(3) + 0.5 * (e + e.T)
+        lat, pos = lat @ M, pos @ M
+        pos = pos + rng.normal(0.0, sigma, pos.shape)
+        out.append((lat, pos, types8 * len(cells)))
+    return out
+
+
+def _fit_setup():
+    """The Tersoff-1989 Si-C parameter set (fitting/registry.py:724-730) and
+    its target parameters theta * U(0.95, 1.05) (seeded), as x vectors."""
+    from akitsushima_b200 import fit
+    from akitsushima_b200.published_parameters import TERSOFF_1989
+    species = ["Si", "C"]
+    el = {s: dict(TERSOFF_1989["elements"][s]) for s in species}
+    ps = fit.Tersoff1989ParameterSet(el, {"Si-C": TERSOFF_1989["chi"]["C-Si"]}, species)
+    x0 = ps.x0
+    u = np.random.default_rng(7).uniform(0.95, 1.05, len(x0))
+    xt = np.array([np.log(np.exp(x) * f) if key in ps._LOG_KEYS else x * f
+                   for x, f, (_, key, _) in zip(x0, u, ps.variables)])
+    return ps, x0, xt
+
+
+def _fit_structs(raw, efs):
+    out = []
+    for (lat, pos, types), (e, f, s) in zip(raw, efs):
+        out.append({"lattice": lat, "positions": pos, "atom_types": types, "natoms": len(pos),
+                    "ref_energy": e / len(pos), "ref_forces": f, "ref_stress": s})
+    return out
+
+
+def time_reference_fit(raw, ps, x0, xt, n_sample):
+    """The reference's gradient: forward differences of the loss, one loss
+    evaluation per variable plus one (fitting/driver.py:802-816), each a
+    loop of force calls (fitting/loss.py:184-242) -- the oracle port under
+    OpenMP with every host thread, on the first n_sample structures;
+    seconds per gradient of the whole set, scaled by atoms."""
+    import oracle
+    threads = cpu_count()
+    oracle.set_threads(threads)
+    sample = raw[:n_sample]
+    rec_t = ps.decode(xt)["tersoff"]
+    efs = [oracle.tersoff_multi(rec_t, ps.species, L, P, T) for L, P, T in sample]
+    st = _fit_structs(sample, efs)
+    pairs = [oracle.nl_build(L, P, 3.0, 0.3)[:2] for L, P, _ in sample]
+    w = {"energy": 1.0, "forces": 1.0, "stress": 0.1}
+    rec0 = ps.decode(x0)["tersoff"]
+    oracle.fit_loss(rec0, ps.species, st, w, pairs)
+    t0 = time.perf_counter()
+    oracle.fit_loss(rec0, ps.species, st, w, pairs)
+    t_loss = time.perf_counter() - t0
+    atoms_sample = sum(len(p) for _, p, _ in sample)
+    atoms_all = sum(len(p) for _, p, _ in raw)
+    return t_loss * (len(x0) + 1) * atoms_all / atoms_sample, threads
+
+
+def run_fit(args, world, rank, local):
+    n_struct = 256
+    raw = make_sic_set(n_struct)
+    n_atoms = sum(len(p) for _, p, _ in raw)
+    cfg = {"workload": "fit_sic256_tersoff1989", "n_structures": n_struct, "n_atoms": n_atoms,
+           "sizes": "zincblende SiC 2^3 / 3^3 cells (64 / 216 atoms)", "a": 4.36, "strain": 0.02,
+           "sigma": 0.1, "parameter_set": "Tersoff1989ParameterSet (A B lambda mu c d h per element, chi)",
+           "targets": "float64 E/F/S at theta * U(0.95, 1.05)",
+           "loss": "w_E 1, w_F 1, w_S 0.1, r0 1, eps0 1 (squared)", "precision": "fp64",
+           "l2": "256 MB scratch write between steps, outside the timed events",
+           "parallelism": f"split{world}"}
+    from akitsushima_b200 import fit
+    ps, x0, xt = _fit_setup()
+    n_var = len(x0)
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        per = []
+        for _ in range(max(1, args.steps)):
+            t, threads = time_reference_fit(raw, ps, x0, xt, 16)
+            per.append(1.0 / t)
+        v = float(np.mean(per))
+        line = {"metric": "fit grads/s", "value": v, "unit": "gradients/s", "impl": "reference",
+                "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": cfg,
+                "cpu_baseline": {"value": v, "unit": "gradients/s", "cores": threads, "kind": "port",
+                                 "sample": f"one loss over the first 16 structures, scaled by atoms to the "
+                                           f"256 and by {n_var + 1} (forward differences)"},
+                "e2e": {"value": v, "unit": "gradients/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    from akitsushima_b200 import _lib
+    # targets: float64 evaluation of every structure at the target parameters
+    tgt = fit.TersoffFit(ps, [{"lattice": L, "positions": P, "atom_types": T, "natoms": len(P),
+                               "ref_energy": 0.0} for L, P, T in raw], device=dev)
+    tb, tri = fit.tables_from_records(ps.decode(xt)["tersoff"], ps.species, dev)
+    E, F, W = tgt.ev.evaluate(tb, tri)
+    E, F, W = E.cpu().numpy(), F.cpu().numpy(), W.cpu().numpy()
+    off = tgt.ev.batch.offsets
+    vols = tgt.ev.batch.volumes
+    efs = [(E[q], F[off[q]:off[q + 1]], W[q].reshape(3, 3) / vols[q]) for q in range(n_struct)]
+    structs = _fit_structs(raw, efs)
+    del tgt
+    f = fit.TersoffFit(ps, structs, {"energy": 1.0, "forces": 1.0, "stress": 0.1}, device=dev,
+                       rank=rank, world=world)
+    # x and its decode live on the host (a few dozen scalars); the batch,
+    # the evaluation, the loss over 38k atoms and the adjoint on the device
+    x_host = torch.tensor(x0, dtype=torch.float64, requires_grad=True)
+
+    def device_step():
+        loss = f._local_loss(x_host)
+        (g,) = torch.autograd.grad(loss, x_host)
+        return torch.cat([loss.detach().reshape(1), g.to(dev)])
+
+    for _ in range(args.warmup):
+        device_step()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            vec = device_step()
+            fit.allreduce_sum(vec, world)
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = 1e3 / ms
+    _lib.profile_begin()
+    device_step()
+    torch.cuda.synchronize()
+    prof = _lib.profile_end()
+    launches = sum(c for c, _ in prof.values())
+    # end to end: numpy x in, (loss, numpy gradient) out, every rank
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        loss, grad = f.loss_and_grad(x0)
+    t_e2e = (time.perf_counter() - t0) / args.e2e_steps
+    if dist:
+        t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t_cpu, threads = time_reference_fit(raw, ps, x0, xt, 16)
+        cpu = {"value": 1.0 / t_cpu, "unit": "gradients/s", "cores": threads, "kind": "port",
+               "sample": f"one loss over the first 16 structures (oracle port), scaled by atoms to the 256 "
+                         f"and by {n_var + 1}: the reference's forward-difference gradient"}
+    clocks = clk.summary()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": "fit grads/s", "value": value, "unit": "gradients/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "atom_force_evals_per_s": n_atoms / (ms * 1e-3), "n_variables": n_var,
+            "gpu_launches": int(launches * args.steps), "gpu_launches_per_step": launches, "clocks": clocks,
+            "kernels": {k: {"launches": c, "ms_per_launch": t / c} for k, (c, t) in prof.items()},
+            "e2e": {"value": 1.0 / t_e2e, "unit": "gradients/s", "h2d_bytes_per_step": 8 * n_var,
+                    "d2h_bytes_per_step": 8 * (n_var + 2), "ms_per_step": t_e2e * 1e3,
+                    "path": "TersoffFit.loss_and_grad(numpy x) -> (loss, numpy gradient)"},
+            "check": {"loss": float(loss), "grad_norm": float(np.linalg.norm(grad))},
+            "cpu_baseline": cpu, "roofline": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def _replicated(lat, pos, r_list):
     from akitsushima_b200.system import replicate_thin
     L2, P2, T2, _ = replicate_thin(lat, pos, np.zeros(len(pos), np.int32), r_list)
@@ -558,7 +764,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--workload", default="eam_cuni_256k",
-                    choices=["eam_cuni_256k", "batched_si512"] + sorted(MD_WORKLOADS))
+                    choices=["eam_cuni_256k", "batched_si512", "fit_sic256"] + sorted(MD_WORKLOADS))
     args = ap.parse_args()
     args.precision_given = "--precision" in sys.argv
     args.warmup = max(3, args.warmup)
@@ -570,6 +776,8 @@ def main():
         return run_batched(args, world, rank, local)
     if args.workload in MD_WORKLOADS:
         return run_md(args, world, rank, local)
+    if args.workload == "fit_sic256":
+        return run_fit(args, world, rank, local)
     lat, pos, ids = make_cuni(args.cells)
     n_atoms = len(pos)
     workload = f"eam_zhou_cuni_fcc{args.cells}^3_{n_atoms}_atoms"
