@@ -236,14 +236,38 @@ __device__ __forceinline__ void adj_leg(const SysView &S, const AdjIn &G, const 
     }
 }
 
+// Per-slot geometry, once per call: d (minimum image), r, the tangent t and
+// a live flag (inside the cutoff), 8 doubles per slot.
+struct SlotGeo {
+    double d[3], r, t[3], live;
+};
+
+__global__ void te_adjoint_prep(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr,
+                                AdjTab P, AdjIn G, int n_slots, SlotGeo *__restrict__ geo) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_slots) return;
+    SlotGeo o;
+    o.live = 0.0;
+    o.d[0] = o.d[1] = o.d[2] = o.r = o.t[0] = o.t[1] = o.t[2] = 0.0;
+    if (s < row_off[S.n_atoms]) {
+        int i = slot_owner(row_off, S.n_atoms, s);
+        int j = nbr[s];
+        int sst = S.n_struct > 1 ? S.atom_struct[i] : 0;
+        adj_leg(S, G, cell_of(S, i), i, j, sst, o.d, o.r, o.t);
+        o.live = (o.r < P.rc && o.r > 1e-12) ? 1.0 : 0.0;
+    }
+    geo[s] = o;
+}
+
 // One pass (sites first .. first + K - 1) over every directed bond slot.
 // site_out (n_slots, W); code[s] = (s_i * ns + s_j) * 2 + (i < j) for a
 // contributing bond, -1 otherwise (written by pass 0).
 template <int K>
 __global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_sites(SysView S, const int *__restrict__ row_off,
                                                               const int *__restrict__ nbr, AdjTab P, AdjIn G,
-                                                              int n_slots, int W, int first,
-                                                              double *__restrict__ site_out, int *__restrict__ code) {
+                                                              const SlotGeo *__restrict__ geo, int n_slots, int W,
+                                                              int first, double *__restrict__ site_out,
+                                                              int *__restrict__ code) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_slots) return;
     const int ns = P.ns;
@@ -254,21 +278,27 @@ __global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_sites(SysView S, const i
         for (int w = first; w < last; ++w) out[w] = 0.0;
         return;
     }
-    int i = slot_owner(row_off, S.n_atoms, s);
-    int j = nbr[s];
-    int sst = S.n_struct > 1 ? S.atom_struct[i] : 0;
-    const double *cell = cell_of(S, i);
-    int si = S.types[i], sj = S.types[j];
-    int lo = i < j ? si : sj, hi = i < j ? sj : si;
-    const double *tp = P.tb + 10 * (lo * ns + hi);
-    double dij[3], rij, tij[3];
-    adj_leg(S, G, cell, i, j, sst, dij, rij, tij);
-    bool live = rij < P.rc && rij > 1e-12 && tp[0] != 0.0;
+    const SlotGeo gs = geo[s];
+    bool live = gs.live != 0.0;
+    int i = 0, j = 0, si = 0, sj = 0;
+    const double *tp = P.tb;
+    if (live) {
+        i = slot_owner(row_off, S.n_atoms, s);
+        j = nbr[s];
+        si = S.types[i];
+        sj = S.types[j];
+        int lo = i < j ? si : sj, hi = i < j ? sj : si;
+        tp = P.tb + 10 * (lo * ns + hi);
+        live = tp[0] != 0.0;
+    }
     if (first == 0) code[s] = live ? ((si * ns + sj) * 2 + (i < j ? 1 : 0)) : -1;
     if (!live) {
         for (int w = first; w < last; ++w) out[w] = 0.0;
         return;
     }
+    int sst = S.n_struct > 1 ? S.atom_struct[i] : 0;
+    const double *dij = gs.d, *tij = gs.t;
+    double rij = gs.r;
     HD<K> r = hd_const<K>(rij);
     r.t = (dij[0] * tij[0] + dij[1] * tij[1] + dij[2] * tij[2]) / rij;
     HD<K> A = hd_param<K>(tp[1], 0, first), B = hd_param<K>(tp[2], 1, first);
@@ -282,10 +312,11 @@ __global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_sites(SysView S, const i
     int beg = row_off[i], end = row_off[i + 1];
     for (int sk_slot = beg; sk_slot < end; ++sk_slot) {
         if (sk_slot == s) continue;
+        const SlotGeo gk = geo[sk_slot];
+        if (gk.live == 0.0) continue;
         int k = nbr[sk_slot];
-        double dik[3], rik, tik[3];
-        adj_leg(S, G, cell, i, k, sst, dik, rik, tik);
-        if (!(rik < P.rc && rik > 1e-12)) continue;
+        const double *dik = gk.d, *tik = gk.t;
+        double rik = gk.r;
         int sk = S.types[k];
         const double *tk = P.tb + 10 * (si * ns + sk);
         const double *t3 = P.tri + 8 * ((si * ns + sj) * ns + sk);
@@ -376,7 +407,7 @@ __global__ void te_adjoint_final(int n_blocks, int ns, const double *__restrict_
 }
 
 struct AdjLayout {
-    size_t site, code, partial, total;
+    size_t site, code, partial, geo, total;
     int W, ne, n_blocks;
 };
 
@@ -393,6 +424,8 @@ static AdjLayout adj_layout(long long n_slots, int ns) {
     o = align256(o + sizeof(int) * (size_t)(n_slots > 0 ? n_slots : 1));
     L.partial = o;
     o = align256(o + sizeof(double) * (size_t)L.n_blocks * L.ne);
+    L.geo = o;
+    o = align256(o + sizeof(SlotGeo) * (size_t)(n_slots > 0 ? n_slots : 1));
     L.total = o;
     return L;
 }
@@ -438,11 +471,13 @@ int mbf_tersoff_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_te
     int *code = ws_at<int>(workspace, L.code);
     double *partial = ws_at<double>(workspace, L.partial);
     int n_slots = (int)nl->n_slots;
+    SlotGeo *geo = ws_at<SlotGeo>(workspace, L.geo);
     int grid = (n_slots + ADJ_BLOCK - 1) / ADJ_BLOCK;
+    te_adjoint_prep<<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, n_slots, geo);
     PROF_BEGIN("te_adjoint_sites", st);
     for (int first = 0; first < L.W; first += ADJ_K)
-        te_adjoint_sites<ADJ_K><<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, n_slots, L.W, first,
-                                                              site, code);
+        te_adjoint_sites<ADJ_K><<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, geo, n_slots, L.W,
+                                                              first, site, code);
     PROF_END("te_adjoint_sites", st);
     MBF_CHECK_LAUNCH();
     int threads = L.ne < 1024 ? ((L.ne + 31) / 32) * 32 : 1024;
