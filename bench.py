@@ -79,6 +79,19 @@ def make_si_set(n=512, a=5.431, strain=0.03, sigma=0.1, seed=0):
     return out
 
 
+def _ncu_traffic(kernel, workload, precision):
+    """DRAM bytes per launch of `kernel` from the committed ncu capture of
+    this workload (profiles/ncu_traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            rec = json.load(f).get(kernel)
+    except (OSError, ValueError):
+        return None
+    if not rec or rec.get("workload") != workload or rec.get("precision") != precision:
+        return None
+    return {"bytes_per_launch": rec["dram_bytes_per_launch"], "source": rec["source"]}
+
+
 def cpu_count():
     try:
         return len(os.sched_getaffinity(0))
@@ -899,7 +912,7 @@ def main():
             "achieved": ach_tf, "peak": peak_tf, "unit": "TFLOP/s", "frac": ach_tf / peak_tf,
             "peak_source": "measured live on this GPU: mbf_peak_probe FMA chains",
             "algorithmic_flops_per_launch": force_flops, "launch_ms": t_dom * 1e3,
-            "traffic": None,
+            "traffic": _ncu_traffic(dom, workload, args.precision),
             "hbm_view": {"achieved": ach_gbs, "peak": hbm_peak, "unit": "GB/s",
                          "frac": ach_gbs / hbm_peak, "peak_source": hbm_src,
                          "algorithmic_bytes_per_launch": force_bytes},
