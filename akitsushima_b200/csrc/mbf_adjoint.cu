@@ -34,7 +34,7 @@ namespace mbf {
 
 constexpr int ADJ_K = 8;        // parameter directions per pass
 constexpr int ADJ_BLOCK = 128;
-constexpr int ADJ_CHUNK = 1024; // slots per reduction block
+constexpr int ADJ_CHUNK = 64;   // bonds per reduction block
 
 // v + t e + sum_p (p_p f_p + q_p e f_p): value, tangent, parameter
 // derivatives and their tangent cross terms.
@@ -242,21 +242,37 @@ struct SlotGeo {
     double d[3], r, t[3], live;
 };
 
+// live[s] = 1 for a bond that contributes (inside the cutoff, pair record
+// valid): the slots the site passes run over, compacted by a scan.
 __global__ void te_adjoint_prep(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr,
-                                AdjTab P, AdjIn G, int n_slots, SlotGeo *__restrict__ geo) {
+                                AdjTab P, AdjIn G, int n_slots, SlotGeo *__restrict__ geo,
+                                int *__restrict__ live) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_slots) return;
     SlotGeo o;
     o.live = 0.0;
     o.d[0] = o.d[1] = o.d[2] = o.r = o.t[0] = o.t[1] = o.t[2] = 0.0;
+    int bond = 0;
     if (s < row_off[S.n_atoms]) {
         int i = slot_owner(row_off, S.n_atoms, s);
         int j = nbr[s];
         int sst = S.n_struct > 1 ? S.atom_struct[i] : 0;
         adj_leg(S, G, cell_of(S, i), i, j, sst, o.d, o.r, o.t);
         o.live = (o.r < P.rc && o.r > 1e-12) ? 1.0 : 0.0;
+        if (o.live != 0.0) {
+            int si = S.types[i], sj = S.types[j];
+            int lo = i < j ? si : sj, hi = i < j ? sj : si;
+            bond = P.tb[10 * (lo * P.ns + hi)] != 0.0 ? 1 : 0;
+        }
     }
     geo[s] = o;
+    live[s] = bond;
+}
+
+__global__ void te_adjoint_compact(int n_slots, const int *__restrict__ live, const int *__restrict__ pos,
+                                   int *__restrict__ bonds) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n_slots && live[s]) bonds[pos[s]] = s;
 }
 
 // One pass (sites first .. first + K - 1) over every directed bond slot.
@@ -265,37 +281,23 @@ __global__ void te_adjoint_prep(SysView S, const int *__restrict__ row_off, cons
 template <int K>
 __global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_sites(SysView S, const int *__restrict__ row_off,
                                                               const int *__restrict__ nbr, AdjTab P, AdjIn G,
-                                                              const SlotGeo *__restrict__ geo, int n_slots, int W,
-                                                              int first, double *__restrict__ site_out,
+                                                              const SlotGeo *__restrict__ geo,
+                                                              const int *__restrict__ bonds,
+                                                              const int *__restrict__ n_bonds, int W, int first,
+                                                              double *__restrict__ site_out,
                                                               int *__restrict__ code) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n_slots) return;
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= *n_bonds) return;
     const int ns = P.ns;
-    double *out = site_out + (size_t)s * W;
-    int last = first + K < W ? first + K : W;
-    if (s >= row_off[S.n_atoms]) {  // capacity beyond the list's slots
-        if (first == 0) code[s] = -1;
-        for (int w = first; w < last; ++w) out[w] = 0.0;
-        return;
-    }
+    int s = bonds[m];
+    double *out = site_out + (size_t)m * W;
     const SlotGeo gs = geo[s];
-    bool live = gs.live != 0.0;
-    int i = 0, j = 0, si = 0, sj = 0;
-    const double *tp = P.tb;
-    if (live) {
-        i = slot_owner(row_off, S.n_atoms, s);
-        j = nbr[s];
-        si = S.types[i];
-        sj = S.types[j];
-        int lo = i < j ? si : sj, hi = i < j ? sj : si;
-        tp = P.tb + 10 * (lo * ns + hi);
-        live = tp[0] != 0.0;
-    }
-    if (first == 0) code[s] = live ? ((si * ns + sj) * 2 + (i < j ? 1 : 0)) : -1;
-    if (!live) {
-        for (int w = first; w < last; ++w) out[w] = 0.0;
-        return;
-    }
+    int i = slot_owner(row_off, S.n_atoms, s);
+    int j = nbr[s];
+    int si = S.types[i], sj = S.types[j];
+    int lo = i < j ? si : sj, hi = i < j ? sj : si;
+    const double *tp = P.tb + 10 * (lo * ns + hi);
+    if (first == 0) code[m] = (si * ns + sj) * 2 + (i < j ? 1 : 0);
     int sst = S.n_struct > 1 ? S.atom_struct[i] : 0;
     const double *dij = gs.d, *tij = gs.t;
     double rij = gs.r;
@@ -356,23 +358,30 @@ __global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_sites(SysView S, const i
         if (first + q < W) out[first + q] = ge * V.p[q] + V.q[q];
 }
 
-// Site values onto table entries: block b sums its chunk of slots for every
-// entry e (one thread each), in slot order.  Entries: tb (ns*ns, 10) then
-// tri (ns^3, 8), the layout of the tables themselves.
-__global__ void te_adjoint_entries(int n_slots, int ns, int W, const double *__restrict__ site_out,
-                                   const int *__restrict__ code, double *__restrict__ partial) {
+// Site values onto table entries: block b stages its chunk of bonds (codes
+// and site rows) in shared memory, then sums it for every entry e (one
+// thread each) in bond order.  Entries: tb (ns*ns, 10) then tri (ns^3, 8),
+// the layout of the tables themselves.
+__global__ void te_adjoint_entries(const int *__restrict__ n_bonds, int ns, int W,
+                                   const double *__restrict__ site_out, const int *__restrict__ code,
+                                   double *__restrict__ partial) {
+    extern __shared__ double sm[];  // ADJ_CHUNK * W site values, then ADJ_CHUNK codes
+    int *scode = reinterpret_cast<int *>(sm + (size_t)ADJ_CHUNK * W);
     int ne = 10 * ns * ns + 8 * ns * ns * ns;
-    int s0 = blockIdx.x * ADJ_CHUNK, s1 = min(n_slots, s0 + ADJ_CHUNK);
+    int m0 = blockIdx.x * ADJ_CHUNK, cnt = min(*n_bonds - m0, ADJ_CHUNK);
+    if (cnt < 0) cnt = 0;
+    for (int q = threadIdx.x; q < cnt * W; q += blockDim.x) sm[q] = site_out[(size_t)m0 * W + q];
+    for (int q = threadIdx.x; q < cnt; q += blockDim.x) scode[q] = code[m0 + q];
+    __syncthreads();
     for (int e = threadIdx.x; e < ne; e += blockDim.x) {
         double acc = 0.0;
         if (e < 10 * ns * ns) {
             int row = e / 10, col = e % 10, a = row / ns, b = row % ns;
-            for (int s = s0; s < s1; ++s) {
-                int c = code[s];
-                if (c < 0) continue;
+            for (int q = 0; q < cnt; ++q) {
+                int c = scode[q];
                 int lower = c & 1, pij = c >> 1, si = pij / ns, sj = pij % ns;
                 int lo = lower ? si : sj, hi = lower ? sj : si;
-                const double *o = site_out + (size_t)s * W;
+                const double *o = sm + (size_t)q * W;
                 if (col >= 1 && col <= 6 && lo == a && hi == b) acc += o[col - 1];
                 if ((col == 7 || col == 8) && si == a && sj == b) acc += o[6 + col - 7];
                 if ((col == 5 || col == 6) && si == a) acc += o[8 + 7 * b + 5 + (col - 5)];
@@ -383,11 +392,9 @@ __global__ void te_adjoint_entries(int n_slots, int ns, int W, const double *__r
             int a = row / (ns * ns), b = (row / ns) % ns, k = row % ns;
             int site = (col >= 1 && col <= 4) ? col - 1 : (col == 6 ? 4 : -1);
             if (site >= 0) {
-                for (int s = s0; s < s1; ++s) {
-                    int c = code[s];
-                    if (c < 0) continue;
-                    int pij = c >> 1, si = pij / ns, sj = pij % ns;
-                    if (si == a && sj == b) acc += site_out[(size_t)s * W + 8 + 7 * k + site];
+                for (int q = 0; q < cnt; ++q) {
+                    int pij = scode[q] >> 1, si = pij / ns, sj = pij % ns;
+                    if (si == a && sj == b) acc += sm[(size_t)q * W + 8 + 7 * k + site];
                 }
             }
         }
@@ -395,19 +402,25 @@ __global__ void te_adjoint_entries(int n_slots, int ns, int W, const double *__r
     }
 }
 
+// One warp per entry: lanes take every 32nd block partial, then a fixed
+// shuffle tree.
 __global__ void te_adjoint_final(int n_blocks, int ns, const double *__restrict__ partial,
                                  double *__restrict__ d_tb, double *__restrict__ d_tri) {
     int ne = 10 * ns * ns + 8 * ns * ns * ns;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
-        double acc = 0.0;
-        for (int b = 0; b < n_blocks; ++b) acc += partial[(size_t)b * ne + e];
+    int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, l = threadIdx.x & 31;
+    if (e >= ne) return;  // whole warps leave together
+    double acc = 0.0;
+    for (int b = l; b < n_blocks; b += 32) acc += partial[(size_t)b * ne + e];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(MBF_FULL, acc, o);
+    if (l == 0) {
         if (e < 10 * ns * ns) d_tb[e] = acc;
         else d_tri[e - 10 * ns * ns] = acc;
     }
 }
 
 struct AdjLayout {
-    size_t site, code, partial, geo, total;
+    size_t site, code, partial, geo, live, pos, bonds, scan, total;
     int W, ne, n_blocks;
 };
 
@@ -426,6 +439,14 @@ static AdjLayout adj_layout(long long n_slots, int ns) {
     o = align256(o + sizeof(double) * (size_t)L.n_blocks * L.ne);
     L.geo = o;
     o = align256(o + sizeof(SlotGeo) * (size_t)(n_slots > 0 ? n_slots : 1));
+    L.live = o;
+    o = align256(o + sizeof(int) * (size_t)(n_slots > 0 ? n_slots : 1));
+    L.pos = o;
+    o = align256(o + sizeof(int) * (size_t)(n_slots + 1));
+    L.bonds = o;
+    o = align256(o + sizeof(int) * (size_t)(n_slots > 0 ? n_slots : 1));
+    L.scan = o;
+    o = align256(o + sizeof(int) * scan_workspace_ints((int)(n_slots > 0 ? n_slots : 1)));
     L.total = o;
     return L;
 }
@@ -472,17 +493,30 @@ int mbf_tersoff_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_te
     double *partial = ws_at<double>(workspace, L.partial);
     int n_slots = (int)nl->n_slots;
     SlotGeo *geo = ws_at<SlotGeo>(workspace, L.geo);
+    int *live = ws_at<int>(workspace, L.live);
+    int *pos = ws_at<int>(workspace, L.pos);
+    int *bonds = ws_at<int>(workspace, L.bonds);
     int grid = (n_slots + ADJ_BLOCK - 1) / ADJ_BLOCK;
-    te_adjoint_prep<<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, n_slots, geo);
+    PROF_BEGIN("te_adjoint_prep", st);
+    te_adjoint_prep<<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, n_slots, geo, live);
+    MBF_CHECK_LAUNCH();
+    int rc = exclusive_scan(live, pos, n_slots, ws_at<int>(workspace, L.scan), st);
+    if (rc != MBF_OK) return rc;
+    te_adjoint_compact<<<grid, ADJ_BLOCK, 0, st>>>(n_slots, live, pos, bonds);
+    PROF_END("te_adjoint_prep", st);
+    const int *n_bonds = pos + n_slots;  // the scan's total
     PROF_BEGIN("te_adjoint_sites", st);
     for (int first = 0; first < L.W; first += ADJ_K)
-        te_adjoint_sites<ADJ_K><<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, geo, n_slots, L.W,
-                                                              first, site, code);
+        te_adjoint_sites<ADJ_K><<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, geo, bonds, n_bonds,
+                                                              L.W, first, site, code);
     PROF_END("te_adjoint_sites", st);
     MBF_CHECK_LAUNCH();
     int threads = L.ne < 1024 ? ((L.ne + 31) / 32) * 32 : 1024;
-    te_adjoint_entries<<<L.n_blocks, threads, 0, st>>>(n_slots, ns, L.W, site, code, partial);
-    te_adjoint_final<<<(L.ne + 127) / 128, 128, 0, st>>>(L.n_blocks, ns, partial, d_tb, d_tri);
+    PROF_BEGIN("te_adjoint_reduce", st);
+    size_t smem = (size_t)ADJ_CHUNK * L.W * sizeof(double) + ADJ_CHUNK * sizeof(int);
+    te_adjoint_entries<<<L.n_blocks, threads, smem, st>>>(n_bonds, ns, L.W, site, code, partial);
+    te_adjoint_final<<<(L.ne * 32 + 127) / 128, 128, 0, st>>>(L.n_blocks, ns, partial, d_tb, d_tri);
+    PROF_END("te_adjoint_reduce", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;
 }
