@@ -249,36 +249,33 @@ __device__ void load_ztab(const EamDev &E, ZTab<T> &Z) {
 }
 
 // phi_{si,sj}, rho'_{sj}, rho'_{si} at r (fused Zhou path).
+// phi_{si,sj}, rho'_{sj}, rho'_{si} at r (fused Zhou path), without a
+// branch on the species: both species' functions are evaluated and combined
+// by the cross-pair rule phi_ab = 1/2 k (q phi_aa + phi_bb / q), q = f_b/f_a
+// (engine/eam_zhou.py:128-207), which for a == b (k = 1, q = 1) is phi_aa
+// up to rounding -- so the lanes of a warp never split between the like and
+// the cross path of a random alloy.
 template <typename T>
 __device__ __forceinline__ void zhou_pair_terms(const ZTab<T> &Z, int si, int sj, T r, T &phi,
                                                 T &dphi, T &drho_j, T &drho_i) {
     T S, dS;
     zswitch_fast<T>(r, Z, S, dS);
-    if (si == sj) {
-        T f, df, pr, dpr;
-        zspecies<T>(Z.sp[si], r, f, df, pr, dpr);
-        phi = pr * S;
-        dphi = dpr * S + pr * dS;
-        drho_j = df * S + f * dS;
-        drho_i = drho_j;
-    } else {
-        int a = si < sj ? si : sj, b = si < sj ? sj : si;
-        T fa, dfa, ua, dua, fb, dfb, ub, dub;
-        zspecies<T>(Z.sp[a], r, fa, dfa, ua, dua);
-        zspecies<T>(Z.sp[b], r, fb, dfb, ub, dub);
-        T k = Z.chi[a * EAM_MAXSP + b];
-        T rfa = fdiv<T>(T(1), fa);
-        T q = fb * rfa;
-        T rq = fdiv<T>(T(1), q);
-        T dq = (dfb * fa - fb * dfa) * rfa * rfa;
-        T v = T(0.5) * k * (q * ua + ub * rq);
-        T dv = T(0.5) * k * (dq * ua + q * dua + dub * rq - ub * dq * rq * rq);
-        phi = v * S;
-        dphi = dv * S + v * dS;
-        T dra = dfa * S + fa * dS, drb = dfb * S + fb * dS;
-        drho_j = sj == a ? dra : drb;
-        drho_i = si == a ? dra : drb;
-    }
+    int a = min(si, sj), b = max(si, sj);
+    T fa, dfa, ua, dua, fb, dfb, ub, dub;
+    zspecies<T>(Z.sp[a], r, fa, dfa, ua, dua);
+    zspecies<T>(Z.sp[b], r, fb, dfb, ub, dub);
+    T k = Z.chi[a * EAM_MAXSP + b];
+    T rfa = fdiv<T>(T(1), fa);
+    T q = fb * rfa;
+    T rq = fdiv<T>(T(1), q);
+    T dq = (dfb * fa - fb * dfa) * rfa * rfa;
+    T v = T(0.5) * k * (q * ua + ub * rq);
+    T dv = T(0.5) * k * (dq * ua + q * dua + dub * rq - ub * dq * rq * rq);
+    phi = v * S;
+    dphi = dv * S + v * dS;
+    T dra = dfa * S + fa * dS, drb = dfb * S + fb * dS;
+    drho_j = sj == a ? dra : drb;
+    drho_i = si == a ? dra : drb;
 }
 
 // Minimum image for the force kernels (fused multiply-add allowed).
