@@ -55,12 +55,15 @@ class PotentialEngine:
     def compute(self, lattice, positions, atom_types, neigh_list=None, use_numba=False,
                 need_stress=True):
         N = len(positions)
-        e_tot = 0.0
-        f_tot = np.zeros((N, 3))
-        s_tot = np.zeros((3, 3)) if need_stress else None
+        if not self.potentials:
+            return 0.0, np.zeros((N, 3)), (np.zeros((3, 3)) if need_stress else None)
+        e_tot = f_tot = s_tot = None
         for p in self.potentials:
             e, f, s = p.compute(lattice, positions, atom_types, neigh_list=neigh_list,
                                 need_stress=need_stress)
+            if f_tot is None:   # the first result is a new array: sum into it
+                e_tot, f_tot, s_tot = e, f, s
+                continue
             e_tot += e
             f_tot += f
             if need_stress:

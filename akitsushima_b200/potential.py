@@ -163,16 +163,18 @@ class DevicePotential:
         ids = species_ids(atom_types, self.species)
         nl, batch, dl = self._resolve_list(lattice, pos, neigh_list, dev)
         batch.set_lattice(0, lattice)
-        batch.set_positions(pos)
+        batch.set_positions(pos, check=False)   # as the reference: no scan of the input
         batch.set_types(ids)
         res = self.evaluate(batch, dl)
-        f = batch.forces_to_host(res.forces)
+        ev = torch.cat([res.energy[:1], res.virial[0]]).to("cpu", non_blocking=True)
+        f = batch.forces_to_host(res.forces)   # synchronises the stream
         self.status()
-        e = float(res.energy[0].item())
+        ev = ev.numpy()
+        e = float(ev[0])
         if not need_stress:
             return e, f, None
         vol = abs(float(np.linalg.det(lattice)))
-        s = res.virial[0].cpu().numpy().reshape(3, 3) / vol
+        s = ev[1:].reshape(3, 3) / vol
         return e, f, s
 
 

@@ -15,6 +15,26 @@ from . import _lib
 REDUCE_CHUNK = 512
 
 
+_COPY_POOL = None
+
+
+def _host_copy(dst, src, min_bytes=1 << 21, parts=4):
+    """dst[...] = src for large host arrays, split over a few threads (numpy
+    releases the GIL while it copies)."""
+    global _COPY_POOL
+    if src.nbytes < min_bytes:
+        np.copyto(dst, src, casting="same_kind")
+        return
+    if _COPY_POOL is None:
+        from concurrent.futures import ThreadPoolExecutor
+        _COPY_POOL = ThreadPoolExecutor(max_workers=parts, thread_name_prefix="mbf-copy")
+    n = len(src)
+    cuts = [n * k // parts for k in range(parts + 1)]
+    futs = [_COPY_POOL.submit(np.copyto, dst[a:b], src[a:b], "same_kind") for a, b in zip(cuts, cuts[1:])]
+    for f in futs:
+        f.result()
+
+
 def cell_metrics(lattice):
     """Perpendicular widths d_i = V / |a_j x a_k| and sigma_min of a lattice
     (rows are lattice vectors); the reference's engine/neighborlist.py:170-267.
@@ -141,10 +161,12 @@ class Batch:
     def single(cls, lattice, positions, type_ids, device=None):
         return cls([lattice], [positions], [type_ids], device=device)
 
-    def set_positions(self, positions):
+    def set_positions(self, positions, check=True):
         """Copy new positions in place: one (N, 3) array or tensor for the
         whole batch, or a sequence of (N_s, 3) arrays, one per structure.
-        Host arrays go through a pinned staging buffer (asynchronous copy)."""
+        Host arrays go through a pinned staging buffer (asynchronous copy).
+        check: refuse NaN / inf in host arrays (no kernel depends on it -- a
+        non-finite coordinate only gives non-finite results)."""
         if isinstance(positions, torch.Tensor):
             src = positions.reshape(-1, 3)
             if tuple(src.shape) != (self.n_atoms, 3):
@@ -158,7 +180,7 @@ class Batch:
                 if len(positions) else np.zeros((0, 3))
         if arr.shape != (self.n_atoms, 3):
             raise ValueError(f"positions have shape {arr.shape}, expected ({self.n_atoms}, 3)")
-        if not np.isfinite(arr).all():
+        if check and not np.isfinite(np.add.reduce(arr, axis=None)):  # NaN and inf survive a sum
             raise ValueError("positions contain NaN or inf")
         if self.device.type != "cuda":
             self.pos.copy_(torch.from_numpy(np.ascontiguousarray(arr, np.float64)))
@@ -167,7 +189,7 @@ class Batch:
         if self._pin_busy.get("pos"):
             # the previous asynchronous copy out of this buffer must finish first
             torch.cuda.current_stream(self.device).synchronize()
-        np.copyto(pin.numpy(), arr, casting="same_kind")
+        _host_copy(pin.numpy(), arr)
         self.pos.copy_(pin, non_blocking=True)
         self._pin_busy["pos"] = True
 
@@ -179,14 +201,16 @@ class Batch:
         return buf
 
     def forces_to_host(self, forces):
-        """Device (N, 3) forces to a host numpy array through a pinned buffer."""
+        """Device (N, 3) forces to a new host numpy array: a pinned block of
+        torch's caching host allocator, copied into directly (no second host
+        copy); the block returns to the cache when the caller drops it."""
         if self.device.type != "cuda":
             return forces.cpu().numpy()
-        pin = self._pinned("forces", (self.n_atoms, 3), torch.float64)
-        pin.copy_(forces, non_blocking=True)
+        out = torch.empty((self.n_atoms, 3), dtype=torch.float64, pin_memory=True)
+        out.copy_(forces, non_blocking=True)
         torch.cuda.current_stream(self.device).synchronize()
         self._pin_busy["pos"] = False
-        return pin.numpy().copy()
+        return out.numpy()
 
     def set_types(self, type_ids):
         """Species ids (torch tensor, or host arrays; an unchanged host array
