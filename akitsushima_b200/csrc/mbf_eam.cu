@@ -17,6 +17,11 @@ constexpr int EAM_NZ = 20;         // Zhou parameters per element row
 constexpr int EAM_NCOL = 2 * EAM_NZ + 3;
 constexpr int EAM_MAXSP = 8;       // species staged in shared memory (fused path)
 constexpr int EAM_BLOCK = 128;
+// Resident blocks per SM the float32 force kernel is compiled for (it sets
+// the register budget: 65536 / (EAM_BLOCK * MBF_EAM_MINB)).
+#ifndef MBF_EAM_MINB
+#define MBF_EAM_MINB 6
+#endif
 
 enum { F_SPLINE = 1, F_SPLINE_R = 2, F_Z_DENS = 3, F_Z_PAIR = 4, F_Z_CROSS = 5, F_Z_EMB = 6 };
 
@@ -427,7 +432,7 @@ template <> struct SlotVec<double> { typedef double3 type; };
 template <> struct SlotVec<float> { typedef float3 type; };
 
 template <typename T, int LPA, bool ZHOU, bool ORTHO>
-__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? 6 : 1) eam_force(SysView S, const int *__restrict__ row_off,
+__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1) eam_force(SysView S, const int *__restrict__ row_off,
                                                        const int *__restrict__ upper,
                                                        const int *__restrict__ nbr,
                                                        const int *__restrict__ rev, EamDev E,
@@ -611,6 +616,8 @@ static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, cons
                             double *aux, void *slot, double *f_local, double *forces, double *per_atom,
                             Chk ck, cudaStream_t st) {
     switch (lpa) {
+        case 1: return eam_launch<T, 1, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
+        case 2: return eam_launch<T, 2, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
         case 4: return eam_launch<T, 4, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
         case 8: return eam_launch<T, 8, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
         case 16: return eam_launch<T, 16, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
