@@ -124,29 +124,12 @@ class BatchedEvaluator:
             o += n
         return e, forces, s
 
-    def autotune(self, candidates=(4, 8, 16), reps=5):
+    def autotune(self, candidates=None, reps=5):
         """Time every lanes-per-atom candidate on this batch and keep the
         fastest (CUDA events; the graph, if any, is recaptured)."""
-        best, best_t = None, float("inf")
-        timings = {}
         had_graph = self._graph is not None
         self._graph = None
-        for c in candidates:
-            self.pot.lanes_per_atom = c
-            self.run()
-            torch.cuda.synchronize(self.device)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
-            for _ in range(reps):
-                self.run()
-            b.record()
-            torch.cuda.synchronize(self.device)
-            t = a.elapsed_time(b) / reps
-            timings[c] = t
-            if t < best_t:
-                best, best_t = c, t
-        self.pot.lanes_per_atom = best
+        self.tuned = self.pot.autotune_lanes(self.batch, self.dlist, candidates, reps, ws=self._ws, out=self.out)
         if had_graph:
             self.capture()
-        self.tuned = {"lanes_per_atom": best, "ms": timings}
         return self.tuned

@@ -124,11 +124,13 @@ class NVE:
                     policy; a fixed interval captures k steps).
     masses        : per-atom amu or {species: amu} (default: the table).
     precision     : 'fp64' or 'mixed' (default: the potential's).
+    autotune      : time the potential's lanes-per-atom tile shapes on this
+                    structure once and keep the fastest.
     """
 
     def __init__(self, potential, lattice, positions, atom_types, temperature=300.0, dt=1.0, seed=None,
                  skin=0.3, rebuild_every=None, steps_per_graph=10, masses=None, velocities=None,
-                 precision=None, device=None, thermo_rows=1 << 16):
+                 precision=None, device=None, thermo_rows=1 << 16, autotune=True):
         if not dt > 0:
             raise ValueError("dt must be positive")
         if rebuild_every is not None and int(rebuild_every) < 1:
@@ -182,6 +184,11 @@ class NVE:
         self._body = torch.cuda.Stream(dev)
         self._graph = None
         self.steps_done = 0
+        if autotune:
+            saved_precision = self.pot.precision
+            self.pot.precision = self.precision
+            self.tuned = self.pot.autotune_lanes(self.batch, self.view, ws=self._ws, out=self.out)
+            self.pot.precision = saved_precision
         self._eval()
         self.e_pot0 = float(self.out.energy[0].item())
         self.e_kin0 = self.kinetic_energy()

@@ -109,6 +109,26 @@ class DevicePotential:
         self._last_ws = ws
         return out
 
+    def autotune_lanes(self, batch, dlist, candidates=None, reps=3, ws=None, out=None):
+        """Time every lanes-per-atom candidate on this batch (CUDA events,
+        after one untimed call each), keep the fastest and return
+        {"lanes_per_atom": best, "ms": {candidate: ms}}."""
+        cands = tuple(candidates or self.lane_choices)
+        timings = {}
+        for c in cands:
+            self.lanes_per_atom = c
+            self.evaluate(batch, dlist, out=out, ws=ws)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                self.evaluate(batch, dlist, out=out, ws=ws)
+            b.record()
+            b.synchronize()
+            timings[c] = a.elapsed_time(b) / reps
+        best = min(cands, key=lambda c: (timings[c], c))
+        self.lanes_per_atom = best
+        return {"lanes_per_atom": best, "ms": timings}
+
     def status(self, device=None):
         """Device status words of the last evaluation (synchronises): raises
         if a kernel reported a bad index or an over-long row."""

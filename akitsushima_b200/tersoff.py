@@ -102,6 +102,7 @@ class TersoffPotential(DevicePotential):
         st = _lib.MbfTersoffTables(len(self.species), _lib.ptr(tb_t), _lib.ptr(tri_t), self.r_cut)
         return (st, tb_t, tri_t)
 
+    lane_choices = (4, 8, 16)
     lanes_per_atom = 8
 
     def _call(self, L, sysd, nld, tabs, plan, prec, ws, nbytes, forces, energy, virial, stream):

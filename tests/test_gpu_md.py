@@ -134,7 +134,7 @@ def test_criterion_graph_equals_eager(cuda_device):
     runs = []
     for graph in (True, False):
         pot = ak.StillingerWeberPotential(SW_SI, species=["Si"])
-        sim = md.NVE(pot, lat, pos, types, temperature=1500.0, seed=3, skin=0.2)
+        sim = md.NVE(pot, lat, pos, types, temperature=1500.0, seed=3, skin=0.2, autotune=False)
         sim.run(60, graph=graph)
         runs.append((sim.positions, sim.results()))
     (p1, r1), (p2, r2) = runs
