@@ -275,15 +275,46 @@ __global__ void te_adjoint_compact(int n_slots, const int *__restrict__ live, co
     if (s < n_slots && live[s]) bonds[pos[s]] = s;
 }
 
-// One pass (sites first .. first + K - 1) over every directed bond slot.
-// site_out (n_slots, W); code[s] = (s_i * ns + s_j) * 2 + (i < j) for a
-// contributing bond, -1 otherwise (written by pass 0).
+// One zeta term gamma fc(r_ik) g(theta) exp((lambda3 (r_ij - r_ik))^m)
+// (engine/tersoff.py:63-101, :528-540) in hyper-dual arithmetic; zero (a
+// constant) where fc(r_ik) = 0, as the reference skips it.
 template <int K>
-__global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_sites(SysView S, const int *__restrict__ row_off,
+__device__ __forceinline__ HD<K> te_zterm(const HD<K> &r, const HD<K> &rk, const HD<K> &dot, const HD<K> &Rk,
+                                          const HD<K> &Dk, const HD<K> &c, const HD<K> &d, const HD<K> &h,
+                                          const HD<K> &l3, const HD<K> &gam, double m) {
+    HD<K> fck = hd_fc<K>(rk, Rk, Dk);
+    if (fck.v == 0.0) return hd_const<K>(0.0);
+    HD<K> cs = dot / (r * rk);
+    HD<K> hc = h - cs;
+    HD<K> d2 = d * d, hc2 = hc * hc;
+    HD<K> g = 1.0 + ((c * c) * hc2) / (d2 * (d2 + hc2));
+    HD<K> ex = hd_cexp<K>(hd_arg<K>(l3, r - rk, m));
+    return gam * fck * g * ex;
+}
+
+// b(zeta) = (1 + (beta zeta)^n)^(-1/(2n)) for zeta > 0 and beta != 0, else 1
+// (engine/tersoff.py:1380-1391).
+template <int K>
+__device__ __forceinline__ HD<K> te_bond_order(const HD<K> &zeta, const HD<K> &beta, const HD<K> &nn) {
+    if (!(zeta.v > 0.0 && beta.v != 0.0)) return hd_const<K>(1.0);
+    HD<K> bz = hd_pow<K>(beta * zeta, nn);
+    return hd_exp<K>(hd_log<K>(1.0 + bz) * ((-0.5) * hd_inv<K>(nn)));
+}
+
+// Every site of one live bond in one pass.  With V = 1/2 fc (fR + b(zeta)
+// fA) and Q = gE V + D_t V:
+//   the pair and bond-order sites (0..7) from one evaluation of V in
+//   hyper-dual arithmetic with zeta held as a (value, tangent) pair;
+//   a leg site theta of term k enters only through zeta, so
+//   dQ/dtheta = (gE V_z + (V_z)') dz_k/dtheta + V_z d(z_k')/dtheta,
+//   V_z = dV/dzeta and (V_z)' its tangent (a dual evaluation), and the
+//   term's own derivatives from a hyper-dual over its 7 leg sites.
+template <int K>
+__global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_bonds(SysView S, const int *__restrict__ row_off,
                                                               const int *__restrict__ nbr, AdjTab P, AdjIn G,
                                                               const SlotGeo *__restrict__ geo,
                                                               const int *__restrict__ bonds,
-                                                              const int *__restrict__ n_bonds, int W, int first,
+                                                              const int *__restrict__ n_bonds, int W,
                                                               double *__restrict__ site_out,
                                                               int *__restrict__ code) {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -297,65 +328,92 @@ __global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_sites(SysView S, const i
     int si = S.types[i], sj = S.types[j];
     int lo = i < j ? si : sj, hi = i < j ? sj : si;
     const double *tp = P.tb + 10 * (lo * ns + hi);
-    if (first == 0) code[m] = (si * ns + sj) * 2 + (i < j ? 1 : 0);
+    code[m] = (si * ns + sj) * 2 + (i < j ? 1 : 0);
     int sst = S.n_struct > 1 ? S.atom_struct[i] : 0;
     const double *dij = gs.d, *tij = gs.t;
-    double rij = gs.r;
-    HD<K> r = hd_const<K>(rij);
-    r.t = (dij[0] * tij[0] + dij[1] * tij[1] + dij[2] * tij[2]) / rij;
-    HD<K> A = hd_param<K>(tp[1], 0, first), B = hd_param<K>(tp[2], 1, first);
-    HD<K> l1 = hd_param<K>(tp[3], 2, first), l2 = hd_param<K>(tp[4], 3, first);
-    HD<K> Rp = hd_param<K>(tp[5], 4, first), Dp = hd_param<K>(tp[6], 5, first);
-    HD<K> fc = hd_fc<K>(r, Rp, Dp);
-    HD<K> fr = A * hd_cexp<K>((-1.0) * (l1 * r));
-    HD<K> fa = (-1.0) * (B * hd_cexp<K>((-1.0) * (l2 * r)));
-    // zeta_ij over the other neighbours k of i (engine/tersoff.py:528-540)
-    HD<K> zeta = hd_const<K>(0.0);
+    double rij = gs.r, rt = (dij[0] * tij[0] + dij[1] * tij[1] + dij[2] * tij[2]) / rij;
     int beg = row_off[i], end = row_off[i + 1];
-    for (int sk_slot = beg; sk_slot < end; ++sk_slot) {
-        if (sk_slot == s) continue;
-        const SlotGeo gk = geo[sk_slot];
+    // 1. zeta and its tangent
+    HD<1> r1 = hd_const<1>(rij);
+    r1.t = rt;
+    HD<1> zeta = hd_const<1>(0.0);
+    for (int q = beg; q < end; ++q) {
+        if (q == s) continue;
+        const SlotGeo gk = geo[q];
         if (gk.live == 0.0) continue;
-        int k = nbr[sk_slot];
-        const double *dik = gk.d, *tik = gk.t;
-        double rik = gk.r;
-        int sk = S.types[k];
+        int sk = S.types[nbr[q]];
         const double *tk = P.tb + 10 * (si * ns + sk);
         const double *t3 = P.tri + 8 * ((si * ns + sj) * ns + sk);
         if (tk[0] == 0.0 || t3[0] == 0.0) continue;
-        int base = 8 + 7 * sk;
-        HD<K> rk = hd_const<K>(rik);
-        rk.t = (dik[0] * tik[0] + dik[1] * tik[1] + dik[2] * tik[2]) / rik;
-        HD<K> Rk = hd_param<K>(tk[5], base + 5, first), Dk = hd_param<K>(tk[6], base + 6, first);
-        HD<K> fck = hd_fc<K>(rk, Rk, Dk);
-        if (fck.v == 0.0) continue;
-        HD<K> dot = hd_const<K>(dij[0] * dik[0] + dij[1] * dik[1] + dij[2] * dik[2]);
-        dot.t = tij[0] * dik[0] + tij[1] * dik[1] + tij[2] * dik[2] + dij[0] * tik[0] + dij[1] * tik[1] +
-                dij[2] * tik[2];
-        HD<K> cs = dot / (r * rk);
-        HD<K> c = hd_param<K>(t3[1], base + 0, first), d = hd_param<K>(t3[2], base + 1, first);
-        HD<K> h = hd_param<K>(t3[3], base + 2, first), l3 = hd_param<K>(t3[4], base + 3, first);
-        HD<K> gam = hd_param<K>(t3[6], base + 4, first);
-        HD<K> hc = h - cs;
-        HD<K> d2 = d * d, hc2 = hc * hc;
-        HD<K> g = 1.0 + ((c * c) * hc2) / (d2 * (d2 + hc2));
-        HD<K> ex = hd_cexp<K>(hd_arg<K>(l3, r - rk, t3[5]));
-        zeta = zeta + gam * fck * g * ex;
+        HD<1> rk = hd_const<1>(gk.r);
+        rk.t = (gk.d[0] * gk.t[0] + gk.d[1] * gk.t[1] + gk.d[2] * gk.t[2]) / gk.r;
+        HD<1> dot = hd_const<1>(dij[0] * gk.d[0] + dij[1] * gk.d[1] + dij[2] * gk.d[2]);
+        dot.t = tij[0] * gk.d[0] + tij[1] * gk.d[1] + tij[2] * gk.d[2] + dij[0] * gk.t[0] + dij[1] * gk.t[1] +
+                dij[2] * gk.t[2];
+        zeta = zeta + te_zterm<1>(r1, rk, dot, hd_const<1>(tk[5]), hd_const<1>(tk[6]), hd_const<1>(t3[1]),
+                                  hd_const<1>(t3[2]), hd_const<1>(t3[3]), hd_const<1>(t3[4]),
+                                  hd_const<1>(t3[6]), t3[5]);
     }
-    // b_ij with beta, n of the centre's record (engine/tersoff.py:1380-1391,
-    // :1693-1702): 1 unless zeta > 0 and beta != 0
-    const double *tij_rec = P.tb + 10 * (si * ns + sj);
-    HD<K> b = hd_const<K>(1.0);
-    if (zeta.v > 0.0 && tij_rec[7] != 0.0) {
-        HD<K> beta = hd_param<K>(tij_rec[7], 6, first), nn = hd_param<K>(tij_rec[8], 7, first);
-        HD<K> bz = hd_pow<K>(beta * zeta, nn);
-        b = hd_exp<K>(hd_log<K>(1.0 + bz) * ((-0.5) * hd_inv<K>(nn)));
-    }
-    HD<K> V = 0.5 * (fc * (fr + b * fa));
     double ge = G.gE ? G.gE[sst] : 0.0;
+    const double *tij_rec = P.tb + 10 * (si * ns + sj);
+    // 2. pair and bond-order sites
+    {
+        HD<K> r = hd_const<K>(rij);
+        r.t = rt;
+        HD<K> z = hd_const<K>(zeta.v);
+        z.t = zeta.t;
+        HD<K> A = hd_param<K>(tp[1], 0, 0), B = hd_param<K>(tp[2], 1, 0);
+        HD<K> l1 = hd_param<K>(tp[3], 2, 0), l2 = hd_param<K>(tp[4], 3, 0);
+        HD<K> Rp = hd_param<K>(tp[5], 4, 0), Dp = hd_param<K>(tp[6], 5, 0);
+        HD<K> beta = hd_param<K>(tij_rec[7], 6, 0), nn = hd_param<K>(tij_rec[8], 7, 0);
+        HD<K> fc = hd_fc<K>(r, Rp, Dp);
+        HD<K> fr = A * hd_cexp<K>((-1.0) * (l1 * r));
+        HD<K> fa = (-1.0) * (B * hd_cexp<K>((-1.0) * (l2 * r)));
+        HD<K> V = 0.5 * (fc * (fr + te_bond_order<K>(z, beta, nn) * fa));
 #pragma unroll
-    for (int q = 0; q < K; ++q)
-        if (first + q < W) out[first + q] = ge * V.p[q] + V.q[q];
+        for (int q = 0; q < 8; ++q) out[q] = ge * V.p[q] + V.q[q];
+    }
+    // 3. V_z = 1/2 fc fA db/dzeta and its tangent
+    double c1 = 0.0, c2 = 0.0;
+    if (zeta.v > 0.0 && tij_rec[7] != 0.0) {
+        HD<1> fc = hd_fc<1>(r1, hd_const<1>(tp[5]), hd_const<1>(tp[6]));
+        HD<1> fa = (-tp[2]) * hd_cexp<1>((-tp[4]) * r1);
+        HD<1> beta = hd_const<1>(tij_rec[7]), nn = hd_const<1>(tij_rec[8]);
+        HD<1> b = te_bond_order<1>(zeta, beta, nn);
+        HD<1> u = hd_pow<1>(beta * zeta, nn);
+        HD<1> db = (-0.5) * (b * u / (zeta * (1.0 + u)));
+        HD<1> Vz = 0.5 * (fc * fa * db);
+        c1 = ge * Vz.v + Vz.t;
+        c2 = Vz.v;
+    }
+    // 4. the leg sites of every term, by the species of k
+    double acc[8 + 7 * 8];
+    for (int w = 8; w < W; ++w) acc[w] = 0.0;
+    if (c1 != 0.0 || c2 != 0.0) {
+        HD<7> r7 = hd_const<7>(rij);
+        r7.t = rt;
+        for (int q = beg; q < end; ++q) {
+            if (q == s) continue;
+            const SlotGeo gk = geo[q];
+            if (gk.live == 0.0) continue;
+            int sk = S.types[nbr[q]];
+            const double *tk = P.tb + 10 * (si * ns + sk);
+            const double *t3 = P.tri + 8 * ((si * ns + sj) * ns + sk);
+            if (tk[0] == 0.0 || t3[0] == 0.0) continue;
+            HD<7> rk = hd_const<7>(gk.r);
+            rk.t = (gk.d[0] * gk.t[0] + gk.d[1] * gk.t[1] + gk.d[2] * gk.t[2]) / gk.r;
+            HD<7> dot = hd_const<7>(dij[0] * gk.d[0] + dij[1] * gk.d[1] + dij[2] * gk.d[2]);
+            dot.t = tij[0] * gk.d[0] + tij[1] * gk.d[1] + tij[2] * gk.d[2] + dij[0] * gk.t[0] + dij[1] * gk.t[1] +
+                    dij[2] * gk.t[2];
+            HD<7> z = te_zterm<7>(r7, rk, dot, hd_param<7>(tk[5], 5, 0), hd_param<7>(tk[6], 6, 0),
+                                  hd_param<7>(t3[1], 0, 0), hd_param<7>(t3[2], 1, 0), hd_param<7>(t3[3], 2, 0),
+                                  hd_param<7>(t3[4], 3, 0), hd_param<7>(t3[6], 4, 0), t3[5]);
+            double *a = acc + 8 + 7 * sk;
+#pragma unroll
+            for (int w = 0; w < 7; ++w) a[w] += c1 * z.p[w] + c2 * z.q[w];
+        }
+    }
+    for (int w = 8; w < W; ++w) out[w] = acc[w];
 }
 
 // Site values onto table entries: block b stages its chunk of bonds (codes
@@ -505,11 +563,10 @@ int mbf_tersoff_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_te
     te_adjoint_compact<<<grid, ADJ_BLOCK, 0, st>>>(n_slots, live, pos, bonds);
     PROF_END("te_adjoint_prep", st);
     const int *n_bonds = pos + n_slots;  // the scan's total
-    PROF_BEGIN("te_adjoint_sites", st);
-    for (int first = 0; first < L.W; first += ADJ_K)
-        te_adjoint_sites<ADJ_K><<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, geo, bonds, n_bonds,
-                                                              L.W, first, site, code);
-    PROF_END("te_adjoint_sites", st);
+    PROF_BEGIN("te_adjoint_bonds", st);
+    te_adjoint_bonds<ADJ_K><<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, geo, bonds, n_bonds, L.W,
+                                                          site, code);
+    PROF_END("te_adjoint_bonds", st);
     MBF_CHECK_LAUNCH();
     int threads = L.ne < 1024 ? ((L.ne + 31) / 32) * 32 : 1024;
     PROF_BEGIN("te_adjoint_reduce", st);
