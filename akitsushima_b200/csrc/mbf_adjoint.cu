@@ -33,8 +33,7 @@
 namespace mbf {
 
 constexpr int ADJ_K = 8;        // parameter directions per pass
-constexpr int ADJ_BLOCK = 128;
-constexpr int ADJ_CHUNK = 64;   // bonds per reduction block
+constexpr int ADJ_BLOCK = 64;
 
 // v + t e + sum_p (p_p f_p + q_p e f_p): value, tangent, parameter
 // derivatives and their tangent cross terms.
@@ -310,25 +309,17 @@ __device__ __forceinline__ HD<K> te_bond_order(const HD<K> &zeta, const HD<K> &b
 //   V_z = dV/dzeta and (V_z)' its tangent (a dual evaluation), and the
 //   term's own derivatives from a hyper-dual over its 7 leg sites.
 template <int K>
-__global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_bonds(SysView S, const int *__restrict__ row_off,
-                                                              const int *__restrict__ nbr, AdjTab P, AdjIn G,
-                                                              const SlotGeo *__restrict__ geo,
-                                                              const int *__restrict__ bonds,
-                                                              const int *__restrict__ n_bonds, int W,
-                                                              double *__restrict__ site_out,
-                                                              int *__restrict__ code) {
-    int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= *n_bonds) return;
+__device__ int adj_bond_sites(const SysView &S, const int *__restrict__ row_off, const int *__restrict__ nbr,
+                              const AdjTab &P, const AdjIn &G, const SlotGeo *__restrict__ geo, int s, int W,
+                              double *__restrict__ out) {
     const int ns = P.ns;
-    int s = bonds[m];
-    double *out = site_out + (size_t)m * W;
     const SlotGeo gs = geo[s];
     int i = slot_owner(row_off, S.n_atoms, s);
     int j = nbr[s];
     int si = S.types[i], sj = S.types[j];
     int lo = i < j ? si : sj, hi = i < j ? sj : si;
     const double *tp = P.tb + 10 * (lo * ns + hi);
-    code[m] = (si * ns + sj) * 2 + (i < j ? 1 : 0);
+    int code = (si * ns + sj) * 2 + (i < j ? 1 : 0);
     int sst = S.n_struct > 1 ? S.atom_struct[i] : 0;
     const double *dij = gs.d, *tij = gs.t;
     double rij = gs.r, rt = (dij[0] * tij[0] + dij[1] * tij[1] + dij[2] * tij[2]) / rij;
@@ -414,59 +405,79 @@ __global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_bonds(SysView S, const i
         }
     }
     for (int w = 8; w < W; ++w) out[w] = acc[w];
+    return code;
 }
 
-// Site values onto table entries: block b stages its chunk of bonds (codes
-// and site rows) in shared memory, then sums it for every entry e (one
-// thread each) in bond order.  Entries: tb (ns*ns, 10) then tri (ns^3, 8),
-// the layout of the tables themselves.
-__global__ void te_adjoint_entries(const int *__restrict__ n_bonds, int ns, int W,
-                                   const double *__restrict__ site_out, const int *__restrict__ code,
-                                   double *__restrict__ partial) {
-    extern __shared__ double sm[];  // ADJ_CHUNK * W site values, then ADJ_CHUNK codes
-    int *scode = reinterpret_cast<int *>(sm + (size_t)ADJ_CHUNK * W);
-    int ne = 10 * ns * ns + 8 * ns * ns * ns;
-    int m0 = blockIdx.x * ADJ_CHUNK, cnt = min(*n_bonds - m0, ADJ_CHUNK);
-    if (cnt < 0) cnt = 0;
-    for (int q = threadIdx.x; q < cnt * W; q += blockDim.x) sm[q] = site_out[(size_t)m0 * W + q];
-    for (int q = threadIdx.x; q < cnt; q += blockDim.x) scode[q] = code[m0 + q];
-    __syncthreads();
-    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-        double acc = 0.0;
-        if (e < 10 * ns * ns) {
-            int row = e / 10, col = e % 10, a = row / ns, b = row % ns;
+// Site values of one entry (tb (ns*ns, 10) then tri (ns^3, 8), the tables'
+// own layout) summed over `cnt` staged bonds in bond order.
+__device__ __forceinline__ double adj_entry_sum(int e, int ns, int W, int cnt, const double *__restrict__ sm,
+                                               const int *__restrict__ scode) {
+    double a = 0.0;
+    if (e < 10 * ns * ns) {
+        int row = e / 10, col = e % 10, ra = row / ns, rb = row % ns;
+        for (int q = 0; q < cnt; ++q) {
+            int c = scode[q];
+            if (c < 0) continue;
+            int lower = c & 1, pij = c >> 1, si = pij / ns, sj = pij % ns;
+            int lo = lower ? si : sj, hi = lower ? sj : si;
+            const double *o = sm + (size_t)q * W;
+            if (col >= 1 && col <= 6 && lo == ra && hi == rb) a += o[col - 1];
+            if ((col == 7 || col == 8) && si == ra && sj == rb) a += o[6 + col - 7];
+            if ((col == 5 || col == 6) && si == ra) a += o[8 + 7 * rb + 5 + (col - 5)];
+        }
+    } else {
+        int e3 = e - 10 * ns * ns;
+        int row = e3 / 8, col = e3 % 8;
+        int ra = row / (ns * ns), rb = (row / ns) % ns, k = row % ns;
+        int site = (col >= 1 && col <= 4) ? col - 1 : (col == 6 ? 4 : -1);
+        if (site >= 0) {
             for (int q = 0; q < cnt; ++q) {
                 int c = scode[q];
-                int lower = c & 1, pij = c >> 1, si = pij / ns, sj = pij % ns;
-                int lo = lower ? si : sj, hi = lower ? sj : si;
-                const double *o = sm + (size_t)q * W;
-                if (col >= 1 && col <= 6 && lo == a && hi == b) acc += o[col - 1];
-                if ((col == 7 || col == 8) && si == a && sj == b) acc += o[6 + col - 7];
-                if ((col == 5 || col == 6) && si == a) acc += o[8 + 7 * b + 5 + (col - 5)];
-            }
-        } else {
-            int e3 = e - 10 * ns * ns;
-            int row = e3 / 8, col = e3 % 8;
-            int a = row / (ns * ns), b = (row / ns) % ns, k = row % ns;
-            int site = (col >= 1 && col <= 4) ? col - 1 : (col == 6 ? 4 : -1);
-            if (site >= 0) {
-                for (int q = 0; q < cnt; ++q) {
-                    int pij = scode[q] >> 1, si = pij / ns, sj = pij % ns;
-                    if (si == a && sj == b) acc += sm[(size_t)q * W + 8 + 7 * k + site];
-                }
+                if (c < 0) continue;
+                int pij = c >> 1, si = pij / ns, sj = pij % ns;
+                if (si == ra && sj == rb) a += sm[(size_t)q * W + 8 + 7 * k + site];
             }
         }
-        partial[(size_t)blockIdx.x * ne + e] = acc;
     }
+    return a;
 }
+
+// Block b takes live bonds b*ADJ_BLOCK ..: every thread one bond, its site
+// values staged in shared memory, then the block's sum of every table entry
+// (one thread per entry, bond order) to partial[b].
+template <int K>
+__global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_bonds(SysView S, const int *__restrict__ row_off,
+                                                              const int *__restrict__ nbr, AdjTab P, AdjIn G,
+                                                              const SlotGeo *__restrict__ geo,
+                                                              const int *__restrict__ bonds,
+                                                              const int *__restrict__ n_bonds, int W,
+                                                              double *__restrict__ partial) {
+    extern __shared__ double sm[];  // ADJ_BLOCK * W site values, then ADJ_BLOCK codes
+    int *scode = reinterpret_cast<int *>(sm + (size_t)ADJ_BLOCK * W);
+    int nb = *n_bonds;
+    int m0 = blockIdx.x * ADJ_BLOCK;
+    if (m0 >= nb) return;  // the whole block leaves together
+    int m = m0 + threadIdx.x;
+    double *out = sm + (size_t)threadIdx.x * W;
+    int c = -1;
+    if (m < nb) c = adj_bond_sites<K>(S, row_off, nbr, P, G, geo, bonds[m], W, out);
+    scode[threadIdx.x] = c;
+    __syncthreads();
+    int cnt = min(ADJ_BLOCK, nb - m0);
+    int ne = 10 * P.ns * P.ns + 8 * P.ns * P.ns * P.ns;
+    for (int e = threadIdx.x; e < ne; e += blockDim.x)
+        partial[(size_t)blockIdx.x * ne + e] = adj_entry_sum(e, P.ns, W, cnt, sm, scode);
+}
+
 
 // One warp per entry: lanes take every 32nd block partial, then a fixed
 // shuffle tree.
-__global__ void te_adjoint_final(int n_blocks, int ns, const double *__restrict__ partial,
+__global__ void te_adjoint_final(const int *__restrict__ n_bonds, int ns, const double *__restrict__ partial,
                                  double *__restrict__ d_tb, double *__restrict__ d_tri) {
     int ne = 10 * ns * ns + 8 * ns * ns * ns;
     int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, l = threadIdx.x & 31;
     if (e >= ne) return;  // whole warps leave together
+    int n_blocks = (*n_bonds + ADJ_BLOCK - 1) / ADJ_BLOCK;
     double acc = 0.0;
     for (int b = l; b < n_blocks; b += 32) acc += partial[(size_t)b * ne + e];
 #pragma unroll
@@ -478,7 +489,7 @@ __global__ void te_adjoint_final(int n_blocks, int ns, const double *__restrict_
 }
 
 struct AdjLayout {
-    size_t site, code, partial, geo, live, pos, bonds, scan, total;
+    size_t partial, geo, live, pos, bonds, scan, total;
     int W, ne, n_blocks;
 };
 
@@ -486,13 +497,9 @@ static AdjLayout adj_layout(long long n_slots, int ns) {
     AdjLayout L;
     L.W = 8 + 7 * ns;
     L.ne = 10 * ns * ns + 8 * ns * ns * ns;
-    L.n_blocks = (int)((n_slots + ADJ_CHUNK - 1) / ADJ_CHUNK);
+    L.n_blocks = (int)((n_slots + ADJ_BLOCK - 1) / ADJ_BLOCK);  // at most one block per live-bond tile
     if (L.n_blocks < 1) L.n_blocks = 1;
     size_t o = 0;
-    L.site = o;
-    o = align256(o + sizeof(double) * (size_t)(n_slots > 0 ? n_slots : 1) * L.W);
-    L.code = o;
-    o = align256(o + sizeof(int) * (size_t)(n_slots > 0 ? n_slots : 1));
     L.partial = o;
     o = align256(o + sizeof(double) * (size_t)L.n_blocks * L.ne);
     L.geo = o;
@@ -546,8 +553,6 @@ int mbf_tersoff_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_te
     G.gE = g_energy;
     G.gF = g_forces;
     G.gW = g_virial;
-    double *site = ws_at<double>(workspace, L.site);
-    int *code = ws_at<int>(workspace, L.code);
     double *partial = ws_at<double>(workspace, L.partial);
     int n_slots = (int)nl->n_slots;
     SlotGeo *geo = ws_at<SlotGeo>(workspace, L.geo);
@@ -563,16 +568,15 @@ int mbf_tersoff_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_te
     te_adjoint_compact<<<grid, ADJ_BLOCK, 0, st>>>(n_slots, live, pos, bonds);
     PROF_END("te_adjoint_prep", st);
     const int *n_bonds = pos + n_slots;  // the scan's total
+    size_t smem = (size_t)ADJ_BLOCK * L.W * sizeof(double) + ADJ_BLOCK * sizeof(int);  // <= 33 KB (ns <= 8)
+    int bgrid = L.n_blocks;
     PROF_BEGIN("te_adjoint_bonds", st);
-    te_adjoint_bonds<ADJ_K><<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, geo, bonds, n_bonds, L.W,
-                                                          site, code);
+    te_adjoint_bonds<ADJ_K><<<bgrid, ADJ_BLOCK, smem, st>>>(S, nl->row_off, nl->nbr, P, G, geo, bonds, n_bonds,
+                                                              L.W, partial);
     PROF_END("te_adjoint_bonds", st);
     MBF_CHECK_LAUNCH();
-    int threads = L.ne < 1024 ? ((L.ne + 31) / 32) * 32 : 1024;
     PROF_BEGIN("te_adjoint_reduce", st);
-    size_t smem = (size_t)ADJ_CHUNK * L.W * sizeof(double) + ADJ_CHUNK * sizeof(int);
-    te_adjoint_entries<<<L.n_blocks, threads, smem, st>>>(n_bonds, ns, L.W, site, code, partial);
-    te_adjoint_final<<<(L.ne * 32 + 127) / 128, 128, 0, st>>>(L.n_blocks, ns, partial, d_tb, d_tri);
+    te_adjoint_final<<<(L.ne * 32 + 127) / 128, 128, 0, st>>>(n_bonds, ns, partial, d_tb, d_tri);
     PROF_END("te_adjoint_reduce", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;

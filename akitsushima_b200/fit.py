@@ -224,6 +224,37 @@ class MultiSpeciesTersoffParameterSet(_Variables):
         """The same with 0-d tensor entries carrying x's autograd history."""
         return self._decode(list(x.unbind(0)))
 
+    _TB_COL = {"A": 1, "B": 2, "lambda1": 3, "lambda2": 4, "R": 5, "D": 6, "beta": 7, "n": 8}
+    _TRI_COL = {"c": 1, "d": 2, "h": 3, "lambda3": 4, "m": 5, "gamma": 6}
+
+    def tables_torch(self, x):
+        """(tb, tri) of decode(x) built directly: the tables of the initial
+        records with every variable's targets overwritten -- a few tensor
+        operations, differentiable in x."""
+        if not hasattr(self, "_plan"):
+            tb0, tri0 = tables_from_records(self.records, self.species, "cpu")
+            idx = {s: a for a, s in enumerate(self.species)}
+            ns = len(self.species)
+            tbp, trip = ([], [], []), ([], [], [])
+            for v, (_, key, targets) in enumerate(self.variables):
+                for (i, j, k), kk in targets:
+                    if kk in self._TB_COL:     # pair and bond keys live on diagonal records
+                        tbp[0].append(v)
+                        tbp[1].append(idx[i] * ns + idx[j])
+                        tbp[2].append(self._TB_COL[kk])
+                    else:
+                        trip[0].append(v)
+                        trip[1].append((idx[i] * ns + idx[j]) * ns + idx[k])
+                        trip[2].append(self._TRI_COL[kk])
+            logm = torch.tensor([key in self._LOG_KEYS for _, key, _ in self.variables])
+            self._plan = (tb0, tri0, [torch.tensor(a, dtype=torch.long) for a in tbp],
+                          [torch.tensor(a, dtype=torch.long) for a in trip], logm)
+        tb0, tri0, tbp, trip, logm = self._plan
+        vals = torch.where(logm, torch.exp(x), x)
+        tb = tb0.clone().index_put((tbp[1], tbp[2]), vals[tbp[0]])
+        tri = tri0.clone().index_put((trip[1], trip[2]), vals[trip[0]])
+        return tb, tri
+
 
 def _mix_1989(el, chi, species, omega):
     """Tersoff (1989) mixing rules (PRB 39, 5566, eqs. 1a-1e) on values that
@@ -320,6 +351,58 @@ class Tersoff1989ParameterSet(_Variables):
     def decode_torch(self, x):
         return self._decode(list(x.unbind(0)), True)
 
+    _EL_KEYS = ("A", "B", "lambda", "mu", "beta", "n", "c", "d", "h", "R", "S")
+
+    def tables_torch(self, x):
+        """(tb, tri) of decode(x) from the mixing rules applied to whole
+        per-element vectors (PRB 39, 5566, eqs. 1a-1e; the same expressions
+        as tersoff1989_to_triplets), differentiable in x."""
+        ns = len(self.species)
+        if not hasattr(self, "_plan"):
+            el0 = torch.tensor([[self.elements[s][k] for k in self._EL_KEYS] for s in self.species],
+                               dtype=torch.float64)
+            chi0 = torch.ones((ns, ns), dtype=torch.float64)
+            for a, sa in enumerate(self.species):
+                for b, sb in enumerate(self.species):
+                    if a != b:
+                        chi0[a, b] = self.chi.get(f"{sa}-{sb}", self.chi.get(f"{sb}-{sa}"))
+            om = torch.ones((ns, ns), dtype=torch.float64)
+            for a, sa in enumerate(self.species):
+                for b, sb in enumerate(self.species):
+                    om[a, b] = float(self.omega.get(f"{sa}-{sb}", self.omega.get(f"{sb}-{sa}", 1.0)))
+            ev, er, ec, cv, cr = [], [], [], [], []
+            idx = {s: a for a, s in enumerate(self.species)}
+            for v, (_, key, target) in enumerate(self.variables):
+                if key == "chi":
+                    a, b = (idx[t] for t in target.split("-"))
+                    cv += [v, v]
+                    cr += [(a, b), (b, a)]
+                else:
+                    ev.append(v)
+                    er.append(idx[target[0]])
+                    ec.append(self._EL_KEYS.index(key))
+            logm = torch.tensor([key in self._LOG_KEYS for _, key, _ in self.variables])
+            self._plan = (el0, chi0, om, torch.tensor(ev, dtype=torch.long), torch.tensor(er, dtype=torch.long),
+                          torch.tensor(ec, dtype=torch.long), torch.tensor(cv, dtype=torch.long),
+                          torch.tensor([c[0] for c in cr], dtype=torch.long),
+                          torch.tensor([c[1] for c in cr], dtype=torch.long), logm)
+        el0, chi0, om, ev, er, ec, cv, c0, c1, logm = self._plan
+        vals = torch.where(logm, torch.exp(x), x)
+        el = el0.clone().index_put((er, ec), vals[ev]) if len(ev) else el0
+        chi = chi0.clone().index_put((c0, c1), vals[cv]) if len(cv) else chi0
+        A, B, lam, mu, beta, n, c, d, h, R, S = el.unbind(1)
+        r = torch.sqrt(R[:, None] * R[None, :])
+        sx = torch.sqrt(S[:, None] * S[None, :])
+        one = torch.ones((ns, ns), dtype=torch.float64)
+        tb = torch.stack([one, torch.sqrt(A[:, None] * A[None, :]), chi * torch.sqrt(B[:, None] * B[None, :]),
+                          0.5 * (lam[:, None] + lam[None, :]), 0.5 * (mu[:, None] + mu[None, :]),
+                          0.5 * (r + sx), 0.5 * (sx - r), beta[:, None] * one, n[:, None] * one, 0.0 * one],
+                         dim=-1).reshape(ns * ns, 10)
+        one3 = torch.ones((ns, ns, ns), dtype=torch.float64)
+        tri = torch.stack([one3, c[:, None, None] * one3, d[:, None, None] * one3, h[:, None, None] * one3,
+                           0.0 * one3, 3.0 * one3, om[:, None, :] * one3, 0.0 * one3], dim=-1).reshape(ns ** 3, 8)
+        return tb, tri
+
 
 # ---- evaluation with explicit tables and its adjoint ----------------------------
 
@@ -333,6 +416,24 @@ class _TableEval:
         self.list_cut = -1.0   # the largest r_cut the current list serves
         self._ws = None
         self._adj_ws = None
+        self.lanes = 8
+
+    def autotune(self, tb, tri, candidates=(4, 8, 16), reps=3):
+        """Keep the fastest lanes-per-atom tile shape of the evaluation on
+        this batch (CUDA events)."""
+        times = {}
+        for c in candidates:
+            self.lanes = c
+            self.evaluate(tb, tri)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                self.evaluate(tb, tri)
+            b.record()
+            b.synchronize()
+            times[c] = a.elapsed_time(b) / reps
+        self.lanes = min(candidates, key=lambda c: (times[c], c))
+        return {"lanes_per_atom": self.lanes, "ms": times}
 
     def _ensure_list(self, r_cut):
         if self.dlist is None or r_cut > self.list_cut:
@@ -359,7 +460,7 @@ class _TableEval:
         F = torch.empty((b.n_atoms, 3), dtype=torch.float64, device=dev)
         W = torch.empty((b.n_struct, 9), dtype=torch.float64, device=dev)
         st = torch.cuda.current_stream(dev).cuda_stream
-        _lib.check(L.mbf_tersoff_eval(b.mbf_system(), dl.mbf_nlist(), tabs, b.reduce_plan(), _lib.MBF_FP64, 8,
+        _lib.check(L.mbf_tersoff_eval(b.mbf_system(), dl.mbf_nlist(), tabs, b.reduce_plan(), _lib.MBF_FP64, self.lanes,
                                       _lib.ptr(self._ws), self._ws.numel(), _lib.ptr(F), _lib.ptr(E), _lib.ptr(W),
                                       st), "mbf_tersoff_eval")
         return E, F, W
@@ -489,6 +590,8 @@ class TersoffFit:
         self.ev = _TableEval(Batch(lats, poss, ids, device=dev), skin) if structs else None
         if not structs:
             return
+        tb0, tri0 = tables_from_records(self.ps.decode(self.ps.x0)["tersoff"], sp, dev)
+        self.tuned = self.ev.autotune(tb0, tri0)
         off = self.ev.batch.offsets
         idx = np.concatenate([np.arange(off[q], off[q] + n) for q, n in enumerate(n_orig)])
         self._orig = torch.as_tensor(idx, device=dev)
@@ -518,8 +621,10 @@ class TersoffFit:
         """This rank's loss as a differentiable torch scalar."""
         if self.ev is None:
             return (x_t.sum() * 0.0).to(self.device)
-        params = self.ps.decode_torch(x_t)
-        tb, tri = tables_from_records(params["tersoff"], self.ps.species, x_t.device)
+        if hasattr(self.ps, "tables_torch"):
+            tb, tri = self.ps.tables_torch(x_t)
+        else:
+            tb, tri = tables_from_records(self.ps.decode_torch(x_t)["tersoff"], self.ps.species, x_t.device)
         E, F, W = TersoffEFS.apply(tb, tri, self.ev)
         w = self.w
         w_E, w_F, w_S = float(w.get("energy", 1.0)), float(w.get("forces", 1.0)), float(w.get("stress", 0.1))

@@ -70,6 +70,21 @@ def test_decode_torch_equals_decode_and_tables(tag):
 
 
 @pytest.mark.parametrize("tag", ["t1989", "multi"])
+def test_vectorised_tables_equal_record_tables(tag):
+    g = golden("fit_sic_t1989")
+    ps = param_sets()[tag]
+    x = torch.tensor(g[f"{tag}_x_test"], dtype=torch.float64, requires_grad=True)
+    tb, tri = ps.tables_torch(x)
+    tb2, tri2 = fit.tables_from_records(ps.decode_torch(x)["tersoff"], SPECIES, "cpu")
+    np.testing.assert_allclose(tb.detach().numpy(), tb2.detach().numpy(), rtol=1e-14, atol=0)
+    np.testing.assert_allclose(tri.detach().numpy(), tri2.detach().numpy(), rtol=1e-14, atol=0)
+    w1, w2 = torch.randn_like(tb), torch.randn_like(tri)
+    (ga,) = torch.autograd.grad((tb * w1).sum() + (tri * w2).sum(), x)
+    (gb,) = torch.autograd.grad((tb2 * w1).sum() + (tri2 * w2).sum(), x)
+    np.testing.assert_allclose(ga.numpy(), gb.numpy(), rtol=1e-12, atol=1e-12 * float(gb.abs().max()))
+
+
+@pytest.mark.parametrize("tag", ["t1989", "multi"])
 def test_oracle_loss_matches_reference(tag):
     g = golden("fit_sic_t1989")
     ps = param_sets()[tag]
