@@ -100,15 +100,13 @@ struct Stencil {
     int pre[33];
 };
 
-__device__ int build_stencil(const SysView &S, const int *__restrict__ grids,
-                             const int *__restrict__ cell_start, const int *__restrict__ atom_cell,
-                             int a, Stencil &st) {
+__device__ int build_stencil_of_cell(const int *__restrict__ grids, const int *__restrict__ cell_start,
+                                     int s, int cell_id, Stencil &st) {
     int lane = threadIdx.x & 31;
-    int s = S.n_struct > 1 ? S.atom_struct[a] : 0;
     const int *g = grids + 8 * s;
     int nc0 = g[0], nc1 = g[1], nc2 = g[2], first = g[3];
     int w0 = g[4], w1 = g[5], w2 = g[6];
-    int local = atom_cell[a] - first;
+    int local = cell_id - first;
     int c2 = local % nc2, c1 = (local / nc2) % nc1, c0 = local / (nc1 * nc2);
     int K = w0 * w1 * w2;
     int len = 0, start = 0;
@@ -145,74 +143,89 @@ __device__ __forceinline__ int stencil_atom(const Stencil &st, const int *__rest
     return cell_atoms[st.start[lo] + (t - st.pre[lo])];
 }
 
-__device__ __forceinline__ bool is_pair(const SysView &S, const double *cell, int a, int b, double rl2) {
-    if (b == a) return false;
+// ---- warp per cell -----------------------------------------------------------
+// The atoms of one cell share their stencil: a warp builds it once, each lane
+// loads one candidate's position per round, and the cell's atoms (32 at a
+// time, one per lane) are broadcast by shuffles and tested against every
+// lane's candidate.  A pair (a, b != a) is listed iff r2 < r_list^2 and
+// r2 > 1e-20, r2 from mic_exact of r_b - r_a: the reference's test in its
+// own operation order (engine/neighborlist.py:350-363).
+__device__ __forceinline__ bool pair_hit(const double *__restrict__ cell, double xa, double ya, double za,
+                                         double xb, double yb, double zb, double rl2) {
     double dx, dy, dz;
-    pair_vec(S, cell, a, b, dx, dy, dz);
+    mic_exact(cell, xb - xa, yb - ya, zb - za, dx, dy, dz);
     double r2 = r2_exact(dx, dy, dz);
     return r2 < rl2 && r2 > 1e-20;
 }
 
-// Warp per atom: count the neighbours within r_list.
-__global__ void nl_count(SysView S, const int *__restrict__ grids, const int *__restrict__ cell_start,
-                         const int *__restrict__ cell_atoms, const int *__restrict__ atom_cell,
-                         double rl2, int *__restrict__ row_cnt, int *__restrict__ max_row) {
+template <bool FILL>
+__global__ void nl_cells(SysView S, const int *__restrict__ grids, const int *__restrict__ cell_start,
+                         const int *__restrict__ cell_atoms, int n_cells, double rl2, int *__restrict__ row_cnt,
+                         int *__restrict__ max_row, const int *__restrict__ row_off, int *__restrict__ nbr) {
     __shared__ Stencil sst[NL_WARPS];
     int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Stencil &st = sst[wid];
-    for (int a = blockIdx.x * NL_WARPS + wid; a < S.n_atoms; a += gridDim.x * NL_WARPS) {
-        int total = build_stencil(S, grids, cell_start, atom_cell, a, st);
-        const double *cell = cell_of(S, a);
-        int cnt = 0;
-        for (int t = lane; t < total; t += 32) {
-            // stencil_atom needs pre[] sorted; empty cells have pre equal to the
-            // next cell's, and the search returns the last such cell, whose
-            // range contains t.
-            int b = stencil_atom(st, cell_atoms, t);
-            cnt += is_pair(S, cell, a, b, rl2) ? 1 : 0;
+    for (int c = blockIdx.x * NL_WARPS + wid; c < n_cells; c += gridDim.x * NL_WARPS) {
+        int cs = cell_start[c], na = cell_start[c + 1] - cs;
+        if (na == 0) continue;  // uniform over the warp
+        int a0 = cell_atoms[cs];
+        int sidx = S.n_struct > 1 ? S.atom_struct[a0] : 0;
+        int total = build_stencil_of_cell(grids, cell_start, sidx, c, st);
+        const double *cell = S.cells + 18 * (size_t)sidx;
+        for (int q0 = 0; q0 < na; q0 += 32) {
+            int nq = min(32, na - q0);
+            int a_l = lane < nq ? cell_atoms[cs + q0 + lane] : 0;
+            double xa_l = S.pos[3 * (size_t)a_l], ya_l = S.pos[3 * (size_t)a_l + 1], za_l = S.pos[3 * (size_t)a_l + 2];
+            int cnt = 0;       // lane q: neighbours of atom q found so far
+            int beg_l = 0, len_l = 0;
+            if (FILL && lane < nq) {
+                beg_l = row_off[a_l];
+                len_l = row_off[a_l + 1] - beg_l;
+            }
+            for (int t0 = 0; t0 < total; t0 += 32) {
+                int t = t0 + lane;
+                int b = -1;
+                double xb = 0, yb = 0, zb = 0;
+                if (t < total) {
+                    b = stencil_atom(st, cell_atoms, t);
+                    xb = S.pos[3 * (size_t)b];
+                    yb = S.pos[3 * (size_t)b + 1];
+                    zb = S.pos[3 * (size_t)b + 2];
+                }
+                for (int q = 0; q < nq; ++q) {
+                    int a = __shfl_sync(MBF_FULL, a_l, q);
+                    double xa = __shfl_sync(MBF_FULL, xa_l, q), ya = __shfl_sync(MBF_FULL, ya_l, q),
+                           za = __shfl_sync(MBF_FULL, za_l, q);
+                    bool hit = b >= 0 && b != a && pair_hit(cell, xa, ya, za, xb, yb, zb, rl2);
+                    unsigned m = __ballot_sync(MBF_FULL, hit);
+                    if (FILL) {
+                        int w = __shfl_sync(MBF_FULL, cnt, q);
+                        int beg = __shfl_sync(MBF_FULL, beg_l, q), len = __shfl_sync(MBF_FULL, len_l, q);
+                        if (hit) {
+                            int pos = w + __popc(m & ((1u << lane) - 1u));
+                            if (pos < len) nbr[beg + pos] = b;
+                        }
+                    }
+                    if (lane == q) cnt += __popc(m);
+                }
+            }
+            if (!FILL && lane < nq) {
+                row_cnt[a_l] = cnt;
+                atomicMax(max_row, cnt);
+            }
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(MBF_FULL, cnt, o);
-        if (lane == 0) {
-            row_cnt[a] = cnt;
-            atomicMax(max_row, cnt);
-        }
-        __syncwarp();
     }
 }
 
-// Warp per atom: write the neighbours (traversal order, by ballot), then
-// sort the row ascending by rank in shared memory.
-__global__ void nl_fill(SysView S, const int *__restrict__ grids, const int *__restrict__ cell_start,
-                        const int *__restrict__ cell_atoms, const int *__restrict__ atom_cell, double rl2,
-                        const int *__restrict__ row_off, int *__restrict__ nbr, int *__restrict__ upper,
-                        int *__restrict__ err) {
-    __shared__ Stencil sst[NL_WARPS];
+// Rows written in traversal order by nl_cells<true>: sort each row
+// ascending (rank sort in shared memory) and record its first upper slot.
+__global__ void nl_sort_rows(int n_atoms, const int *__restrict__ row_off, int *__restrict__ nbr,
+                             int *__restrict__ upper, int *__restrict__ err) {
     __shared__ int srow[NL_WARPS][NL_MAXROW];
     int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    Stencil &st = sst[wid];
     int *row = srow[wid];
-    for (int a = blockIdx.x * NL_WARPS + wid; a < S.n_atoms; a += gridDim.x * NL_WARPS) {
-        int total = build_stencil(S, grids, cell_start, atom_cell, a, st);
-        const double *cell = cell_of(S, a);
+    for (int a = blockIdx.x * NL_WARPS + wid; a < n_atoms; a += gridDim.x * NL_WARPS) {
         int beg = row_off[a], n = row_off[a + 1] - beg;
-        int w = 0;
-        int rounds = (total + 31) & ~31;
-        for (int t = lane; t < rounds; t += 32) {
-            int b = -1;
-            bool hit = false;
-            if (t < total) {
-                b = stencil_atom(st, cell_atoms, t);
-                hit = is_pair(S, cell, a, b, rl2);
-            }
-            unsigned m = __ballot_sync(MBF_FULL, hit);
-            if (hit) {
-                int pos = w + __popc(m & ((1u << lane) - 1u));
-                if (pos < n) nbr[beg + pos] = b;
-            }
-            w += __popc(m);
-        }
-        __syncwarp();
         if (n > NL_MAXROW) {
             if (lane == 0) {
                 atomicOr(err, MBF_DEV_ROW_TOO_LONG);
@@ -400,25 +413,29 @@ static int nl_prepare(const SysView &S, const int *grids, int n_cells_total, dou
     nl_fill_cells<<<(N + 255) / 256, 256, 0, st>>>(N, atom_cell, cursor, cell_atoms);
     nl_sort_cells<<<(n_cells_total + 127) / 128, 128, 0, st>>>(n_cells_total, cell_start, cell_atoms);
     MBF_CHECK_LAUNCH();
-    int blocks = (N + NL_WARPS - 1) / NL_WARPS;
-    int g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_count);
+    int cblocks = (n_cells_total + NL_WARPS - 1) / NL_WARPS;
+    int g = persistent_grid(cblocks, 32 * NL_WARPS, (const void *)nl_cells<false>);
     PROF_BEGIN("nl_count", st);
-    nl_count<<<g, 32 * NL_WARPS, 0, st>>>(S, grids, cell_start, cell_atoms, atom_cell, rl2, row_cnt, mrow);
+    nl_cells<false><<<g, 32 * NL_WARPS, 0, st>>>(S, grids, cell_start, cell_atoms, n_cells_total, rl2, row_cnt, mrow,
+                                                 nullptr, nullptr);
     PROF_END("nl_count", st);
     MBF_CHECK_LAUNCH();
     return exclusive_scan(row_cnt, row_off, N, scan_ws, st);
 }
 
-static int nl_finish(const SysView &S, const int *grids, double rl2, void *workspace, const NlLayout &L,
-                     const int *row_off, int *nbr, int *rev, int *upper, cudaStream_t st) {
+static int nl_finish(const SysView &S, const int *grids, int n_cells_total, double rl2, void *workspace,
+                     const NlLayout &L, const int *row_off, int *nbr, int *rev, int *upper, cudaStream_t st) {
     int N = S.n_atoms;
     int *err = ws_at<int>(workspace, L.err);
     int blocks = (N + NL_WARPS - 1) / NL_WARPS;
-    int g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_fill);
+    int cblocks = (n_cells_total + NL_WARPS - 1) / NL_WARPS;
+    int g = persistent_grid(cblocks, 32 * NL_WARPS, (const void *)nl_cells<true>);
     PROF_BEGIN("nl_fill", st);
-    nl_fill<<<g, 32 * NL_WARPS, 0, st>>>(S, grids, ws_at<int>(workspace, L.cell_start),
-                                         ws_at<int>(workspace, L.cell_atoms), ws_at<int>(workspace, L.atom_cell),
-                                         rl2, row_off, nbr, upper, err);
+    nl_cells<true><<<g, 32 * NL_WARPS, 0, st>>>(S, grids, ws_at<int>(workspace, L.cell_start),
+                                                ws_at<int>(workspace, L.cell_atoms), n_cells_total, rl2, nullptr,
+                                                nullptr, row_off, nbr);
+    g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_sort_rows);
+    nl_sort_rows<<<g, 32 * NL_WARPS, 0, st>>>(N, row_off, nbr, upper, err);
     PROF_END("nl_fill", st);
     MBF_CHECK_LAUNCH();
     g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_reverse);
@@ -460,7 +477,7 @@ int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total, dou
     if ((long long)host[0] > nbr_capacity || !nbr || !rev) return MBF_ERR_CAPACITY;
     if (!upper) return MBF_ERR_ARGUMENT;
     if (host[1] > NL_MAXROW) return MBF_ERR_ROW_TOO_LONG;
-    rc = nl_finish(S, grids, rl2, workspace, L, row_off, nbr, rev, upper, st);
+    rc = nl_finish(S, grids, n_cells_total, rl2, workspace, L, row_off, nbr, rev, upper, st);
     if (rc != MBF_OK) return rc;
     int herr = 0;
     if (cudaMemcpyAsync(&herr, ws_at<int>(workspace, L.err), sizeof(int), cudaMemcpyDeviceToHost, st) !=
@@ -492,7 +509,7 @@ int mbf_nl_rebuild_async(const mbf_system *sys, const int *grids, int n_cells_to
                                err + 4);
     nl_clear_if<<<(N + 256) / 256, 256, 0, st>>>(N, err + 4, row_off, upper);
     MBF_CHECK_LAUNCH();
-    rc = nl_finish(S, grids, rl2, workspace, L, row_off, nbr, rev, upper, st);
+    rc = nl_finish(S, grids, n_cells_total, rl2, workspace, L, row_off, nbr, rev, upper, st);
     if (rc != MBF_OK) return rc;
     nl_status_merge<<<1, 32, 0, st>>>(err, status);
     MBF_CHECK_LAUNCH();
