@@ -94,6 +94,15 @@ _SIGS = {
     "mbf_tersoff_eval": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                               ctypes.POINTER(MbfTersoffTables), ctypes.POINTER(MbfReducePlan), _i, _i,
                               _vp, _sz, _vp, _vp, _vp, _vp]),
+    "mbf_tersoff_eval_sites": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
+                                    ctypes.POINTER(MbfTersoffTables), ctypes.POINTER(MbfReducePlan), _i, _i,
+                                    _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "mbf_sw_eval_sites": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
+                               ctypes.POINTER(MbfSwTables), ctypes.POINTER(MbfReducePlan), _i, _i,
+                               _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "mbf_eam_eval_sites": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
+                                ctypes.POINTER(MbfEamTables), ctypes.POINTER(MbfReducePlan), _i, _i,
+                                _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mbf_tersoff_adjoint_workspace_bytes": (_sz, [_ll, _i]),
     "mbf_tersoff_adjoint": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                                  ctypes.POINTER(MbfTersoffTables), _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp]),

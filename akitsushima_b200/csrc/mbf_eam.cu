@@ -579,9 +579,73 @@ __global__ void eam_gather(int n_atoms, const int *__restrict__ row_off, const i
     }
 }
 
+// Site terms (engine/site_terms.py:440-479): U_i = F_i(rho-bar_i) + 1/2
+// sum_j phi_ij and dU_i/dv_ij = (F'_i rho'_{s_j}(r) + 1/2 phi'(r)) v / r over
+// the full row, after the density and embedding passes; v for every slot.
+template <typename T, int LPA, bool ZHOU, bool ORTHO>
+__global__ void __launch_bounds__(EAM_BLOCK) eam_site(SysView S, const int *__restrict__ row_off,
+                                                      const int *__restrict__ nbr, EamDev E,
+                                                      const double4 *__restrict__ pk,
+                                                      const double *__restrict__ aux, SiteOut so, Chk ck) {
+    __shared__ ZTab<T> Z;
+    if (ZHOU) load_ztab<T>(E, Z);
+    const int sub = threadIdx.x & (LPA - 1);
+    const int gpb = EAM_BLOCK / LPA;
+    const double rc = E.r_cut, rc2 = rc * rc;
+    for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
+        int i = base + threadIdx.x / LPA;
+        double e = 0.0;
+        if (i < S.n_atoms) {
+            int si = S.types[i];
+            if (!MBF_OK_IDX(ck, 51, si, 0, ck.ns)) si = 0;
+            CellView<ORTHO> cv;
+            cv.load(S, i);
+            double4 pi = ld_pack(pk, i);
+            double Fp = aux[2 * (size_t)i];
+            int end = row_off[i + 1];
+            if (!MBF_OK_IDX(ck, 52, end, 0, ck.n_slots + 1)) end = row_off[i];
+            for (int s = row_off[i] + sub; s < end; s += LPA) {
+                int j = nbr[s];
+                if (!MBF_OK_IDX(ck, 53, j, 0, ck.n_atoms)) continue;
+                int sj = __ldg(S.types + j);
+                if (!MBF_OK_IDX(ck, 54, sj, 0, ck.ns)) sj = 0;
+                double4 pj = ld_pack(pk, j);
+                double dx, dy, dz;
+                cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
+                double r2 = dx * dx + dy * dy + dz * dz;
+                size_t o = 3 * (size_t)s;
+                so.vec[o] = dx;
+                so.vec[o + 1] = dy;
+                so.vec[o + 2] = dz;
+                double c = 0.0;
+                if (r2 < rc2 && r2 > 1e-24) {
+                    T phi, dphi, drho_j, drho_i;
+                    if (ZHOU) {
+                        zhou_pair_terms<T>(Z, si, sj, pair_dist<T>(r2), phi, dphi, drho_j, drho_i);
+                    } else {
+                        double rr = sqrt(r2);
+                        T rj;
+                        feval<T>(E, E.phi_f[si * E.ns + sj], rr, phi, dphi);
+                        feval<T>(E, E.rho_f[sj], rr, rj, drho_j);
+                    }
+                    double r = sqrt(r2);
+                    e += 0.5 * (double)phi;
+                    c = (Fp * (double)drho_j + 0.5 * (double)dphi) / r;
+                }
+                so.dudv[o] = c * dx;
+                so.dudv[o + 1] = c * dy;
+                so.dudv[o + 2] = c * dz;
+            }
+        }
+        e = group_sum<LPA>(e);
+        if (sub == 0 && i < S.n_atoms) so.e[i] = e + aux[2 * (size_t)i + 1];
+    }
+}
+
 template <typename T, int LPA, bool ZHOU, bool ORTHO>
 static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, double4 *pk, double *aux,
-                      void *slot, double *f_local, double *forces, double *per_atom, Chk ck, cudaStream_t st) {
+                      void *slot, double *f_local, double *forces, double *per_atom, Chk ck, const SiteOut &so,
+                      cudaStream_t st) {
     typedef typename SlotVec<T>::type V3;
     int gpb = EAM_BLOCK / LPA;
     int blocks = (S.n_atoms + gpb - 1) / gpb;
@@ -608,20 +672,25 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, do
                                                              (const V3 *)slot, f_local, forces, ck);
     PROF_END("eam_gather", st);
     MBF_CHECK_LAUNCH();
+    if (so.e) {
+        g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_site<T, LPA, ZHOU, ORTHO>);
+        eam_site<T, LPA, ZHOU, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, E, pk, aux, so, ck);
+        MBF_CHECK_LAUNCH();
+    }
     return MBF_OK;
 }
 
 template <typename T, bool ZHOU, bool ORTHO>
 static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E, double4 *pk,
                             double *aux, void *slot, double *f_local, double *forces, double *per_atom,
-                            Chk ck, cudaStream_t st) {
+                            Chk ck, const SiteOut &so, cudaStream_t st) {
     switch (lpa) {
-        case 1: return eam_launch<T, 1, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
-        case 2: return eam_launch<T, 2, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
-        case 4: return eam_launch<T, 4, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
-        case 8: return eam_launch<T, 8, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
-        case 16: return eam_launch<T, 16, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
-        case 32: return eam_launch<T, 32, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
+        case 1: return eam_launch<T, 1, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
+        case 2: return eam_launch<T, 2, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
+        case 4: return eam_launch<T, 4, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
+        case 8: return eam_launch<T, 8, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
+        case 16: return eam_launch<T, 16, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
+        case 32: return eam_launch<T, 32, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
         default: return MBF_ERR_ARGUMENT;
     }
 }
@@ -629,22 +698,22 @@ static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, cons
 template <typename T>
 static int eam_dispatch(bool zhou, int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E,
                         double4 *pk, double *aux, void *slot, double *f_local, double *forces,
-                        double *per_atom, Chk ck, cudaStream_t st) {
+                        double *per_atom, Chk ck, const SiteOut &so, cudaStream_t st) {
     if (zhou)
-        return S.ortho ? eam_dispatch_lpa<T, true, true>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st)
-                       : eam_dispatch_lpa<T, true, false>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
-    return S.ortho ? eam_dispatch_lpa<T, false, true>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st)
-                   : eam_dispatch_lpa<T, false, false>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, st);
+        return S.ortho ? eam_dispatch_lpa<T, true, true>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st)
+                       : eam_dispatch_lpa<T, true, false>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
+    return S.ortho ? eam_dispatch_lpa<T, false, true>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st)
+                   : eam_dispatch_lpa<T, false, false>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
 }
 
 }  // namespace mbf
 
 using namespace mbf;
 
-extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
-                            const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
-                            void *workspace, size_t workspace_bytes, double *forces, double *energy,
-                            double *virial, void *stream) {
+static int eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                    const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
+                    size_t workspace_bytes, double *forces, double *energy, double *virial, const SiteOut &so,
+                    void *stream) {
     if (!sys || !nl || !tab || !plan || !workspace || !forces || !energy || !virial) return MBF_ERR_ARGUMENT;
     if (precision != MBF_FP64 && precision != MBF_MIXED) return MBF_ERR_ARGUMENT;
     if (nl->n_atoms != sys->n_atoms || tab->ns <= 0) return MBF_ERR_ARGUMENT;
@@ -680,11 +749,30 @@ extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mb
     bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
     int rc;
     if (precision == MBF_FP64)
-        rc = eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, st);
+        rc = eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, so, st);
     else
-        rc = eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, st);
+        rc = eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, so, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
+}
+
+extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                            const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
+                            void *workspace, size_t workspace_bytes, double *forces, double *energy,
+                            double *virial, void *stream) {
+    SiteOut none = {nullptr, nullptr, nullptr};
+    return eam_eval(sys, nl, tab, plan, precision, lanes_per_atom, workspace, workspace_bytes, forces, energy,
+                    virial, none, stream);
+}
+
+extern "C" int mbf_eam_eval_sites(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                                  const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
+                                  size_t workspace_bytes, double *forces, double *energy, double *virial,
+                                  double *site_e, double *site_dudv, double *site_vec, void *stream) {
+    if (!site_e || !site_dudv || !site_vec) return MBF_ERR_ARGUMENT;
+    SiteOut so = {site_e, site_dudv, site_vec};
+    return eam_eval(sys, nl, tab, plan, precision, lanes_per_atom, workspace, workspace_bytes, forces, energy,
+                    virial, so, stream);
 }
 
 // ---- the same evaluation without any allocation -----------------------------
@@ -765,9 +853,9 @@ extern "C" int mbf_eam_eval_static(const mbf_system *sys, const mbf_nlist *nl, c
     int lpa = lanes_per_atom > 0 ? lanes_per_atom : 8;
     bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
     if (precision == MBF_FP64)
-        rc = eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, st);
+        rc = eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, SiteOut{}, st);
     else
-        rc = eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, st);
+        rc = eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, SiteOut{}, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
 }

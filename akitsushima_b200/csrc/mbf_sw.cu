@@ -69,7 +69,7 @@ struct SwRow {
 template <typename T, int MAXN, bool SYM, int LPA>
 __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr,
                          const int *__restrict__ rev, SwDev P, double *__restrict__ slot_G, double *__restrict__ f_local,
-                         double *__restrict__ per_atom, int *__restrict__ err) {
+                         double *__restrict__ per_atom, int *__restrict__ err, SiteOut so) {
     constexpr int GPB = SwGeom<MAXN, LPA>::GPB;
     __shared__ SwRow<T, MAXN> rows[GPB];
     const int sub = threadIdx.x & (LPA - 1);
@@ -105,6 +105,12 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
                               S.pos[3 * (size_t)j + 2] - zi, dx, dy, dz);
                     double r = sqrt(dx * dx + dy * dy + dz * dz);
                     ok = r < P.rc && r > 1e-12;
+                    if (so.vec) {
+                        size_t os = 3 * (size_t)(beg + s);
+                        so.vec[os] = dx;
+                        so.vec[os + 1] = dy;
+                        so.vec[os + 2] = dz;
+                    }
                     if (ok) {
                         int sj = S.types[j];
                         const double *ls = P.leg + 4 * (si * ns + sj);
@@ -221,6 +227,12 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
                 v[6] += -hz * dx + Gz * dx;
                 v[7] += -hz * dy + Gz * dy;
                 v[8] += -hz * dz + Gz * dz;
+                if (so.dudv) {  // U_i = 1/2 sum V2 + angles at i (engine/site_terms.py:179-300)
+                    size_t os = 3 * (size_t)(beg + s);
+                    so.dudv[os] = 0.5 * cx * dx - Gx;
+                    so.dudv[os + 1] = 0.5 * cx * dy - Gy;
+                    so.dudv[os + 2] = 0.5 * cx * dz - Gz;
+                }
                 // the force on neighbour j goes to j's own slot (j -> i)
                 size_t o = 3 * (size_t)rev[beg + s];
                 slot_G[o] = Gx;
@@ -234,6 +246,7 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
         e = group_sum<LPA>(e);
 #pragma unroll
         for (int q = 0; q < 9; ++q) v[q] = group_sum<LPA>(v[q]);
+        if (sub == 0 && i < S.n_atoms && so.e) so.e[i] = e;
         if (sub == 0 && i < S.n_atoms) {
             f_local[3 * (size_t)i] = fx;
             f_local[3 * (size_t)i + 1] = fy;
@@ -250,12 +263,13 @@ __global__ void sw_force(SysView S, const int *__restrict__ row_off, const int *
 
 template <typename T, int MAXN, bool SYM, int LPA>
 static int sw_launch(const SysView &S, const mbf_nlist *nl, const SwDev &P, double *slot_G, double *f_local,
-                     double *per_atom, double *forces, int *err, cudaStream_t st) {
+                     double *per_atom, double *forces, int *err, const SiteOut &so, cudaStream_t st) {
     constexpr int GPB = SwGeom<MAXN, LPA>::GPB, BLOCK = SwGeom<MAXN, LPA>::BLOCK;
     int blocks = (S.n_atoms + GPB - 1) / GPB;
     int g = persistent_grid(blocks, BLOCK, (const void *)sw_force<T, MAXN, SYM, LPA>);
     PROF_BEGIN("sw_force", st);
-    sw_force<T, MAXN, SYM, LPA><<<g, BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, nl->rev, P, slot_G, f_local, per_atom, err);
+    sw_force<T, MAXN, SYM, LPA><<<g, BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, nl->rev, P, slot_G, f_local, per_atom, err,
+                                                     so);
     PROF_END("sw_force", st);
     MBF_CHECK_LAUNCH();
     return gather_forces(S.n_atoms, nl->row_off, slot_G, f_local, forces, st);
@@ -263,32 +277,33 @@ static int sw_launch(const SysView &S, const mbf_nlist *nl, const SwDev &P, doub
 
 template <typename T, int MAXN, bool SYM>
 static int sw_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const SwDev &P, double *slot_G, double *f_local,
-                  double *per_atom, double *forces, int *err, cudaStream_t st) {
+                  double *per_atom, double *forces, int *err, const SiteOut &so, cudaStream_t st) {
     switch (lpa) {
-        case 4: return sw_launch<T, MAXN, SYM, 4>(S, nl, P, slot_G, f_local, per_atom, forces, err, st);
-        case 8: return sw_launch<T, MAXN, SYM, 8>(S, nl, P, slot_G, f_local, per_atom, forces, err, st);
-        case 16: return sw_launch<T, MAXN, SYM, 16>(S, nl, P, slot_G, f_local, per_atom, forces, err, st);
+        case 4: return sw_launch<T, MAXN, SYM, 4>(S, nl, P, slot_G, f_local, per_atom, forces, err, so, st);
+        case 8: return sw_launch<T, MAXN, SYM, 8>(S, nl, P, slot_G, f_local, per_atom, forces, err, so, st);
+        case 16: return sw_launch<T, MAXN, SYM, 16>(S, nl, P, slot_G, f_local, per_atom, forces, err, so, st);
         default: return MBF_ERR_ARGUMENT;
     }
 }
 
 template <typename T, bool SYM>
 static int sw_dispatch(int mr, int lpa, const SysView &S, const mbf_nlist *nl, const SwDev &P, double *slot_G,
-                       double *f_local, double *per_atom, double *forces, int *err, cudaStream_t st) {
+                       double *f_local, double *per_atom, double *forces, int *err, const SiteOut &so,
+                       cudaStream_t st) {
     if (lpa <= 0) lpa = 8;
-    if (mr <= 32) return sw_lpa<T, 32, SYM>(lpa, S, nl, P, slot_G, f_local, per_atom, forces, err, st);
-    if (mr <= 64) return sw_lpa<T, 64, SYM>(lpa, S, nl, P, slot_G, f_local, per_atom, forces, err, st);
-    return sw_lpa<T, 128, SYM>(lpa, S, nl, P, slot_G, f_local, per_atom, forces, err, st);
+    if (mr <= 32) return sw_lpa<T, 32, SYM>(lpa, S, nl, P, slot_G, f_local, per_atom, forces, err, so, st);
+    if (mr <= 64) return sw_lpa<T, 64, SYM>(lpa, S, nl, P, slot_G, f_local, per_atom, forces, err, so, st);
+    return sw_lpa<T, 128, SYM>(lpa, S, nl, P, slot_G, f_local, per_atom, forces, err, so, st);
 }
 
 }  // namespace mbf
 
 using namespace mbf;
 
-extern "C" int mbf_sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables *tab,
-                           const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
-                           size_t workspace_bytes,
-                           double *forces, double *energy, double *virial, void *stream) {
+static int sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables *tab,
+                   const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
+                   size_t workspace_bytes, double *forces, double *energy, double *virial, const SiteOut &so,
+                   void *stream) {
     if (!sys || !nl || !tab || !plan || !workspace || !forces || !energy || !virial) return MBF_ERR_ARGUMENT;
     if (precision != MBF_FP64 && precision != MBF_MIXED) return MBF_ERR_ARGUMENT;
     if (nl->n_atoms != sys->n_atoms || tab->ns <= 0) return MBF_ERR_ARGUMENT;
@@ -318,11 +333,32 @@ extern "C" int mbf_sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf
     bool sym = tab->ns == 1;
     int rc;
     if (precision == MBF_FP64)
-        rc = sym ? sw_dispatch<double, true>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, st)
-                 : sw_dispatch<double, false>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, st);
+        rc = sym ? sw_dispatch<double, true>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, so, st)
+                 : sw_dispatch<double, false>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, so, st);
     else
-        rc = sym ? sw_dispatch<float, true>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, st)
-                 : sw_dispatch<float, false>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, st);
+        rc = sym ? sw_dispatch<float, true>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, so, st)
+                 : sw_dispatch<float, false>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, so, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
+}
+
+extern "C" int mbf_sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables *tab,
+                           const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
+                           size_t workspace_bytes, double *forces, double *energy, double *virial, void *stream) {
+    SiteOut none = {nullptr, nullptr, nullptr};
+    return sw_eval(sys, nl, tab, plan, precision, lanes_per_atom, workspace, workspace_bytes, forces, energy, virial,
+                   none, stream);
+}
+
+extern "C" int mbf_sw_eval_sites(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables *tab,
+                                 const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
+                                 size_t workspace_bytes, double *forces, double *energy, double *virial,
+                                 double *site_e, double *site_dudv, double *site_vec, void *stream) {
+    if (!site_e || !site_dudv || !site_vec) return MBF_ERR_ARGUMENT;
+    if (nl && nl->n_slots > 0 &&
+        cudaMemsetAsync(site_dudv, 0, sizeof(double) * 3 * (size_t)nl->n_slots, (cudaStream_t)stream) != cudaSuccess)
+        return MBF_ERR_CUDA;
+    SiteOut so = {site_e, site_dudv, site_vec};
+    return sw_eval(sys, nl, tab, plan, precision, lanes_per_atom, workspace, workspace_bytes, forces, energy, virial,
+                   so, stream);
 }

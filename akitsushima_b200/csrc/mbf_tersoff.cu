@@ -187,7 +187,7 @@ template <typename T, int MAXN, int LPA>
 __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr,
                          const int *__restrict__ rev, TeDev P, const double *__restrict__ slot_b,
                          double *__restrict__ slot_G, double *__restrict__ f_local,
-                         double *__restrict__ per_atom, int *__restrict__ err) {
+                         double *__restrict__ per_atom, int *__restrict__ err, SiteOut so) {
     constexpr int GPB = TeGeom<MAXN, LPA>::GPB;
     __shared__ TeRow<T, MAXN> rows[GPB];
     const int sub = threadIdx.x & (LPA - 1);
@@ -207,11 +207,12 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
         }
         if (live) te_stage<T, MAXN, LPA>(S, nbr, i, beg, n, P.rc, R, sub);
         __syncwarp();
-        double fx = 0, fy = 0, fz = 0, e = 0, npair = 0;
+        double fx = 0, fy = 0, fz = 0, e = 0, npair = 0, e_site = 0;
         double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         int si = live ? S.types[i] : 0;
         // pass 1: pair terms and the zeta-gradient coefficients
         double cxs[(MAXN + LPA - 1) / LPA];
+        double cxs_site[(MAXN + LPA - 1) / LPA];  // site split: own bond order (engine/site_terms.py:312-437)
         double pair_r[(MAXN + LPA - 1) / LPA];
         if (live) {
             const double *cell = cell_of(S, i);
@@ -226,7 +227,7 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
                     pair_r[q] = sqrt(dx * dx + dy * dy + dz * dz);
                 }
                 T coef = T(0);
-                double cx = 0.0;
+                double cx = 0.0, cx_site = 0.0;
                 if (R.ok[s]) {
                     int j = nbr[beg + s];
                     int sj = R.sp[s];
@@ -249,12 +250,17 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
                             e += 0.5 * (fc * (fr + bavg * fa));
                             double dEdr = dfc * (fr + bavg * fa) + fc * (-l1 * fr + bavg * (-l2 * fa));
                             cx = dEdr / r;
+                            if (so.dudv) {
+                                e_site += 0.5 * (fc * (fr + b_own * fa));
+                                cx_site = 0.5 * (dfc * (fr + b_own * fa) + fc * (-l1 * fr - l2 * b_own * fa)) / r;
+                            }
                             if (fabs(db_own) > 1e-30) coef = (T)(0.5 * fc * fa * db_own);
                         }
                     }
                 }
                 R.coef[s] = coef;
                 cxs[q] = cx;
+                cxs_site[q] = cx_site;
             }
         }
         __syncwarp();
@@ -325,6 +331,16 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
                 v[7] += -hz * dy + Gz * dy;
                 v[8] += -hz * dz + Gz * dz;
                 npair += R.ok[s] ? 1.0 : 0.0;
+                if (so.dudv) {
+                    size_t os = 3 * (size_t)(beg + s);
+                    double cs_ = cxs_site[q];
+                    so.dudv[os] = cs_ * dx - Gx;
+                    so.dudv[os + 1] = cs_ * dy - Gy;
+                    so.dudv[os + 2] = cs_ * dz - Gz;
+                    so.vec[os] = dx;
+                    so.vec[os + 1] = dy;
+                    so.vec[os + 2] = dz;
+                }
                 // the force on neighbour x goes to x's own slot (x -> i)
                 size_t o = 3 * (size_t)rev[beg + s];
                 slot_G[o] = Gx;
@@ -337,8 +353,10 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
         fz = group_sum<LPA>(fz);
         e = group_sum<LPA>(e);
         npair = group_sum<LPA>(npair);
+        e_site = group_sum<LPA>(e_site);
 #pragma unroll
         for (int q = 0; q < 9; ++q) v[q] = group_sum<LPA>(v[q]);
+        if (sub == 0 && i < S.n_atoms && so.e) so.e[i] = e_site;
         if (sub == 0 && i < S.n_atoms) {
             f_local[3 * (size_t)i] = fx;
             f_local[3 * (size_t)i + 1] = fy;
@@ -355,7 +373,8 @@ __global__ void te_force(SysView S, const int *__restrict__ row_off, const int *
 
 template <typename T, int MAXN, int LPA>
 static int te_launch(const SysView &S, const mbf_nlist *nl, const TeDev &P, double *slot_b, double *slot_G,
-                     double *f_local, double *per_atom, double *forces, int *err, cudaStream_t st) {
+                     double *f_local, double *per_atom, double *forces, int *err, const SiteOut &so,
+                     cudaStream_t st) {
     constexpr int GPB = TeGeom<MAXN, LPA>::GPB, BLOCK = TeGeom<MAXN, LPA>::BLOCK;
     int blocks = (S.n_atoms + GPB - 1) / GPB;
     int g = persistent_grid(blocks, BLOCK, (const void *)te_zeta<T, MAXN, LPA>);
@@ -366,7 +385,7 @@ static int te_launch(const SysView &S, const mbf_nlist *nl, const TeDev &P, doub
     g = persistent_grid(blocks, BLOCK, (const void *)te_force<T, MAXN, LPA>);
     PROF_BEGIN("te_force", st);
     te_force<T, MAXN, LPA><<<g, BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, nl->rev, P, slot_b, slot_G, f_local,
-                                         per_atom, err);
+                                         per_atom, err, so);
     PROF_END("te_force", st);
     MBF_CHECK_LAUNCH();
     return gather_forces(S.n_atoms, nl->row_off, slot_G, f_local, forces, st);
@@ -374,40 +393,42 @@ static int te_launch(const SysView &S, const mbf_nlist *nl, const TeDev &P, doub
 
 template <typename T, int MAXN>
 static int te_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const TeDev &P, double *slot_b,
-                  double *slot_G, double *f_local, double *per_atom, double *forces, int *err, cudaStream_t st) {
+                  double *slot_G, double *f_local, double *per_atom, double *forces, int *err, const SiteOut &so,
+                  cudaStream_t st) {
     switch (lpa) {
-        case 4: return te_launch<T, MAXN, 4>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
-        case 8: return te_launch<T, MAXN, 8>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
-        case 16: return te_launch<T, MAXN, 16>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
+        case 4: return te_launch<T, MAXN, 4>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, so, st);
+        case 8: return te_launch<T, MAXN, 8>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, so, st);
+        case 16: return te_launch<T, MAXN, 16>(S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, so, st);
         default: return MBF_ERR_ARGUMENT;
     }
 }
 
 template <typename T>
 static int te_rows(int mr, int lpa, const SysView &S, const mbf_nlist *nl, const TeDev &P, double *slot_b,
-                   double *slot_G, double *f_local, double *per_atom, double *forces, int *err, cudaStream_t st) {
-    if (mr <= 32) return te_lpa<T, 32>(lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
-    if (mr <= 64) return te_lpa<T, 64>(lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
-    return te_lpa<T, 128>(lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
+                   double *slot_G, double *f_local, double *per_atom, double *forces, int *err, const SiteOut &so,
+                   cudaStream_t st) {
+    if (mr <= 32) return te_lpa<T, 32>(lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, so, st);
+    if (mr <= 64) return te_lpa<T, 64>(lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, so, st);
+    return te_lpa<T, 128>(lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, so, st);
 }
 
 static int te_dispatch(int precision, int mr, int lpa, const SysView &S, const mbf_nlist *nl, const TeDev &P,
                        double *slot_b, double *slot_G, double *f_local, double *per_atom, double *forces,
-                       int *err, cudaStream_t st) {
+                       int *err, const SiteOut &so, cudaStream_t st) {
     if (lpa <= 0) lpa = 8;
     return precision == MBF_FP64
-               ? te_rows<double>(mr, lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st)
-               : te_rows<float>(mr, lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, st);
+               ? te_rows<double>(mr, lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, so, st)
+               : te_rows<float>(mr, lpa, S, nl, P, slot_b, slot_G, f_local, per_atom, forces, err, so, st);
 }
 
 }  // namespace mbf
 
 using namespace mbf;
 
-extern "C" int mbf_tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_tersoff_tables *tab,
-                                const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
-                                size_t workspace_bytes, double *forces, double *energy, double *virial,
-                                void *stream) {
+static int tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_tersoff_tables *tab,
+                        const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
+                        size_t workspace_bytes, double *forces, double *energy, double *virial, const SiteOut &so,
+                        void *stream) {
     if (!sys || !nl || !tab || !plan || !workspace || !forces || !energy || !virial) return MBF_ERR_ARGUMENT;
     if (precision != MBF_FP64 && precision != MBF_MIXED) return MBF_ERR_ARGUMENT;
     if (nl->n_atoms != sys->n_atoms || tab->ns <= 0) return MBF_ERR_ARGUMENT;
@@ -434,7 +455,30 @@ extern "C" int mbf_tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, cons
     double *slot_b = ws_at<double>(workspace, L.slot_b);
     double *partial = ws_at<double>(workspace, L.partial);
     int rc = te_dispatch(precision, nl->max_row, lanes_per_atom, S, nl, P, slot_b, slot_G, f_local, per_atom,
-                         forces, err, st);
+                         forces, err, so, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
+}
+
+extern "C" int mbf_tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_tersoff_tables *tab,
+                                const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
+                                size_t workspace_bytes, double *forces, double *energy, double *virial,
+                                void *stream) {
+    SiteOut none = {nullptr, nullptr, nullptr};
+    return tersoff_eval(sys, nl, tab, plan, precision, lanes_per_atom, workspace, workspace_bytes, forces, energy,
+                        virial, none, stream);
+}
+
+extern "C" int mbf_tersoff_eval_sites(const mbf_system *sys, const mbf_nlist *nl, const mbf_tersoff_tables *tab,
+                                      const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
+                                      void *workspace, size_t workspace_bytes, double *forces, double *energy,
+                                      double *virial, double *site_e, double *site_dudv, double *site_vec,
+                                      void *stream) {
+    if (!site_e || !site_dudv || !site_vec) return MBF_ERR_ARGUMENT;
+    if (nl && nl->n_slots > 0 &&
+        cudaMemsetAsync(site_dudv, 0, sizeof(double) * 3 * (size_t)nl->n_slots, (cudaStream_t)stream) != cudaSuccess)
+        return MBF_ERR_CUDA;
+    SiteOut so = {site_e, site_dudv, site_vec};
+    return tersoff_eval(sys, nl, tab, plan, precision, lanes_per_atom, workspace, workspace_bytes, forces, energy,
+                        virial, so, stream);
 }

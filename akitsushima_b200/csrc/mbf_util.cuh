@@ -22,6 +22,16 @@ int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, in
 int gather_forces(int n_atoms, const int *row_off, const double *G, const double *f_local, double *forces,
                   cudaStream_t st);
 
+// Optional site-term outputs of an evaluation (all null: none): the site
+// energy U_i per atom and, per list slot, dU_centre/dv and v (the
+// minimum-image vector centre -> neighbour); slots outside the cutoff get
+// dU/dv = 0.
+struct SiteOut {
+    double *e;     // (n_atoms,)
+    double *dudv;  // (n_slots, 3)
+    double *vec;   // (n_slots, 3)
+};
+
 // Layout of the evaluation workspace (all offsets 256-byte aligned):
 //   err      device error word (int)
 //   per_atom (n_atoms, ATOM_ACC) doubles

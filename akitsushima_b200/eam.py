@@ -268,6 +268,7 @@ class EAMPotential(DevicePotential):
         return (st, keep)
 
     # lanes of one atom's group: 2 measured fastest on B200 (256k Cu-Ni, both precisions)
+    sites_entry = "mbf_eam_eval_sites"
     lane_choices = (1, 2, 4, 8, 16, 32)
     lanes_per_atom = 2
 

@@ -109,6 +109,30 @@ class DevicePotential:
         self._last_ws = ws
         return out
 
+    def evaluate_sites(self, batch, dlist, precision=None):
+        """evaluate() plus the site-energy decomposition (heat flux): returns
+        (EvalResult, site_e (N,), dU/dv (n_slots, 3), v (n_slots, 3)) on the
+        device; slots beyond the cutoff have dU/dv = 0."""
+        prec = precision_code(precision or self.precision)
+        dev = batch.device
+        L = _lib.lib()
+        nbytes = int(L.mbf_eval_workspace_bytes(batch.n_atoms, dlist.n_slots, batch.n_chunks))
+        ws = workspace(dev, nbytes)
+        f64 = dict(dtype=torch.float64, device=dev)
+        out = EvalResult(torch.empty(batch.n_struct, **f64), torch.empty((batch.n_atoms, 3), **f64),
+                         torch.empty((batch.n_struct, 9), **f64))
+        e = torch.empty(batch.n_atoms, **f64)
+        dudv = torch.zeros((max(int(dlist.n_slots), 1), 3), **f64)
+        vec = torch.zeros((max(int(dlist.n_slots), 1), 3), **f64)
+        tabs = self.tables(dev)
+        rc = getattr(L, self.sites_entry)(batch.mbf_system(), dlist.mbf_nlist(), tabs[0], batch.reduce_plan(), prec,
+                                          int(self.lanes_per_atom), _lib.ptr(ws), ws.numel(), _lib.ptr(out.forces),
+                                          _lib.ptr(out.energy), _lib.ptr(out.virial), _lib.ptr(e), _lib.ptr(dudv),
+                                          _lib.ptr(vec), torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(rc, type(self).__name__ + ".evaluate_sites")
+        self._last_ws = ws
+        return out, e, dudv, vec
+
     def autotune_lanes(self, batch, dlist, candidates=None, reps=3, ws=None, out=None):
         """Time every lanes-per-atom candidate on this batch (CUDA events,
         after one untimed call each), keep the fastest and return

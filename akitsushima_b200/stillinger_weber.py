@@ -124,6 +124,7 @@ class StillingerWeberPotential(DevicePotential):
         st = _lib.MbfSwTables(len(self.species), _lib.ptr(t[0]), _lib.ptr(t[1]), _lib.ptr(t[2]), rc)
         return (st, *t)
 
+    sites_entry = "mbf_sw_eval_sites"
     lane_choices = (4, 8, 16)
     lanes_per_atom = 8
 

@@ -102,6 +102,7 @@ class TersoffPotential(DevicePotential):
         st = _lib.MbfTersoffTables(len(self.species), _lib.ptr(tb_t), _lib.ptr(tri_t), self.r_cut)
         return (st, tb_t, tri_t)
 
+    sites_entry = "mbf_tersoff_eval_sites"
     lane_choices = (4, 8, 16)
     lanes_per_atom = 8
 

@@ -282,6 +282,34 @@ int mbf_sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables 
  * and writes "name launches total_ms" lines to buf.  Returns the number of
  * kernels listed.  No counterpart in the reference (its timing is
  * benchmarks/bench_force.py's wall clock).                                */
+/* ---- site terms (heat flux) --------------------------------------------
+ * mbf_*_eval_sites: the evaluation above plus the site-energy
+ * decomposition of the reference's engine/site_terms.py:1-83 (Green-Kubo
+ * heat flux, Fan et al. PRB 92, 094301): site_e (n_atoms) U_i, and per list
+ * slot (centre i -> neighbour j) site_dudv (n_slots, 3) = dU_i/dv_ij and
+ * site_vec (n_slots, 3) = v_ij (minimum image); slots beyond the cutoff get
+ * dU/dv = 0.  Energy conventions per potential as the reference's
+ * tersoff_site_terms (:312-437, U_i += fc (fR + b_ij fA) / 2 with the
+ * centre's own bond order), sw_site_terms (:179-300, half the two-body term
+ * plus the angles centred on i) and eam_site_terms (:440-479, F_i + half
+ * the pair terms).  F_k = sum_m dUdv_m (delta_k,centre - delta_k,nbr)
+ * rebuilds the forces.                                                    */
+int mbf_tersoff_eval_sites(const mbf_system *sys, const mbf_nlist *nl,
+                           const mbf_tersoff_tables *tab, const mbf_reduce_plan *plan,
+                           int precision, int lanes_per_atom, void *workspace,
+                           size_t workspace_bytes, double *forces, double *energy, double *virial,
+                           double *site_e, double *site_dudv, double *site_vec, void *stream);
+int mbf_sw_eval_sites(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables *tab,
+                      const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
+                      void *workspace, size_t workspace_bytes, double *forces, double *energy,
+                      double *virial, double *site_e, double *site_dudv, double *site_vec,
+                      void *stream);
+int mbf_eam_eval_sites(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                       const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
+                       void *workspace, size_t workspace_bytes, double *forces, double *energy,
+                       double *virial, double *site_e, double *site_dudv, double *site_vec,
+                       void *stream);
+
 /* ---- velocity-Verlet NVE on the device ---------------------------------
  * The integrator of NVESimulation.run (solvers/molecular_dynamics.py:
  * 1969-2000) split around the force call: velocities in A/fs, masses in

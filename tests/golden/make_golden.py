@@ -267,6 +267,28 @@ def main():
                                                   "c", "d", "h", "lambda3", "m", "gamma")] for k in keys])})
     save("fit_sic_t1989", **out)
 
+    # ---- site terms (heat flux): the reference's engine/site_terms.py -----------
+    from akitsushima.engine.site_terms import eam_site_terms, sw_site_terms, tersoff_site_terms
+    cases = [
+        ("sites_tersoff_si216", {"type": "Tersoff", "species": ["Si"], "params": TERSOFF_SI},
+         cubic(DIAMOND, 5.431, 3, ["Si"] * 8, rattle=0.08, seed=51), tersoff_site_terms),
+        ("sites_tersoff1989_sic216", sic_cfg, cubic(DIAMOND, 4.36, 3, zb, rattle=0.08, seed=52),
+         tersoff_site_terms),
+        ("sites_sw_si216", {"type": "SW", "species": ["Si"], "params": SW_SI},
+         cubic(DIAMOND, 5.431, 3, ["Si"] * 8, rattle=0.08, seed=53), sw_site_terms),
+        ("sites_eam_cuni256", {"type": "EAM", "form": "zhou2004", "elements": ["Cu", "Ni"],
+                               "species": ["Cu", "Ni"]},
+         cubic(FCC, 3.58, 4, ["Cu", "Ni", "Cu", "Ni"], rattle=0.08, seed=54), eam_site_terms),
+    ]
+    for name, cfg, (L, P, T), fun in cases:
+        fn = ak.force_fn_from_config(cfg)
+        pot = fn.engine._potentials[0]
+        st = fun(pot, L, P, list(T))
+        vel = np.random.default_rng(55).normal(0, 0.01, P.shape)
+        save(name, lattice=L, positions=P, atom_types=np.array(T), e_site=st.e_site, centre=st.centre,
+             nbr=st.nbr, vec=st.vec, dUdv=st.dUdv, velocities=vel, virial_flux=st.virial_flux(vel),
+             stress=st.stress(abs(np.linalg.det(L))), forces=st.forces())
+
 
 if __name__ == "__main__":
     main()
