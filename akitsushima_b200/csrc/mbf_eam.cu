@@ -58,12 +58,24 @@ template <typename T>
 __device__ __forceinline__ void spline_eval(const EamDev &E, int f, double r, T &v, T &dv) {
     int o = E.xo[f], n = E.nx[f];
     const double *X = E.X + o;
-    int lo = 0, hi = n;
-    while (lo < hi) {  // searchsorted(side='right')
-        int mid = (lo + hi) >> 1;
-        if (X[mid] <= r) lo = mid + 1; else hi = mid;
+    const double *Pf = E.P + (size_t)f * EAM_NCOL;
+    int i;
+    if (Pf[0] == 1.0) {
+        // uniform knots: the interval from the spacing, then moved by at most
+        // one so that it is the last knot <= r, as the search below gives
+        double t = (r - Pf[1]) * Pf[2];
+        int k = t < 0.0 ? 0 : (t > (double)(n - 1) ? n - 1 : (int)t);
+        if (k + 1 < n && X[k + 1] <= r) ++k;
+        else if (k > 0 && X[k] > r) --k;
+        i = k;
+    } else {
+        int lo = 0, hi = n;
+        while (lo < hi) {  // searchsorted(side='right')
+            int mid = (lo + hi) >> 1;
+            if (X[mid] <= r) lo = mid + 1; else hi = mid;
+        }
+        i = lo - 1;
     }
-    int i = lo - 1;
     i = i < 0 ? 0 : (i > n - 2 ? n - 2 : i);
     T dx = (T)(r - X[i]);
     T c0 = (T)E.C[o + i], c1 = (T)E.C[E.nX + o + i];

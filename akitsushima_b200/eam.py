@@ -229,6 +229,9 @@ class EAMPotential(DevicePotential):
                 if c.shape[0] != 4:
                     raise ValueError("EAM: only cubic splines are supported")
                 xo[f], nx[f] = off, len(x)
+                h = (x[-1] - x[0]) / (len(x) - 1) if len(x) > 1 else 0.0
+                if len(x) > 2 and h > 0 and np.allclose(np.diff(x), h, rtol=1e-9, atol=0.0):
+                    P[f, 0], P[f, 1], P[f, 2] = 1.0, x[0], 1.0 / h   # uniform knots
                 Xs.append(x)
                 cc = np.zeros((4, len(x)))
                 cc[:, :len(x) - 1] = c
@@ -267,9 +270,9 @@ class EAMPotential(DevicePotential):
                                self.r_cut, 1 if t["fused"] else 0)
         return (st, keep)
 
-    # lanes of one atom's group: 2 measured fastest on B200 (256k Cu-Ni, both precisions)
     sites_entry = "mbf_eam_eval_sites"
     lane_choices = (1, 2, 4, 8, 16, 32)
+    # lanes of one atom's group: 2 measured fastest on B200 (256k Cu-Ni, both precisions)
     lanes_per_atom = 2
 
     def _call(self, L, sysd, nld, tabs, plan, prec, ws, nbytes, forces, energy, virial, stream):
@@ -348,6 +351,31 @@ def zhou_eam(elements, species, r_cut=None, chi=None, width=0.5, tol=1e-6,
     pot.zhou_params = P
     pot.zhou_chi = {f"{a}-{b}": cfac(a, b) for i, a in enumerate(species) for b in species[i + 1:]}
     return pot
+
+
+def tabulate(pot, n_r=2000, n_rho=2000, rho_max=None, precision=None):
+    """The setfl form of an EAMPotential: F on a uniform rho grid, rho and
+    r*phi on a uniform r grid up to r_cut, each a cubic spline (scipy
+    CubicSpline) -- what writing the potential to an eam/alloy file and
+    reading it back with read_setfl gives (reference engine/eam_zhou.py:
+    258-315).  rho_max defaults to twice the largest rho-bar of a perfect
+    lattice's worth of neighbours (50 x the largest rho(r) on the grid)."""
+    from scipy.interpolate import CubicSpline
+    r_g = np.linspace(0.0, pot.r_cut, n_r)
+    r_pos = np.where(r_g > 0.0, r_g, r_g[1])
+    if rho_max is None:
+        rho_max = 50.0 * max(float(np.max(pot._rho[s](r_pos))) for s in pot.species)
+    rho_g = np.linspace(0.0, rho_max, n_rho)
+
+    def spline(x, y, kind):
+        cs = CubicSpline(x, y)
+        return SpecFunction((kind, np.asarray(cs.x, float), np.asarray(cs.c, float)))
+
+    F_tab = {s: spline(rho_g, pot._F[s](rho_g), "spline") for s in pot.species}
+    rho_tab = {s: spline(r_g, pot._rho[s](r_pos), "spline") for s in pot.species}
+    phi_tab = {k: spline(r_g, r_g * f(r_pos), "spline_over_r") for k, f in pot._phi.items()}
+    return EAMPotential(F_tab, rho_tab, phi_tab, r_cut=pot.r_cut, species=pot.species,
+                        precision=precision or pot.precision)
 
 
 def read_setfl(path, species=None, precision="fp64"):

@@ -82,25 +82,40 @@ def default_device():
     return torch.device("cuda", torch.cuda.current_device())
 
 
+_IDS_CACHE = {}
+
+
 def species_ids(atom_types, species):
     """Species index of every atom.  ``atom_types`` is a list / array of
-    symbols, or an integer array of indices into ``species``."""
+    symbols, or an integer array of indices into ``species``.  A list of
+    symbols equal to the previous call's (the solvers pass the same list
+    every step) reuses its ids: comparing two lists of the same string
+    objects is much cheaper than converting one."""
+    if isinstance(atom_types, list) and atom_types and isinstance(atom_types[0], str):
+        key = tuple(species)
+        hit = _IDS_CACHE.get(key)
+        if hit is not None and len(hit[0]) == len(atom_types) and hit[0] == atom_types:
+            return hit[1]
     a = np.asarray(atom_types)
     if a.dtype.kind in "iu":
         ids = a.astype(np.int32, copy=False)
         if len(ids) and (ids.min() < 0 or ids.max() >= len(species)):
             raise ValueError("atom type index out of range of the potential's species")
         return ids
-    index = {s: k for k, s in enumerate(species)}
     if len(a) == 0:
         return np.zeros(0, np.int32)
-    uniq, inv = np.unique(a.astype(str), return_inverse=True)
-    try:
-        lut = np.array([index[str(u)] for u in uniq], np.int32)
-    except KeyError as exc:
-        raise ValueError(f"atom type {exc.args[0]!r} is not among the potential's species "
-                         f"{list(species)}") from None
-    return lut[inv.reshape(-1)]
+    a = a.astype(str)
+    ids = np.full(len(a), -1, np.int32)
+    for k, sp in enumerate(species):
+        ids[a == sp] = k
+    if (ids < 0).any():
+        bad = a[np.argmax(ids < 0)]
+        raise ValueError(f"atom type {str(bad)!r} is not among the potential's species {list(species)}")
+    ids.setflags(write=False)
+    if isinstance(atom_types, list):
+        _IDS_CACHE.clear()
+        _IDS_CACHE[tuple(species)] = (list(atom_types), ids)
+    return ids
 
 
 class Batch:
@@ -228,7 +243,8 @@ class Batch:
             raise ValueError("type_ids do not match the atom count")
         if self._types_host is not None and np.array_equal(arr, self._types_host):
             return
-        self.types.copy_(torch.from_numpy(np.ascontiguousarray(arr)))
+        host = np.ascontiguousarray(arr)
+        self.types.copy_(torch.from_numpy(host if host.flags.writeable else host.copy()))
         self._types_host = arr.copy()
 
     def set_lattice(self, s, lattice):

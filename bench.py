@@ -760,6 +760,157 @@ def run_fit(args, world, rank, local):
     return 0
 
 
+def _gesn(n_cells=20, a=5.762, sigma=0.1, seed=0, frac_sn=0.25):
+    lat, pos, _ = make_si(n_cells, a=a, sigma=sigma, seed=seed)
+    types = [str(t) for t in np.random.default_rng(seed + 1).choice(["Ge", "Sn"], len(pos),
+                                                                    p=[1 - frac_sn, frac_sn])]
+    return lat, pos, types
+
+
+def _perf_case(name, precision):
+    """(lattice, positions, species names, potential, oracle evaluator) of a
+    performance-path workload."""
+    import oracle
+    import akitsushima_b200 as ak
+    from akitsushima_b200 import eam as eam_mod
+    from akitsushima_b200.published_parameters import SW_GESN_TOMITA_2018, ZHOU_2004
+    if name == "eam_setfl_cuni_256k":
+        lat, pos, ids = make_cuni(40)
+        types = list(np.array(["Cu", "Ni"])[ids])
+        zp = ak.zhou_eam({s: ZHOU_2004[s] for s in ("Cu", "Ni")}, ["Cu", "Ni"])
+        pot = eam_mod.tabulate(zp, precision=precision)
+        sp = ["Cu", "Ni"]
+        specs = ([pot.rho_spec[s] for s in sp] + [pot.F_spec[s] for s in sp]
+                 + [pot.phi_spec[frozenset(k)] for k in (("Cu",), ("Cu", "Ni"), ("Ni",))])
+        ospec = oracle.EAMSpec(sp, specs, [0, 1], [2, 3], np.array([[4, 5], [5, 6]]), pot.r_cut)
+
+        def ref(L, P, T, pairs):
+            return oracle.eam(ospec, L, P, T, pairs)
+        desc = "Zhou 2004 Cu-Ni as setfl cubic splines (2000 r and rho knots), fcc 40^3"
+    else:
+        lat, pos, types = _gesn()
+        pot = ak.StillingerWeberPotential(SW_GESN_TOMITA_2018, species=["Ge", "Sn"], precision=precision)
+        recs = {(r["i"], r["j"], r["k"]): {k: v for k, v in r.items() if k not in "ijk"}
+                for r in SW_GESN_TOMITA_2018}
+
+        def ref(L, P, T, pairs):
+            return oracle.sw_multi(recs, ["Ge", "Sn"], L, P, T, pairs)
+        desc = "Tomita 2018 Ge-Sn Stillinger-Weber, diamond 20^3 (a 5.762 A), 25 % Sn at random"
+    return lat, pos, types, pot, ref, desc
+
+
+def run_perf_path(args, world, rank, local):
+    """One evaluation of a large structure through the spline-EAM or the
+    multi-species SW path (SURVEY next-row performance paths)."""
+    import oracle
+    lat, pos, types, pot, ref, desc = _perf_case(args.workload, args.precision)
+    n_atoms = len(pos)
+    cfg = {"workload": args.workload, "potential": desc, "n_atoms": n_atoms, "skin": 0.3,
+           "precision": args.precision, "l2": "256 MB scratch write between steps, outside the timed events",
+           "parallelism": f"replicas{world}"}
+
+    def cpu_time(n):
+        threads = cpu_count()
+        oracle.set_threads(threads)
+        pairs = oracle.nl_build(lat, pos, float(pot.r_cut), 0.3)[:2]
+        ref(lat, pos, types, pairs)
+        t0 = time.perf_counter()
+        for _ in range(n):
+            ref(lat, pos, types, pairs)
+        return (time.perf_counter() - t0) / n, threads
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        t, threads = cpu_time(max(1, min(args.steps, 3)))
+        v = n_atoms / t
+        line = {"metric": METRIC, "value": v, "unit": "atoms/s", "impl": "reference", "n_gpus": 0,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(cfg, precision="fp64"),
+                "cpu_baseline": {"value": v, "unit": "atoms/s", "cores": threads, "kind": "port",
+                                 "sample": "force calls of the whole structure, prebuilt pair list"},
+                "e2e": {"value": v, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    import akitsushima_b200 as ak
+    from akitsushima_b200 import _lib
+    from akitsushima_b200.system import species_ids
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    batch = ak.Batch.single(lat, pos, species_ids(types, pot.species), device=dev)
+    dnl = ak.DeviceNeighbourList(float(pot.r_cut) + 0.3).build(batch)
+    tuned = pot.autotune_lanes(batch, dnl)
+    out = pot.evaluate(batch, dnl)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        pot.evaluate(batch, dnl, out=out)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            pot.evaluate(batch, dnl, out=out)
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    _lib.profile_begin()
+    pot.evaluate(batch, dnl, out=out)
+    prof = _lib.profile_end()
+    nl = ak.NeighbourList(float(pot.r_cut), skin_width=0.3, device=dev)
+    nl.build_batch(batch)
+    fn = ak.make_force_fn(pot)
+    fn(lat, pos, types, nl)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        fn(lat, pos, types, nl)
+    t_e2e = (time.perf_counter() - t0) / args.e2e_steps
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t_cpu, threads = cpu_time(1)
+        cpu = {"value": n_atoms / t_cpu, "unit": "atoms/s", "cores": threads, "kind": "port",
+               "sample": "one force call of the whole structure (oracle port), prebuilt pair list"}
+    clocks = clk.summary()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": world * n_atoms / (ms * 1e-3), "unit": "atoms/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+            "data": "synthetic", "config": cfg, "autotune": tuned,
+            "gpu_launches": int(sum(c for c, _ in prof.values()) * args.steps),
+            "kernels": {k: {"launches": c, "ms_per_launch": t / c} for k, (c, t) in prof.items()},
+            "clocks": clocks,
+            "e2e": {"value": world * n_atoms / t_e2e, "unit": "atoms/s", "h2d_bytes_per_step": n_atoms * 28,
+                    "d2h_bytes_per_step": n_atoms * 24 + 80, "ms_per_step": t_e2e * 1e3,
+                    "path": "force_fn(lattice, numpy positions, species names, NeighbourList) -> numpy"},
+            "cpu_baseline": cpu, "roofline": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def _replicated(lat, pos, r_list):
     from akitsushima_b200.system import replicate_thin
     L2, P2, T2, _ = replicate_thin(lat, pos, np.zeros(len(pos), np.int32), r_list)
@@ -780,7 +931,8 @@ def main():
     ap.add_argument("--skip-singles", action="store_true",
                     help="batched workload: skip the per-structure-launch comparison (profiling runs)")
     ap.add_argument("--workload", default="eam_cuni_256k",
-                    choices=["eam_cuni_256k", "batched_si512", "fit_sic256"] + sorted(MD_WORKLOADS))
+                    choices=["eam_cuni_256k", "batched_si512", "fit_sic256", "eam_setfl_cuni_256k",
+                             "sw_gesn_64k"] + sorted(MD_WORKLOADS))
     args = ap.parse_args()
     args.precision_given = "--precision" in sys.argv
     args.warmup = max(3, args.warmup)
@@ -794,6 +946,8 @@ def main():
         return run_md(args, world, rank, local)
     if args.workload == "fit_sic256":
         return run_fit(args, world, rank, local)
+    if args.workload in ("eam_setfl_cuni_256k", "sw_gesn_64k"):
+        return run_perf_path(args, world, rank, local)
     lat, pos, ids = make_cuni(args.cells)
     n_atoms = len(pos)
     workload = f"eam_zhou_cuni_fcc{args.cells}^3_{n_atoms}_atoms"

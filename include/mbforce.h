@@ -162,7 +162,11 @@ int mbf_eval_status(const void *workspace, int *host_words, void *stream);
  *   codes (nf,) int32: 1 spline, 2 spline/r, 3 Zhou density, 4 Zhou pair,
  *         5 Zhou cross pair, 6 Zhou embedding
  *   P     (nf, 43) float64 parameter rows; spline xo/nx (nf,) int32,
- *         X (nX,), C (4, nX)
+ *         X (nX,), C (4, nX).  A spline's P row may declare its knots
+ *         uniform: P[0] = 1, P[1] = the first knot, P[2] = 1 / spacing
+ *         (setfl tables are); its interval is then computed, not searched
+ *         -- the same interval as searchsorted(side='right').  P row 0
+ *         otherwise (binary search).
  *   rho_f, F_f (ns,) int32 and phi_f (ns, ns) int32 function ids.        */
 typedef struct mbf_eam_tables {
     int ns;
