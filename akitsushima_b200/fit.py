@@ -1,5 +1,5 @@
-"""Tersoff fitting on the GPU: the reference's weighted E/F/S loss and its
-exact gradient with respect to the parameters.
+"""Tersoff and Zhou-EAM fitting on the GPU: the reference's weighted E/F/S
+loss and its exact gradient with respect to the parameters.
 
 The reference evaluates its fit loss structure by structure on the CPU
 (fitting/loss.py:51-260) and gets gradients by forward differences, one
@@ -12,9 +12,14 @@ with respect to the dense parameter tables, which torch chains back
 through the parameter decoding (log variables, Tersoff-1989 mixing rules,
 tied records) to the optimisation vector x.
 
-Parameter sets mirror the reference's (fitting/parameter_sets.py:1035-1296):
+The Zhou (2004) EAM fit is the same construction over the analytic EAM
+table: the rows P (nf, 43) built differentiably from the element
+parameters (continuity of F included), one mbf_eam_eval and one
+mbf_eam_adjoint call.
+
+Parameter sets mirror the reference's (fitting/parameter_sets.py:1035-1400):
 the same variables, names, x0, bounds, log-space keys and decode(); each
-also decodes differentiably (decode_torch).
+also builds its device tables differentiably in x.
 """
 import math
 
@@ -25,6 +30,7 @@ from . import _lib
 from .force_fn import PotentialEngine
 from .neighbourlist import DeviceNeighbourList
 from .system import Batch, default_device, replicate_thin, species_ids
+from .eam import ZHOU_KEYS, continuous, zhou_cutoff, zhou_eam
 from .tersoff import TERSOFF1989_ELEMENT_KEYS, TersoffPotential, tersoff1989_to_triplets
 
 _TB_KEYS = (("A", 0.0), ("B", 0.0), ("lambda1", 0.0), ("lambda2", 0.0), ("R", 1.0), ("D", 1.0),
@@ -404,6 +410,166 @@ class Tersoff1989ParameterSet(_Variables):
         return tb, tri
 
 
+# ---- Zhou (2004) EAM -------------------------------------------------------------
+
+_ZCOL = {k: c for c, k in enumerate(ZHOU_KEYS)}
+ZHOU_DERIVED = ("Fn0", "Fn1", "F0", "F_e")
+
+
+def continuous_torch(el):
+    """continuous() (F and dF/drho continuous at rho_n = 0.85 rho_e and
+    rho_0 = 1.15 rho_e, engine/eam_zhou.py:47-64) on every row of a (ns, 20)
+    tensor of element parameters in ZHOU_KEYS order, differentiable."""
+    c = _ZCOL
+    re, rs, eta = el[:, c["rho_e"]], el[:, c["rho_s"]], el[:, c["eta"]]
+    F1, F2, F3 = el[:, c["F1"]], el[:, c["F2"]], el[:, c["F3"]]
+    y, x = 0.15, -0.15
+    t0 = 1.15 * re / rs
+    lt0 = torch.log(t0)
+    slope0 = (F1 + 2 * F2 * y + 3 * F3 * y * y) / re
+    dg = -eta * eta * lt0 * t0 ** (eta - 1.0) / rs
+    if bool((dg == 0.0).any()):
+        raise ValueError("Zhou EAM: rho_0 = rho_s (or eta = 0) leaves F_e undetermined")
+    Fe = slope0 / dg
+    F0 = Fe * (1 - eta * lt0) * t0 ** eta - (F1 * y + F2 * y * y + F3 * y ** 3)
+    cols = list(el.unbind(1))
+    cols[c["F_e"]] = Fe
+    cols[c["F0"]] = F0
+    cols[c["Fn0"]] = F0 + F1 * x + F2 * x * x + F3 * x ** 3
+    cols[c["Fn1"]] = 0.85 * (F1 + 2 * F2 * x + 3 * F3 * x * x)
+    return torch.stack(cols, 1)
+
+
+def zhou_table_torch(el, chi, r_cut, width=0.5):
+    """The rows P (nf, 43) of zhou_eam's function table (EAMPotential.
+    function_table: a density row per species, an embedding row per
+    species, a pair row per a <= b) from element rows el (ns, 20, ZHOU_KEYS
+    order, already continuous) and the cross factors chi (ns, ns);
+    differentiable in both."""
+    ns = el.shape[0]
+    f64 = dict(dtype=el.dtype, device=el.device)
+    sw = torch.tensor([float(r_cut), float(width)], **f64)
+    z20 = torch.zeros(20, **f64)
+    z1 = torch.zeros(1, **f64)
+    rows = [torch.cat([el[a], z20, sw, z1]) for a in range(ns)]
+    rows += [torch.cat([el[a], z20, torch.zeros(3, **f64)]) for a in range(ns)]
+    for a in range(ns):
+        for b in range(a, ns):
+            rows.append(torch.cat([el[a], z20, sw, z1]) if a == b else
+                        torch.cat([el[a], el[b], sw, chi[a, b].reshape(1)]))
+    return torch.stack(rows)
+
+
+class ZhouEAMParameterSet(_Variables):
+    """Alloy EAM in the analytic form of Zhou, Johnson and Wadley, PRB 69,
+    144113 (2004) (reference fitting/parameter_sets.py:1306-1400).
+
+    Variables (default, per element): A, B, alpha, beta, Fn2, Fn3, F2, F3,
+    eta; Fn0, Fn1, F0, F_e follow from the continuity of F and are never
+    variables; r_e, f_e, rho_e, rho_s, kappa, lambda, F1 fixed by default;
+    "chi" in fit_keys adds one cross factor per pair of distinct elements.
+    The cutoff is fixed for the whole fit (r_cut, default the largest
+    zhou_cutoff of the start parameters)."""
+
+    _DEFAULT_FIX = ("r_e", "f_e", "rho_e", "rho_s", "kappa", "lambda", "F1")
+    _DEFAULT_FIT = ("A", "B", "alpha", "beta", "Fn2", "Fn3", "F2", "F3", "eta")
+    _LOG_KEYS = frozenset({"A", "B", "alpha", "beta", "chi", "r_e", "f_e", "rho_e", "rho_s"})
+    _BOUNDS = {"A": (1e-3, 10.0), "B": (1e-3, 10.0), "alpha": (1.0, 30.0), "beta": (0.5, 20.0),
+               "Fn2": (-20.0, 20.0), "Fn3": (-20.0, 20.0), "F2": (-20.0, 20.0), "F3": (-20.0, 20.0),
+               "eta": (-3.0, 3.0), "F1": (-20.0, 20.0), "chi": (0.2, 5.0), "r_e": (1.5, 5.0),
+               "f_e": (0.05, 20.0), "rho_e": (0.5, 100.0), "rho_s": (0.5, 100.0), "kappa": (0.05, 2.0),
+               "lambda": (0.05, 2.0)}
+    width = 0.5
+
+    def __init__(self, elements, species, chi=None, fix_params=None, fit_keys=None, r_cut=None):
+        self.species = list(species)
+        self.elements = {}
+        for s in self.species:
+            if s not in elements:
+                raise ValueError(f"ZhouEAMParameterSet: no parameters for '{s}'")
+            self.elements[s] = continuous(elements[s])
+        self.chi = {}
+        for a_i, a in enumerate(self.species):
+            for b in self.species[a_i + 1:]:
+                v = (chi or {}).get(f"{a}-{b}", (chi or {}).get(f"{b}-{a}", 1.0))
+                self.chi[f"{a}-{b}"] = float(v)
+        self.r_cut = float(r_cut) if r_cut else max(zhou_cutoff(self.elements[s]) for s in self.species)
+        fixed = set(self._DEFAULT_FIX) | set(fix_params or ())
+        keys = list(fit_keys) if fit_keys else list(self._DEFAULT_FIT)
+        bad = [k for k in keys if k in ZHOU_DERIVED]
+        if bad:
+            raise ValueError(f"ZhouEAMParameterSet: {bad} follow from the continuity of F and cannot be fitted")
+        self.fit_keys = [k for k in keys if k not in fixed]
+        unknown = [k for k in self.fit_keys if k not in ZHOU_KEYS and k != "chi"]
+        if unknown:
+            raise ValueError(f"ZhouEAMParameterSet: unknown fit key(s) {unknown}")
+        self.variables, init = [], []
+        for s in self.species:
+            for key in self.fit_keys:
+                if key != "chi":
+                    self.variables.append((f"{s}:{key}", key, (s, key)))
+                    init.append(self.elements[s][key])
+        if "chi" in self.fit_keys:
+            for pair, v in self.chi.items():
+                self.variables.append((f"chi:{pair}", "chi", pair))
+                init.append(v)
+        self._setup_vector(init, "ZhouEAMParameterSet")
+
+    def decode(self, x):
+        """{'eam': {'form': 'zhou2004', 'elements', 'chi', 'r_cut'}}."""
+        el = {s: dict(p) for s, p in self.elements.items()}
+        chi = dict(self.chi)
+        for xi, (_, key, target) in zip(np.asarray(x, float), self.variables):
+            v = self._value(key, xi)
+            if key == "chi":
+                chi[target] = v
+            else:
+                el[target[0]][key] = v
+        el = {s: continuous(p) for s, p in el.items()}
+        return {"eam": {"form": "zhou2004", "elements": el, "chi": chi, "r_cut": self.r_cut}}
+
+    def build_engine(self, params):
+        p = params["eam"]
+        return PotentialEngine().add(zhou_eam(p["elements"], self.species, r_cut=p["r_cut"], chi=p["chi"]))
+
+    def potential(self, x=None):
+        """The EAMPotential of decode(x) (x0 by default)."""
+        p = self.decode(self.x0 if x is None else x)["eam"]
+        return zhou_eam(p["elements"], self.species, r_cut=p["r_cut"], chi=p["chi"], width=self.width)
+
+    def table_torch(self, x):
+        """P (nf, 43) of decode(x), differentiable in x: the variables set
+        into the element rows, continuity re-derived, rows assembled."""
+        ns = len(self.species)
+        if not hasattr(self, "_plan"):
+            el0 = torch.tensor([[self.elements[s][k] for k in ZHOU_KEYS] for s in self.species],
+                               dtype=torch.float64)
+            chi0 = torch.ones((ns, ns), dtype=torch.float64)
+            idx = {s: a for a, s in enumerate(self.species)}
+            for pair, v in self.chi.items():
+                a, b = (idx[t] for t in pair.split("-"))
+                chi0[a, b] = chi0[b, a] = v
+            ev, er, ec, cv, c0, c1 = [], [], [], [], [], []
+            for v, (_, key, target) in enumerate(self.variables):
+                if key == "chi":
+                    a, b = (idx[t] for t in target.split("-"))
+                    cv += [v, v]
+                    c0 += [a, b]
+                    c1 += [b, a]
+                else:
+                    ev.append(v)
+                    er.append(idx[target[0]])
+                    ec.append(_ZCOL[key])
+            logm = torch.tensor([key in self._LOG_KEYS for _, key, _ in self.variables])
+            L = lambda q: torch.tensor(q, dtype=torch.long)
+            self._plan = (el0, chi0, L(ev), L(er), L(ec), L(cv), L(c0), L(c1), logm)
+        el0, chi0, ev, er, ec, cv, c0, c1, logm = self._plan
+        vals = torch.where(logm, torch.exp(x), x)
+        el = el0.clone().index_put((er, ec), vals[ev]) if len(ev) else el0
+        chi = chi0.clone().index_put((c0, c1), vals[cv]) if len(cv) else chi0
+        return zhou_table_torch(continuous_torch(el), chi, self.r_cut, self.width)
+
+
 # ---- evaluation with explicit tables and its adjoint ----------------------------
 
 class _TableEval:
@@ -510,6 +676,100 @@ class TersoffEFS(torch.autograd.Function):
         return d_tb.to(ctx.home), d_tri.to(ctx.home), None
 
 
+class _EamTableEval:
+    """A batch, its device list and workspaces, evaluated with given Zhou
+    rows P (nf, 43) over a fixed function-table skeleton (codes, function
+    ids per species; the cutoff is fixed)."""
+
+    def __init__(self, batch, skin, skeleton, r_cut):
+        self.batch = batch
+        dev = batch.device
+        self.r_cut = float(r_cut)
+        self.dlist = DeviceNeighbourList(self.r_cut + float(skin)).build(batch)
+        self.keep = {k: torch.as_tensor(np.ascontiguousarray(skeleton[k]), device=dev)
+                     for k in ("codes", "xo", "nx", "X", "C", "rho_f", "F_f", "phi_f")}
+        self.ns = len(skeleton["rho_f"])
+        self.nf = len(skeleton["codes"])
+        self.fused = 1 if skeleton["fused"] else 0
+        self._ws = None
+        self._adj_ws = None
+        self.lanes = 2
+
+    def _tab(self, P):
+        k = self.keep
+        return _lib.MbfEamTables(self.ns, self.nf, int(k["X"].shape[0]), _lib.ptr(k["codes"]), _lib.ptr(P),
+                                 _lib.ptr(k["xo"]), _lib.ptr(k["nx"]), _lib.ptr(k["X"]), _lib.ptr(k["C"]),
+                                 _lib.ptr(k["rho_f"]), _lib.ptr(k["F_f"]), _lib.ptr(k["phi_f"]), self.r_cut,
+                                 self.fused)
+
+    def autotune(self, P, candidates=(1, 2, 4, 8), reps=3):
+        """Keep the fastest lanes-per-atom of the evaluation (CUDA events)."""
+        times = {}
+        for c in candidates:
+            self.lanes = c
+            self.evaluate(P)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                self.evaluate(P)
+            b.record()
+            b.synchronize()
+            times[c] = a.elapsed_time(b) / reps
+        self.lanes = min(candidates, key=lambda c: (times[c], c))
+        return {"lanes_per_atom": self.lanes, "ms": times}
+
+    def evaluate(self, P):
+        b, dl = self.batch, self.dlist
+        dev = b.device
+        L = _lib.lib()
+        need = int(L.mbf_eval_workspace_bytes(b.n_atoms, dl.n_slots, b.n_chunks))
+        if self._ws is None or self._ws.numel() < need:
+            self._ws = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
+        E = torch.empty(b.n_struct, dtype=torch.float64, device=dev)
+        F = torch.empty((b.n_atoms, 3), dtype=torch.float64, device=dev)
+        W = torch.empty((b.n_struct, 9), dtype=torch.float64, device=dev)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(L.mbf_eam_eval(b.mbf_system(), dl.mbf_nlist(), self._tab(P), b.reduce_plan(), _lib.MBF_FP64,
+                                  self.lanes, _lib.ptr(self._ws), self._ws.numel(), _lib.ptr(F), _lib.ptr(E),
+                                  _lib.ptr(W), st), "mbf_eam_eval")
+        return E, F, W
+
+    def adjoint(self, P, gE, gF, gW):
+        b, dl = self.batch, self.dlist
+        dev = b.device
+        L = _lib.lib()
+        need = int(L.mbf_eam_adjoint_workspace_bytes(b.n_atoms, self.nf))
+        if self._adj_ws is None or self._adj_ws.numel() < need:
+            self._adj_ws = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
+        d_P = torch.empty_like(P)
+        g = [None if t is None else t.to(torch.float64).contiguous() for t in (gE, gF, gW)]
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(L.mbf_eam_adjoint(b.mbf_system(), dl.mbf_nlist(), self._tab(P), _lib.ptr(g[0]), _lib.ptr(g[1]),
+                                     _lib.ptr(g[2]), _lib.ptr(self._adj_ws), self._adj_ws.numel(), _lib.ptr(d_P),
+                                     st), "mbf_eam_adjoint")
+        return d_P
+
+
+class EamEFS(torch.autograd.Function):
+    """(energy (S,), forces (N, 3), virial (S, 9)) of a batch as a function
+    of the Zhou rows P (nf, 43); backward is one mbf_eam_adjoint call.  P
+    may live on the host; its gradient comes back there."""
+
+    @staticmethod
+    def forward(ctx, P, ev):
+        P_d = P.detach().to(ev.batch.device, non_blocking=True).contiguous()
+        E, F, W = ev.evaluate(P_d)
+        ctx.ev = ev
+        ctx.home = P.device
+        ctx.save_for_backward(P_d)
+        return E, F, W
+
+    @staticmethod
+    def backward(ctx, gE, gF, gW):
+        (P,) = ctx.saved_tensors
+        return ctx.ev.adjoint(P, gE, gF, gW).to(ctx.home), None
+
+
 def shard_structures(n_atoms, world):
     """Greedy atom-count balance: largest structures first, each to the
     rank with the fewest atoms so far (lowest rank on ties); returns one
@@ -539,9 +799,57 @@ def _huber_of_squared(sq, delta):
     return torch.where(r <= delta, sq, 2.0 * delta * r - delta * delta)
 
 
-class TersoffFit:
+class _TersoffModel:
+    """Tersoff parameter sets: dense (tb, tri) tables, TersoffEFS."""
+
+    def __init__(self, ps):
+        self.ps = ps
+
+    def _tables0(self, device):
+        return tables_from_records(self.ps.decode(self.ps.x0)["tersoff"], self.ps.species, device)
+
+    def list_cut(self):
+        return table_cutoff(self._tables0("cpu")[0])
+
+    def evaluator(self, batch, skin):
+        ev = _TableEval(batch, skin)
+        return ev, ev.autotune(*self._tables0(batch.device))
+
+    def efs(self, x_t, ev):
+        if hasattr(self.ps, "tables_torch"):
+            tb, tri = self.ps.tables_torch(x_t)
+        else:
+            tb, tri = tables_from_records(self.ps.decode_torch(x_t)["tersoff"], self.ps.species, x_t.device)
+        return TersoffEFS.apply(tb, tri, ev)
+
+
+class _ZhouModel:
+    """Zhou EAM parameter sets: the analytic rows P (nf, 43), EamEFS."""
+
+    def __init__(self, ps):
+        self.ps = ps
+
+    def list_cut(self):
+        return self.ps.r_cut
+
+    def evaluator(self, batch, skin):
+        ev = _EamTableEval(batch, skin, self.ps.potential().function_table(), self.ps.r_cut)
+        P0 = self.ps.table_torch(torch.as_tensor(self.ps.x0)).to(batch.device)
+        return ev, ev.autotune(P0)
+
+    def efs(self, x_t, ev):
+        return EamEFS.apply(self.ps.table_torch(x_t), ev)
+
+
+def _model_of(ps):
+    return _ZhouModel(ps) if hasattr(ps, "table_torch") else _TersoffModel(ps)
+
+
+class PotentialFit:
     """The reference's fit loss (fitting/loss.py:51-260) over a training set
-    on the GPU, and its gradient in x.
+    on the GPU, and its gradient in x, for the Tersoff parameter sets
+    (MultiSpeciesTersoffParameterSet, Tersoff1989ParameterSet) and
+    ZhouEAMParameterSet.
 
     structures : dicts with lattice, positions, atom_types, natoms,
                  ref_energy (eV/atom), optional ref_forces (N, 3),
@@ -565,6 +873,7 @@ class TersoffFit:
                 if key not in weights:
                     raise ValueError(f"loss_type='huber' requires weights['{key}'] (eV)")
         self.ps = param_set
+        self.model = _model_of(param_set)
         self.loss_type = loss_type
         self.w = weights
         self.rank, self.world, self.group = int(rank), int(world), group
@@ -576,7 +885,7 @@ class TersoffFit:
         dev = self.device
         sp = self.ps.species
         lats, poss, ids, reps, n_orig, vols = [], [], [], [], [], []
-        r_guess = table_cutoff(tables_from_records(self.ps.decode(self.ps.x0)["tersoff"], sp, "cpu")[0])
+        r_guess = self.model.list_cut()
         for s in structs:
             t = species_ids(s["atom_types"], sp)
             L2, P2, T2, k = replicate_thin(s["lattice"], s["positions"], t, r_guess + skin)
@@ -587,11 +896,10 @@ class TersoffFit:
             n_orig.append(len(s["positions"]))
             vols.append(float(s.get("volume", abs(np.linalg.det(np.asarray(s["lattice"], float))))))
         self.n_struct = len(structs)
-        self.ev = _TableEval(Batch(lats, poss, ids, device=dev), skin) if structs else None
+        self.ev = None
         if not structs:
             return
-        tb0, tri0 = tables_from_records(self.ps.decode(self.ps.x0)["tersoff"], sp, dev)
-        self.tuned = self.ev.autotune(tb0, tri0)
+        self.ev, self.tuned = self.model.evaluator(Batch(lats, poss, ids, device=dev), skin)
         off = self.ev.batch.offsets
         idx = np.concatenate([np.arange(off[q], off[q] + n) for q, n in enumerate(n_orig)])
         self._orig = torch.as_tensor(idx, device=dev)
@@ -621,11 +929,7 @@ class TersoffFit:
         """This rank's loss as a differentiable torch scalar."""
         if self.ev is None:
             return (x_t.sum() * 0.0).to(self.device)
-        if hasattr(self.ps, "tables_torch"):
-            tb, tri = self.ps.tables_torch(x_t)
-        else:
-            tb, tri = tables_from_records(self.ps.decode_torch(x_t)["tersoff"], self.ps.species, x_t.device)
-        E, F, W = TersoffEFS.apply(tb, tri, self.ev)
+        E, F, W = self.model.efs(x_t, self.ev)
         w = self.w
         w_E, w_F, w_S = float(w.get("energy", 1.0)), float(w.get("forces", 1.0)), float(w.get("stress", 0.1))
         r0, eps0 = float(w.get("r0", 1.0)), float(w.get("eps0", 1.0))
@@ -681,19 +985,22 @@ class TersoffFit:
         return 1e30 if vec[1] > 0.0 else float(vec[0])
 
 
+TersoffFit = PotentialFit
+
 _FITS = {}
 
 
 def generic_loss_function(x, param_set, structures, weights, r_cut=None, ewald_alpha=None,
                           coulomb_method="ewald", loss_type="squared"):
-    """fitting/loss.py:51 on the GPU for Tersoff parameter sets: the same
-    value (eV^2; 1e30 when the parameters cannot be evaluated).  r_cut,
-    ewald_alpha and coulomb_method concern charges, which Tersoff sets do
-    not carry; the list radius follows the decoded records."""
+    """fitting/loss.py:51 on the GPU for Tersoff and Zhou EAM parameter
+    sets: the same value (eV^2; 1e30 when the parameters cannot be
+    evaluated).  r_cut, ewald_alpha and coulomb_method concern charges,
+    which these sets do not carry; the list radius follows the decoded
+    records (Tersoff) or the set's fixed cutoff (EAM)."""
     if loss_type not in ("squared", "huber"):
         raise ValueError(f"generic_loss_function: unknown loss_type '{loss_type}'. Choose 'squared' or 'huber'.")
     key = (id(param_set), id(structures), loss_type, tuple(sorted((k, float(v)) for k, v in weights.items())))
     fit = _FITS.get(key)
     if fit is None:
-        fit = _FITS[key] = TersoffFit(param_set, structures, weights, loss_type=loss_type)
+        fit = _FITS[key] = PotentialFit(param_set, structures, weights, loss_type=loss_type)
     return fit.loss(x)

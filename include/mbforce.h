@@ -220,6 +220,29 @@ int mbf_eam_eval_static(const mbf_system *sys, const mbf_nlist *nl, const mbf_ea
                         const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
                         double *forces, double *energy, double *virial, void *stream);
 
+/* Zhou EAM adjoint for fitting: the vector-Jacobian product of (energy,
+ * forces, virial) with respect to the function rows P (nf, 43) of an
+ * analytic Zhou table (density rows code 3, embedding rows code 6, pair
+ * rows code 4 / 5, as the table layout above), in float64.  Given upstream
+ * gradients g_energy (n_struct), g_forces (n_atoms, 3) and g_virial
+ * (n_struct, 9) -- any may be NULL for zero -- writes
+ *   d_P[f, c] = sum_s gE_s dE_s/dP[f, c] + sum_a gF_a . dF_a/dP[f, c]
+ *               + sum_s gW_s : dW_s/dP[f, c]
+ * for the columns each row's function reads: density r_e, f_e, beta,
+ * lambda; embedding rho_e, rho_s, Fn0..3, F0..3, eta, F_e; pair the element
+ * columns of one (like) or both (cross) species and the cross factor
+ * (column 42).  The switch columns 40, 41 and unread columns get 0.  The
+ * derivative is of the float64 evaluation, with respect to the rows the
+ * generic evaluation reads (rho_f, F_f, phi_f).  Replaces the
+ * forward-difference Jacobian of the reference's fit over
+ * ZhouEAMParameterSet (fitting/driver.py:802-816,
+ * fitting/parameter_sets.py:1306-1400).  Deterministic.  ns <= 8; the
+ * workspace needs mbf_eam_adjoint_workspace_bytes(n_atoms, nf).         */
+size_t mbf_eam_adjoint_workspace_bytes(int n_atoms, int nf);
+int mbf_eam_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                    const double *g_energy, const double *g_forces, const double *g_virial,
+                    void *workspace, size_t workspace_bytes, double *d_P, void *stream);
+
 /* ---- Tersoff ----------------------------------------------------------
  * Replaces TersoffPotential.compute (engine/tersoff.py:1208-1711): both the
  * single-species flat form (m = 3, gamma = 1; :1233-1513) and the

@@ -708,6 +708,12 @@ def eam(spec, lattice, positions, atom_types, pairs=None):
     return float(e), forces, vir / _volume(lattice)
 
 
+def zhou_force(elements, species, r_cut=None, chi=None, width=0.5):
+    """The force call of a Zhou EAM (zhou_spec) for fit_loss."""
+    spec = zhou_spec(elements, species, r_cut, chi, width)
+    return lambda lat, pos, types, pairs=None: eam(spec, lat, pos, types, pairs)
+
+
 # ---- molecular dynamics ------------------------------------------------------
 EV_ANG_TO_AMU_ANG_FS2 = (1.60217663e-19 / 1.0e-10) / (1.66053906660e-27) * 1.0e-20
 K_B = 1.380649e-23 * 6.241509074e18
@@ -755,11 +761,13 @@ def nve(force, lattice, positions, masses, velocities, dt, n_steps):
 
 
 # ---- fitting -------------------------------------------------------------------
-def fit_loss(records, species, structures, weights, pairs=None):
+def fit_loss(records, species, structures, weights, pairs=None, force=None):
     """fitting/loss.py:184-260 (squared loss) with the multi-species Tersoff
     force call: sum_s w_trust c_s^2 [w_E (E - N e_ref)^2 + w_F r0^2
     mean|dF|^2 + w_S (V eps0)^2 mean|dsigma|^2].  pairs: optional list of
-    prebuilt (i, j) per structure."""
+    prebuilt (i, j) per structure.  force: optional callable (lattice,
+    positions, atom_types, pairs) -> (E, F, stress) used instead of the
+    Tersoff call (records is then ignored)."""
     w_E = weights.get("energy", 1.0)
     w_F = weights.get("forces", 1.0)
     w_S = weights.get("stress", 0.1)
@@ -769,8 +777,11 @@ def fit_loss(records, species, structures, weights, pairs=None):
     for q, s in enumerate(structures):
         N = s["natoms"]
         vol = float(s.get("volume", abs(np.linalg.det(s["lattice"]))))
-        e, f, st = tersoff_multi(records, species, s["lattice"], s["positions"], s["atom_types"],
-                                 None if pairs is None else pairs[q])
+        pq = None if pairs is None else pairs[q]
+        if force is not None:
+            e, f, st = force(s["lattice"], s["positions"], s["atom_types"], pq)
+        else:
+            e, f, st = tersoff_multi(records, species, s["lattice"], s["positions"], s["atom_types"], pq)
         tot = w_E * (N * (e / N - s["ref_energy"])) ** 2
         if s.get("ref_forces") is not None:
             tot += w_F * r0 ** 2 * float(np.mean((f - s["ref_forces"]) ** 2))

@@ -77,6 +77,7 @@ def strained(lat, pos, amp, seed):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", default=None, help="write only this section ('fit_eam')")
     args = ap.parse_args()
     sys.path.insert(0, args.reference)
     os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache")
@@ -86,6 +87,10 @@ def main():
     def save(name, **kw):
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **kw)
         print("wrote", name)
+
+    if args.only == "fit_eam":
+        fit_eam(save)
+        return
 
     def nl_pairs(lat, pos, r_cut, skin):
         nl = NeighbourList(r_cut=r_cut, skin_width=skin, backend="cll")
@@ -267,6 +272,8 @@ def main():
                                                   "c", "d", "h", "lambda3", "m", "gamma")] for k in keys])})
     save("fit_sic_t1989", **out)
 
+    fit_eam(save)
+
     # ---- site terms (heat flux): the reference's engine/site_terms.py -----------
     from akitsushima.engine.site_terms import eam_site_terms, sw_site_terms, tersoff_site_terms
     cases = [
@@ -288,6 +295,62 @@ def main():
         save(name, lattice=L, positions=P, atom_types=np.array(T), e_site=st.e_site, centre=st.centre,
              nbr=st.nbr, vec=st.vec, dUdv=st.dUdv, velocities=vel, virial_flux=st.virial_flux(vel),
              stress=st.stress(abs(np.linalg.det(L))), forces=st.forces())
+
+
+def fit_eam(save):
+    """Zhou (2004) Al-Ni EAM fit: the reference's ZhouEAMParameterSet, its
+    loss (fitting/loss.py:51) and the forward-difference gradient of its
+    fit (fitting/driver.py:802-816) on two rattled, strained L1_2 Ni3Al
+    cells whose targets come from a perturbed parameter set."""
+    from akitsushima.engine.published_parameters import ZHOU_2004
+    from akitsushima.fitting.loss import generic_loss_function, generic_residuals
+    from akitsushima.fitting.parameter_sets import ZhouEAMParameterSet
+    species = ["Al", "Ni"]
+    el0 = {s: dict(ZHOU_2004[s]) for s in species}
+    rng = np.random.default_rng(61)
+    el_t = {s: {k: (v * rng.uniform(0.97, 1.03) if k in ("A", "B", "alpha", "beta", "F2", "F3", "eta") else v)
+                for k, v in el0[s].items()} for s in species}
+    target = ZhouEAMParameterSet(el_t, species, chi={"Al-Ni": 1.04})
+    eng = target.build_engine(target.decode(target.x0))
+    structs, geo = [], {}
+    for q, (n, seed) in enumerate(((4, 62), (5, 63))):
+        L, P, T = cubic(FCC, 3.57, n, ["Al", "Ni", "Ni", "Ni"], rattle=0.06, seed=seed)
+        L, P = strained(L, P, 0.015, seed + 100)
+        e, f, s = eng.compute(L, P, list(T))
+        structs.append({"lattice": L, "positions": P, "atom_types": list(T), "natoms": len(P),
+                        "ref_energy": float(e) / len(P), "ref_forces": np.asarray(f),
+                        "ref_stress": np.asarray(s)})
+        geo.update({f"lattice{q}": L, f"positions{q}": P, f"atom_types{q}": np.array(T),
+                    f"ref_energy{q}": float(e) / len(P), f"ref_forces{q}": np.asarray(f),
+                    f"ref_stress{q}": np.asarray(s)})
+    weights = {"energy": 1.0, "forces": 1.0, "stress": 1.0, "r0": 0.1, "eps0": 0.01}
+    out = dict(geo, n_structures=len(structs))
+    for tag, ps in (("zhou", ZhouEAMParameterSet(el0, species)),
+                    ("zhou_chi", ZhouEAMParameterSet(el0, species, fit_keys=["A", "B", "F2", "eta", "chi"]))):
+        x0 = ps.x0
+        lo_b = np.array([b[0] for b in ps.bounds])
+        hi_b = np.array([b[1] for b in ps.bounds])
+        r0 = generic_residuals(x0, ps, structs, weights, ps.r_cut, None)
+        J = np.empty((len(r0), len(x0)))
+        for q in range(len(x0)):   # the fit's jacobian_fn (fitting/driver.py:802-816)
+            h = 1e-7 * max(1.0, abs(x0[q]))
+            if x0[q] + h > hi_b[q]:
+                h = -h
+            xp = np.array(x0, float)
+            xp[q] += h
+            J[:, q] = (generic_residuals(xp, ps, structs, weights, ps.r_cut, None) - r0) / h
+        x_test = np.clip(x0 + np.random.default_rng(64).uniform(-0.02, 0.02, len(x0)), lo_b, hi_b)
+        dec = ps.decode(x_test)["eam"]
+        out.update({f"{tag}_x0": x0, f"{tag}_names": np.array(ps.variable_names), f"{tag}_lo": lo_b,
+                    f"{tag}_hi": hi_b, f"{tag}_r_cut": ps.r_cut,
+                    f"{tag}_loss0": generic_loss_function(x0, ps, structs, weights, ps.r_cut, None),
+                    f"{tag}_grad_fd": 2.0 * J.T @ r0, f"{tag}_x_test": x_test,
+                    f"{tag}_loss_test": generic_loss_function(x_test, ps, structs, weights, ps.r_cut, None),
+                    f"{tag}_decoded_keys": np.array(list(dec["elements"]["Al"])),
+                    f"{tag}_decoded": np.array([[dec["elements"][s][k] for k in dec["elements"]["Al"]]
+                                                for s in species]),
+                    f"{tag}_decoded_chi": dec["chi"]["Al-Ni"]})
+    save("fit_alni_zhou", **out)
 
 
 if __name__ == "__main__":
