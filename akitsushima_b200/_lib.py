@@ -103,7 +103,7 @@ _SIGS = {
     "mbf_eam_eval_sites": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                                 ctypes.POINTER(MbfEamTables), ctypes.POINTER(MbfReducePlan), _i, _i,
                                 _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
-    "mbf_eam_adjoint_workspace_bytes": (_sz, [_i, _i]),
+    "mbf_eam_adjoint_workspace_bytes": (_sz, [_i, _ll, _i]),
     "mbf_eam_adjoint": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                              ctypes.POINTER(MbfEamTables), _vp, _vp, _vp, _vp, _sz, _vp, _vp]),
     "mbf_tersoff_adjoint_workspace_bytes": (_sz, [_ll, _i]),

@@ -19,6 +19,10 @@
 // The embedding's 12 parameters and rho-bar itself are the 13 directions of
 // one evaluation of F; with c1 = gE F' + F'' D_t rho-bar and c2 = F', a
 // density parameter's site value is c1 d(rho)/dtheta + c2 d(D_t rho)/dtheta.
+// Density and pair functions are built from decays
+// g(r; r_e, exponent, shift), each differentiated in its own three
+// parameters only; an element's eight parameters and the cross pair's
+// (f_a, u_a, f_b, u_b) dependence are chained by hand from those.
 //
 // Sites of atom i (W = 12 + 21 ns):
 //   0..11               rho_e, rho_s, Fn0..Fn3, F0..F3, eta, F_e of row F_f[s_i]
@@ -38,7 +42,6 @@
 
 namespace mbf {
 
-constexpr int EADJ_BLOCK = 64;
 constexpr int EADJ_NCOL = 43;
 constexpr int EADJ_NZ = 20;
 
@@ -49,51 +52,52 @@ struct EamAdjTab {
     double rc;
 };
 
-// pre exp(-expo (x - 1)) / (1 + (x - shift)^20), x = r / re
-// (engine/eam_zhou.py:20-45).
+// g = exp(-expo (x - 1)) / (1 + (x - shift)^20), x = r / re, the decay
+// every Zhou function is built from (engine/eam_zhou.py:20-45), with r's
+// tangent rt; as HD<3> its directions are (re, expo, shift).
 template <int K>
-__device__ __forceinline__ HD<K> hz_decay(const HD<K> &r, const HD<K> &re, const HD<K> &pre, const HD<K> &expo,
+__device__ __forceinline__ HD<K> hz_decay(double r, double rt, const HD<K> &re, const HD<K> &expo,
                                           const HD<K> &shift) {
-    HD<K> x = r / re;
-    HD<K> e = pre * hd_exp<K>((-1.0) * (expo * (x + (-1.0))));
+    HD<K> R = hd_const<K>(r);
+    R.t = rt;
+    HD<K> x = R / re;
+    HD<K> e = hd_exp<K>((-1.0) * (expo * (x + (-1.0))));
     HD<K> u = x - shift;
     double u2 = u.v * u.v, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8, u18 = u16 * u2;
     HD<K> den = 1.0 + hd_apply<K>(u, u18 * u2, 20.0 * u18 * u.v, 380.0 * u18);
     return e / den;
 }
 
-// One element's density f and pair phi_aa (both unswitched) from the 20
-// Zhou columns at p; parameter k of the 8 (r_e, f_e, alpha, beta, A, B,
-// kappa, lambda) is direction first + k (no direction if out of range).
-template <int K>
-__device__ __forceinline__ void hz_species(const double *p, int first, const HD<K> &r, HD<K> &f, HD<K> &u) {
-    HD<K> re = hd_param<K>(p[0], first + 0, 0), fe = hd_param<K>(p[1], first + 1, 0);
-    HD<K> al = hd_param<K>(p[4], first + 2, 0), be = hd_param<K>(p[5], first + 3, 0);
-    HD<K> A = hd_param<K>(p[6], first + 4, 0), B = hd_param<K>(p[7], first + 5, 0);
-    HD<K> ka = hd_param<K>(p[8], first + 6, 0), la = hd_param<K>(p[9], first + 7, 0);
-    HD<K> one = hd_const<K>(1.0);
-    HD<K> gB = hz_decay<K>(r, re, one, be, la);
-    HD<K> gA = hz_decay<K>(r, re, one, al, ka);
-    f = fe * gB;
-    u = A * gA - B * gB;
+__device__ __forceinline__ HD<3> hz_g3(double r, double rt, double re, double expo, double shift) {
+    return hz_decay<3>(r, rt, hd_param<3>(re, 0, 0), hd_param<3>(expo, 1, 0), hd_param<3>(shift, 2, 0));
 }
 
-// The quintic switch of a row (columns 40, 41) as a function of r only.
-template <int K>
-__device__ __forceinline__ HD<K> hz_switch(const double *row, const HD<K> &r) {
+// The quintic switch of a row (columns 40, 41) at r: value and tangent.
+__device__ __forceinline__ void hz_switch(const double *row, double r, double rt, double &S, double &St) {
     double rc = row[2 * EADJ_NZ], w = row[2 * EADJ_NZ + 1];
-    double s = (r.v - (rc - w)) / w;
+    double s = (r - (rc - w)) / w;
     s = s < 0.0 ? 0.0 : (s > 1.0 ? 1.0 : s);
-    double S = 1.0 - s * s * s * (10.0 - 15.0 * s + 6.0 * s * s);
-    double dS = -30.0 * s * s * (1.0 - s) * (1.0 - s) / w;
-    return hd_apply<K>(r, S, dS, 0.0);  // r carries no parameter direction
+    S = 1.0 - s * s * s * (10.0 - 15.0 * s + 6.0 * s * s);
+    St = -30.0 * s * s * (1.0 - s) * (1.0 - s) / w * rt;
 }
 
-template <int K, int J>
-__device__ __forceinline__ HD<K> hd_lift(const HD<J> &a) {
-    HD<K> r = hd_const<K>(a.v);
-    r.t = a.t;
-    return r;
+// One element's density f = f_e gB and pair u = A gA - B gB (unswitched),
+// gA = g(r; r_e, alpha, kappa), gB = g(r; r_e, beta, lambda), enter a site
+// value through their parameter derivatives (p) and the tangent of those
+// (q): site_k += af f.p_k + bf f.q_k + au u.p_k + bu u.q_k, for the 8
+// element parameters r_e, f_e, alpha, beta, A, B, kappa, lambda (columns 0,
+// 1, 4..9 of p).
+__device__ __forceinline__ void hz_species_sites(double *o, const HD<3> &gA, const HD<3> &gB, const double *p,
+                                                 double af, double bf, double au, double bu) {
+    double fe = p[1], A = p[6], B = p[7];
+    o[0] += fe * (af * gB.p[0] + bf * gB.q[0]) + au * (A * gA.p[0] - B * gB.p[0]) + bu * (A * gA.q[0] - B * gB.q[0]);
+    o[1] += af * gB.v + bf * gB.t;
+    o[2] += A * (au * gA.p[1] + bu * gA.q[1]);
+    o[3] += (fe * af - B * au) * gB.p[1] + (fe * bf - B * bu) * gB.q[1];
+    o[4] += au * gA.v + bu * gA.t;
+    o[5] -= au * gB.v + bu * gB.t;
+    o[6] += A * (au * gA.p[2] + bu * gA.q[2]);
+    o[7] += (fe * af - B * au) * gB.p[2] + (fe * bf - B * bu) * gB.q[2];
 }
 
 // Zhou embedding F(rho), eqs. (A6)-(A8) (engine/eam_zhou.py:66-115), with
@@ -122,100 +126,256 @@ __device__ __forceinline__ HD<13> hz_embed(const double *p, double rho, double r
 
 __device__ __forceinline__ const double *row_of(const EamAdjTab &T, int f) { return T.P + (size_t)f * EADJ_NCOL; }
 
-// Site values of atom i into out[0..W).  Returns s_i.
-__device__ int eam_atom_sites(const SysView &S, const int *__restrict__ row_off, const int *__restrict__ nbr,
-                              const EamAdjTab &T, const AdjIn &G, int i, int W, double *out) {
+// Value and r-tangent of f_e g(r; r_e, beta, lambda) S(r) for pass 1.
+__device__ __forceinline__ void dens_value(const double *row, double r, double rt, double &v, double &vt) {
+    double x = r / row[0];
+    double e = exp(-row[5] * (x - 1.0));
+    double u = x - row[9];
+    double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8, u19 = u16 * u2 * u;
+    double id = 1.0 / (1.0 + u19 * u);
+    double g = e * id;
+    double dg = g * (-row[5] - 20.0 * u19 * id) / row[0];
+    double Sw, St;
+    hz_switch(row, r, 1.0, Sw, St);  // St = dS/dr here
+    v = row[1] * g * Sw;
+    vt = row[1] * (dg * Sw + g * St) * rt;
+}
+
+// Tiles: EADJ_TA atoms (embedding pass) or EADJ_TP pairs (pair pass) per
+// iteration of a block; blocks stride over tiles in a fixed order and keep
+// their own sums, so every reduction below is in a fixed order.
+constexpr int EADJ_TA = 128;
+constexpr int EADJ_TP = 64;
+constexpr int EADJ_GRID = 148 * 16;  // pair-kernel blocks at most (16 per SM of a B200)
+constexpr int EADJ_PS = 25;          // staged values of one pair
+constexpr int EADJ_STRIDE = 25;      // odd: conflict-free 8-byte shared accesses
+
+// Pass 1, a thread per atom: rho-bar and its tangent over the full row, the
+// embedding sites (12; summed per species of the centre into the block's
+// partialF row) and the coefficients c1 = gE F' + F'' D_t rho-bar, c2 = F'
+// through which every density parameter acts on this atom's site term.
+// Also flags the live pairs above the diagonal (j > i, inside the cutoff):
+// flag[s] for like-species pairs, flag[n_slots + s] for cross pairs.
+__global__ void __launch_bounds__(EADJ_TA) eam_adjoint_embed(SysView S, const int *__restrict__ row_off,
+                                                             const int *__restrict__ upper,
+                                                             const int *__restrict__ nbr, EamAdjTab T, AdjIn G,
+                                                             int n_slots, double2 *__restrict__ cc,
+                                                             int *__restrict__ flag, double *__restrict__ partialF) {
+    __shared__ double sf[EADJ_TA * 13];  // 12 sites per atom, odd stride
+    __shared__ int scode[EADJ_TA];
+    extern __shared__ double accF[];     // ns * 12
+    const int ns = T.ns, nf = 12 * ns;
+    for (int k = threadIdx.x; k < nf; k += blockDim.x) accF[k] = 0.0;
+    const double rc2 = T.rc * T.rc;
+    int n_tiles = (S.n_atoms + EADJ_TA - 1) / EADJ_TA;
+    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        int i = tile * EADJ_TA + threadIdx.x;
+        int code = -1;
+        double *o = sf + 13 * threadIdx.x;
+        if (i < S.n_atoms) {
+            int si = S.types[i];
+            int sst = S.n_struct > 1 ? S.atom_struct[i] : 0;
+            double gE = G.gE ? G.gE[sst] : 0.0;
+            const double *cell = cell_of(S, i);
+            double rho = 0.0, rho_t = 0.0;
+            int up = upper[i];
+            for (int s = row_off[i]; s < row_off[i + 1]; ++s) {
+                int j = nbr[s];
+                double d[3], r, tg[3];
+                adj_leg(S, G, cell, i, j, sst, d, r, tg);
+                if (!(r * r < rc2 && r * r > 1e-24)) continue;
+                int sj = S.types[j];
+                if (s >= up) flag[(si == sj ? 0 : n_slots) + s] = 1;
+                double rt = (d[0] * tg[0] + d[1] * tg[1] + d[2] * tg[2]) / r;
+                double v, vt;
+                dens_value(row_of(T, T.rho_f[sj]), r, rt, v, vt);
+                rho += v;
+                rho_t += vt;
+            }
+            // the embedding, rho-bar clamped at 0 as the evaluation does
+            double rb = rho > 0.0 ? rho : 0.0;
+            HD<13> F = hz_embed(row_of(T, T.F_f[si]), rb, rho_t);
+#pragma unroll
+            for (int k = 0; k < 12; ++k) o[k] = gE * F.p[k] + F.q[k];
+            cc[i] = make_double2(rho > 0.0 ? gE * F.p[12] + F.q[12] : 0.0, F.p[12]);
+            code = si;
+        }
+        scode[threadIdx.x] = code;
+        __syncthreads();
+        int cnt = min(EADJ_TA, S.n_atoms - tile * EADJ_TA);
+        for (int item = threadIdx.x; item < nf; item += blockDim.x) {
+            int sp = item / 12, k = item % 12;
+            double a = 0.0;
+            for (int q = 0; q < cnt; ++q)
+                if (scode[q] == sp) a += sf[13 * q + k];
+            accF[item] += a;
+        }
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < nf; k += blockDim.x) partialF[(size_t)blockIdx.x * nf + k] = accF[k];
+}
+
+// Compacted pair list: like pairs first, then cross pairs (slot indices).
+__global__ void eam_adjoint_compact(int n2, const int *__restrict__ flag, const int *__restrict__ pos,
+                                    int n_slots, int *__restrict__ pairs) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n2 && flag[q]) pairs[pos[q]] = q < n_slots ? q : q - n_slots;
+}
+
+// The slot's owning atom: rows are sorted, so a binary search in row_off.
+__device__ __forceinline__ int eadj_owner(const int *__restrict__ row_off, int n_atoms, int s) {
+    int lo = 0, hi = n_atoms - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (row_off[mid] <= s) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Density sites of one centre's view of a neighbour of species s at r:
+// rho_s = f_e gB S, contributing c1 d(rho)/dtheta + c2 d(D_t rho)/dtheta to
+// r_e, f_e, beta, lambda (o[0..3]).
+__device__ __forceinline__ void dens_sites(double *o, const HD<3> &gB, const double *row, double Sw, double St,
+                                           double c1, double c2) {
+    double a = c1 * Sw + c2 * St, bq = c2 * Sw;
+    double af = a * row[1], bf = bq * row[1];
+    o[0] += af * gB.p[0] + bf * gB.q[0];
+    o[1] += a * gB.v + bq * gB.t;
+    o[2] += af * gB.p[1] + bf * gB.q[1];
+    o[3] += af * gB.p[2] + bf * gB.q[2];
+}
+
+// The density decay of species row `dr` at r: the pair's decay of the same
+// element when the density row holds the same (r_e, beta, lambda), else its
+// own.
+__device__ __forceinline__ HD<3> dens_decay(const double *dr, const double *blk, const HD<3> &gB_blk, double r,
+                                            double rt) {
+    if (dr[0] == blk[0] && dr[5] == blk[5] && dr[9] == blk[9]) return gB_blk;
+    return hz_g3(r, rt, dr[0], dr[5], dr[9]);
+}
+
+// The 25 staged values of the live pair at slot s (i < j): 0..16 the pair
+// sites of row phi_f[s_i, s_j] (weight 1: the two halves 1/2 phi of the
+// site terms of i and j), 17..20 the density sites of i's view of rho_{s_j}
+// (coefficients of i), 21..24 those of j's view of rho_{s_i}.  Returns the
+// code s_i ns + s_j.
+template <bool LIKE>
+__device__ int eam_pair_sites(const SysView &S, const int *__restrict__ row_off, const int *__restrict__ nbr,
+                              const EamAdjTab &T, const AdjIn &G, const double2 *__restrict__ cc, int s, double *o) {
     const int ns = T.ns;
-    for (int w = 0; w < W; ++w) out[w] = 0.0;
-    int si = S.types[i];
+    int i = eadj_owner(row_off, S.n_atoms, s);
+    int j = nbr[s];
+    int si = S.types[i], sj = S.types[j];
     int sst = S.n_struct > 1 ? S.atom_struct[i] : 0;
     double gE = G.gE ? G.gE[sst] : 0.0;
-    const double *cell = cell_of(S, i);
-    const double rc2 = T.rc * T.rc;
-    int b = row_off[i], e = row_off[i + 1];
-    // pass 1: rho-bar and its tangent
-    double rho = 0.0, rho_t = 0.0;
-    for (int s = b; s < e; ++s) {
-        int j = nbr[s];
-        double d[3], r, tg[3];
-        adj_leg(S, G, cell, i, j, sst, d, r, tg);
-        if (!(r * r < rc2 && r * r > 1e-24)) continue;
-        HD<1> rr = hd_const<1>(r);
-        rr.t = (d[0] * tg[0] + d[1] * tg[1] + d[2] * tg[2]) / r;
-        const double *row = row_of(T, T.rho_f[S.types[j]]);
-        HD<1> fs = hz_decay<1>(rr, hd_const<1>(row[0]), hd_const<1>(row[1]), hd_const<1>(row[5]),
-                               hd_const<1>(row[9])) *
-                   hz_switch<1>(row, rr);
-        rho += fs.v;
-        rho_t += fs.t;
+    double d[3], r, tg[3];
+    adj_leg(S, G, cell_of(S, i), i, j, sst, d, r, tg);
+    double rt = (d[0] * tg[0] + d[1] * tg[1] + d[2] * tg[2]) / r;
+    for (int k = 0; k < EADJ_PS; ++k) o[k] = 0.0;
+    const double *row = row_of(T, T.phi_f[si * ns + sj]);
+    const double *rho_i = row_of(T, T.rho_f[si]), *rho_j = row_of(T, T.rho_f[sj]);
+    const double2 ci = cc[i], cj = cc[j];
+    double Sw, St, Dw, Dt;
+    hz_switch(row, r, rt, Sw, St);
+    HD<3> gAa = hz_g3(r, rt, row[0], row[4], row[8]);
+    HD<3> gBa = hz_g3(r, rt, row[0], row[5], row[9]);
+    if (LIKE) {
+        // phi = u S
+        hz_species_sites(o, gAa, gBa, row, 0.0, 0.0, gE * Sw + St, Sw);
+        HD<3> gD = dens_decay(rho_j, row, gBa, r, rt);
+        hz_switch(rho_j, r, rt, Dw, Dt);
+        dens_sites(o + 17, gD, rho_j, Dw, Dt, ci.x, ci.y);
+        dens_sites(o + 21, gD, rho_i, Dw, Dt, cj.x, cj.y);
+    } else {
+        // phi = k psi, psi = 1/2 S (q u_a + u_b / q), q = f_b / f_a, a the
+        // earlier species: psi's derivatives in (f_a, u_a, f_b, u_b), then
+        // each element's chain
+        const double *pb = row + EADJ_NZ;
+        HD<3> gAb = hz_g3(r, rt, pb[0], pb[4], pb[8]);
+        HD<3> gBb = hz_g3(r, rt, pb[0], pb[5], pb[9]);
+        HD<4> fa = hd_param<4>(row[1] * gBa.v, 0, 0), ua = hd_param<4>(row[6] * gAa.v - row[7] * gBa.v, 1, 0);
+        HD<4> fb = hd_param<4>(pb[1] * gBb.v, 2, 0), ub = hd_param<4>(pb[6] * gAb.v - pb[7] * gBb.v, 3, 0);
+        fa.t = row[1] * gBa.t;
+        ua.t = row[6] * gAa.t - row[7] * gBa.t;
+        fb.t = pb[1] * gBb.t;
+        ub.t = pb[6] * gAb.t - pb[7] * gBb.t;
+        HD<4> Sh = hd_const<4>(Sw);
+        Sh.t = St;
+        HD<4> q = fb / fa;
+        HD<4> psi = 0.5 * (Sh * (q * ua + ub / q));
+        double h = row[2 * EADJ_NZ + 2];
+        hz_species_sites(o, gAa, gBa, row, h * (gE * psi.p[0] + psi.q[0]), h * psi.p[0],
+                         h * (gE * psi.p[1] + psi.q[1]), h * psi.p[1]);
+        hz_species_sites(o + 8, gAb, gBb, pb, h * (gE * psi.p[2] + psi.q[2]), h * psi.p[2],
+                         h * (gE * psi.p[3] + psi.q[3]), h * psi.p[3]);
+        o[16] = gE * psi.v + psi.t;
+        // the element blocks of s_i and s_j in the cross row
+        bool i_first = si < sj;
+        const double *bi = i_first ? row : pb, *bj = i_first ? pb : row;
+        HD<3> gDj = dens_decay(rho_j, bj, i_first ? gBb : gBa, r, rt);
+        hz_switch(rho_j, r, rt, Dw, Dt);
+        dens_sites(o + 17, gDj, rho_j, Dw, Dt, ci.x, ci.y);
+        HD<3> gDi = dens_decay(rho_i, bi, i_first ? gBa : gBb, r, rt);
+        hz_switch(rho_i, r, rt, Dw, Dt);
+        dens_sites(o + 21, gDi, rho_i, Dw, Dt, cj.x, cj.y);
     }
-    // the embedding, rho-bar clamped at 0 as the evaluation does
-    double rb = rho > 0.0 ? rho : 0.0;
-    HD<13> F = hz_embed(row_of(T, T.F_f[si]), rb, rho_t);
-#pragma unroll
-    for (int k = 0; k < 12; ++k) out[k] = gE * F.p[k] + F.q[k];
-    double c1 = rho > 0.0 ? gE * F.p[12] + F.q[12] : 0.0;
-    double c2 = F.p[12];
-    // pass 2: density and pair sites per neighbour
-    double *dens = out + 12, *pair = out + 12 + 4 * ns;
-    for (int s = b; s < e; ++s) {
-        int j = nbr[s];
-        double d[3], r, tg[3];
-        adj_leg(S, G, cell, i, j, sst, d, r, tg);
-        if (!(r * r < rc2 && r * r > 1e-24)) continue;
-        int sj = S.types[j];
-        double rt = (d[0] * tg[0] + d[1] * tg[1] + d[2] * tg[2]) / r;
-        {
-            HD<4> r4 = hd_const<4>(r);
-            r4.t = rt;
-            const double *row = row_of(T, T.rho_f[sj]);
-            HD<4> re = hd_param<4>(row[0], 0, 0), fe = hd_param<4>(row[1], 1, 0);
-            HD<4> be = hd_param<4>(row[5], 2, 0), la = hd_param<4>(row[9], 3, 0);
-            HD<4> f = hz_decay<4>(r4, re, fe, be, la) * hz_switch<4>(row, r4);
-            double *o = dens + 4 * sj;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) o[k] += c1 * f.p[k] + c2 * f.q[k];
+    return si * ns + sj;
+}
+
+// Pass 2, a thread per live pair of one segment of the compacted list
+// (like pairs [0, pos[n_slots]) or cross pairs [pos[n_slots], pos[2
+// n_slots])), EADJ_TP pairs per tile: the staged values are sorted by code
+// inside the tile (a counting sort, ranks from warp matches, so the order
+// is fixed), then each (code, value) item is summed over its segment into
+// the block's partialP row (ns^2 * 25).  The two segments are separate
+// instantiations: the like pairs' kernel keeps a smaller register budget.
+template <bool LIKE>
+__global__ void __launch_bounds__(EADJ_TP) eam_adjoint_pairs(SysView S, const int *__restrict__ row_off,
+                                                             const int *__restrict__ nbr, EamAdjTab T, AdjIn G,
+                                                             const double2 *__restrict__ cc,
+                                                             const int *__restrict__ pairs,
+                                                             const int *__restrict__ seg_begin,
+                                                             const int *__restrict__ seg_end,
+                                                             double *__restrict__ partialP) {
+    __shared__ double st[EADJ_TP * EADJ_STRIDE];
+    __shared__ int order[EADJ_TP];
+    __shared__ int wcnt[2][65], start[66];
+    extern __shared__ double accP[];     // ns^2 * 25
+    const int ns = T.ns, nc = ns * ns, ni = nc * EADJ_PS;
+    for (int k = threadIdx.x; k < ni; k += blockDim.x) accP[k] = 0.0;
+    const int p0 = *seg_begin, np = *seg_end - p0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int tile = blockIdx.x; tile * EADJ_TP < np; tile += gridDim.x) {
+        int m = tile * EADJ_TP + threadIdx.x;
+        int code = nc;  // past the last code: not summed
+        if (m < np)
+            code = eam_pair_sites<LIKE>(S, row_off, nbr, T, G, cc, pairs[p0 + m], st + EADJ_STRIDE * threadIdx.x);
+        for (int k = threadIdx.x; k < 2 * 65; k += blockDim.x) (&wcnt[0][0])[k] = 0;
+        __syncthreads();
+        unsigned same = __match_any_sync(MBF_FULL, code);
+        int rank = __popc(same & ((1u << lane) - 1u));
+        if (rank == 0) wcnt[w][code] = __popc(same);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int a = 0;
+            for (int c = 0; c <= nc; ++c) {
+                start[c] = a;
+                a += wcnt[0][c] + wcnt[1][c];
+            }
+            start[nc + 1] = a;
         }
-        HD<8> r8 = hd_const<8>(r);
-        r8.t = rt;
-        const double *row = row_of(T, T.phi_f[si * ns + sj]);
-        HD<8> Sw = hz_switch<8>(row, r8);
-        double *o = pair + 17 * sj;
-        if (si == sj) {
-            HD<8> f, u;
-            hz_species<8>(row, 0, r8, f, u);
-            HD<8> phi = u * Sw;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) o[k] += 0.5 * (gE * phi.p[k] + phi.q[k]);
-        } else {
-            // psi = 1/2 S (q u_a + u_b / q), q = f_b / f_a, phi = k psi
-            double kf = row[2 * EADJ_NZ + 2];
-            HD<1> r1 = hd_const<1>(r);
-            r1.t = rt;
-            HD<1> f1, u1;
-            HD<8> fa, ua, fb, ub;
-            // the earlier species' directions
-            hz_species<8>(row, 0, r8, fa, ua);
-            hz_species<1>(row + EADJ_NZ, -100, r1, f1, u1);
-            fb = hd_lift<8, 1>(f1);
-            ub = hd_lift<8, 1>(u1);
-            HD<8> q = fb / fa;
-            HD<8> psi = 0.5 * (Sw * (q * ua + ub / q));
-#pragma unroll
-            for (int k = 0; k < 8; ++k) o[k] += 0.5 * kf * (gE * psi.p[k] + psi.q[k]);
-            o[16] += 0.5 * (gE * psi.v + psi.t);
-            // the later species' directions
-            hz_species<1>(row, -100, r1, f1, u1);
-            fa = hd_lift<8, 1>(f1);
-            ua = hd_lift<8, 1>(u1);
-            hz_species<8>(row + EADJ_NZ, 0, r8, fb, ub);
-            q = fb / fa;
-            psi = 0.5 * (Sw * (q * ua + ub / q));
-#pragma unroll
-            for (int k = 0; k < 8; ++k) o[8 + k] += 0.5 * kf * (gE * psi.p[k] + psi.q[k]);
+        __syncthreads();
+        order[start[code] + (w ? wcnt[0][code] : 0) + rank] = threadIdx.x;
+        __syncthreads();
+        for (int item = threadIdx.x; item < ni; item += blockDim.x) {
+            int c = item / EADJ_PS, k = item % EADJ_PS;
+            double a = 0.0;
+            for (int q = start[c]; q < start[c + 1]; ++q) a += st[EADJ_STRIDE * order[q] + k];
+            accP[item] += a;
         }
+        __syncthreads();
     }
-    return si;
+    for (int k = threadIdx.x; k < ni; k += blockDim.x) partialP[(size_t)blockIdx.x * ni + k] = accP[k];
 }
 
 // Column -> site of a role (-1: not differentiated).
@@ -229,73 +389,78 @@ __device__ __forceinline__ int p_site(int c) {
     return c == 42 ? 16 : -1;
 }
 
-// Sum of entry e = row * 43 + col over `cnt` staged atoms, in atom order.
-__device__ double eam_entry_sum(const EamAdjTab &T, int e, int W, int cnt, const double *__restrict__ sm,
-                                const int *__restrict__ scode) {
-    const int ns = T.ns;
+// One warp per entry (row f, column c) of d_P: the block partials that feed
+// it -- the embedding sums of the row's species, the density values of
+// every code with that neighbour (i's view) or centre (j's view) species,
+// the pair values of the row's code(s) -- summed over blocks by lanes, then
+// a fixed shuffle tree.
+__global__ void eam_adjoint_final(EamAdjTab T, int gA, const double *__restrict__ partialF, int gP,
+                                  const double *__restrict__ partialP, double *__restrict__ d_P) {
+    const int ns = T.ns, nfs = 12 * ns, ni = ns * ns * EADJ_PS;
+    int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, l = threadIdx.x & 31;
+    if (e >= T.nf * EADJ_NCOL) return;  // whole warps leave together
     int f = e / EADJ_NCOL, c = e % EADJ_NCOL;
-    double a = 0.0;
+    int idx[16], n = 0;  // items of partialP feeding this entry (<= 2 ns)
+    int fitem = -1;      // item of partialF
     for (int s = 0; s < ns; ++s) {
-        if (T.F_f[s] == f) {
-            int k = f_site(c);
-            if (k >= 0)
-                for (int q = 0; q < cnt; ++q)
-                    if (scode[q] == s) a += sm[(size_t)q * W + k];
-        }
-        if (T.rho_f[s] == f) {
-            int k = d_site(c);
-            if (k >= 0)
-                for (int q = 0; q < cnt; ++q)
-                    if (scode[q] >= 0) a += sm[(size_t)q * W + 12 + 4 * s + k];
-        }
+        if (T.F_f[s] == f && f_site(c) >= 0) fitem = 12 * s + f_site(c);
+        if (T.rho_f[s] == f && d_site(c) >= 0)
+            for (int x = 0; x < ns; ++x) {
+                idx[n++] = (x * ns + s) * EADJ_PS + 17 + d_site(c);  // centre x, neighbour s
+                idx[n++] = (s * ns + x) * EADJ_PS + 21 + d_site(c);  // centre s: j's view
+            }
     }
     for (int x = 0; x < ns; ++x)
         for (int y = x; y < ns; ++y) {
-            if (T.phi_f[x * ns + y] != f) continue;
             int k = p_site(c);
-            if (k < 0 || (x == y && k >= 8)) continue;
-            for (int q = 0; q < cnt; ++q) {
-                int si = scode[q];
-                if (si == x) a += sm[(size_t)q * W + 12 + 4 * ns + 17 * y + k];
-                else if (si == y) a += sm[(size_t)q * W + 12 + 4 * ns + 17 * x + k];
-            }
+            if (T.phi_f[x * ns + y] != f || k < 0 || (x == y && k >= 8)) continue;
+            idx[n++] = (x * ns + y) * EADJ_PS + k;
+            if (x != y) idx[n++] = (y * ns + x) * EADJ_PS + k;
         }
-    return a;
-}
-
-// Block b takes atoms b*EADJ_BLOCK ..: a thread per atom, site values staged
-// in shared memory, then the block's sum of every entry to partial[b].
-__global__ void __launch_bounds__(EADJ_BLOCK) eam_adjoint_atoms(SysView S, const int *__restrict__ row_off,
-                                                                const int *__restrict__ nbr, EamAdjTab T,
-                                                                AdjIn G, int W, double *__restrict__ partial) {
-    extern __shared__ double sm[];  // EADJ_BLOCK * W site values, then EADJ_BLOCK codes
-    int *scode = reinterpret_cast<int *>(sm + (size_t)EADJ_BLOCK * W);
-    int i0 = blockIdx.x * EADJ_BLOCK;
-    int i = i0 + threadIdx.x;
-    int c = -1;
-    if (i < S.n_atoms) c = eam_atom_sites(S, row_off, nbr, T, G, i, W, sm + (size_t)threadIdx.x * W);
-    scode[threadIdx.x] = c;
-    __syncthreads();
-    int cnt = min(EADJ_BLOCK, S.n_atoms - i0);
-    int ne = T.nf * EADJ_NCOL;
-    for (int e = threadIdx.x; e < ne; e += blockDim.x)
-        partial[(size_t)blockIdx.x * ne + e] = eam_entry_sum(T, e, W, cnt, sm, scode);
-}
-
-// One warp per entry: lanes take every 32nd block partial, then a fixed
-// shuffle tree.
-__global__ void eam_adjoint_final(int n_blocks, int ne, const double *__restrict__ partial,
-                                  double *__restrict__ d_P) {
-    int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, l = threadIdx.x & 31;
-    if (e >= ne) return;  // whole warps leave together
     double acc = 0.0;
-    for (int b = l; b < n_blocks; b += 32) acc += partial[(size_t)b * ne + e];
+    if (fitem >= 0)
+        for (int b = l; b < gA; b += 32) acc += partialF[(size_t)b * nfs + fitem];
+    for (int b = l; b < gP; b += 32) {  // the like and the cross kernels' rows
+        const double *pp = partialP + (size_t)b * ni;
+        for (int q = 0; q < n; ++q) acc += pp[idx[q]];
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(MBF_FULL, acc, o);
     if (l == 0) d_P[e] = acc;
 }
 
-static int eadj_blocks(int n_atoms) { return n_atoms > 0 ? (n_atoms + EADJ_BLOCK - 1) / EADJ_BLOCK : 1; }
+// Workspace of one call.
+struct EadjLayout {
+    size_t partialF, partialP, cc, flag, pos, pairs, scan, total;
+    int gA, gP;
+};
+
+static EadjLayout eadj_layout(int n_atoms, long long n_slots, int ns) {
+    EadjLayout L;
+    long long ns2 = n_slots > 0 ? n_slots : 1;
+    int tiles_a = (int)((n_atoms + EADJ_TA - 1) / EADJ_TA);
+    long long tiles_p = (ns2 + EADJ_TP - 1) / EADJ_TP;  // the live pairs are at most the slots
+    L.gA = tiles_a < 1 ? 1 : (tiles_a < 65535 ? tiles_a : 65535);
+    L.gP = (int)(tiles_p < EADJ_GRID ? tiles_p : EADJ_GRID);  // rows per pair kernel, at most
+    if (L.gP < 1) L.gP = 1;
+    size_t o = 0;
+    L.partialF = o;
+    o = align256(o + sizeof(double) * (size_t)L.gA * 12 * ns);
+    L.partialP = o;
+    o = align256(o + sizeof(double) * (size_t)2 * L.gP * ns * ns * EADJ_PS);
+    L.cc = o;
+    o = align256(o + sizeof(double2) * (size_t)(n_atoms > 0 ? n_atoms : 1));
+    L.flag = o;
+    o = align256(o + sizeof(int) * (size_t)(2 * ns2));
+    L.pos = o;
+    o = align256(o + sizeof(int) * (size_t)(2 * ns2 + 1));
+    L.pairs = o;
+    o = align256(o + sizeof(int) * (size_t)ns2);
+    L.scan = o;
+    o = align256(o + sizeof(int) * scan_workspace_ints((int)(2 * ns2)));
+    L.total = o;
+    return L;
+}
 
 }  // namespace mbf
 
@@ -303,9 +468,9 @@ using namespace mbf;
 
 extern "C" {
 
-size_t mbf_eam_adjoint_workspace_bytes(int n_atoms, int nf) {
-    if (n_atoms < 0 || nf <= 0) return 0;
-    return align256(sizeof(double) * (size_t)eadj_blocks(n_atoms) * nf * EADJ_NCOL);
+size_t mbf_eam_adjoint_workspace_bytes(int n_atoms, long long n_slots, int ns) {
+    if (n_atoms < 0 || n_slots < 0 || ns <= 0 || ns > 8 || 2 * n_slots + 1 > 0x7fffffffLL) return 0;
+    return eadj_layout(n_atoms, n_slots, ns).total;
 }
 
 int mbf_eam_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab, const double *g_energy,
@@ -313,8 +478,9 @@ int mbf_eam_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
                     double *d_P, void *stream) {
     if (!sys || !nl || !tab || !workspace || !d_P || tab->ns <= 0 || tab->ns > 8 || tab->nf <= 0)
         return MBF_ERR_ARGUMENT;
-    if (nl->n_atoms != sys->n_atoms) return MBF_ERR_ARGUMENT;
-    if (workspace_bytes < mbf_eam_adjoint_workspace_bytes(sys->n_atoms, tab->nf)) return MBF_ERR_WORKSPACE;
+    if (nl->n_atoms != sys->n_atoms || !nl->upper || 2 * nl->n_slots + 1 > 0x7fffffffLL) return MBF_ERR_ARGUMENT;
+    EadjLayout L = eadj_layout(sys->n_atoms, nl->n_slots, tab->ns);
+    if (workspace_bytes < L.total) return MBF_ERR_WORKSPACE;
     cudaStream_t st = (cudaStream_t)stream;
     int ne = tab->nf * EADJ_NCOL;
     if (sys->n_atoms == 0) {
@@ -334,20 +500,38 @@ int mbf_eam_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
     G.gE = g_energy;
     G.gF = g_forces;
     G.gW = g_virial;
-    int W = 12 + 21 * tab->ns;
-    size_t smem = (size_t)EADJ_BLOCK * W * sizeof(double) + EADJ_BLOCK * sizeof(int);  // <= 93 KB (ns <= 8)
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(eam_adjoint_atoms, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
-        return MBF_ERR_CUDA;
-    int nb = eadj_blocks(sys->n_atoms);
-    double *partial = ws_at<double>(workspace, 0);
-    PROF_BEGIN("eam_adjoint_atoms", st);
-    eam_adjoint_atoms<<<nb, EADJ_BLOCK, smem, st>>>(S, nl->row_off, nl->nbr, T, G, W, partial);
-    PROF_END("eam_adjoint_atoms", st);
+    int n_slots = (int)(nl->n_slots > 0 ? nl->n_slots : 1);
+    double *partialF = ws_at<double>(workspace, L.partialF);
+    double *partialP = ws_at<double>(workspace, L.partialP);
+    double2 *cc = ws_at<double2>(workspace, L.cc);
+    int *flag = ws_at<int>(workspace, L.flag);
+    int *pos = ws_at<int>(workspace, L.pos);
+    int *pairs = ws_at<int>(workspace, L.pairs);
+    if (cudaMemsetAsync(flag, 0, sizeof(int) * 2 * (size_t)n_slots, st) != cudaSuccess) return MBF_ERR_CUDA;
+    PROF_BEGIN("eam_adjoint_embed", st);
+    eam_adjoint_embed<<<L.gA, EADJ_TA, sizeof(double) * 12 * T.ns, st>>>(S, nl->row_off, nl->upper, nl->nbr, T, G,
+                                                                          n_slots, cc, flag, partialF);
+    MBF_CHECK_LAUNCH();
+    int rc = exclusive_scan(flag, pos, 2 * n_slots, ws_at<int>(workspace, L.scan), st);
+    if (rc != MBF_OK) return rc;
+    eam_adjoint_compact<<<(2 * n_slots + 255) / 256, 256, 0, st>>>(2 * n_slots, flag, pos, n_slots, pairs);
+    PROF_END("eam_adjoint_embed", st);
+    MBF_CHECK_LAUNCH();
+    // like pairs [pos[0], pos[n_slots]), cross pairs [pos[n_slots], pos[2 n_slots])
+    size_t psm = sizeof(double) * T.ns * T.ns * EADJ_PS;
+    int gL = persistent_grid(L.gP, EADJ_TP, (const void *)eam_adjoint_pairs<true>, psm);
+    int gC = persistent_grid(L.gP, EADJ_TP, (const void *)eam_adjoint_pairs<false>, psm);
+    size_t ni = (size_t)T.ns * T.ns * EADJ_PS;
+    PROF_BEGIN("eam_adjoint_pairs", st);
+    eam_adjoint_pairs<true><<<gL, EADJ_TP, psm, st>>>(S, nl->row_off, nl->nbr, T, G, cc, pairs, pos, pos + n_slots,
+                                                       partialP);
+    MBF_CHECK_LAUNCH();
+    eam_adjoint_pairs<false><<<gC, EADJ_TP, psm, st>>>(S, nl->row_off, nl->nbr, T, G, cc, pairs, pos + n_slots,
+                                                        pos + 2 * n_slots, partialP + (size_t)gL * ni);
+    PROF_END("eam_adjoint_pairs", st);
     MBF_CHECK_LAUNCH();
     PROF_BEGIN("eam_adjoint_reduce", st);
-    eam_adjoint_final<<<(ne * 32 + 127) / 128, 128, 0, st>>>(nb, ne, partial, d_P);
+    eam_adjoint_final<<<(ne * 32 + 127) / 128, 128, 0, st>>>(T, L.gA, partialF, gL + gC, partialP, d_P);
     PROF_END("eam_adjoint_reduce", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;

@@ -738,7 +738,7 @@ class _EamTableEval:
         b, dl = self.batch, self.dlist
         dev = b.device
         L = _lib.lib()
-        need = int(L.mbf_eam_adjoint_workspace_bytes(b.n_atoms, self.nf))
+        need = int(L.mbf_eam_adjoint_workspace_bytes(b.n_atoms, dl.n_slots, self.ns))
         if self._adj_ws is None or self._adj_ws.numel() < need:
             self._adj_ws = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
         d_P = torch.empty_like(P)

@@ -595,6 +595,63 @@ def _fit_setup():
     return ps, x0, xt
 
 
+def make_ni3al_set(n=256, a=3.57, strain=0.02, sigma=0.08, seed=0):
+    """L1_2 Ni3Al (Al on the cube corners), 4^3 or 5^3 conventional cells
+    (256 or 500 atoms), symmetric strain entries uniform +-2 %, Gaussian
+    displacements."""
+    rng = np.random.default_rng(seed)
+    fcc = np.array([[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0]], float)
+    types4 = ["Al", "Ni", "Ni", "Ni"]
+    out = []
+    for _ in range(n):
+        m = int(rng.integers(4, 6))
+        g = np.arange(m)
+        cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+        frac = (fcc[None] + cells[:, None]).reshape(-1, 3)
+        lat = np.eye(3) * a * m
+        pos = frac * a
+        e = rng.uniform(-strain, strain, (3, 3))
+        M = np.eye(3) + 0.5 * (e + e.T)
+        lat, pos = lat @ M, pos @ M
+        pos = pos + rng.normal(0.0, sigma, pos.shape)
+        out.append((lat, pos, types4 * len(cells)))
+    return out
+
+
+def _fit_setup_zhou():
+    """The Zhou (2004) Al-Ni parameter set (ZhouEAMParameterSet defaults:
+    A B alpha beta Fn2 Fn3 F2 F3 eta per element) and its target
+    parameters theta * U(0.97, 1.03) (seeded), as x vectors."""
+    from akitsushima_b200 import fit
+    from akitsushima_b200.published_parameters import ZHOU_2004
+    species = ["Al", "Ni"]
+    ps = fit.ZhouEAMParameterSet({s: dict(ZHOU_2004[s]) for s in species}, species)
+    x0 = ps.x0
+    u = np.random.default_rng(7).uniform(0.97, 1.03, len(x0))
+    xt = np.array([np.log(np.exp(x) * f) if key in ps._LOG_KEYS else x * f
+                   for x, f, (_, key, _) in zip(x0, u, ps.variables)])
+    return ps, x0, xt
+
+
+FIT_WORKLOADS = {
+    # name: (structure set, parameter set, loss weights, config)
+    "fit_sic256": (lambda: make_sic_set(256), _fit_setup, {"energy": 1.0, "forces": 1.0, "stress": 0.1},
+                   {"workload": "fit_sic256_tersoff1989",
+                    "sizes": "zincblende SiC 2^3 / 3^3 cells (64 / 216 atoms)", "a": 4.36, "strain": 0.02,
+                    "sigma": 0.1, "parameter_set": "Tersoff1989ParameterSet (A B lambda mu c d h per element, chi)",
+                    "targets": "float64 E/F/S at theta * U(0.95, 1.05)",
+                    "loss": "w_E 1, w_F 1, w_S 0.1, r0 1, eps0 1 (squared)"}),
+    "fit_ni3al256_zhou": (lambda: make_ni3al_set(256), _fit_setup_zhou,
+                          {"energy": 1.0, "forces": 1.0, "stress": 1.0, "r0": 0.1, "eps0": 0.01},
+                          {"workload": "fit_ni3al256_zhou2004",
+                           "sizes": "L1_2 Ni3Al 4^3 / 5^3 cells (256 / 500 atoms)", "a": 3.57, "strain": 0.02,
+                           "sigma": 0.08,
+                           "parameter_set": "ZhouEAMParameterSet (A B alpha beta Fn2 Fn3 F2 F3 eta per element)",
+                           "targets": "float64 E/F/S at theta * U(0.97, 1.03)",
+                           "loss": "w_E 1, w_F 1, w_S 1, r0 0.1, eps0 0.01 (squared)"}),
+}
+
+
 def _fit_structs(raw, efs):
     out = []
     for (lat, pos, types), (e, f, s) in zip(raw, efs):
@@ -603,7 +660,7 @@ def _fit_structs(raw, efs):
     return out
 
 
-def time_reference_fit(raw, ps, x0, xt, n_sample):
+def time_reference_fit(raw, ps, x0, xt, n_sample, w):
     """The reference's gradient: forward differences of the loss, one loss
     evaluation per variable plus one (fitting/driver.py:802-816), each a
     loop of force calls (fitting/loss.py:184-242) -- the oracle port under
@@ -613,15 +670,24 @@ def time_reference_fit(raw, ps, x0, xt, n_sample):
     threads = cpu_count()
     oracle.set_threads(threads)
     sample = raw[:n_sample]
-    rec_t = ps.decode(xt)["tersoff"]
-    efs = [oracle.tersoff_multi(rec_t, ps.species, L, P, T) for L, P, T in sample]
+    if "eam" in ps.decode(x0):
+        def force_of(x):
+            d = ps.decode(x)["eam"]
+            return oracle.zhou_force(d["elements"], ps.species, d["r_cut"], d["chi"])
+        r_list = ps.r_cut + 0.3
+    else:
+        def force_of(x):
+            rec = ps.decode(x)["tersoff"]
+            return lambda L, P, T, pairs: oracle.tersoff_multi(rec, ps.species, L, P, T, pairs)
+        r_list = 3.0 + 0.3
+    pairs = [oracle.nl_build(L, P, r_list - 0.3, 0.3)[:2] for L, P, _ in sample]
+    ft = force_of(xt)
+    efs = [ft(L, P, T, pq) for (L, P, T), pq in zip(sample, pairs)]
     st = _fit_structs(sample, efs)
-    pairs = [oracle.nl_build(L, P, 3.0, 0.3)[:2] for L, P, _ in sample]
-    w = {"energy": 1.0, "forces": 1.0, "stress": 0.1}
-    rec0 = ps.decode(x0)["tersoff"]
-    oracle.fit_loss(rec0, ps.species, st, w, pairs)
+    f0 = force_of(x0)
+    oracle.fit_loss(None, ps.species, st, w, pairs, force=f0)
     t0 = time.perf_counter()
-    oracle.fit_loss(rec0, ps.species, st, w, pairs)
+    oracle.fit_loss(None, ps.species, st, w, pairs, force=f0)
     t_loss = time.perf_counter() - t0
     atoms_sample = sum(len(p) for _, p, _ in sample)
     atoms_all = sum(len(p) for _, p, _ in raw)
@@ -629,25 +695,22 @@ def time_reference_fit(raw, ps, x0, xt, n_sample):
 
 
 def run_fit(args, world, rank, local):
-    n_struct = 256
-    raw = make_sic_set(n_struct)
+    make_set, setup, weights, cfg0 = FIT_WORKLOADS[args.workload]
+    raw = make_set()
+    n_struct = len(raw)
     n_atoms = sum(len(p) for _, p, _ in raw)
-    cfg = {"workload": "fit_sic256_tersoff1989", "n_structures": n_struct, "n_atoms": n_atoms,
-           "sizes": "zincblende SiC 2^3 / 3^3 cells (64 / 216 atoms)", "a": 4.36, "strain": 0.02,
-           "sigma": 0.1, "parameter_set": "Tersoff1989ParameterSet (A B lambda mu c d h per element, chi)",
-           "targets": "float64 E/F/S at theta * U(0.95, 1.05)",
-           "loss": "w_E 1, w_F 1, w_S 0.1, r0 1, eps0 1 (squared)", "precision": "fp64",
-           "l2": "256 MB scratch write between steps, outside the timed events",
-           "parallelism": f"split{world}"}
+    cfg = dict(cfg0, n_structures=n_struct, n_atoms=n_atoms, precision="fp64",
+               l2="256 MB scratch write between steps, outside the timed events", parallelism=f"split{world}")
+    n_sample = 16 if args.workload == "fit_sic256" else 4
     from akitsushima_b200 import fit
-    ps, x0, xt = _fit_setup()
+    ps, x0, xt = setup()
     n_var = len(x0)
     if args.impl == "reference":
         if rank != 0:
             return 0
         per = []
         for _ in range(max(1, args.steps)):
-            t, threads = time_reference_fit(raw, ps, x0, xt, 16)
+            t, threads = time_reference_fit(raw, ps, x0, xt, n_sample, weights)
             per.append(1.0 / t)
         v = float(np.mean(per))
         line = {"metric": "fit grads/s", "value": v, "unit": "gradients/s", "impl": "reference",
@@ -655,8 +718,8 @@ def run_fit(args, world, rank, local):
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": cfg,
                 "cpu_baseline": {"value": v, "unit": "gradients/s", "cores": threads, "kind": "port",
-                                 "sample": f"one loss over the first 16 structures, scaled by atoms to the "
-                                           f"256 and by {n_var + 1} (forward differences)"},
+                                 "sample": f"one loss over the first {n_sample} structures, scaled by atoms to "
+                                           f"the {n_struct} and by {n_var + 1} (forward differences)"},
                 "e2e": {"value": v, "unit": "gradients/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
@@ -674,18 +737,17 @@ def run_fit(args, world, rank, local):
     dev = torch.device("cuda", torch.cuda.current_device())
     from akitsushima_b200 import _lib
     # targets: float64 evaluation of every structure at the target parameters
-    tgt = fit.TersoffFit(ps, [{"lattice": L, "positions": P, "atom_types": T, "natoms": len(P),
-                               "ref_energy": 0.0} for L, P, T in raw], device=dev)
-    tb, tri = fit.tables_from_records(ps.decode(xt)["tersoff"], ps.species, dev)
-    E, F, W = tgt.ev.evaluate(tb, tri)
+    tgt = fit.PotentialFit(ps, [{"lattice": L, "positions": P, "atom_types": T, "natoms": len(P),
+                                 "ref_energy": 0.0} for L, P, T in raw], device=dev)
+    with torch.no_grad():
+        E, F, W = tgt.model.efs(torch.as_tensor(xt), tgt.ev)
     E, F, W = E.cpu().numpy(), F.cpu().numpy(), W.cpu().numpy()
     off = tgt.ev.batch.offsets
     vols = tgt.ev.batch.volumes
     efs = [(E[q], F[off[q]:off[q + 1]], W[q].reshape(3, 3) / vols[q]) for q in range(n_struct)]
     structs = _fit_structs(raw, efs)
     del tgt
-    f = fit.TersoffFit(ps, structs, {"energy": 1.0, "forces": 1.0, "stress": 0.1}, device=dev,
-                       rank=rank, world=world)
+    f = fit.PotentialFit(ps, structs, weights, device=dev, rank=rank, world=world)
     # x and its decode live on the host (a few dozen scalars); the batch,
     # the evaluation, the loss over 38k atoms and the adjoint on the device
     x_host = torch.tensor(x0, dtype=torch.float64, requires_grad=True)
@@ -735,10 +797,10 @@ def run_fit(args, world, rank, local):
         t_e2e = float(t.item())
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        t_cpu, threads = time_reference_fit(raw, ps, x0, xt, 16)
+        t_cpu, threads = time_reference_fit(raw, ps, x0, xt, n_sample, weights)
         cpu = {"value": 1.0 / t_cpu, "unit": "gradients/s", "cores": threads, "kind": "port",
-               "sample": f"one loss over the first 16 structures (oracle port), scaled by atoms to the 256 "
-                         f"and by {n_var + 1}: the reference's forward-difference gradient"}
+               "sample": f"one loss over the first {n_sample} structures (oracle port), scaled by atoms to the "
+                         f"{n_struct} and by {n_var + 1}: the reference's forward-difference gradient"}
     clocks = clk.summary()
     if dist:
         dist.barrier()
@@ -753,7 +815,7 @@ def run_fit(args, world, rank, local):
             "kernels": {k: {"launches": c, "ms_per_launch": t / c} for k, (c, t) in prof.items()},
             "e2e": {"value": 1.0 / t_e2e, "unit": "gradients/s", "h2d_bytes_per_step": 8 * n_var,
                     "d2h_bytes_per_step": 8 * (n_var + 2), "ms_per_step": t_e2e * 1e3,
-                    "path": "TersoffFit.loss_and_grad(numpy x) -> (loss, numpy gradient)"},
+                    "path": "PotentialFit.loss_and_grad(numpy x) -> (loss, numpy gradient)"},
             "check": {"loss": float(loss), "grad_norm": float(np.linalg.norm(grad))},
             "cpu_baseline": cpu, "roofline": None}
     print(json.dumps(line), flush=True)
@@ -931,8 +993,8 @@ def main():
     ap.add_argument("--skip-singles", action="store_true",
                     help="batched workload: skip the per-structure-launch comparison (profiling runs)")
     ap.add_argument("--workload", default="eam_cuni_256k",
-                    choices=["eam_cuni_256k", "batched_si512", "fit_sic256", "eam_setfl_cuni_256k",
-                             "sw_gesn_64k"] + sorted(MD_WORKLOADS))
+                    choices=["eam_cuni_256k", "batched_si512", "eam_setfl_cuni_256k",
+                             "sw_gesn_64k"] + sorted(FIT_WORKLOADS) + sorted(MD_WORKLOADS))
     args = ap.parse_args()
     args.precision_given = "--precision" in sys.argv
     args.warmup = max(3, args.warmup)
@@ -944,7 +1006,7 @@ def main():
         return run_batched(args, world, rank, local)
     if args.workload in MD_WORKLOADS:
         return run_md(args, world, rank, local)
-    if args.workload == "fit_sic256":
+    if args.workload in FIT_WORKLOADS:
         return run_fit(args, world, rank, local)
     if args.workload in ("eam_setfl_cuni_256k", "sw_gesn_64k"):
         return run_perf_path(args, world, rank, local)

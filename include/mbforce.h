@@ -236,9 +236,10 @@ int mbf_eam_eval_static(const mbf_system *sys, const mbf_nlist *nl, const mbf_ea
  * generic evaluation reads (rho_f, F_f, phi_f).  Replaces the
  * forward-difference Jacobian of the reference's fit over
  * ZhouEAMParameterSet (fitting/driver.py:802-816,
- * fitting/parameter_sets.py:1306-1400).  Deterministic.  ns <= 8; the
- * workspace needs mbf_eam_adjoint_workspace_bytes(n_atoms, nf).         */
-size_t mbf_eam_adjoint_workspace_bytes(int n_atoms, int nf);
+ * fitting/parameter_sets.py:1306-1400).  Each unordered pair is visited
+ * once; deterministic.  ns <= 8; the workspace needs
+ * mbf_eam_adjoint_workspace_bytes(n_atoms, n_slots, ns).                 */
+size_t mbf_eam_adjoint_workspace_bytes(int n_atoms, long long n_slots, int ns);
 int mbf_eam_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
                     const double *g_energy, const double *g_forces, const double *g_virial,
                     void *workspace, size_t workspace_bytes, double *d_P, void *stream);
