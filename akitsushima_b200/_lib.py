@@ -44,6 +44,14 @@ class MbfEamTables(ctypes.Structure):
                 ("phi_f", _vp), ("r_cut", _d), ("zhou_fused", _i)]
 
 
+class MbfFitSet(ctypes.Structure):
+    _fields_ = [("n_struct", _i), ("n_atoms", _i)] + \
+        [(k, _vp) for k in ("struct_off", "atom_struct", "n_orig", "fref_off", "inv_k", "e_ref", "f_ref",
+                            "s_ref", "vol", "vsup", "fmask", "smask", "cw")] + \
+        [(k, _d) for k in ("w_e", "w_f", "w_s", "r0", "eps0")] + [("huber", _i)] + \
+        [(k, _d) for k in ("delta_e", "delta_f", "delta_s")]
+
+
 class MbfTersoffTables(ctypes.Structure):
     _fields_ = [("ns", _i), ("tb", _vp), ("tri", _vp), ("r_cut", _d)]
 
@@ -103,6 +111,8 @@ _SIGS = {
     "mbf_eam_eval_sites": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                                 ctypes.POINTER(MbfEamTables), ctypes.POINTER(MbfReducePlan), _i, _i,
                                 _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "mbf_fit_loss_workspace_bytes": (_sz, [_i]),
+    "mbf_fit_loss": (_i, [ctypes.POINTER(MbfFitSet), _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp, _vp]),
     "mbf_eam_adjoint_workspace_bytes": (_sz, [_i, _ll, _i]),
     "mbf_eam_adjoint": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                              ctypes.POINTER(MbfEamTables), _vp, _vp, _vp, _vp, _sz, _vp, _vp]),

@@ -73,7 +73,7 @@ def tables_from_records(records, species, device):
 
 def table_cutoff(tb):
     """Largest R + D over the valid pair records (the list radius)."""
-    t = tb.detach().cpu().numpy()
+    t = tb.detach().cpu().numpy() if torch.is_tensor(tb) else np.asarray(tb)
     valid = t[:, 0] != 0.0
     return float(np.max(t[valid, 5] + t[valid, 6])) if valid.any() else 0.0
 
@@ -120,6 +120,30 @@ class _Variables:
 
     def build_engine(self, params):
         return PotentialEngine().add(TersoffPotential(params["tersoff"], species=self.species))
+
+    def _vals_np(self, X):
+        """Variable values of the rows of X (B, n_var), exp of the log keys."""
+        logm = np.array([key in self._LOG_KEYS for _, key, _ in self.variables], bool)
+        V = np.array(X, dtype=X.dtype, copy=True)
+        V[:, logm] = np.exp(X[:, logm])
+        return V
+
+    def tables_np(self, x):
+        """The device tables of decode(x) as float64 numpy arrays."""
+        return [t[0].real.copy() for t in self._tables_np(np.asarray(x, float)[None].astype(complex))]
+
+    def table_jacobian(self, x):
+        """(tables at x, d tables / dx): every variable's derivative by the
+        complex step (Squire and Trapp, SIAM Rev. 40, 110 (1998)) in one
+        vectorised evaluation -- exact to rounding, as the table maps are
+        analytic.  Jacobians have shape (n_var,) + table shape."""
+        x = np.asarray(x, float)
+        n = len(x)
+        h = 1e-30
+        X = np.repeat(x[None].astype(complex), n + 1, axis=0)
+        X[1:] += 1j * h * np.eye(n)
+        outs = self._tables_np(X)
+        return [o[0].real.copy() for o in outs], [o[1:].imag / h for o in outs]
 
 
 def _nested(records):
@@ -259,6 +283,20 @@ class MultiSpeciesTersoffParameterSet(_Variables):
         vals = torch.where(logm, torch.exp(x), x)
         tb = tb0.clone().index_put((tbp[1], tbp[2]), vals[tbp[0]])
         tri = tri0.clone().index_put((trip[1], trip[2]), vals[trip[0]])
+        return tb, tri
+
+    def _tables_np(self, X):
+        """tables_torch over the rows of X (B, n_var): (tb (B, ns^2, 10),
+        tri (B, ns^3, 8)) in X's dtype."""
+        if not hasattr(self, "_plan"):
+            self.tables_torch(torch.as_tensor(self.x0))
+        tb0, tri0, tbp, trip, _ = self._plan
+        V = self._vals_np(X)
+        B = X.shape[0]
+        tb = np.repeat(tb0.numpy()[None].astype(X.dtype), B, axis=0)
+        tri = np.repeat(tri0.numpy()[None].astype(X.dtype), B, axis=0)
+        tb[:, tbp[1].numpy(), tbp[2].numpy()] = V[:, tbp[0].numpy()]
+        tri[:, trip[1].numpy(), trip[2].numpy()] = V[:, trip[0].numpy()]
         return tb, tri
 
 
@@ -409,6 +447,34 @@ class Tersoff1989ParameterSet(_Variables):
                            0.0 * one3, 3.0 * one3, om[:, None, :] * one3, 0.0 * one3], dim=-1).reshape(ns ** 3, 8)
         return tb, tri
 
+    def _tables_np(self, X):
+        """tables_torch over the rows of X (B, n_var), in X's dtype."""
+        ns = len(self.species)
+        if not hasattr(self, "_plan"):
+            self.tables_torch(torch.as_tensor(self.x0))
+        el0, chi0, om, ev, er, ec, cv, c0, c1, _ = [t.numpy() if torch.is_tensor(t) else t for t in self._plan]
+        V = self._vals_np(X)
+        B = X.shape[0]
+        el = np.repeat(el0[None].astype(X.dtype), B, axis=0)
+        chi = np.repeat(chi0[None].astype(X.dtype), B, axis=0)
+        if len(ev):
+            el[:, er, ec] = V[:, ev]
+        if len(cv):
+            chi[:, c0, c1] = V[:, cv]
+        A, Bb, lam, mu, beta, n, c, d, h, R, S = np.moveaxis(el, -1, 0)
+        r = np.sqrt(R[:, :, None] * R[:, None, :])
+        sx = np.sqrt(S[:, :, None] * S[:, None, :])
+        one = np.ones((B, ns, ns), X.dtype)
+        tb = np.stack([one, np.sqrt(A[:, :, None] * A[:, None, :]), chi * np.sqrt(Bb[:, :, None] * Bb[:, None, :]),
+                       0.5 * (lam[:, :, None] + lam[:, None, :]), 0.5 * (mu[:, :, None] + mu[:, None, :]),
+                       0.5 * (r + sx), 0.5 * (sx - r), beta[:, :, None] * one, n[:, :, None] * one, 0.0 * one],
+                      axis=-1).reshape(B, ns * ns, 10)
+        one3 = np.ones((B, ns, ns, ns), X.dtype)
+        tri = np.stack([one3, c[:, :, None, None] * one3, d[:, :, None, None] * one3, h[:, :, None, None] * one3,
+                        0.0 * one3, 3.0 * one3, om[None, :, None, :] * one3, 0.0 * one3],
+                       axis=-1).reshape(B, ns ** 3, 8)
+        return tb, tri
+
 
 # ---- Zhou (2004) EAM -------------------------------------------------------------
 
@@ -458,6 +524,28 @@ def zhou_table_torch(el, chi, r_cut, width=0.5):
             rows.append(torch.cat([el[a], z20, sw, z1]) if a == b else
                         torch.cat([el[a], el[b], sw, chi[a, b].reshape(1)]))
     return torch.stack(rows)
+
+
+def continuous_np(el):
+    """continuous_torch on a numpy array (..., 20), real or complex."""
+    c = _ZCOL
+    re, rs, eta = el[..., c["rho_e"]], el[..., c["rho_s"]], el[..., c["eta"]]
+    F1, F2, F3 = el[..., c["F1"]], el[..., c["F2"]], el[..., c["F3"]]
+    y, x = 0.15, -0.15
+    t0 = 1.15 * re / rs
+    lt0 = np.log(t0)
+    slope0 = (F1 + 2 * F2 * y + 3 * F3 * y * y) / re
+    dg = -eta * eta * lt0 * np.exp((eta - 1.0) * lt0) / rs
+    if np.any(np.real(dg) == 0.0):
+        raise ValueError("Zhou EAM: rho_0 = rho_s (or eta = 0) leaves F_e undetermined")
+    Fe = slope0 / dg
+    F0 = Fe * (1 - eta * lt0) * np.exp(eta * lt0) - (F1 * y + F2 * y * y + F3 * y ** 3)
+    out = np.array(el, copy=True)
+    out[..., c["F_e"]] = Fe
+    out[..., c["F0"]] = F0
+    out[..., c["Fn0"]] = F0 + F1 * x + F2 * x * x + F3 * x ** 3
+    out[..., c["Fn1"]] = 0.85 * (F1 + 2 * F2 * x + 3 * F3 * x * x)
+    return out
 
 
 class ZhouEAMParameterSet(_Variables):
@@ -568,6 +656,40 @@ class ZhouEAMParameterSet(_Variables):
         el = el0.clone().index_put((er, ec), vals[ev]) if len(ev) else el0
         chi = chi0.clone().index_put((c0, c1), vals[cv]) if len(cv) else chi0
         return zhou_table_torch(continuous_torch(el), chi, self.r_cut, self.width)
+
+    def _tables_np(self, X):
+        """(P (B, nf, 43),) over the rows of X (B, n_var), in X's dtype: the
+        element rows and cross factors set, continuity re-derived, P
+        gathered from them by a fixed index map (zhou_table_torch's layout)."""
+        ns = len(self.species)
+        if not hasattr(self, "_plan"):
+            self.table_torch(torch.as_tensor(self.x0))
+        el0, chi0, ev, er, ec, cv, c0, c1, _ = [t.numpy() for t in self._plan]
+        if not hasattr(self, "_pmap"):
+            # src = [el (ns*20), chi (ns*ns), r_cut, width, 0]; P.flat = src[pmap]
+            zero = ns * 20 + ns * ns + 2
+            rows = []
+            for a in range(ns):
+                rows.append(list(range(a * 20, a * 20 + 20)) + [zero] * 20 + [zero - 2, zero - 1, zero])
+            for a in range(ns):
+                rows.append(list(range(a * 20, a * 20 + 20)) + [zero] * 23)
+            for a in range(ns):
+                for b in range(a, ns):
+                    tail = [zero] * 20 if a == b else list(range(b * 20, b * 20 + 20))
+                    k = zero if a == b else ns * 20 + a * ns + b
+                    rows.append(list(range(a * 20, a * 20 + 20)) + tail + [zero - 2, zero - 1, k])
+            self._pmap = np.array(rows, np.int64)
+        V = self._vals_np(X)
+        B = X.shape[0]
+        el = np.repeat(el0[None].astype(X.dtype), B, axis=0)
+        chi = np.repeat(chi0[None].astype(X.dtype), B, axis=0)
+        if len(ev):
+            el[:, er, ec] = V[:, ev]
+        if len(cv):
+            chi[:, c0, c1] = V[:, cv]
+        src = np.concatenate([continuous_np(el).reshape(B, -1), chi.reshape(B, -1),
+                              np.broadcast_to(np.array([self.r_cut, self.width, 0.0], X.dtype), (B, 3))], axis=1)
+        return (src[:, self._pmap],)
 
 
 # ---- evaluation with explicit tables and its adjoint ----------------------------
@@ -822,6 +944,12 @@ class _TersoffModel:
             tb, tri = tables_from_records(self.ps.decode_torch(x_t)["tersoff"], self.ps.species, x_t.device)
         return TersoffEFS.apply(tb, tri, ev)
 
+    def evaluate(self, ev, dtabs, tabs):
+        return ev.evaluate(dtabs[0], dtabs[1], table_cutoff(tabs[0]))
+
+    def adjoint(self, ev, dtabs, tabs, gE, gF, gW):
+        return ev.adjoint(dtabs[0], dtabs[1], gE, gF, gW, table_cutoff(tabs[0]))
+
 
 class _ZhouModel:
     """Zhou EAM parameter sets: the analytic rows P (nf, 43), EamEFS."""
@@ -839,6 +967,12 @@ class _ZhouModel:
 
     def efs(self, x_t, ev):
         return EamEFS.apply(self.ps.table_torch(x_t), ev)
+
+    def evaluate(self, ev, dtabs, tabs):
+        return ev.evaluate(dtabs[0])
+
+    def adjoint(self, ev, dtabs, tabs, gE, gF, gW):
+        return (ev.adjoint(dtabs[0], gE, gF, gW),)
 
 
 def _model_of(ps):
@@ -924,6 +1058,27 @@ class PotentialFit:
         self._smask = torch.tensor(smask, **f64)
         self._cw = torch.tensor([float(s.get("weight", 1.0)) * float(s.get("scale", 1.0)) ** 2 for s in structs],
                                 **f64)
+        # the fused device loss (mbf_fit_loss): its set description and outputs
+        i32 = dict(dtype=torch.int32, device=dev)
+        b = self.ev.batch
+        fo = np.zeros(len(n_orig), np.int64)
+        fo[1:] = np.cumsum(n_orig)[:-1]
+        w = self.w
+        self._fs_keep = dict(n_orig=torch.tensor(n_orig, **i32), fref_off=torch.as_tensor(fo.astype(np.int32), **i32))
+        hub = self.loss_type == "huber"
+        self._fs = _lib.MbfFitSet(
+            len(structs), b.n_atoms, _lib.ptr(b.struct_off), _lib.ptr(b.atom_struct),
+            _lib.ptr(self._fs_keep["n_orig"]), _lib.ptr(self._fs_keep["fref_off"]), _lib.ptr(self._inv_k),
+            _lib.ptr(self._eref), _lib.ptr(self._fref), _lib.ptr(self._sref), _lib.ptr(self._vol), _lib.ptr(self._vsup),
+            _lib.ptr(self._fmask), _lib.ptr(self._smask), _lib.ptr(self._cw),
+            float(w.get("energy", 1.0)), float(w.get("forces", 1.0)), float(w.get("stress", 0.1)),
+            float(w.get("r0", 1.0)), float(w.get("eps0", 1.0)), 1 if hub else 0,
+            float(w["huber_delta_energy"]) if hub else 0.0, float(w["huber_delta_forces"]) if hub else 0.0,
+            float(w["huber_delta_stress"]) if hub else 0.0)
+        nws = int(_lib.lib().mbf_fit_loss_workspace_bytes(len(structs)))
+        self._fws = torch.empty(max(nws, 256), dtype=torch.uint8, device=dev)
+        self._gout = (torch.empty(1, **f64), torch.empty(len(structs), **f64), torch.empty((b.n_atoms, 3), **f64),
+                      torch.empty((len(structs), 9), **f64))
 
     def _local_loss(self, x_t):
         """This rank's loss as a differentiable torch scalar."""
@@ -952,36 +1107,71 @@ class PotentialFit:
     def _reduce(self, vec):
         return allreduce_sum(vec, self.world, self.group)
 
+    def device_step(self, x, grad=True):
+        """One step on the device: the tables of x (host, with their
+        x-Jacobians by the complex step when grad), the batch evaluation,
+        the fused loss (mbf_fit_loss) and, when grad, the adjoint.  Returns
+        (loss (1,), table gradients, Jacobians): device tensors, the
+        Jacobians numpy; nothing is synchronised."""
+        x = np.asarray(x, float)
+        if grad:
+            tabs, jac = self.ps.table_jacobian(x)
+        else:
+            tabs, jac = self.ps.tables_np(x), None
+        dev = self.device
+        dtabs = [torch.from_numpy(t).to(dev, non_blocking=False) for t in tabs]
+        E, F, W = self.model.evaluate(self.ev, dtabs, tabs)
+        loss, gE, gF, gW = self._gout
+        L = _lib.lib()
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(L.mbf_fit_loss(self._fs, _lib.ptr(E), _lib.ptr(F), _lib.ptr(W), _lib.ptr(self._fws),
+                                  self._fws.numel(), _lib.ptr(loss), _lib.ptr(gE), _lib.ptr(gF), _lib.ptr(gW), st),
+                   "mbf_fit_loss")
+        if not grad:
+            return loss, (), None
+        return loss, self.model.adjoint(self.ev, dtabs, tabs, gE, gF, gW), jac
+
+    def _local(self, x, grad):
+        """(loss, gradient or None) of this rank's structures, host numpy."""
+        if self.ev is None:
+            return 0.0, (np.zeros(len(x)) if grad else None)
+        loss, d, jac = self.device_step(x, grad)
+        flat = torch.cat([loss] + [t.reshape(-1) for t in d]).cpu().numpy()
+        if not grad:
+            return float(flat[0]), None
+        g = np.zeros(len(x))
+        o = 1
+        for J, t in zip(jac, d):
+            k = t.numel()
+            g += np.tensordot(J, flat[o:o + k].reshape(tuple(t.shape)), axes=t.dim())
+            o += k
+        return float(flat[0]), g
+
+    def _combine(self, vec):
+        if self.world > 1:
+            vec = self._reduce(torch.as_tensor(vec, device=self.device)).cpu().numpy()
+        return vec
+
     def loss_and_grad(self, x):
         """(loss, dloss/dx) at x; every rank of a group must call it."""
-        x_t = torch.tensor(np.asarray(x, float), dtype=torch.float64, requires_grad=True)
         failed = 0.0
         try:
-            loss = self._local_loss(x_t)
-            (g,) = torch.autograd.grad(loss, x_t, allow_unused=True)
-            g = torch.zeros_like(x_t) if g is None else g
-            vec = torch.cat([loss.detach().reshape(1), g.detach().to(self.device),
-                             torch.zeros(1, dtype=torch.float64, device=self.device)])
+            loss, g = self._local(x, True)
         except (ValueError, RuntimeError, _lib.MbfError):
-            failed = 1.0
-            vec = torch.zeros(len(x) + 2, dtype=torch.float64, device=self.device)
-        vec[-1] = failed
-        vec = self._reduce(vec).cpu().numpy()
+            failed, loss, g = 1.0, 0.0, np.zeros(len(x))
+        vec = self._combine(np.concatenate([[loss], g, [failed]]))
         if vec[-1] > 0.0:
             return 1e30, np.zeros(len(x))
         return float(vec[0]), vec[1:-1]
 
     def loss(self, x):
         """The loss at x (1e30 if the parameters cannot be evaluated)."""
-        x_t = torch.tensor(np.asarray(x, float), dtype=torch.float64)
         failed = 0.0
         try:
-            with torch.no_grad():
-                val = self._local_loss(x_t).reshape(1)
+            val, _ = self._local(x, False)
         except (ValueError, RuntimeError, _lib.MbfError):
-            failed, val = 1.0, torch.zeros(1, dtype=torch.float64, device=self.device)
-        vec = self._reduce(torch.cat([val, torch.tensor([failed], dtype=torch.float64, device=self.device)]))
-        vec = vec.cpu().numpy()
+            failed, val = 1.0, 0.0
+        vec = self._combine(np.array([val, failed]))
         return 1e30 if vec[1] > 0.0 else float(vec[0])
 
 

@@ -748,14 +748,14 @@ def run_fit(args, world, rank, local):
     structs = _fit_structs(raw, efs)
     del tgt
     f = fit.PotentialFit(ps, structs, weights, device=dev, rank=rank, world=world)
-    # x and its decode live on the host (a few dozen scalars); the batch,
-    # the evaluation, the loss over 38k atoms and the adjoint on the device
-    x_host = torch.tensor(x0, dtype=torch.float64, requires_grad=True)
+    # x, its tables and their x-Jacobians live on the host (a few dozen
+    # scalars); the batch, the evaluation, the fused loss and the adjoint on
+    # the device; the step ends with the loss and the table gradients on the
+    # device (their sum over ranks is the whole set's)
 
     def device_step():
-        loss = f._local_loss(x_host)
-        (g,) = torch.autograd.grad(loss, x_host)
-        return torch.cat([loss.detach().reshape(1), g.to(dev)])
+        loss, d, _ = f.device_step(x0, True)
+        return torch.cat([loss] + [t.reshape(-1) for t in d])
 
     for _ in range(args.warmup):
         device_step()

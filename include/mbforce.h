@@ -284,6 +284,48 @@ int mbf_tersoff_adjoint(const mbf_system *sys, const mbf_nlist *nl,
                         const double *g_forces, const double *g_virial, void *workspace,
                         size_t workspace_bytes, double *d_tb, double *d_tri, void *stream);
 
+/* ---- fit loss ----------------------------------------------------------
+ * The reference's fit loss over a batch (fitting/loss.py:184-260, squared or
+ * Huber, fitting/loss.py:29-48) and its gradient with respect to the
+ * batch's energies, forces and virials -- the upstream gradients that
+ * mbf_tersoff_adjoint / mbf_eam_adjoint take.  Structure s holds atoms
+ * struct_off[s] .. struct_off[s+1]; its first n_orig[s] atoms are the
+ * original cell's (the rest replicas of a thin cell, k_s = 1 / inv_k[s]
+ * copies), with reference forces f_ref[fref_off[s] + a].  Per structure:
+ *   e_sq = (E_s inv_k_s - n_s e_ref_s)^2
+ *   f_sq = r0^2 sum_a |F_a - f_ref_a|^2 / (3 n_s)
+ *   s_sq = (vol_s eps0)^2 mean_9 (W_s / vsup_s - s_ref_s)^2
+ *   loss = sum_s cw_s [w_e h(e_sq) + fmask_s w_f h(f_sq) + smask_s w_s h(s_sq)]
+ * h the identity (huber = 0) or sq -> 2 delta sqrt(sq) - delta^2 above
+ * delta^2 (huber = 1, delta_e / delta_f / delta_s).  All pointers are device
+ * arrays.  Sums run in a fixed order.                                    */
+typedef struct mbf_fit_set {
+    int n_struct, n_atoms;
+    const int *struct_off;     /* (n_struct + 1) */
+    const int *atom_struct;    /* (n_atoms,) */
+    const int *n_orig;         /* (n_struct,) */
+    const int *fref_off;       /* (n_struct,) first row of the structure in f_ref */
+    const double *inv_k;       /* (n_struct,) 1 / replicas of the evaluated cell */
+    const double *e_ref;       /* (n_struct,) reference energy per atom */
+    const double *f_ref;       /* (sum n_orig, 3) */
+    const double *s_ref;       /* (n_struct, 9) reference stress */
+    const double *vol;         /* (n_struct,) volume of the original cell */
+    const double *vsup;        /* (n_struct,) volume of the evaluated cell */
+    const double *fmask;       /* (n_struct,) 1 if forces are fitted */
+    const double *smask;       /* (n_struct,) 1 if stress is fitted */
+    const double *cw;          /* (n_struct,) trust weight * scale^2 */
+    double w_e, w_f, w_s, r0, eps0;
+    int huber;
+    double delta_e, delta_f, delta_s;
+} mbf_fit_set;
+
+size_t mbf_fit_loss_workspace_bytes(int n_struct);
+/* Writes loss[0] and g_energy (n_struct), g_forces (n_atoms, 3), g_virial
+ * (n_struct, 9), all device arrays; two launches on `stream`.            */
+int mbf_fit_loss(const mbf_fit_set *set, const double *energy, const double *forces, const double *virial,
+                 void *workspace, size_t workspace_bytes, double *loss, double *g_energy, double *g_forces,
+                 double *g_virial, void *stream);
+
 /* ---- Stillinger-Weber -------------------------------------------------
  * Replaces StillingerWeberPotential.compute (engine/stillinger_weber.py:
  * 900-1451), single- and multi-species.  tb (ns*ns, 8) rows [valid, eps,

@@ -141,3 +141,22 @@ def test_two_rank_loss_sum_equals_whole_set():
     for _, total, count in res:
         assert count == 4
         assert total == pytest.approx(float(g["t1989_loss0"]), rel=1e-11)
+
+
+@pytest.mark.parametrize("tag", ["t1989", "multi"])
+def test_table_jacobian_equals_autograd(tag):
+    """The complex-step tables and x-Jacobians (the fused fit step's) equal
+    tables_torch and its autograd vector-Jacobian product."""
+    g = golden("fit_sic_t1989")
+    ps = param_sets()[tag]
+    x = g[f"{tag}_x_test"]
+    tabs, jac = ps.table_jacobian(x)
+    xt = torch.tensor(x, requires_grad=True)
+    tt = ps.tables_torch(xt)
+    rng = np.random.default_rng(3)
+    ws = [rng.normal(size=a.shape) for a in tabs]
+    (gt,) = torch.autograd.grad(sum((b * torch.from_numpy(w)).sum() for b, w in zip(tt, ws)), xt)
+    gn = sum(np.tensordot(J, w, axes=w.ndim) for J, w in zip(jac, ws))
+    for a, b in zip(tabs, tt):
+        np.testing.assert_allclose(a, b.detach().numpy(), rtol=1e-15, atol=1e-15)
+    np.testing.assert_allclose(gn, gt.numpy(), rtol=1e-13, atol=1e-13 * np.abs(gn).max())

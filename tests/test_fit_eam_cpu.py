@@ -108,3 +108,21 @@ def test_oracle_loss_matches_reference(tag):
         force = oracle.zhou_force(d["elements"], SPECIES, d["r_cut"], d["chi"])
         got = oracle.fit_loss(None, SPECIES, st, WEIGHTS, force=force)
         assert got == pytest.approx(float(g[f"{tag}_{key}"]), rel=1e-10)
+
+
+@pytest.mark.parametrize("tag", ["zhou", "zhou_chi"])
+def test_table_jacobian_equals_autograd(tag):
+    """The complex-step table and x-Jacobian (the fused fit step's) equal
+    table_torch and its autograd vector-Jacobian product."""
+    g = golden("fit_alni_zhou")
+    ps = param_sets()[tag]
+    x = g[f"{tag}_x_test"]
+    (P,), (J,) = ps.table_jacobian(x)
+    xt = torch.tensor(x, requires_grad=True)
+    Pt = ps.table_torch(xt)
+    w = np.random.default_rng(4).normal(size=P.shape)
+    (gt,) = torch.autograd.grad((Pt * torch.from_numpy(w)).sum(), xt)
+    np.testing.assert_allclose(P, Pt.detach().numpy(), rtol=1e-14, atol=1e-15)
+    gn = np.tensordot(J, w, axes=2)
+    np.testing.assert_allclose(gn, gt.numpy(), rtol=1e-12, atol=1e-12 * np.abs(gn).max())
+    np.testing.assert_allclose(ps.tables_np(x)[0], P, rtol=0, atol=0)

@@ -121,3 +121,29 @@ def test_eam_gradient_matches_central_differences_and_reference(cuda_device, tag
     # O(h) truncation error of their own
     ref = g[f"{tag}_grad_fd"]
     np.testing.assert_allclose(grad, ref, rtol=1e-3, atol=1e-4 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("which", ["zhou", "t1989"])
+def test_fused_step_equals_autograd_path(cuda_device, which):
+    """loss_and_grad (fused loss kernel, complex-step table Jacobian) equals
+    the torch autograd composition (EamEFS / TersoffEFS under the torch
+    loss), Huber weights and a structure without stress included."""
+    if which == "zhou":
+        g = golden("fit_alni_zhou")
+        ps, st, x = param_sets()["zhou_chi"], structures(), g["zhou_chi_x_test"]
+        w = dict(WEIGHTS, huber_delta_energy=3.0, huber_delta_forces=0.05, huber_delta_stress=1.0)
+    else:
+        import test_fit_cpu as tc
+        g = golden("fit_sic_t1989")
+        ps, st, x = tc.param_sets()["t1989"], tc.structures(), g["t1989_x_test"]
+        w = {"energy": 1.0, "forces": 1.0, "stress": 0.1, "huber_delta_energy": 2.0,
+             "huber_delta_forces": 0.5, "huber_delta_stress": 1.0}
+    st[1] = dict(st[1], weight=0.5, scale=2.0, ref_stress=None)
+    f = fit.PotentialFit(ps, st, w, loss_type="huber", device=cuda_device)
+    loss, grad = f.loss_and_grad(x)
+    xt = torch.tensor(x, requires_grad=True)
+    lt = f._local_loss(xt)
+    (gt,) = torch.autograd.grad(lt, xt)
+    assert loss == pytest.approx(float(lt.detach()), rel=1e-12)
+    np.testing.assert_allclose(grad, gt.numpy(), rtol=1e-10, atol=1e-12 * np.abs(gt.numpy()).max())
+    assert f.loss(x) == pytest.approx(loss, rel=1e-14)
