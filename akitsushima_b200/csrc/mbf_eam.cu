@@ -380,21 +380,23 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *_
             int end = row_off[i + 1];
             int s = row_off[i] + sub;
             if (!MBF_OK_IDX(ck, 11, end, 0, ck.n_slots + 1)) end = s;
-            int jn = i;
-            if (s < end && MBF_OK_IDX(ck, 12, s, 0, ck.n_slots)) jn = nbr[s];
-            if (!MBF_OK_IDX(ck, 13, jn, 0, ck.n_atoms)) jn = i;
-            double4 pn = ld_pack(pk, jn);
-            int tn = __ldg(S.types + jn);
+            // two-stage prefetch, as in eam_force
+            int j0 = i, j1 = i;
+            if (s < end && MBF_OK_IDX(ck, 12, s, 0, ck.n_slots)) j0 = nbr[s];
+            if (s + LPA < end && MBF_OK_IDX(ck, 15, s + LPA, 0, ck.n_slots)) j1 = nbr[s + LPA];
+            if (!MBF_OK_IDX(ck, 13, j0, 0, ck.n_atoms)) j0 = i;
+            double4 pn = ld_pack(pk, j0);
+            int tn = __ldg(S.types + j0);
             for (; s < end; s += LPA) {
                 double4 pj = pn;
                 int sj = tn;
                 if (!MBF_OK_IDX(ck, 14, sj, 0, ck.ns)) sj = 0;
                 if (s + LPA < end) {
-                    jn = MBF_OK_IDX(ck, 15, s + LPA, 0, ck.n_slots) ? nbr[s + LPA] : i;
-                    if (!MBF_OK_IDX(ck, 16, jn, 0, ck.n_atoms)) jn = i;
-                    pn = ld_pack(pk, jn);
-                    tn = __ldg(S.types + jn);
+                    if (!MBF_OK_IDX(ck, 16, j1, 0, ck.n_atoms)) j1 = i;
+                    pn = ld_pack(pk, j1);
+                    tn = __ldg(S.types + j1);
                 }
+                if (s + 2 * LPA < end && MBF_OK_IDX(ck, 15, s + 2 * LPA, 0, ck.n_slots)) j1 = nbr[s + 2 * LPA];
                 double dx, dy, dz;
                 cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
                 double r2 = dx * dx + dy * dy + dz * dz;
@@ -473,27 +475,35 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1) 
             int end = row_off[i + 1];
             int up = upper[i];
             if (!MBF_OK_IDX(ck, 21, up, row_off[i], end + 1)) up = end;
+            // two-stage prefetch: slot indices two iterations ahead, the
+            // neighbour's record and species one ahead, so the record load
+            // never waits on the index load of the same iteration
             int s = up + sub;
-            int jn = i, rn = 0;
+            int j0 = i, r0 = 0, j1 = i, r1 = 0;
             if (s < end && MBF_OK_IDX(ck, 22, s, 0, ck.n_slots)) {
-                jn = nbr[s];
-                rn = rev[s];
+                j0 = nbr[s];
+                r0 = rev[s];
             }
-            if (!MBF_OK_IDX(ck, 23, jn, 0, ck.n_atoms)) jn = i;
-            double4 pn = ld_pack(pk, jn);
-            int tn = __ldg(S.types + jn);
+            if (s + LPA < end && MBF_OK_IDX(ck, 25, s + LPA, 0, ck.n_slots)) {
+                j1 = nbr[s + LPA];
+                r1 = rev[s + LPA];
+            }
+            if (!MBF_OK_IDX(ck, 23, j0, 0, ck.n_atoms)) j0 = i;
+            double4 pn = ld_pack(pk, j0);
+            int tn = __ldg(S.types + j0);
             for (; s < end; s += LPA) {
                 double4 pj = pn;
-                int sj = tn, rs = rn;
+                int sj = tn, rs = r0;
                 if (!MBF_OK_IDX(ck, 24, sj, 0, ck.ns)) sj = 0;
                 if (s + LPA < end) {
-                    if (MBF_OK_IDX(ck, 25, s + LPA, 0, ck.n_slots)) {
-                        jn = nbr[s + LPA];
-                        rn = rev[s + LPA];
-                    }
-                    if (!MBF_OK_IDX(ck, 26, jn, 0, ck.n_atoms)) jn = i;
-                    pn = ld_pack(pk, jn);
-                    tn = __ldg(S.types + jn);
+                    if (!MBF_OK_IDX(ck, 26, j1, 0, ck.n_atoms)) j1 = i;
+                    pn = ld_pack(pk, j1);
+                    tn = __ldg(S.types + j1);
+                }
+                r0 = r1;
+                if (s + 2 * LPA < end && MBF_OK_IDX(ck, 25, s + 2 * LPA, 0, ck.n_slots)) {
+                    j1 = nbr[s + 2 * LPA];
+                    r1 = rev[s + 2 * LPA];
                 }
                 double dx, dy, dz;
                 cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
