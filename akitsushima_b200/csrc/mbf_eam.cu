@@ -20,7 +20,7 @@ constexpr int EAM_BLOCK = 128;
 // Resident blocks per SM the float32 force kernel is compiled for (it sets
 // the register budget: 65536 / (EAM_BLOCK * MBF_EAM_MINB)).
 #ifndef MBF_EAM_MINB
-#define MBF_EAM_MINB 6
+#define MBF_EAM_MINB 5
 #endif
 
 enum { F_SPLINE = 1, F_SPLINE_R = 2, F_Z_DENS = 3, F_Z_PAIR = 4, F_Z_CROSS = 5, F_Z_EMB = 6 };
