@@ -154,13 +154,13 @@ constexpr int EADJ_STRIDE = 25;      // odd: conflict-free 8-byte shared accesse
 // embedding sites (12; summed per species of the centre into the block's
 // partialF row) and the coefficients c1 = gE F' + F'' D_t rho-bar, c2 = F'
 // through which every density parameter acts on this atom's site term.
-// Also flags the live pairs above the diagonal (j > i, inside the cutoff):
-// flag[s] for like-species pairs, flag[n_slots + s] for cross pairs.
+// Also counts the live pairs above the diagonal (j > i, inside the cutoff):
+// cnt[i] like-species pairs, cnt[n_atoms + i] cross pairs.
 __global__ void __launch_bounds__(EADJ_TA) eam_adjoint_embed(SysView S, const int *__restrict__ row_off,
                                                              const int *__restrict__ upper,
                                                              const int *__restrict__ nbr, EamAdjTab T, AdjIn G,
-                                                             int n_slots, double2 *__restrict__ cc,
-                                                             int *__restrict__ flag, double *__restrict__ partialF) {
+                                                             double2 *__restrict__ cc, int *__restrict__ cnt,
+                                                             double *__restrict__ partialF) {
     __shared__ double sf[EADJ_TA * 13];  // 12 sites per atom, odd stride
     __shared__ int scode[EADJ_TA];
     extern __shared__ double accF[];     // ns * 12
@@ -178,14 +178,17 @@ __global__ void __launch_bounds__(EADJ_TA) eam_adjoint_embed(SysView S, const in
             double gE = G.gE ? G.gE[sst] : 0.0;
             const double *cell = cell_of(S, i);
             double rho = 0.0, rho_t = 0.0;
-            int up = upper[i];
+            int up = upper[i], n_like = 0, n_cross = 0;
             for (int s = row_off[i]; s < row_off[i + 1]; ++s) {
                 int j = nbr[s];
                 double d[3], r, tg[3];
                 adj_leg(S, G, cell, i, j, sst, d, r, tg);
                 if (!(r * r < rc2 && r * r > 1e-24)) continue;
                 int sj = S.types[j];
-                if (s >= up) flag[(si == sj ? 0 : n_slots) + s] = 1;
+                if (s >= up) {
+                    if (si == sj) ++n_like;
+                    else ++n_cross;
+                }
                 double rt = (d[0] * tg[0] + d[1] * tg[1] + d[2] * tg[2]) / r;
                 double v, vt;
                 dens_value(row_of(T, T.rho_f[sj]), r, rt, v, vt);
@@ -198,6 +201,8 @@ __global__ void __launch_bounds__(EADJ_TA) eam_adjoint_embed(SysView S, const in
 #pragma unroll
             for (int k = 0; k < 12; ++k) o[k] = gE * F.p[k] + F.q[k];
             cc[i] = make_double2(rho > 0.0 ? gE * F.p[12] + F.q[12] : 0.0, F.p[12]);
+            cnt[i] = n_like;
+            cnt[S.n_atoms + i] = n_cross;
             code = si;
         }
         scode[threadIdx.x] = code;
@@ -215,11 +220,28 @@ __global__ void __launch_bounds__(EADJ_TA) eam_adjoint_embed(SysView S, const in
     for (int k = threadIdx.x; k < nf; k += blockDim.x) partialF[(size_t)blockIdx.x * nf + k] = accF[k];
 }
 
-// Compacted pair list: like pairs first, then cross pairs (slot indices).
-__global__ void eam_adjoint_compact(int n2, const int *__restrict__ flag, const int *__restrict__ pos,
-                                    int n_slots, int *__restrict__ pairs) {
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < n2 && flag[q]) pairs[pos[q]] = q < n_slots ? q : q - n_slots;
+// Compacted pair list, a thread per atom: its live upper slots (the same
+// test as eam_adjoint_embed's, so the same count) at its scanned offsets,
+// like pairs in [pos[0], pos[N]), cross pairs in [pos[N], pos[2N]), each in
+// atom then slot order.
+__global__ void eam_adjoint_compact(SysView S, const int *__restrict__ row_off, const int *__restrict__ upper,
+                                    const int *__restrict__ nbr, EamAdjTab T, AdjIn G,
+                                    const int *__restrict__ pos, int *__restrict__ pairs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n_atoms) return;
+    int si = S.types[i];
+    int sst = S.n_struct > 1 ? S.atom_struct[i] : 0;
+    const double *cell = cell_of(S, i);
+    const double rc2 = T.rc * T.rc;
+    int ol = pos[i], oc = pos[S.n_atoms + i];
+    for (int s = upper[i]; s < row_off[i + 1]; ++s) {
+        int j = nbr[s];
+        double d[3], r, tg[3];
+        adj_leg(S, G, cell, i, j, sst, d, r, tg);
+        if (!(r * r < rc2 && r * r > 1e-24)) continue;
+        if (S.types[j] == si) pairs[ol++] = s;
+        else pairs[oc++] = s;
+    }
 }
 
 // The slot's owning atom: rows are sorted, so a binary search in row_off.
@@ -323,8 +345,8 @@ __device__ int eam_pair_sites(const SysView &S, const int *__restrict__ row_off,
 }
 
 // Pass 2, a thread per live pair of one segment of the compacted list
-// (like pairs [0, pos[n_slots]) or cross pairs [pos[n_slots], pos[2
-// n_slots])), EADJ_TP pairs per tile: the staged values are sorted by code
+// (like pairs [0, pos[N]) or cross pairs [pos[N], pos[2 N])), EADJ_TP
+// pairs per tile: the staged values are sorted by code
 // inside the tile (a counting sort, ranks from warp matches, so the order
 // is fixed), then each (code, value) item is summed over its segment into
 // the block's partialP row (ns^2 * 25).  The two segments are separate
@@ -431,7 +453,7 @@ __global__ void eam_adjoint_final(EamAdjTab T, int gA, const double *__restrict_
 
 // Workspace of one call.
 struct EadjLayout {
-    size_t partialF, partialP, cc, flag, pos, pairs, scan, total;
+    size_t partialF, partialP, cc, cnt, pos, pairs, scan, total;
     int gA, gP;
 };
 
@@ -450,14 +472,15 @@ static EadjLayout eadj_layout(int n_atoms, long long n_slots, int ns) {
     o = align256(o + sizeof(double) * (size_t)2 * L.gP * ns * ns * EADJ_PS);
     L.cc = o;
     o = align256(o + sizeof(double2) * (size_t)(n_atoms > 0 ? n_atoms : 1));
-    L.flag = o;
-    o = align256(o + sizeof(int) * (size_t)(2 * ns2));
+    size_t na = (size_t)(n_atoms > 0 ? n_atoms : 1);
+    L.cnt = o;
+    o = align256(o + sizeof(int) * 2 * na);
     L.pos = o;
-    o = align256(o + sizeof(int) * (size_t)(2 * ns2 + 1));
+    o = align256(o + sizeof(int) * (2 * na + 1));
     L.pairs = o;
     o = align256(o + sizeof(int) * (size_t)ns2);
     L.scan = o;
-    o = align256(o + sizeof(int) * scan_workspace_ints((int)(2 * ns2)));
+    o = align256(o + sizeof(int) * scan_workspace_ints((int)(2 * na)));
     L.total = o;
     return L;
 }
@@ -469,7 +492,7 @@ using namespace mbf;
 extern "C" {
 
 size_t mbf_eam_adjoint_workspace_bytes(int n_atoms, long long n_slots, int ns) {
-    if (n_atoms < 0 || n_slots < 0 || ns <= 0 || ns > 8 || 2 * n_slots + 1 > 0x7fffffffLL) return 0;
+    if (n_atoms < 0 || n_slots < 0 || ns <= 0 || ns > 8 || n_slots > 0x7fffffffLL) return 0;
     return eadj_layout(n_atoms, n_slots, ns).total;
 }
 
@@ -478,7 +501,7 @@ int mbf_eam_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
                     double *d_P, void *stream) {
     if (!sys || !nl || !tab || !workspace || !d_P || tab->ns <= 0 || tab->ns > 8 || tab->nf <= 0)
         return MBF_ERR_ARGUMENT;
-    if (nl->n_atoms != sys->n_atoms || !nl->upper || 2 * nl->n_slots + 1 > 0x7fffffffLL) return MBF_ERR_ARGUMENT;
+    if (nl->n_atoms != sys->n_atoms || !nl->upper || nl->n_slots > 0x7fffffffLL) return MBF_ERR_ARGUMENT;
     EadjLayout L = eadj_layout(sys->n_atoms, nl->n_slots, tab->ns);
     if (workspace_bytes < L.total) return MBF_ERR_WORKSPACE;
     cudaStream_t st = (cudaStream_t)stream;
@@ -500,34 +523,33 @@ int mbf_eam_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
     G.gE = g_energy;
     G.gF = g_forces;
     G.gW = g_virial;
-    int n_slots = (int)(nl->n_slots > 0 ? nl->n_slots : 1);
     double *partialF = ws_at<double>(workspace, L.partialF);
     double *partialP = ws_at<double>(workspace, L.partialP);
     double2 *cc = ws_at<double2>(workspace, L.cc);
-    int *flag = ws_at<int>(workspace, L.flag);
+    int *cnt = ws_at<int>(workspace, L.cnt);
     int *pos = ws_at<int>(workspace, L.pos);
     int *pairs = ws_at<int>(workspace, L.pairs);
-    if (cudaMemsetAsync(flag, 0, sizeof(int) * 2 * (size_t)n_slots, st) != cudaSuccess) return MBF_ERR_CUDA;
+    const int N = sys->n_atoms;
     PROF_BEGIN("eam_adjoint_embed", st);
     eam_adjoint_embed<<<L.gA, EADJ_TA, sizeof(double) * 12 * T.ns, st>>>(S, nl->row_off, nl->upper, nl->nbr, T, G,
-                                                                          n_slots, cc, flag, partialF);
+                                                                          cc, cnt, partialF);
     MBF_CHECK_LAUNCH();
-    int rc = exclusive_scan(flag, pos, 2 * n_slots, ws_at<int>(workspace, L.scan), st);
+    int rc = exclusive_scan(cnt, pos, 2 * N, ws_at<int>(workspace, L.scan), st);
     if (rc != MBF_OK) return rc;
-    eam_adjoint_compact<<<(2 * n_slots + 255) / 256, 256, 0, st>>>(2 * n_slots, flag, pos, n_slots, pairs);
+    eam_adjoint_compact<<<(N + 127) / 128, 128, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, T, G, pos, pairs);
     PROF_END("eam_adjoint_embed", st);
     MBF_CHECK_LAUNCH();
-    // like pairs [pos[0], pos[n_slots]), cross pairs [pos[n_slots], pos[2 n_slots])
+    // like pairs [pos[0], pos[N]), cross pairs [pos[N], pos[2 N])
     size_t psm = sizeof(double) * T.ns * T.ns * EADJ_PS;
     int gL = persistent_grid(L.gP, EADJ_TP, (const void *)eam_adjoint_pairs<true>, psm);
     int gC = persistent_grid(L.gP, EADJ_TP, (const void *)eam_adjoint_pairs<false>, psm);
     size_t ni = (size_t)T.ns * T.ns * EADJ_PS;
     PROF_BEGIN("eam_adjoint_pairs", st);
-    eam_adjoint_pairs<true><<<gL, EADJ_TP, psm, st>>>(S, nl->row_off, nl->nbr, T, G, cc, pairs, pos, pos + n_slots,
+    eam_adjoint_pairs<true><<<gL, EADJ_TP, psm, st>>>(S, nl->row_off, nl->nbr, T, G, cc, pairs, pos, pos + N,
                                                        partialP);
     MBF_CHECK_LAUNCH();
-    eam_adjoint_pairs<false><<<gC, EADJ_TP, psm, st>>>(S, nl->row_off, nl->nbr, T, G, cc, pairs, pos + n_slots,
-                                                        pos + 2 * n_slots, partialP + (size_t)gL * ni);
+    eam_adjoint_pairs<false><<<gC, EADJ_TP, psm, st>>>(S, nl->row_off, nl->nbr, T, G, cc, pairs, pos + N, pos + 2 * N,
+                                                        partialP + (size_t)gL * ni);
     PROF_END("eam_adjoint_pairs", st);
     MBF_CHECK_LAUNCH();
     PROF_BEGIN("eam_adjoint_reduce", st);
