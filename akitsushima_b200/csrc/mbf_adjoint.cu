@@ -80,7 +80,7 @@ struct SlotGeo {
 // valid): the slots the site passes run over, compacted by a scan.
 __global__ void te_adjoint_prep(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr,
                                 AdjTab P, AdjIn G, int n_slots, SlotGeo *__restrict__ geo,
-                                int *__restrict__ live) {
+                                int *__restrict__ live, int *__restrict__ inside) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_slots) return;
     SlotGeo o;
@@ -101,6 +101,7 @@ __global__ void te_adjoint_prep(SysView S, const int *__restrict__ row_off, cons
     }
     geo[s] = o;
     live[s] = bond;
+    inside[s] = o.live != 0.0 ? 1 : 0;
 }
 
 __global__ void te_adjoint_compact(int n_slots, const int *__restrict__ live, const int *__restrict__ pos,
@@ -145,7 +146,8 @@ __device__ __forceinline__ HD<K> te_bond_order(const HD<K> &zeta, const HD<K> &b
 //   term's own derivatives from a hyper-dual over its 7 leg sites.
 template <int K>
 __device__ int adj_bond_sites(const SysView &S, const int *__restrict__ row_off, const int *__restrict__ nbr,
-                              const AdjTab &P, const AdjIn &G, const SlotGeo *__restrict__ geo, int s, int W,
+                              const AdjTab &P, const AdjIn &G, const SlotGeo *__restrict__ geo,
+                              const int *__restrict__ legs, const int *__restrict__ lpos, int s, int W,
                               double *__restrict__ out) {
     const int ns = P.ns;
     const SlotGeo gs = geo[s];
@@ -163,10 +165,10 @@ __device__ int adj_bond_sites(const SysView &S, const int *__restrict__ row_off,
     HD<1> r1 = hd_const<1>(rij);
     r1.t = rt;
     HD<1> zeta = hd_const<1>(0.0);
-    for (int q = beg; q < end; ++q) {
+    for (int t = lpos[beg]; t < lpos[end]; ++t) {
+        int q = legs[t];
         if (q == s) continue;
         const SlotGeo gk = geo[q];
-        if (gk.live == 0.0) continue;
         int sk = S.types[nbr[q]];
         const double *tk = P.tb + 10 * (si * ns + sk);
         const double *t3 = P.tri + 8 * ((si * ns + sj) * ns + sk);
@@ -218,10 +220,10 @@ __device__ int adj_bond_sites(const SysView &S, const int *__restrict__ row_off,
     if (c1 != 0.0 || c2 != 0.0) {
         HD<7> r7 = hd_const<7>(rij);
         r7.t = rt;
-        for (int q = beg; q < end; ++q) {
+        for (int t = lpos[beg]; t < lpos[end]; ++t) {
+            int q = legs[t];
             if (q == s) continue;
             const SlotGeo gk = geo[q];
-            if (gk.live == 0.0) continue;
             int sk = S.types[nbr[q]];
             const double *tk = P.tb + 10 * (si * ns + sk);
             const double *t3 = P.tri + 8 * ((si * ns + sj) * ns + sk);
@@ -284,6 +286,8 @@ template <int K>
 __global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_bonds(SysView S, const int *__restrict__ row_off,
                                                               const int *__restrict__ nbr, AdjTab P, AdjIn G,
                                                               const SlotGeo *__restrict__ geo,
+                                                              const int *__restrict__ legs,
+                                                              const int *__restrict__ lpos,
                                                               const int *__restrict__ bonds,
                                                               const int *__restrict__ n_bonds, int W,
                                                               double *__restrict__ partial) {
@@ -295,7 +299,7 @@ __global__ void __launch_bounds__(ADJ_BLOCK) te_adjoint_bonds(SysView S, const i
     int m = m0 + threadIdx.x;
     double *out = sm + (size_t)threadIdx.x * W;
     int c = -1;
-    if (m < nb) c = adj_bond_sites<K>(S, row_off, nbr, P, G, geo, bonds[m], W, out);
+    if (m < nb) c = adj_bond_sites<K>(S, row_off, nbr, P, G, geo, legs, lpos, bonds[m], W, out);
     scode[threadIdx.x] = c;
     __syncthreads();
     int cnt = min(ADJ_BLOCK, nb - m0);
@@ -324,7 +328,7 @@ __global__ void te_adjoint_final(const int *__restrict__ n_bonds, int ns, const 
 }
 
 struct AdjLayout {
-    size_t partial, geo, live, pos, bonds, scan, total;
+    size_t partial, geo, live, pos, bonds, inside, lpos, legs, scan, total;
     int W, ne, n_blocks;
 };
 
@@ -344,6 +348,12 @@ static AdjLayout adj_layout(long long n_slots, int ns) {
     L.pos = o;
     o = align256(o + sizeof(int) * (size_t)(n_slots + 1));
     L.bonds = o;
+    o = align256(o + sizeof(int) * (size_t)(n_slots > 0 ? n_slots : 1));
+    L.inside = o;
+    o = align256(o + sizeof(int) * (size_t)(n_slots > 0 ? n_slots : 1));
+    L.lpos = o;
+    o = align256(o + sizeof(int) * (size_t)(n_slots + 1));
+    L.legs = o;
     o = align256(o + sizeof(int) * (size_t)(n_slots > 0 ? n_slots : 1));
     L.scan = o;
     o = align256(o + sizeof(int) * scan_workspace_ints((int)(n_slots > 0 ? n_slots : 1)));
@@ -394,20 +404,28 @@ int mbf_tersoff_adjoint(const mbf_system *sys, const mbf_nlist *nl, const mbf_te
     int *live = ws_at<int>(workspace, L.live);
     int *pos = ws_at<int>(workspace, L.pos);
     int *bonds = ws_at<int>(workspace, L.bonds);
+    int *inside = ws_at<int>(workspace, L.inside);
+    int *lpos = ws_at<int>(workspace, L.lpos);
+    int *legs = ws_at<int>(workspace, L.legs);
     int grid = (n_slots + ADJ_BLOCK - 1) / ADJ_BLOCK;
     PROF_BEGIN("te_adjoint_prep", st);
-    te_adjoint_prep<<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, n_slots, geo, live);
+    te_adjoint_prep<<<grid, ADJ_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, G, n_slots, geo, live, inside);
     MBF_CHECK_LAUNCH();
     int rc = exclusive_scan(live, pos, n_slots, ws_at<int>(workspace, L.scan), st);
     if (rc != MBF_OK) return rc;
     te_adjoint_compact<<<grid, ADJ_BLOCK, 0, st>>>(n_slots, live, pos, bonds);
+    // the slots inside the cutoff, each row's contiguous and in slot order: the
+    // zeta loops of a bond run over these only
+    rc = exclusive_scan(inside, lpos, n_slots, ws_at<int>(workspace, L.scan), st);
+    if (rc != MBF_OK) return rc;
+    te_adjoint_compact<<<grid, ADJ_BLOCK, 0, st>>>(n_slots, inside, lpos, legs);
     PROF_END("te_adjoint_prep", st);
     const int *n_bonds = pos + n_slots;  // the scan's total
     size_t smem = (size_t)ADJ_BLOCK * L.W * sizeof(double) + ADJ_BLOCK * sizeof(int);  // <= 33 KB (ns <= 8)
     int bgrid = L.n_blocks;
     PROF_BEGIN("te_adjoint_bonds", st);
-    te_adjoint_bonds<ADJ_K><<<bgrid, ADJ_BLOCK, smem, st>>>(S, nl->row_off, nl->nbr, P, G, geo, bonds, n_bonds,
-                                                              L.W, partial);
+    te_adjoint_bonds<ADJ_K><<<bgrid, ADJ_BLOCK, smem, st>>>(S, nl->row_off, nl->nbr, P, G, geo, legs, lpos, bonds,
+                                                              n_bonds, L.W, partial);
     PROF_END("te_adjoint_bonds", st);
     MBF_CHECK_LAUNCH();
     PROF_BEGIN("te_adjoint_reduce", st);

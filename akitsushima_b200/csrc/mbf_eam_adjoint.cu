@@ -351,8 +351,14 @@ __device__ int eam_pair_sites(const SysView &S, const int *__restrict__ row_off,
 // is fixed), then each (code, value) item is summed over its segment into
 // the block's partialP row (ns^2 * 25).  The two segments are separate
 // instantiations: the like pairs' kernel keeps a smaller register budget.
+// Resident blocks per SM the cross-pair instantiation is compiled for (its
+// register budget: 65536 / (EADJ_TP * MBF_EADJ_CROSS_MINB)).
+#ifndef MBF_EADJ_CROSS_MINB
+#define MBF_EADJ_CROSS_MINB 8
+#endif
+
 template <bool LIKE>
-__global__ void __launch_bounds__(EADJ_TP) eam_adjoint_pairs(SysView S, const int *__restrict__ row_off,
+__global__ void __launch_bounds__(EADJ_TP, LIKE ? 1 : MBF_EADJ_CROSS_MINB) eam_adjoint_pairs(SysView S, const int *__restrict__ row_off,
                                                              const int *__restrict__ nbr, EamAdjTab T, AdjIn G,
                                                              const double2 *__restrict__ cc,
                                                              const int *__restrict__ pairs,
