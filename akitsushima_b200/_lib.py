@@ -82,7 +82,9 @@ _SIGS = {
     "mbf_nl_max_displacement": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _vp]),
     "mbf_md_kick_drift": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _vp, _d, _vp]),
     "mbf_md_partial_count": (_i, [_i]),
-    "mbf_md_kick": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _d, _vp, _vp, _vp, _i, _vp, _vp]),
+    "mbf_md_kick": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _d, _vp, _vp, _vp, _i, _vp, _vp, _vp]),
+    "mbf_md_kick_drift_check": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _vp, _d, _vp, _d, _d, _vp, _vp,
+                                     _vp, _i, _vp, _vp, ctypes.c_ulonglong, _vp]),
     "mbf_md_skin_check": (_i, [ctypes.POINTER(MbfSystem), _vp, _d, _d, _vp, _vp, _i, _vp, _vp, _vp,
                                ctypes.c_ulonglong, _vp]),
     "mbf_md_rebuild_done": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp]),

@@ -1,6 +1,10 @@
 // Velocity-Verlet NVE on the device: the two half kicks, the drift with the
 // wrap into the cell, and a fixed-order kinetic-energy sum, split around the
 // force call so a whole rebuild interval can be captured in one CUDA graph.
+// The first half kick also carries the step's list-validity check, the
+// second the kinetic-energy sum (completion counters: the block that
+// finishes last does the per-step serial work), so a step is the force
+// call plus two launches.
 //
 // Replaces the integrator of NVESimulation.run
 // (solvers/molecular_dynamics.py:1969-2000) and _kinetic_energy (:239-244);
@@ -43,6 +47,82 @@ __global__ void md_kick_drift(SysView S, double *__restrict__ pos, double *__res
     vel[o + 2] = vz;
 }
 
+// md_kick_drift fused with the list-validity check of the same step: each
+// atom's minimum-image displacement from the reference positions (the
+// lattice is fixed, engine/neighborlist.py:661-668), its per-structure
+// maximum (warp max, then one atomic per warp; max is order-free), and in
+// the block that finishes last the reference's rebuild decision
+// r_list - 2 d <= r_cut (:653-673): d logged, the gate word and the graph
+// conditional set, the maxima and the completion word reset to 0.
+__global__ void md_kick_drift_check(SysView S, double *__restrict__ pos, double *__restrict__ vel,
+                                    const double *__restrict__ F, const double *__restrict__ im, double dt,
+                                    const double *__restrict__ ref, unsigned long long *__restrict__ dmax,
+                                    unsigned *__restrict__ done, double r_list, double r_cut,
+                                    double *__restrict__ d_log, int rows, int *__restrict__ counter,
+                                    int *__restrict__ gate, unsigned long long cond) {
+    __shared__ bool last;
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = a < S.n_atoms;
+    int s = 0;
+    unsigned long long bits = 0ull;
+    if (valid) {
+        size_t o = 3 * (size_t)a;
+        double h = 0.5 * dt * im[a];
+        double vx = vel[o] + h * F[o], vy = vel[o + 1] + h * F[o + 1], vz = vel[o + 2] + h * F[o + 2];
+        double x = pos[o] + dt * vx, y = pos[o + 1] + dt * vy, z = pos[o + 2] + dt * vz;
+        s = S.n_struct > 1 ? S.atom_struct[a] : 0;
+        const double *c = S.cells + 18 * (size_t)s;
+        double s0 = x * c[9] + y * c[12] + z * c[15];
+        double s1 = x * c[10] + y * c[13] + z * c[16];
+        double s2 = x * c[11] + y * c[14] + z * c[17];
+        s0 -= floor(s0);
+        s1 -= floor(s1);
+        s2 -= floor(s2);
+        if (s0 >= 1.0) s0 = 0.0;
+        if (s1 >= 1.0) s1 = 0.0;
+        if (s2 >= 1.0) s2 = 0.0;
+        double px = s0 * c[0] + s1 * c[3] + s2 * c[6];
+        double py = s0 * c[1] + s1 * c[4] + s2 * c[7];
+        double pz = s0 * c[2] + s1 * c[5] + s2 * c[8];
+        pos[o] = px;
+        pos[o + 1] = py;
+        pos[o + 2] = pz;
+        vel[o] = vx;
+        vel[o + 1] = vy;
+        vel[o + 2] = vz;
+        double dx, dy, dz;
+        mic_exact(c, px - ref[o], py - ref[o + 1], pz - ref[o + 2], dx, dy, dz);
+        bits = (unsigned long long)__double_as_longlong(sqrt(dx * dx + dy * dy + dz * dz));
+    }
+    int s_first = __shfl_sync(MBF_FULL, s, 0);
+    if (__all_sync(MBF_FULL, s == s_first || !valid)) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long b = __shfl_xor_sync(MBF_FULL, bits, o);
+            bits = b > bits ? b : bits;
+        }
+        if ((threadIdx.x & 31) == 0 && bits) atomicMax(dmax + s_first, bits);
+    } else if (valid) {
+        atomicMax(dmax + s, bits);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    int row = *counter % rows;
+    int need = 0;
+    for (int q = 0; q < S.n_struct; ++q) {
+        double d = __longlong_as_double((long long)atomicExch(dmax + q, 0ull));
+        d_log[(size_t)row * S.n_struct + q] = d;
+        if (r_list - 2.0 * d <= r_cut) need = 1;
+    }
+    *gate = need;
+    if (cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, need ? 1u : 0u);
+    *counter += 1;
+    *done = 0u;
+}
+
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double *sh) {
 #pragma unroll
@@ -61,11 +141,21 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
 
 // Second half kick and m v^2 over chunk blockIdx.x of structure blockIdx.y
 // (mass = 1 / inv_mass in amu / conv units: conv cancels in m v^2 / conv).
+// The block that finishes last then sums the partials into the thermo row
+// (md_thermo's arithmetic, so the same bits) and resets `done`.
+__device__ void md_thermo_body(int n_struct, int P, const double *__restrict__ partial,
+                               const double *__restrict__ energy, double *__restrict__ thermo, int rows,
+                               int *__restrict__ counter, double *sh);
+
 __global__ void __launch_bounds__(MD_BLOCK) md_kick(SysView S, double *__restrict__ vel,
                                                     const double *__restrict__ F,
                                                     const double *__restrict__ im, double dt, int P,
-                                                    double *__restrict__ partial) {
+                                                    double *__restrict__ partial,
+                                                    const double *__restrict__ energy,
+                                                    double *__restrict__ thermo, int rows,
+                                                    int *__restrict__ counter, unsigned *__restrict__ done) {
     __shared__ double sh[MD_BLOCK / 32];
+    __shared__ bool last;
     int s = blockIdx.y;
     int beg = S.n_struct > 1 ? S.struct_off[s] : 0;
     int end = S.n_struct > 1 ? S.struct_off[s + 1] : S.n_atoms;
@@ -86,21 +176,27 @@ __global__ void __launch_bounds__(MD_BLOCK) md_kick(SysView S, double *__restric
         }
     }
     acc = block_sum<MD_BLOCK>(acc, sh);
-    if (threadIdx.x == 0) partial[(size_t)s * P + blockIdx.x] = acc;
+    if (threadIdx.x == 0) {
+        partial[(size_t)s * P + blockIdx.x] = acc;
+        __threadfence();
+        last = atomicAdd(done, 1u) == gridDim.x * gridDim.y - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    md_thermo_body(S.n_struct, P, partial, energy, thermo, rows, counter, sh);
+    if (threadIdx.x == 0) *done = 0u;
 }
 
 // With inv_mass = conv / m the partials hold sum m v^2 / conv, so the
 // kinetic energy is half their sum, in eV (the reference's
 // 0.5 sum m v^2 / EV_ANG_TO_AMU_ANG_FS2, :243-244).
-__global__ void __launch_bounds__(MD_BLOCK) md_thermo(int n_struct, int P, const double *__restrict__ partial,
-                                                      const double *__restrict__ energy,
-                                                      double *__restrict__ thermo, int rows,
-                                                      int *__restrict__ counter) {
-    __shared__ double sh[MD_BLOCK / 32];
+__device__ void md_thermo_body(int n_struct, int P, const double *__restrict__ partial,
+                               const double *__restrict__ energy, double *__restrict__ thermo, int rows,
+                               int *__restrict__ counter, double *sh) {
     int row = *counter % rows;
     for (int s = 0; s < n_struct; ++s) {
         double v = 0.0;
-        for (int k = threadIdx.x; k < P; k += MD_BLOCK) v += partial[(size_t)s * P + k];
+        for (int k = threadIdx.x; k < P; k += MD_BLOCK) v += __ldcg(partial + (size_t)s * P + k);
         v = block_sum<MD_BLOCK>(v, sh);
         if (threadIdx.x == 0) {
             double *t = thermo + 2 * ((size_t)row * n_struct + s);
@@ -137,18 +233,36 @@ int mbf_md_partial_count(int n_atoms) { return n_atoms <= 0 ? 1 : (n_atoms + MD_
 
 int mbf_md_kick(const mbf_system *sys, double *velocities, const double *forces, const double *inv_mass,
                 double dt, const double *energy, double *partial, double *thermo, int thermo_rows,
-                int *counter, void *stream) {
-    if (!sys || !velocities || !forces || !inv_mass || !energy || !partial || !thermo || !counter ||
+                int *counter, unsigned *done, void *stream) {
+    if (!sys || !velocities || !forces || !inv_mass || !energy || !partial || !thermo || !counter || !done ||
         thermo_rows <= 0 || sys->n_struct <= 0 || sys->n_struct > 65535)
         return MBF_ERR_ARGUMENT;
     SysView S = make_view(sys);
     cudaStream_t st = (cudaStream_t)stream;
     int P = mbf_md_partial_count(sys->n_atoms);
     PROF_BEGIN("md_kick", st);
-    md_kick<<<dim3(P, sys->n_struct), MD_BLOCK, 0, st>>>(S, velocities, forces, inv_mass, dt, P, partial);
+    md_kick<<<dim3(P, sys->n_struct), MD_BLOCK, 0, st>>>(S, velocities, forces, inv_mass, dt, P, partial, energy,
+                                                         thermo, thermo_rows, counter, done);
     PROF_END("md_kick", st);
     MBF_CHECK_LAUNCH();
-    md_thermo<<<1, MD_BLOCK, 0, st>>>(sys->n_struct, P, partial, energy, thermo, thermo_rows, counter);
+    return MBF_OK;
+}
+
+int mbf_md_kick_drift_check(const mbf_system *sys, double *positions, double *velocities, const double *forces,
+                            const double *inv_mass, double dt, const double *ref_positions, double r_list,
+                            double r_cut, unsigned long long *d_max, unsigned *done, double *d_log, int rows,
+                            int *counter, int *gate, unsigned long long cond_handle, void *stream) {
+    if (!sys || !positions || !velocities || !forces || !inv_mass || positions != sys->positions ||
+        !ref_positions || !d_max || !done || !d_log || !counter || !gate || rows <= 0 || !(r_list > r_cut) ||
+        !(r_cut > 0.0) || sys->n_struct <= 0 || sys->n_atoms <= 0)
+        return MBF_ERR_ARGUMENT;
+    SysView S = make_view(sys);
+    cudaStream_t st = (cudaStream_t)stream;
+    PROF_BEGIN("md_kick_drift", st);
+    md_kick_drift_check<<<(sys->n_atoms + MD_BLOCK - 1) / MD_BLOCK, MD_BLOCK, 0, st>>>(
+        S, positions, velocities, forces, inv_mass, dt, ref_positions, d_max, done, r_list, r_cut, d_log, rows,
+        counter, gate, cond_handle);
+    PROF_END("md_kick_drift", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;
 }

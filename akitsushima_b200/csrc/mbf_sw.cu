@@ -324,7 +324,7 @@ static int sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tabl
     P.tri = tab->tri;
     P.rc = tab->r_cut;
     int *err = ws_at<int>(workspace, L.err);
-    if (cudaMemsetAsync(err, 0, 16, st) != cudaSuccess) return MBF_ERR_CUDA;
+    if (cudaMemsetAsync(err, 0, ERR_CLEAR_BYTES, st) != cudaSuccess) return MBF_ERR_CUDA;
     double *per_atom = ws_at<double>(workspace, L.per_atom);
     double *f_local = ws_at<double>(workspace, L.f_local);
     double *slot_G = ws_at<double>(workspace, L.slot);
@@ -339,7 +339,8 @@ static int sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tabl
         rc = sym ? sw_dispatch<float, true>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, so, st)
                  : sw_dispatch<float, false>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, so, st);
     if (rc != MBF_OK) return rc;
-    return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
+    return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial,
+                                (unsigned *)(err + RED_COUNTER_WORD), st);
 }
 
 extern "C" int mbf_sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables *tab,

@@ -448,7 +448,7 @@ static int tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_te
     P.tri = tab->tri;
     P.rc = tab->r_cut;
     int *err = ws_at<int>(workspace, L.err);
-    if (cudaMemsetAsync(err, 0, 16, st) != cudaSuccess) return MBF_ERR_CUDA;
+    if (cudaMemsetAsync(err, 0, ERR_CLEAR_BYTES, st) != cudaSuccess) return MBF_ERR_CUDA;
     double *per_atom = ws_at<double>(workspace, L.per_atom);
     double *f_local = ws_at<double>(workspace, L.f_local);
     double *slot_G = ws_at<double>(workspace, L.slot);
@@ -457,7 +457,8 @@ static int tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_te
     int rc = te_dispatch(precision, nl->max_row, lanes_per_atom, S, nl, P, slot_b, slot_G, f_local, per_atom,
                          forces, err, so, st);
     if (rc != MBF_OK) return rc;
-    return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial, st);
+    return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial,
+                                (unsigned *)(err + RED_COUNTER_WORD), st);
 }
 
 extern "C" int mbf_tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_tersoff_tables *tab,

@@ -127,7 +127,7 @@ constexpr int RED_BLOCK = 128;
 // chunk of atoms (chunks never straddle structures); each thread sums its
 // atoms' ATOM_ACC values in registers, then a shuffle tree per warp and the
 // warps in order.  Stage 2: one warp per structure sums its chunks the same
-// way.
+// way, in the last block to finish (a completion counter).
 template <int NW>
 __device__ __forceinline__ void warp_sum_acc(double (&v)[ATOM_ACC]) {
 #pragma unroll
@@ -138,11 +138,14 @@ __device__ __forceinline__ void warp_sum_acc(double (&v)[ATOM_ACC]) {
 
 __global__ void __launch_bounds__(RED_BLOCK) reduce_chunks(const double *__restrict__ per_atom,
                                                            const int *__restrict__ chunk, int n_chunks,
-                                                           double *__restrict__ partial) {
+                                                           double *__restrict__ partial,
+                                                           const int *__restrict__ chunk_first, int n_struct,
+                                                           double *__restrict__ energy, double *__restrict__ virial,
+                                                           unsigned *__restrict__ counter) {
     constexpr int NW = RED_BLOCK / 32;
     __shared__ double sh[NW][ATOM_ACC];
+    __shared__ bool last;
     int c = blockIdx.x;
-    if (c >= n_chunks) return;
     int a0 = chunk[3 * c + 1], a1 = chunk[3 * c + 2];
     double v[ATOM_ACC];
 #pragma unroll
@@ -164,37 +167,39 @@ __global__ void __launch_bounds__(RED_BLOCK) reduce_chunks(const double *__restr
 #pragma unroll
         for (int k = 0; k < NW; ++k) t += sh[k][threadIdx.x];
         partial[(size_t)c * ATOM_ACC + threadIdx.x] = t;
+        __threadfence();
     }
-}
-
-__global__ void reduce_structs(const double *__restrict__ partial, const int *__restrict__ chunk_first,
-                               int n_struct, double *__restrict__ energy, double *__restrict__ virial) {
-    int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int l = threadIdx.x & 31;
-    if (s >= n_struct) return;  // whole warps leave together
-    double v[ATOM_ACC];
+    __syncthreads();
+    // Stage 2 in the block that finishes last: a warp per structure sums its
+    // chunks (lane-strided, then the shuffle tree), as a separate launch would.
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == (unsigned)(n_chunks - 1);
+    __syncthreads();
+    if (!last) return;
+    for (int s = w; s < n_struct; s += NW) {
 #pragma unroll
-    for (int q = 0; q < ATOM_ACC; ++q) v[q] = 0.0;
-    for (int c = chunk_first[s] + l; c < chunk_first[s + 1]; c += 32) {
-        const double *p = partial + (size_t)c * ATOM_ACC;
+        for (int q = 0; q < ATOM_ACC; ++q) v[q] = 0.0;
+        for (int k = chunk_first[s] + l; k < chunk_first[s + 1]; k += 32) {
+            const double *p = partial + (size_t)k * ATOM_ACC;
 #pragma unroll
-        for (int q = 0; q < ATOM_ACC; ++q) v[q] += p[q];
+            for (int q = 0; q < ATOM_ACC; ++q) v[q] += __ldcg(p + q);
+        }
+        warp_sum_acc<1>(v);
+        if (l == 0) {
+            energy[s] = v[10] > 0.0 ? v[0] : 0.0;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) virial[9 * s + q] = v[1 + q];
+        }
     }
-    warp_sum_acc<1>(v);
-    if (l == 0) {
-        energy[s] = v[10] > 0.0 ? v[0] : 0.0;
-#pragma unroll
-        for (int q = 0; q < 9; ++q) virial[9 * s + q] = v[1 + q];
-    }
+    if (threadIdx.x == 0) *counter = 0u;  // ready for the next evaluation
 }
 
 int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, int n_struct,
-                         double *partial, double *energy, double *virial, cudaStream_t st) {
-    if (plan->n_chunks <= 0) return MBF_ERR_ARGUMENT;
+                         double *partial, double *energy, double *virial, unsigned *counter, cudaStream_t st) {
+    if (plan->n_chunks <= 0 || !counter) return MBF_ERR_ARGUMENT;
     PROF_BEGIN("reduce_chunks", st);
-    reduce_chunks<<<plan->n_chunks, RED_BLOCK, 0, st>>>(per_atom, plan->chunk, plan->n_chunks, partial);
+    reduce_chunks<<<plan->n_chunks, RED_BLOCK, 0, st>>>(per_atom, plan->chunk, plan->n_chunks, partial,
+                                                        plan->chunk_first, n_struct, energy, virial, counter);
     PROF_END("reduce_chunks", st);
-    reduce_structs<<<(n_struct + 3) / 4, 128, 0, st>>>(partial, plan->chunk_first, n_struct, energy, virial);
     MBF_CHECK_LAUNCH();
     return MBF_OK;
 }

@@ -16,8 +16,10 @@ size_t scan_workspace_ints(int n);
 // scan_workspace_ints(n) ints.
 int exclusive_scan(const int *in, int *out, int n, int *ws, cudaStream_t st);
 
+// `counter` must be 0 at the call (it is left at 0): the evaluation
+// workspace's word RED_COUNTER_WORD, cleared with the error words.
 int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, int n_struct,
-                         double *partial, double *energy, double *virial, cudaStream_t st);
+                         double *partial, double *energy, double *virial, unsigned *counter, cudaStream_t st);
 
 int gather_forces(int n_atoms, const int *row_off, const double *G, const double *f_local, double *forces,
                   cudaStream_t st);
@@ -32,8 +34,14 @@ struct SiteOut {
     double *vec;   // (n_slots, 3)
 };
 
+// Words of the evaluation workspace's `err` region that each evaluation
+// clears at its start (ERR_CLEAR_BYTES): the error words 0..3 and the
+// completion counter of the per-structure reduction.
+constexpr int RED_COUNTER_WORD = 8;
+constexpr int ERR_CLEAR_BYTES = 64;
+
 // Layout of the evaluation workspace (all offsets 256-byte aligned):
-//   err      device error word (int)
+//   err      device error words (ints; see ERR_CLEAR_BYTES)
 //   per_atom (n_atoms, ATOM_ACC) doubles
 //   f_local  (n_atoms, 3) doubles (three-body potentials: centre-local force)
 //   atom_aux (n_atoms, 2) doubles (EAM F'(rho), F(rho))

@@ -176,10 +176,12 @@ class NVE:
         self.thermo_rows = int(thermo_rows)
         self.thermo = torch.zeros((self.thermo_rows, 1, 2), dtype=torch.float64, device=dev)
         self.skin_log = torch.zeros((self.thermo_rows, 1), dtype=torch.float64, device=dev)
-        # device words: thermo row, skin row, status, rebuilds, rebuild gate
+        # device words: thermo row, skin row, status, rebuilds, rebuild gate,
+        # and the completion counters of the two fused kick launches
         self._counters = torch.zeros(8, dtype=torch.int32, device=dev)
         self._partial = torch.empty(int(L.mbf_md_partial_count(self.n_atoms)), dtype=torch.float64, device=dev)
         self._dscratch = torch.empty(1, dtype=torch.float64, device=dev)
+        self._dmax = torch.zeros(1, dtype=torch.int64, device=dev)   # left at 0 by every check
         self._ref = self.batch.pos.clone()
         self._body = torch.cuda.Stream(dev)
         self._graph = None
@@ -234,21 +236,30 @@ class NVE:
                                                 self._word(1), self._word(4), self._word(2) if assert_only else None,
                                                 cond, stream), "mbf_md_skin_check")
 
+    def _kick_drift_check(self, stream, cond=0):
+        """First half kick, drift and the criterion check in one launch."""
+        _lib.check(_lib.lib().mbf_md_kick_drift_check(
+            self.batch.mbf_system(), _lib.ptr(self.batch.pos), _lib.ptr(self.vel), _lib.ptr(self.out.forces),
+            _lib.ptr(self.inv_mass), self.dt, _lib.ptr(self._ref), self.dlist.r_list, float(self.pot.r_cut),
+            _lib.ptr(self._dmax), self._word(5), _lib.ptr(self.skin_log), self.thermo_rows, self._word(1),
+            self._word(4), cond, stream), "mbf_md_kick_drift_check")
+
     def _step(self, k, capturing):
         """MD step number k of a block (k counts from 0)."""
         L = _lib.lib()
         st = torch.cuda.current_stream(self.device).cuda_stream
         sysd = self.batch.mbf_system()
-        _lib.check(L.mbf_md_kick_drift(sysd, _lib.ptr(self.batch.pos), _lib.ptr(self.vel), _lib.ptr(self.out.forces),
-                                       _lib.ptr(self.inv_mass), self.dt, st), "mbf_md_kick_drift")
         if self.rebuild_every is not None:
+            _lib.check(L.mbf_md_kick_drift(sysd, _lib.ptr(self.batch.pos), _lib.ptr(self.vel),
+                                           _lib.ptr(self.out.forces), _lib.ptr(self.inv_mass), self.dt, st),
+                       "mbf_md_kick_drift")
             if k % self.rebuild_every == 0:
                 self._skin_check(st, assert_only=True)
                 self._rebuild(st)
         elif capturing:
             h = ctypes.c_ulonglong(0)
             _lib.check(L.mbf_capture_cond_create(st, ctypes.byref(h)), "mbf_capture_cond_create")
-            self._skin_check(st, assert_only=False, cond=h.value)
+            self._kick_drift_check(st, cond=h.value)
             body = self._body.cuda_stream
             _lib.check(L.mbf_capture_if_begin(st, body, h.value), "mbf_capture_if_begin")
             try:
@@ -256,13 +267,14 @@ class NVE:
             finally:
                 _lib.check(L.mbf_capture_if_end(body), "mbf_capture_if_end")
         else:
-            self._skin_check(st, assert_only=False)
+            self._kick_drift_check(st)
             if int(self._counters[4].item()):
                 self._rebuild(st)
         self._eval()
         _lib.check(L.mbf_md_kick(sysd, _lib.ptr(self.vel), _lib.ptr(self.out.forces), _lib.ptr(self.inv_mass),
                                  self.dt, _lib.ptr(self.out.energy), _lib.ptr(self._partial),
-                                 _lib.ptr(self.thermo), self.thermo_rows, self._word(0), st), "mbf_md_kick")
+                                 _lib.ptr(self.thermo), self.thermo_rows, self._word(0), self._word(6), st),
+                   "mbf_md_kick")
 
     def _run_block(self, capturing=False):
         for k in range(self.block):

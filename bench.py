@@ -618,6 +618,25 @@ def make_ni3al_set(n=256, a=3.57, strain=0.02, sigma=0.08, seed=0):
     return out
 
 
+def _fit_setup_multi():
+    """The multi-species Si-C record set (fitting/parameter_sets.py:1068-1203;
+    A, B, lambda1, lambda2 per unordered pair and c, d, h per (i, j, k)
+    record: every species triplet) at the Tersoff-1989 Si-C values, and its
+    target parameters theta * U(0.95, 1.05) (seeded), as x vectors."""
+    from akitsushima_b200 import fit
+    from akitsushima_b200.published_parameters import TERSOFF_1989
+    from akitsushima_b200.tersoff import tersoff1989_to_triplets
+    species = ["Si", "C"]
+    el = {s: dict(TERSOFF_1989["elements"][s]) for s in species}
+    recs = tersoff1989_to_triplets(el, {"Si-C": TERSOFF_1989["chi"]["C-Si"]}, species)
+    ps = fit.MultiSpeciesTersoffParameterSet(recs, species)
+    x0 = ps.x0
+    u = np.random.default_rng(7).uniform(0.95, 1.05, len(x0))
+    xt = np.array([np.log(np.exp(x) * f) if key in ps._LOG_KEYS else x * f
+                   for x, f, (_, key, _) in zip(x0, u, ps.variables)])
+    return ps, x0, xt
+
+
 def _fit_setup_zhou():
     """The Zhou (2004) Al-Ni parameter set (ZhouEAMParameterSet defaults:
     A B alpha beta Fn2 Fn3 F2 F3 eta per element) and its target
@@ -635,7 +654,15 @@ def _fit_setup_zhou():
 
 FIT_WORKLOADS = {
     # name: (structure set, parameter set, loss weights, config)
-    "fit_sic256": (lambda: make_sic_set(256), _fit_setup, {"energy": 1.0, "forces": 1.0, "stress": 0.1},
+    "fit_sic256": (lambda: make_sic_set(256), _fit_setup_multi, {"energy": 1.0, "forces": 1.0, "stress": 0.1},
+                   {"workload": "fit_sic256_multispecies",
+                    "sizes": "zincblende SiC 2^3 / 3^3 cells (64 / 216 atoms)", "a": 4.36, "strain": 0.02,
+                    "sigma": 0.1,
+                    "parameter_set": "MultiSpeciesTersoffParameterSet (A B lambda1 lambda2 per pair, c d h per "
+                                     "(i, j, k) record), Tersoff-1989 Si-C start",
+                    "targets": "float64 E/F/S at theta * U(0.95, 1.05)",
+                    "loss": "w_E 1, w_F 1, w_S 0.1, r0 1, eps0 1 (squared)"}),
+    "fit_sic256_t1989": (lambda: make_sic_set(256), _fit_setup, {"energy": 1.0, "forces": 1.0, "stress": 0.1},
                    {"workload": "fit_sic256_tersoff1989",
                     "sizes": "zincblende SiC 2^3 / 3^3 cells (64 / 216 atoms)", "a": 4.36, "strain": 0.02,
                     "sigma": 0.1, "parameter_set": "Tersoff1989ParameterSet (A B lambda mu c d h per element, chi)",
@@ -701,7 +728,7 @@ def run_fit(args, world, rank, local):
     n_atoms = sum(len(p) for _, p, _ in raw)
     cfg = dict(cfg0, n_structures=n_struct, n_atoms=n_atoms, precision="fp64",
                l2="256 MB scratch write between steps, outside the timed events", parallelism=f"split{world}")
-    n_sample = 16 if args.workload == "fit_sic256" else 4
+    n_sample = 4 if "zhou" in args.workload else 16
     from akitsushima_b200 import fit
     ps, x0, xt = setup()
     n_var = len(x0)

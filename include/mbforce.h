@@ -399,11 +399,22 @@ int mbf_md_kick_drift(const mbf_system *sys, double *positions, double *velociti
  * per structure) is scratch, and the pair (potential energy energy[s],
  * kinetic energy) is written to thermo at row (*counter) mod thermo_rows
  * (thermo: (thermo_rows, n_struct, 2)); *counter (device) then advances
- * by one.                                                               */
+ * by one.  One launch: *done (device word) must be 0 and is left at 0.  */
 int mbf_md_partial_count(int n_atoms);
 int mbf_md_kick(const mbf_system *sys, double *velocities, const double *forces,
                 const double *inv_mass, double dt, const double *energy,
-                double *partial, double *thermo, int thermo_rows, int *counter, void *stream);
+                double *partial, double *thermo, int thermo_rows, int *counter, unsigned *done,
+                void *stream);
+
+/* mbf_md_kick_drift and mbf_md_skin_check (below, with a graph condition
+ * handle or 0 and no status word) in one launch: the displacement maxima
+ * d_max (n_struct device words) and *done must be 0 and are left at 0;
+ * the other arguments are mbf_md_skin_check's.                           */
+int mbf_md_kick_drift_check(const mbf_system *sys, double *positions, double *velocities,
+                            const double *forces, const double *inv_mass, double dt,
+                            const double *ref_positions, double r_list, double r_cut,
+                            unsigned long long *d_max, unsigned *done, double *d_log, int rows,
+                            int *counter, int *gate, unsigned long long cond_handle, void *stream);
 
 /* The reference's rebuild decision (engine/neighborlist.py:613-673 with
  * the lattice fixed: rebuild iff r_list - 2 d <= r_cut, d = max_a |MIC(r_a -
