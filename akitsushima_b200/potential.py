@@ -163,6 +163,9 @@ class DevicePotential:
         _lib.check(_lib.lib().mbf_eval_status(_lib.ptr(ws), words,
                                               torch.cuda.current_stream(ws.device).cuda_stream),
                    "mbf_eval_status")
+        self._raise_status(list(words))
+
+    def _raise_status(self, words):
         if words[0] or words[1]:
             raise RuntimeError(f"{type(self).__name__}: device check failed (bits {words[0]}, "
                                f"site {words[1]}, index {words[2]})")
@@ -210,15 +213,18 @@ class DevicePotential:
         batch.set_positions(pos, check=False)   # as the reference: no scan of the input
         batch.set_types(ids)
         res = self.evaluate(batch, dl)
-        ev = torch.cat([res.energy[:1], res.virial[0]]).to("cpu", non_blocking=True)
+        # energy, virial and the device status words (the first 16 bytes of
+        # the workspace, carried as two doubles) in one copy
+        words = self._last_ws[:16].view(torch.float64)
+        ev = torch.cat([res.energy[:1], res.virial[0], words]).to("cpu", non_blocking=True)
         f = batch.forces_to_host(res.forces)   # synchronises the stream
-        self.status()
         ev = ev.numpy()
+        self._raise_status(np.frombuffer(ev[10:12].tobytes(), dtype=np.int32))
         e = float(ev[0])
         if not need_stress:
             return e, f, None
         vol = abs(float(np.linalg.det(lattice)))
-        s = ev[1:].reshape(3, 3) / vol
+        s = ev[1:10].reshape(3, 3) / vol
         return e, f, s
 
 

@@ -1017,7 +1017,7 @@ def main():
     ap.add_argument("--cells", type=int, default=40)
     ap.add_argument("--lanes", type=int, default=2, help="EAM lanes per atom (1, 2, 4, 8, 16, 32)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--skip-singles", action="store_true",
                     help="batched workload: skip the per-structure-launch comparison (profiling runs)")
     ap.add_argument("--workload", default="eam_cuni_256k",
@@ -1171,9 +1171,12 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    calls = []
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
+        c0 = time.perf_counter()
         e, f, st = fn(lat, pos_host, ids, nl)
+        calls.append(time.perf_counter() - c0)
     t_e2e = (time.perf_counter() - t0) / args.e2e_steps
     if dist:
         t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
@@ -1181,8 +1184,11 @@ def main():
         t_e2e = float(t.item())
     e2e = {"value": world * n_atoms / t_e2e, "unit": "atoms/s",
            "h2d_bytes_per_step": n_atoms * (24 + 4), "d2h_bytes_per_step": n_atoms * 24 + 8 + 72,
-           "ms_per_step": t_e2e * 1e3, "path": "force_fn(lattice, numpy positions, species ids, "
-                                             "NeighbourList) -> numpy"}
+           "ms_per_step": t_e2e * 1e3,
+           "ms_per_call_min_median_max": [round(1e3 * float(np.min(calls)), 4),
+                                          round(1e3 * float(np.median(calls)), 4),
+                                          round(1e3 * float(np.max(calls)), 4)],
+           "path": "force_fn(lattice, numpy positions, species ids, NeighbourList) -> numpy"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
