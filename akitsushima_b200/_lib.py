@@ -113,8 +113,6 @@ _SIGS = {
     "mbf_eam_eval_sites": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                                 ctypes.POINTER(MbfEamTables), ctypes.POINTER(MbfReducePlan), _i, _i,
                                 _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
-    "mbf_host_register": (_i, [_vp, _sz]),
-    "mbf_host_unregister": (_i, [_vp]),
     "mbf_fit_loss_workspace_bytes": (_sz, [_i]),
     "mbf_fit_loss": (_i, [ctypes.POINTER(MbfFitSet), _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp, _vp]),
     "mbf_eam_adjoint_workspace_bytes": (_sz, [_i, _ll, _i]),

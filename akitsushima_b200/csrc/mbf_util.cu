@@ -258,24 +258,6 @@ const char *mbf_error_string(int code) {
 
 int mbf_version(void) { return 10000; }
 
-int mbf_host_register(void *ptr, size_t bytes) {
-    if (!ptr || bytes == 0) return MBF_ERR_ARGUMENT;
-    if (cudaHostRegister(ptr, bytes, cudaHostRegisterDefault) != cudaSuccess) {
-        cudaGetLastError();  // not sticky; clear it for later error checks
-        return MBF_ERR_CUDA;
-    }
-    return MBF_OK;
-}
-
-int mbf_host_unregister(void *ptr) {
-    if (!ptr) return MBF_ERR_ARGUMENT;
-    if (cudaHostUnregister(ptr) != cudaSuccess) {
-        cudaGetLastError();
-        return MBF_ERR_CUDA;
-    }
-    return MBF_OK;
-}
-
 size_t mbf_eval_workspace_bytes(int n_atoms, long long n_slots, int n_chunks) {
     return mbf::eval_layout(n_atoms, n_slots, n_chunks).total;
 }

@@ -6,8 +6,6 @@ inverse, and the per-structure reduction plan the kernels use to sum energy
 and virial.  A single structure is a batch of one.  Torch supplies the device
 memory and the stream; every computation runs in libmbforce.so.
 """
-import ctypes
-
 import numpy as np
 import torch
 
@@ -138,7 +136,6 @@ class Batch:
         self.pos = torch.empty((self.n_atoms, 3), dtype=torch.float64, device=dev)
         self.types = torch.empty(self.n_atoms, dtype=torch.int32, device=dev)
         self._types_host = None
-        self._host_reg = None
         self.set_positions(positions)
         self.set_types(type_ids)
         # reduction plan: chunks of REDUCE_CHUNK atoms inside one structure
@@ -180,35 +177,7 @@ class Batch:
             raise ValueError(f"positions have shape {arr.shape}, expected ({self.n_atoms}, 3)")
         if check and not np.isfinite(np.add.reduce(arr, axis=None)):  # NaN and inf survive a sum
             raise ValueError("positions contain NaN or inf")
-        arr = np.ascontiguousarray(arr, np.float64)
-        self.pos.copy_(torch.from_numpy(arr) if self.device.type != "cuda" else self._host_source(arr))
-
-    def _host_source(self, arr):
-        """arr as a host tensor; page-locked in place (mbf_host_register)
-        when the same array object was passed last time -- solvers that
-        update one buffer in place then copy at pinned speed.  The batch
-        keeps that array alive while it is registered and releases it when
-        another array comes."""
-        key = (arr.ctypes.data, arr.nbytes)
-        reg = self._host_reg
-        if reg is not None and reg[1] is arr and reg[0] == key:
-            if not reg[2] and arr.nbytes >= (1 << 20):
-                reg[2] = _lib.lib().mbf_host_register(ctypes.c_void_p(key[0]), key[1]) == 0
-            return torch.from_numpy(arr)
-        self._release_host()
-        self._host_reg = [key, arr, False]
-        return torch.from_numpy(arr)
-
-    def _release_host(self):
-        reg, self._host_reg = getattr(self, "_host_reg", None), None
-        if reg is not None and reg[2]:
-            _lib.lib().mbf_host_unregister(ctypes.c_void_p(reg[0][0]))
-
-    def __del__(self):
-        try:
-            self._release_host()
-        except Exception:
-            pass
+        self.pos.copy_(torch.from_numpy(np.ascontiguousarray(arr, np.float64)))
 
     def forces_to_host(self, forces):
         """Device (N, 3) forces to a new host numpy array: a pinned block of

@@ -86,14 +86,6 @@ typedef struct mbf_reduce_plan {
 const char *mbf_error_string(int code);
 int mbf_version(void);
 
-/* Page-lock (and release) a caller's host buffer in place, so that copies
- * from it run at pinned-memory speed: cudaHostRegister / cudaHostUnregister.
- * The buffer must stay allocated until it is unregistered.  The Python
- * layer registers a positions array the second time the same array is
- * passed (solvers that update one buffer in place), never a new one.     */
-int mbf_host_register(void *ptr, size_t bytes);
-int mbf_host_unregister(void *ptr);
-
 /* ---- neighbour list ---------------------------------------------------
  * Replaces NeighbourList.build / _build_cell_linked / _canonical_pair_order
  * (engine/neighborlist.py:574-585, :935-1024, :1166-1181) and the two-way CSR
