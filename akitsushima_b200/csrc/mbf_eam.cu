@@ -776,7 +776,7 @@ static int eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
         rc = eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, so, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial,
-                                (unsigned *)(ck.err + RED_COUNTER_WORD), st);
+                                ws_at<unsigned>(workspace, L.sdone), st);
 }
 
 extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
@@ -868,9 +868,9 @@ extern "C" int mbf_eam_eval_static(const mbf_system *sys, const mbf_nlist *nl, c
     ck.n_atoms = sys->n_atoms;
     ck.n_slots = nl->n_slots;
     ck.ns = tab->ns;
-    // the scratch keeps the previous call's contents: the error words and the
-    // reduction's completion counter must start at zero; every other region
-    // is fully written before it is read
+    // the scratch keeps the previous call's contents: the error words must
+    // start at zero (the reduction clears its own counters); every other
+    // region is fully written before it is read
     if (cudaMemsetAsync(ck.err, 0, ERR_CLEAR_BYTES, st) != cudaSuccess) return MBF_ERR_CUDA;
     double *f_local = ws_at<double>(workspace, L.f_local);
     double4 *pk = ws_at<double4>(workspace, L.pack);
@@ -882,5 +882,5 @@ extern "C" int mbf_eam_eval_static(const mbf_system *sys, const mbf_nlist *nl, c
         rc = eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, SiteOut{}, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial,
-                                (unsigned *)(ck.err + RED_COUNTER_WORD), st);
+                                ws_at<unsigned>(workspace, L.sdone), st);
 }

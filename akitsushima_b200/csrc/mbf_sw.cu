@@ -340,7 +340,7 @@ static int sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tabl
                  : sw_dispatch<float, false>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, so, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial,
-                                (unsigned *)(err + RED_COUNTER_WORD), st);
+                                ws_at<unsigned>(workspace, L.sdone), st);
 }
 
 extern "C" int mbf_sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables *tab,

@@ -458,7 +458,7 @@ static int tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_te
                          forces, err, so, st);
     if (rc != MBF_OK) return rc;
     return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial,
-                                (unsigned *)(err + RED_COUNTER_WORD), st);
+                                ws_at<unsigned>(workspace, L.sdone), st);
 }
 
 extern "C" int mbf_tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_tersoff_tables *tab,

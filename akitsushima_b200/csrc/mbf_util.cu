@@ -127,7 +127,7 @@ constexpr int RED_BLOCK = 128;
 // chunk of atoms (chunks never straddle structures); each thread sums its
 // atoms' ATOM_ACC values in registers, then a shuffle tree per warp and the
 // warps in order.  Stage 2: one warp per structure sums its chunks the same
-// way, in the last block to finish (a completion counter).
+// way, in the block that completes the structure.
 template <int NW>
 __device__ __forceinline__ void warp_sum_acc(double (&v)[ATOM_ACC]) {
 #pragma unroll
@@ -139,14 +139,14 @@ __device__ __forceinline__ void warp_sum_acc(double (&v)[ATOM_ACC]) {
 __global__ void __launch_bounds__(RED_BLOCK) reduce_chunks(const double *__restrict__ per_atom,
                                                            const int *__restrict__ chunk, int n_chunks,
                                                            double *__restrict__ partial,
-                                                           const int *__restrict__ chunk_first, int n_struct,
+                                                           const int *__restrict__ chunk_first,
                                                            double *__restrict__ energy, double *__restrict__ virial,
-                                                           unsigned *__restrict__ counter) {
+                                                           unsigned *__restrict__ sdone) {
     constexpr int NW = RED_BLOCK / 32;
     __shared__ double sh[NW][ATOM_ACC];
     __shared__ bool last;
     int c = blockIdx.x;
-    int a0 = chunk[3 * c + 1], a1 = chunk[3 * c + 2];
+    int s = chunk[3 * c], a0 = chunk[3 * c + 1], a1 = chunk[3 * c + 2];
     double v[ATOM_ACC];
 #pragma unroll
     for (int q = 0; q < ATOM_ACC; ++q) v[q] = 0.0;
@@ -170,35 +170,35 @@ __global__ void __launch_bounds__(RED_BLOCK) reduce_chunks(const double *__restr
         __threadfence();
     }
     __syncthreads();
-    // Stage 2 in the block that finishes last: a warp per structure sums its
-    // chunks (lane-strided, then the shuffle tree), as a separate launch would.
-    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == (unsigned)(n_chunks - 1);
+    // Stage 2 in the block that finishes its structure's last chunk (a
+    // completion counter per structure): its first warp sums the
+    // structure's chunks (lane-strided, then the shuffle tree).
+    int c0 = chunk_first[s], c1 = chunk_first[s + 1];
+    if (threadIdx.x == 0) last = atomicAdd(sdone + s, 1u) == (unsigned)(c1 - c0 - 1);
     __syncthreads();
-    if (!last) return;
-    for (int s = w; s < n_struct; s += NW) {
+    if (!last || w != 0) return;
 #pragma unroll
-        for (int q = 0; q < ATOM_ACC; ++q) v[q] = 0.0;
-        for (int k = chunk_first[s] + l; k < chunk_first[s + 1]; k += 32) {
-            const double *p = partial + (size_t)k * ATOM_ACC;
+    for (int q = 0; q < ATOM_ACC; ++q) v[q] = 0.0;
+    for (int k = c0 + l; k < c1; k += 32) {
+        const double *p = partial + (size_t)k * ATOM_ACC;
 #pragma unroll
-            for (int q = 0; q < ATOM_ACC; ++q) v[q] += __ldcg(p + q);
-        }
-        warp_sum_acc<1>(v);
-        if (l == 0) {
-            energy[s] = v[10] > 0.0 ? v[0] : 0.0;
-#pragma unroll
-            for (int q = 0; q < 9; ++q) virial[9 * s + q] = v[1 + q];
-        }
+        for (int q = 0; q < ATOM_ACC; ++q) v[q] += __ldcg(p + q);
     }
-    if (threadIdx.x == 0) *counter = 0u;  // ready for the next evaluation
+    warp_sum_acc<1>(v);
+    if (l == 0) {
+        energy[s] = v[10] > 0.0 ? v[0] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) virial[9 * s + q] = v[1 + q];
+    }
 }
 
 int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, int n_struct,
-                         double *partial, double *energy, double *virial, unsigned *counter, cudaStream_t st) {
-    if (plan->n_chunks <= 0 || !counter) return MBF_ERR_ARGUMENT;
+                         double *partial, double *energy, double *virial, unsigned *sdone, cudaStream_t st) {
+    if (plan->n_chunks <= 0 || n_struct <= 0 || !sdone) return MBF_ERR_ARGUMENT;
+    if (cudaMemsetAsync(sdone, 0, sizeof(unsigned) * (size_t)n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
     PROF_BEGIN("reduce_chunks", st);
     reduce_chunks<<<plan->n_chunks, RED_BLOCK, 0, st>>>(per_atom, plan->chunk, plan->n_chunks, partial,
-                                                        plan->chunk_first, n_struct, energy, virial, counter);
+                                                        plan->chunk_first, energy, virial, sdone);
     PROF_END("reduce_chunks", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;

@@ -16,10 +16,10 @@ size_t scan_workspace_ints(int n);
 // scan_workspace_ints(n) ints.
 int exclusive_scan(const int *in, int *out, int n, int *ws, cudaStream_t st);
 
-// `counter` must be 0 at the call (it is left at 0): the evaluation
-// workspace's word RED_COUNTER_WORD, cleared with the error words.
+// `sdone` (n_struct words, the workspace's sdone region) holds the
+// per-structure completion counters; the call clears it.
 int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, int n_struct,
-                         double *partial, double *energy, double *virial, unsigned *counter, cudaStream_t st);
+                         double *partial, double *energy, double *virial, unsigned *sdone, cudaStream_t st);
 
 int gather_forces(int n_atoms, const int *row_off, const double *G, const double *f_local, double *forces,
                   cudaStream_t st);
@@ -34,11 +34,9 @@ struct SiteOut {
     double *vec;   // (n_slots, 3)
 };
 
-// Words of the evaluation workspace's `err` region that each evaluation
-// clears at its start (ERR_CLEAR_BYTES): the error words 0..3 and the
-// completion counter of the per-structure reduction.
-constexpr int RED_COUNTER_WORD = 8;
-constexpr int ERR_CLEAR_BYTES = 64;
+// Bytes of the evaluation workspace's `err` region (the error words 0..3)
+// that each evaluation clears at its start.
+constexpr int ERR_CLEAR_BYTES = 16;
 
 // Layout of the evaluation workspace (all offsets 256-byte aligned):
 //   err      device error words (ints; see ERR_CLEAR_BYTES)
@@ -49,8 +47,9 @@ constexpr int ERR_CLEAR_BYTES = 64;
 //   slot     (n_slots, 3) doubles (three-body force left on each neighbour)
 //   slot_b   (n_slots, 2) doubles (Tersoff bond order and its derivative)
 //   partial  (n_chunks, ATOM_ACC) doubles
+//   sdone    (n_chunks,) completion counters of the per-structure sums
 struct EvalLayout {
-    size_t err, per_atom, f_local, atom_aux, pack, slot, slot_b, partial, total;
+    size_t err, per_atom, f_local, atom_aux, pack, slot, slot_b, partial, sdone, total;
 };
 
 static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -74,6 +73,8 @@ static inline EvalLayout eval_layout(int n_atoms, long long n_slots, int n_chunk
     o = align256(o + sizeof(double) * (size_t)n_slots * 2);
     L.partial = o;
     o = align256(o + sizeof(double) * (size_t)(n_chunks > 0 ? n_chunks : 1) * ATOM_ACC);
+    L.sdone = o;
+    o = align256(o + sizeof(unsigned) * (size_t)(n_chunks > 0 ? n_chunks : 1));
     L.total = o;
     return L;
 }
