@@ -77,6 +77,7 @@ _SIGS = {
     "mbf_nl_workspace_bytes": (_sz, [_i, _i]),
     "mbf_nl_build": (_i, [ctypes.POINTER(MbfSystem), _vp, _i, _d, _vp, _sz, _vp, _vp, _vp, _vp, _ll,
                           ctypes.POINTER(_ll), ctypes.POINTER(_i), _vp]),
+    "mbf_nl_rebuild_workspace_bytes": (_sz, [_i, _i, _i]),
     "mbf_nl_rebuild_async": (_i, [ctypes.POINTER(MbfSystem), _vp, _i, _d, _vp, _sz, _vp, _vp, _vp, _vp,
                                   _ll, _i, _vp, _vp]),
     "mbf_nl_max_displacement": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _vp]),

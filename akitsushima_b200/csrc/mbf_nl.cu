@@ -42,6 +42,11 @@ static NlLayout nl_layout(int n_atoms, int n_cells) {
     return L;
 }
 
+// The rebuild's staging rows (n_atoms x max_row_limit ints) after the layout.
+static size_t nl_staged_bytes(const NlLayout &L, int n_atoms, int max_row_limit) {
+    return L.total + align256(sizeof(int) * (size_t)n_atoms * (size_t)max_row_limit);
+}
+
 // Bin every atom: fractional coordinate wrapped to [0, 1), sub-cell index
 // floor(frac * nc) clipped to [0, nc - 1] (engine/neighborlist.py:982-989).
 __global__ void nl_assign(SysView S, const int *__restrict__ grids, int *__restrict__ atom_cell,
@@ -158,10 +163,17 @@ __device__ __forceinline__ bool pair_hit(const double *__restrict__ cell, double
     return r2 < rl2 && r2 > 1e-20;
 }
 
-template <bool FILL>
+// MODE 0 counts each atom's neighbours (row_cnt, max_row); MODE 1 writes
+// them into the CSR rows (row_off, nbr); MODE 2 counts and writes them at a
+// fixed stride into a staging array (`nbr` = stage, row a at a * stride,
+// at most stride entries kept), so one pass serves a list of known row
+// bound.
+template <int MODE>
 __global__ void nl_cells(SysView S, const int *__restrict__ grids, const int *__restrict__ cell_start,
                          const int *__restrict__ cell_atoms, int n_cells, double rl2, int *__restrict__ row_cnt,
-                         int *__restrict__ max_row, const int *__restrict__ row_off, int *__restrict__ nbr) {
+                         int *__restrict__ max_row, const int *__restrict__ row_off, int *__restrict__ nbr,
+                         int stride) {
+    constexpr bool FILL = MODE != 0, COUNT = MODE != 1;
     __shared__ Stencil sst[NL_WARPS];
     int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Stencil &st = sst[wid];
@@ -179,8 +191,8 @@ __global__ void nl_cells(SysView S, const int *__restrict__ grids, const int *__
             int cnt = 0;       // lane q: neighbours of atom q found so far
             int beg_l = 0, len_l = 0;
             if (FILL && lane < nq) {
-                beg_l = row_off[a_l];
-                len_l = row_off[a_l + 1] - beg_l;
+                beg_l = MODE == 1 ? row_off[a_l] : a_l * stride;
+                len_l = MODE == 1 ? row_off[a_l + 1] - beg_l : stride;
             }
             for (int t0 = 0; t0 < total; t0 += 32) {
                 int t = t0 + lane;
@@ -209,7 +221,7 @@ __global__ void nl_cells(SysView S, const int *__restrict__ grids, const int *__
                     if (lane == q) cnt += __popc(m);
                 }
             }
-            if (!FILL && lane < nq) {
+            if (COUNT && lane < nq) {
                 row_cnt[a_l] = cnt;
                 atomicMax(max_row, cnt);
             }
@@ -234,6 +246,42 @@ __global__ void nl_sort_rows(int n_atoms, const int *__restrict__ row_off, int *
             continue;
         }
         for (int k = lane; k < n; k += 32) row[k] = nbr[beg + k];
+        __syncwarp();
+        int lower = 0;
+        for (int k = lane; k < n; k += 32) {
+            int v = row[k], rank = 0;
+            for (int q = 0; q < n; ++q) rank += row[q] < v ? 1 : 0;
+            nbr[beg + rank] = v;
+            lower += v < a ? 1 : 0;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lower += __shfl_xor_sync(MBF_FULL, lower, o);
+        if (lane == 0) upper[a] = beg + lower;
+        __syncwarp();
+    }
+}
+
+// The staged rows (nl_cells<2>) into the CSR: each row read from its
+// stride-spaced staging slot, rank-sorted ascending in shared memory (as
+// nl_sort_rows) and written at its scanned offset; its first upper slot
+// recorded.  Rows longer than the stride were refused by the guard (their
+// rows are empty by then).
+__global__ void nl_unstage_rows(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ stage,
+                                int stride, int *__restrict__ nbr, int *__restrict__ upper, int *__restrict__ err) {
+    __shared__ int srow[NL_WARPS][NL_MAXROW];
+    int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *row = srow[wid];
+    for (int a = blockIdx.x * NL_WARPS + wid; a < n_atoms; a += gridDim.x * NL_WARPS) {
+        int beg = row_off[a], n = row_off[a + 1] - beg;
+        if (n > stride || n > NL_MAXROW) {
+            if (lane == 0) {
+                atomicOr(err, MBF_DEV_ROW_TOO_LONG);
+                upper[a] = beg;
+            }
+            continue;
+        }
+        const int *src = stage + (size_t)a * stride;
+        for (int k = lane; k < n; k += 32) row[k] = src[k];
         __syncwarp();
         int lower = 0;
         for (int k = lane; k < n; k += 32) {
@@ -385,8 +433,13 @@ size_t mbf_nl_workspace_bytes(int n_atoms, int n_cells_total) {
     return nl_layout(n_atoms, n_cells_total).total;
 }
 
+size_t mbf_nl_rebuild_workspace_bytes(int n_atoms, int n_cells_total, int max_row_limit) {
+    if (n_atoms < 0 || n_cells_total <= 0 || max_row_limit <= 0) return 0;
+    return nl_staged_bytes(nl_layout(n_atoms, n_cells_total), n_atoms, max_row_limit);
+}
+
 static int nl_prepare(const SysView &S, const int *grids, int n_cells_total, double rl2, void *workspace,
-                      const NlLayout &L, int *row_off, cudaStream_t st) {
+                      const NlLayout &L, int *row_off, cudaStream_t st, int *stage = nullptr, int stride = 0) {
     int N = S.n_atoms;
     int *err = ws_at<int>(workspace, L.err);
     int *atom_cell = ws_at<int>(workspace, L.atom_cell);
@@ -414,28 +467,40 @@ static int nl_prepare(const SysView &S, const int *grids, int n_cells_total, dou
     nl_sort_cells<<<(n_cells_total + 127) / 128, 128, 0, st>>>(n_cells_total, cell_start, cell_atoms);
     MBF_CHECK_LAUNCH();
     int cblocks = (n_cells_total + NL_WARPS - 1) / NL_WARPS;
-    int g = persistent_grid(cblocks, 32 * NL_WARPS, (const void *)nl_cells<false>);
+    int g = persistent_grid(cblocks, 32 * NL_WARPS, (const void *)nl_cells<0>);
     PROF_BEGIN("nl_count", st);
-    nl_cells<false><<<g, 32 * NL_WARPS, 0, st>>>(S, grids, cell_start, cell_atoms, n_cells_total, rl2, row_cnt, mrow,
-                                                 nullptr, nullptr);
+    if (stage) {
+        g = persistent_grid(cblocks, 32 * NL_WARPS, (const void *)nl_cells<2>);
+        nl_cells<2><<<g, 32 * NL_WARPS, 0, st>>>(S, grids, cell_start, cell_atoms, n_cells_total, rl2, row_cnt, mrow,
+                                                 nullptr, stage, stride);
+    } else {
+        nl_cells<0><<<g, 32 * NL_WARPS, 0, st>>>(S, grids, cell_start, cell_atoms, n_cells_total, rl2, row_cnt, mrow,
+                                                 nullptr, nullptr, 0);
+    }
     PROF_END("nl_count", st);
     MBF_CHECK_LAUNCH();
     return exclusive_scan(row_cnt, row_off, N, scan_ws, st);
 }
 
 static int nl_finish(const SysView &S, const int *grids, int n_cells_total, double rl2, void *workspace,
-                     const NlLayout &L, const int *row_off, int *nbr, int *rev, int *upper, cudaStream_t st) {
+                     const NlLayout &L, const int *row_off, int *nbr, int *rev, int *upper, cudaStream_t st,
+                     const int *stage = nullptr, int stride = 0) {
     int N = S.n_atoms;
     int *err = ws_at<int>(workspace, L.err);
     int blocks = (N + NL_WARPS - 1) / NL_WARPS;
     int cblocks = (n_cells_total + NL_WARPS - 1) / NL_WARPS;
-    int g = persistent_grid(cblocks, 32 * NL_WARPS, (const void *)nl_cells<true>);
+    int g = persistent_grid(cblocks, 32 * NL_WARPS, (const void *)nl_cells<1>);
     PROF_BEGIN("nl_fill", st);
-    nl_cells<true><<<g, 32 * NL_WARPS, 0, st>>>(S, grids, ws_at<int>(workspace, L.cell_start),
-                                                ws_at<int>(workspace, L.cell_atoms), n_cells_total, rl2, nullptr,
-                                                nullptr, row_off, nbr);
-    g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_sort_rows);
-    nl_sort_rows<<<g, 32 * NL_WARPS, 0, st>>>(N, row_off, nbr, upper, err);
+    if (stage) {
+        g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_unstage_rows);
+        nl_unstage_rows<<<g, 32 * NL_WARPS, 0, st>>>(N, row_off, stage, stride, nbr, upper, err);
+    } else {
+        nl_cells<1><<<g, 32 * NL_WARPS, 0, st>>>(S, grids, ws_at<int>(workspace, L.cell_start),
+                                                 ws_at<int>(workspace, L.cell_atoms), n_cells_total, rl2, nullptr,
+                                                 nullptr, row_off, nbr, 0);
+        g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_sort_rows);
+        nl_sort_rows<<<g, 32 * NL_WARPS, 0, st>>>(N, row_off, nbr, upper, err);
+    }
     PROF_END("nl_fill", st);
     MBF_CHECK_LAUNCH();
     g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_reverse);
@@ -502,14 +567,19 @@ int mbf_nl_rebuild_async(const mbf_system *sys, const int *grids, int n_cells_to
     if (workspace_bytes < L.total) return MBF_ERR_WORKSPACE;
     SysView S = make_view(sys);
     double rl2 = r_list * r_list;
-    int rc = nl_prepare(S, grids, n_cells_total, rl2, workspace, L, row_off, st);
+    // with room for the staging rows the search runs once (count and stage),
+    // else it counts, then fills
+    int *stage = nullptr;
+    if (workspace_bytes >= nl_staged_bytes(L, N, max_row_limit) && (long long)N * max_row_limit < 0x7fffffffLL)
+        stage = ws_at<int>(workspace, L.total);
+    int rc = nl_prepare(S, grids, n_cells_total, rl2, workspace, L, row_off, st, stage, max_row_limit);
     if (rc != MBF_OK) return rc;
     int *err = ws_at<int>(workspace, L.err);
     nl_guard<<<1, 32, 0, st>>>(N, row_off, ws_at<int>(workspace, L.maxrow), nbr_capacity, max_row_limit, status,
                                err + 4);
     nl_clear_if<<<(N + 256) / 256, 256, 0, st>>>(N, err + 4, row_off, upper);
     MBF_CHECK_LAUNCH();
-    rc = nl_finish(S, grids, n_cells_total, rl2, workspace, L, row_off, nbr, rev, upper, st);
+    rc = nl_finish(S, grids, n_cells_total, rl2, workspace, L, row_off, nbr, rev, upper, st, stage, max_row_limit);
     if (rc != MBF_OK) return rc;
     nl_status_merge<<<1, 32, 0, st>>>(err, status);
     MBF_CHECK_LAUNCH();

@@ -160,7 +160,7 @@ class NVE:
         nbytes = int(L.mbf_eval_workspace_bytes(self.n_atoms, cap, self.batch.n_chunks))
         self._ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=dev)
         self._n_cells = self.dlist._grid_table(self.batch)[1]
-        nl_bytes = int(L.mbf_nl_workspace_bytes(self.n_atoms, self._n_cells))
+        nl_bytes = int(L.mbf_nl_rebuild_workspace_bytes(self.n_atoms, self._n_cells, self.view.max_row))
         self._nl_ws = torch.empty(max(nl_bytes, 256), dtype=torch.uint8, device=dev)
         if velocities is None:
             rng = np.random.default_rng(seed)

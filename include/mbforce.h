@@ -96,6 +96,12 @@ int mbf_version(void);
  * (engine/neighborlist.py:350-363), so the pair set equals the reference's
  * bit for bit.  n_cells_total = sum over structures of nc0*nc1*nc2.      */
 size_t mbf_nl_workspace_bytes(int n_atoms, int n_cells_total);
+/* The workspace with which mbf_nl_rebuild_async searches once instead of
+ * twice: mbf_nl_workspace_bytes plus n_atoms x max_row_limit staging ints
+ * (each row kept at a fixed stride during the count, then sorted into
+ * the CSR).  A smaller workspace, of at least mbf_nl_workspace_bytes, runs
+ * the count-then-fill search.                                            */
+size_t mbf_nl_rebuild_workspace_bytes(int n_atoms, int n_cells_total, int max_row_limit);
 
 /* Counts, scans and fills.  If nbr_capacity < the number of slots it stops
  * after the count, stores the need in *n_slots (host) and returns
