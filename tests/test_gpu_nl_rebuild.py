@@ -1,0 +1,83 @@
+"""The in-place list rebuild of device MD (mbf_nl_rebuild_async), through
+the C ABI: with the staged workspace (one search: rows kept at the row
+bound's stride, then sorted into the CSR) and with the plain one (count,
+then fill) it gives exactly the general build's rows, reverse slots and
+upper offsets; a row bound below the longest row is reported, with every
+row left empty."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import DIAMOND, FCC, cubic, strained
+
+pytestmark = pytest.mark.gpu
+
+ak = pytest.importorskip("akitsushima_b200")
+from akitsushima_b200 import _lib  # noqa: E402
+from akitsushima_b200.neighbourlist import DeviceNeighbourList  # noqa: E402
+
+STATUS_ROW_TOO_LONG = 1
+
+
+def _cases():
+    lat, pos, _ = cubic(DIAMOND, 5.431, 4, ["Si"] * 8, rattle=0.1, seed=21)
+    one = ([lat], [pos], 4.07)
+    l2, p2, _ = cubic(FCC, 3.58, 5, ["Cu"] * 4, rattle=0.08, seed=22)
+    l2, p2 = strained(l2, p2, 0.03, 23)
+    l3, p3, _ = cubic(DIAMOND, 5.431, 3, ["Si"] * 8, rattle=0.1, seed=24)
+    many = ([l2, l3], [p2, p3], 6.1)
+    return {"si512": one, "batch_fcc_si": many}
+
+
+def _rebuild(batch, ref, limit, staged):
+    L = _lib.lib()
+    dev = batch.device
+    grids, n_cells = ref._grid_table(batch)
+    grids_t = torch.as_tensor(grids, device=dev)
+    N = batch.n_atoms
+    plain = int(L.mbf_nl_workspace_bytes(N, n_cells))
+    need = int(L.mbf_nl_rebuild_workspace_bytes(N, n_cells, limit)) if staged else plain
+    assert need > plain if staged else True
+    ws = torch.empty(need, dtype=torch.uint8, device=dev)
+    cap = ref.n_slots + 1024
+    row_off = torch.full((N + 1,), -7, dtype=torch.int32, device=dev)
+    upper = torch.full((N,), -7, dtype=torch.int32, device=dev)
+    nbr = torch.full((cap,), -7, dtype=torch.int32, device=dev)
+    rev = torch.full((cap,), -7, dtype=torch.int32, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    _lib.check(L.mbf_nl_rebuild_async(batch.mbf_system(), _lib.ptr(grids_t), n_cells, ref.r_list, _lib.ptr(ws), need,
+                                      _lib.ptr(row_off), _lib.ptr(nbr), _lib.ptr(rev), _lib.ptr(upper), cap, limit,
+                                      _lib.ptr(status), st), "mbf_nl_rebuild_async")
+    torch.cuda.synchronize(dev)
+    return row_off.cpu().numpy(), upper.cpu().numpy(), nbr.cpu().numpy(), rev.cpu().numpy(), int(status.item())
+
+
+@pytest.mark.parametrize("case", ["si512", "batch_fcc_si"])
+@pytest.mark.parametrize("staged", [True, False])
+def test_rebuild_equals_general_build(cuda_device, case, staged):
+    lats, poss, r_list = _cases()[case]
+    ids = [np.zeros(len(p), np.int32) for p in poss]
+    batch = ak.Batch(lats, poss, ids, device=cuda_device)
+    ref = DeviceNeighbourList(r_list).build(batch)
+    N, ns = batch.n_atoms, ref.n_slots
+    want = (ref.row_off[:N + 1].cpu().numpy(), ref.upper[:N].cpu().numpy(), ref.nbr[:ns].cpu().numpy(),
+            ref.rev[:ns].cpu().numpy())
+    limit = ref.max_row + 3
+    for _ in range(2):   # the second call reuses the same workspace contents
+        row_off, upper, nbr, rev, status = _rebuild(batch, ref, limit, staged)
+        assert status == 0
+        np.testing.assert_array_equal(row_off, want[0])
+        np.testing.assert_array_equal(upper, want[1])
+        np.testing.assert_array_equal(nbr[:ns], want[2])
+        np.testing.assert_array_equal(rev[:ns], want[3])
+
+
+@pytest.mark.parametrize("staged", [True, False])
+def test_row_bound_too_small_is_reported(cuda_device, staged):
+    lats, poss, r_list = _cases()["si512"]
+    batch = ak.Batch(lats, poss, [np.zeros(len(poss[0]), np.int32)], device=cuda_device)
+    ref = DeviceNeighbourList(r_list).build(batch)
+    row_off, upper, _, _, status = _rebuild(batch, ref, ref.max_row - 2, staged)
+    assert status & STATUS_ROW_TOO_LONG
+    assert not row_off.any() and not upper.any()
