@@ -207,11 +207,14 @@ class DevicePotential:
         if dev is None:
             from .system import default_device
             dev = default_device()
-        ids = species_ids(atom_types, self.species)
         nl, batch, dl = self._resolve_list(lattice, pos, neigh_list, dev)
         batch.set_lattice(0, lattice)
         batch.set_positions(pos, check=False)   # as the reference: no scan of the input
-        batch.set_types(ids)
+        # an integer id array equal to the one on the device was validated
+        # and uploaded before: one comparison instead of a range check and
+        # a comparison
+        if not batch.types_unchanged(atom_types, len(self.species)):
+            batch.set_types(species_ids(atom_types, self.species))
         res = self.evaluate(batch, dl)
         # energy, virial and the device status words (the first 16 bytes of
         # the workspace, carried as two doubles) in one copy

@@ -190,6 +190,13 @@ class Batch:
         torch.cuda.current_stream(self.device).synchronize()
         return out.numpy()
 
+    def types_unchanged(self, type_ids, n_species):
+        """True if type_ids is an integer array equal to the ids last
+        uploaded from the host, all of them below n_species."""
+        return (isinstance(type_ids, np.ndarray) and type_ids.dtype.kind in "iu" and self._types_host is not None
+                and self._types_max < n_species and type_ids.shape == self._types_host.shape
+                and np.array_equal(type_ids, self._types_host))
+
     def set_types(self, type_ids):
         """Species ids (torch tensor, or host arrays; an unchanged host array
         is not uploaded again)."""
@@ -209,6 +216,7 @@ class Batch:
         host = np.ascontiguousarray(arr)
         self.types.copy_(torch.from_numpy(host if host.flags.writeable else host.copy()))
         self._types_host = arr.copy()
+        self._types_max = int(arr.max()) if len(arr) else -1
 
     def set_lattice(self, s, lattice):
         lat = np.asarray(lattice, np.float64).reshape(3, 3)

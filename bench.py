@@ -1024,7 +1024,7 @@ def main():
     ap.add_argument("--cells", type=int, default=40)
     ap.add_argument("--lanes", type=int, default=2, help="EAM lanes per atom (1, 2, 4, 8, 16, 32)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--e2e-steps", type=int, default=200)
     ap.add_argument("--skip-singles", action="store_true",
                     help="batched workload: skip the per-structure-launch comparison (profiling runs)")
     ap.add_argument("--workload", default="eam_cuni_256k",
