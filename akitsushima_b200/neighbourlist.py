@@ -66,10 +66,13 @@ class DeviceNeighbourList:
         if self.row_off is None or self.row_off.numel() < N + 1 or self.row_off.device != dev:
             self.row_off = torch.empty(N + 1, dtype=torch.int32, device=dev)
             self.upper = torch.empty(max(N, 1), dtype=torch.int32, device=dev)
+        # the slots expected from each structure's number density (the sphere
+        # of radius r_list), 20 % over, so one search usually suffices
+        cnt = np.asarray(batch.counts, float)
+        est = int(1.2 * float(np.sum(cnt * cnt / batch.volumes)) * 4.0 / 3.0 * np.pi * self.r_list ** 3) + 1024
         if self.nbr is None or self.nbr.device != dev:
-            cap = max(1024, int(N * 8))
-            self.nbr = torch.empty(cap, dtype=torch.int32, device=dev)
-            self.rev = torch.empty(cap, dtype=torch.int32, device=dev)
+            self.nbr = torch.empty(est, dtype=torch.int32, device=dev)
+            self.rev = torch.empty(est, dtype=torch.int32, device=dev)
         sysd = batch.mbf_system()
         stream = torch.cuda.current_stream(dev).cuda_stream
         n_slots = _lib._ll(0)

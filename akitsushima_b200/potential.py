@@ -11,6 +11,7 @@ Stress is compressive-positive and divided by the volume, as the reference
 returns it (engine/tersoff.py:1512).
 """
 import threading
+import weakref
 
 import numpy as np
 import torch
@@ -22,6 +23,17 @@ from .system import Batch, species_ids
 PRECISIONS = {"fp64": _lib.MBF_FP64, "mixed": _lib.MBF_MIXED}
 
 _ws_local = threading.local()
+
+
+def _set_last_ws(pot, ws):
+    """The workspace of this thread's last evaluation with `pot` (its status
+    words are read back after the call); held weakly."""
+    _ws_local.__dict__.setdefault("last", {})[id(pot)] = weakref.ref(ws)
+
+
+def _get_last_ws(pot):
+    ref = getattr(_ws_local, "last", {}).get(id(pot))
+    return ref() if ref is not None else None
 
 
 def workspace(device, nbytes):
@@ -106,7 +118,7 @@ class DevicePotential:
                         _lib.ptr(ws), ws.numel(), _lib.ptr(out.forces), _lib.ptr(out.energy),
                         _lib.ptr(out.virial), stream)
         _lib.check(rc, type(self).__name__ + ".evaluate")
-        self._last_ws = ws
+        _set_last_ws(self, ws)
         return out
 
     def evaluate_sites(self, batch, dlist, precision=None):
@@ -130,7 +142,7 @@ class DevicePotential:
                                           _lib.ptr(out.energy), _lib.ptr(out.virial), _lib.ptr(e), _lib.ptr(dudv),
                                           _lib.ptr(vec), torch.cuda.current_stream(dev).cuda_stream)
         _lib.check(rc, type(self).__name__ + ".evaluate_sites")
-        self._last_ws = ws
+        _set_last_ws(self, ws)
         return out, e, dudv, vec
 
     def autotune_lanes(self, batch, dlist, candidates=None, reps=3, ws=None, out=None):
@@ -156,7 +168,7 @@ class DevicePotential:
     def status(self, device=None):
         """Device status words of the last evaluation (synchronises): raises
         if a kernel reported a bad index or an over-long row."""
-        ws = getattr(self, "_last_ws", None)
+        ws = _get_last_ws(self)
         if ws is None:
             return
         words = (_lib._i * 4)()
@@ -218,7 +230,7 @@ class DevicePotential:
         res = self.evaluate(batch, dl)
         # energy, virial and the device status words (the first 16 bytes of
         # the workspace, carried as two doubles) in one copy
-        words = self._last_ws[:16].view(torch.float64)
+        words = _get_last_ws(self)[:16].view(torch.float64)
         ev = torch.cat([res.energy[:1], res.virial[0], words]).to("cpu", non_blocking=True)
         f = batch.forces_to_host(res.forces)   # synchronises the stream
         ev = ev.numpy()
