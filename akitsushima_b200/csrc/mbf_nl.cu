@@ -5,6 +5,8 @@
 // (_cell_linked_pairs_numpy), :1166-1181 (_canonical_pair_order) and the
 // two-way CSR of engine/tersoff.py:1297-1307.  The pair test reproduces the
 // reference's rounding exactly (mic_exact), so the pair set is bit-exact.
+#include <type_traits>
+
 #include "mbf_util.cuh"
 
 namespace mbf {
@@ -163,6 +165,35 @@ __device__ __forceinline__ bool pair_hit(const double *__restrict__ cell, double
     return r2 < rl2 && r2 > 1e-20;
 }
 
+// A cell whose lattice and inverse have exact zeros off the diagonal.
+__device__ __forceinline__ bool cell_is_diagonal(const double *__restrict__ c) {
+    bool z = true;
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        const double *q = c + 9 * m;
+        z = z && q[1] == 0.0 && q[2] == 0.0 && q[3] == 0.0 && q[5] == 0.0 && q[6] == 0.0 && q[7] == 0.0;
+    }
+    return z;
+}
+
+// pair_hit for a diagonal cell (d = inverse diagonal, l = lattice
+// diagonal).  Each dropped term of mic_exact's dot products is a product
+// with an exact zero, i.e. +-0, and x + (+-0) == x for every x != 0, so
+// every component equals mic_exact's up to the sign of a zero, and r2 --
+// a sum of squares -- is the same double bit for bit.
+__device__ __forceinline__ bool pair_hit_diag(double d0, double d1, double d2, double l0, double l1, double l2,
+                                              double xa, double ya, double za, double xb, double yb, double zb,
+                                              double rl2) {
+    double sx = __dmul_rn(__dsub_rn(xb, xa), d0);
+    double sy = __dmul_rn(__dsub_rn(yb, ya), d1);
+    double sz = __dmul_rn(__dsub_rn(zb, za), d2);
+    sx = __dsub_rn(sx, rint_shift(sx));
+    sy = __dsub_rn(sy, rint_shift(sy));
+    sz = __dsub_rn(sz, rint_shift(sz));
+    double r2 = r2_exact(__dmul_rn(sx, l0), __dmul_rn(sy, l1), __dmul_rn(sz, l2));
+    return r2 < rl2 && r2 > 1e-20;
+}
+
 // MODE 0 counts each atom's neighbours (row_cnt, max_row); MODE 1 writes
 // them into the CSR rows (row_off, nbr); MODE 2 counts and writes them at a
 // fixed stride into a staging array (`nbr` = stage, row a at a * stride,
@@ -184,6 +215,8 @@ __global__ void nl_cells(SysView S, const int *__restrict__ grids, const int *__
         int sidx = S.n_struct > 1 ? S.atom_struct[a0] : 0;
         int total = build_stencil_of_cell(grids, cell_start, sidx, c, st);
         const double *cell = S.cells + 18 * (size_t)sidx;
+        const bool diag = cell_is_diagonal(cell);
+        const double d0 = cell[9], d1 = cell[13], d2 = cell[17], l0 = cell[0], l1 = cell[4], l2 = cell[8];
         for (int q0 = 0; q0 < na; q0 += 32) {
             int nq = min(32, na - q0);
             int a_l = lane < nq ? cell_atoms[cs + q0 + lane] : 0;
@@ -204,22 +237,33 @@ __global__ void nl_cells(SysView S, const int *__restrict__ grids, const int *__
                     yb = S.pos[3 * (size_t)b + 1];
                     zb = S.pos[3 * (size_t)b + 2];
                 }
-                for (int q = 0; q < nq; ++q) {
-                    int a = __shfl_sync(MBF_FULL, a_l, q);
-                    double xa = __shfl_sync(MBF_FULL, xa_l, q), ya = __shfl_sync(MBF_FULL, ya_l, q),
-                           za = __shfl_sync(MBF_FULL, za_l, q);
-                    bool hit = b >= 0 && b != a && pair_hit(cell, xa, ya, za, xb, yb, zb, rl2);
-                    unsigned m = __ballot_sync(MBF_FULL, hit);
-                    if (FILL) {
-                        int w = __shfl_sync(MBF_FULL, cnt, q);
-                        int beg = __shfl_sync(MBF_FULL, beg_l, q), len = __shfl_sync(MBF_FULL, len_l, q);
-                        if (hit) {
-                            int pos = w + __popc(m & ((1u << lane) - 1u));
-                            if (pos < len) nbr[beg + pos] = b;
+                // the cell's atoms against this round's candidates, with
+                // the test specialised once per cell (warp-uniform)
+                auto rounds = [&](auto diag_tag) {
+                    constexpr bool DIAG = decltype(diag_tag)::value;
+                    for (int q = 0; q < nq; ++q) {
+                        int a = __shfl_sync(MBF_FULL, a_l, q);
+                        double xa = __shfl_sync(MBF_FULL, xa_l, q), ya = __shfl_sync(MBF_FULL, ya_l, q),
+                               za = __shfl_sync(MBF_FULL, za_l, q);
+                        bool hit = b >= 0 && b != a &&
+                                   (DIAG ? pair_hit_diag(d0, d1, d2, l0, l1, l2, xa, ya, za, xb, yb, zb, rl2)
+                                         : pair_hit(cell, xa, ya, za, xb, yb, zb, rl2));
+                        unsigned m = __ballot_sync(MBF_FULL, hit);
+                        if (FILL) {
+                            int w = __shfl_sync(MBF_FULL, cnt, q);
+                            int beg = __shfl_sync(MBF_FULL, beg_l, q), len = __shfl_sync(MBF_FULL, len_l, q);
+                            if (hit) {
+                                int pos = w + __popc(m & ((1u << lane) - 1u));
+                                if (pos < len) nbr[beg + pos] = b;
+                            }
                         }
+                        if (lane == q) cnt += __popc(m);
                     }
-                    if (lane == q) cnt += __popc(m);
-                }
+                };
+                if (diag)
+                    rounds(std::true_type{});
+                else
+                    rounds(std::false_type{});
             }
             if (COUNT && lane < nq) {
                 row_cnt[a_l] = cnt;
@@ -229,13 +273,84 @@ __global__ void nl_cells(SysView S, const int *__restrict__ grids, const int *__
     }
 }
 
-// Rows written in traversal order by nl_cells<true>: sort each row
-// ascending (rank sort in shared memory) and record its first upper slot.
+// ---- row sorts -----------------------------------------------------------------
+// Rows come out of the search in traversal order; the CSR keeps them
+// ascending.  A row of at most 128 entries is sorted in registers by a
+// bitonic network over four entries per lane (entry e = 4 lane + j, padded
+// with INT_MAX, which sorts last since atom indices are smaller); a longer
+// one by rank in shared memory.  Entries of a row are distinct.
+constexpr int NL_PAD = 0x7fffffff;
+
+__device__ __forceinline__ void cmp_swap(int &lo, int &hi, bool asc) {
+    int mn = min(lo, hi), mx = max(lo, hi);
+    lo = asc ? mn : mx;
+    hi = asc ? mx : mn;
+}
+
+__device__ __forceinline__ void bitonic128(int (&v)[4]) {
+    int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 128; k <<= 1) {
+#pragma unroll
+        for (int d = k >> 1; d > 0; d >>= 1) {
+            if (d >= 4) {  // partner in lane ^ (d / 4), same register
+                bool low = (lane & (d >> 2)) == 0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    int o = __shfl_xor_sync(MBF_FULL, v[j], d >> 2);
+                    bool asc = ((4 * lane + j) & k) == 0;
+                    v[j] = (low == asc) ? min(v[j], o) : max(v[j], o);
+                }
+            } else {  // partner in register j ^ d of this lane
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if ((j & d) == 0) cmp_swap(v[j], v[j ^ d], ((4 * lane + j) & k) == 0);
+            }
+        }
+    }
+}
+
+// Sorts the n entries src[0..n) (n <= NL_MAXROW) ascending into out[0..n)
+// (src and out may be the same row: every entry is read before any is
+// written) and returns how many are below `a` (warp-uniform).  `row` is
+// the warp's shared scratch of NL_MAXROW ints.
+__device__ __forceinline__ int sort_row(const int *src, int n, int *out, int a, int *row) {
+    int lane = threadIdx.x & 31;
+    int lower = 0;
+    if (n <= 128) {
+        int v[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = 4 * lane + j < n ? src[4 * lane + j] : NL_PAD;
+        __syncwarp();
+        bitonic128(v);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (4 * lane + j < n) {
+                out[4 * lane + j] = v[j];
+                lower += v[j] < a ? 1 : 0;
+            }
+    } else {
+        for (int k = lane; k < n; k += 32) row[k] = src[k];
+        __syncwarp();
+        for (int k = lane; k < n; k += 32) {
+            int v = row[k], rank = 0;
+            for (int q = 0; q < n; ++q) rank += row[q] < v ? 1 : 0;
+            out[rank] = v;
+            lower += v < a ? 1 : 0;
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lower += __shfl_xor_sync(MBF_FULL, lower, o);
+    return lower;
+}
+
+// Rows written in traversal order by nl_cells<1>: sorted in place, and
+// each row's first upper slot recorded.
 __global__ void nl_sort_rows(int n_atoms, const int *__restrict__ row_off, int *__restrict__ nbr,
                              int *__restrict__ upper, int *__restrict__ err) {
     __shared__ int srow[NL_WARPS][NL_MAXROW];
     int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int *row = srow[wid];
     for (int a = blockIdx.x * NL_WARPS + wid; a < n_atoms; a += gridDim.x * NL_WARPS) {
         int beg = row_off[a], n = row_off[a + 1] - beg;
         if (n > NL_MAXROW) {
@@ -245,32 +360,19 @@ __global__ void nl_sort_rows(int n_atoms, const int *__restrict__ row_off, int *
             }
             continue;
         }
-        for (int k = lane; k < n; k += 32) row[k] = nbr[beg + k];
-        __syncwarp();
-        int lower = 0;
-        for (int k = lane; k < n; k += 32) {
-            int v = row[k], rank = 0;
-            for (int q = 0; q < n; ++q) rank += row[q] < v ? 1 : 0;
-            nbr[beg + rank] = v;
-            lower += v < a ? 1 : 0;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) lower += __shfl_xor_sync(MBF_FULL, lower, o);
+        int lower = sort_row(nbr + beg, n, nbr + beg, a, srow[wid]);
         if (lane == 0) upper[a] = beg + lower;
-        __syncwarp();
     }
 }
 
 // The staged rows (nl_cells<2>) into the CSR: each row read from its
-// stride-spaced staging slot, rank-sorted ascending in shared memory (as
-// nl_sort_rows) and written at its scanned offset; its first upper slot
-// recorded.  Rows longer than the stride were refused by the guard (their
-// rows are empty by then).
+// stride-spaced staging slot, sorted and written at its scanned offset;
+// its first upper slot recorded.  Rows longer than the stride were refused
+// by the guard (their rows are empty by then).
 __global__ void nl_unstage_rows(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ stage,
                                 int stride, int *__restrict__ nbr, int *__restrict__ upper, int *__restrict__ err) {
     __shared__ int srow[NL_WARPS][NL_MAXROW];
     int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int *row = srow[wid];
     for (int a = blockIdx.x * NL_WARPS + wid; a < n_atoms; a += gridDim.x * NL_WARPS) {
         int beg = row_off[a], n = row_off[a + 1] - beg;
         if (n > stride || n > NL_MAXROW) {
@@ -280,32 +382,22 @@ __global__ void nl_unstage_rows(int n_atoms, const int *__restrict__ row_off, co
             }
             continue;
         }
-        const int *src = stage + (size_t)a * stride;
-        for (int k = lane; k < n; k += 32) row[k] = src[k];
-        __syncwarp();
-        int lower = 0;
-        for (int k = lane; k < n; k += 32) {
-            int v = row[k], rank = 0;
-            for (int q = 0; q < n; ++q) rank += row[q] < v ? 1 : 0;
-            nbr[beg + rank] = v;
-            lower += v < a ? 1 : 0;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) lower += __shfl_xor_sync(MBF_FULL, lower, o);
+        int lower = sort_row(stage + (size_t)a * stride, n, nbr + beg, a, srow[wid]);
         if (lane == 0) upper[a] = beg + lower;
-        __syncwarp();
     }
 }
 
-// Reverse slot of every slot: rows are sorted, so binary search for a in
-// the row of b.
-__global__ void nl_reverse(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ nbr,
-                           int *__restrict__ rev, int *__restrict__ err) {
+// Reverse slot of every slot.  rev is an involution, so only the upper
+// slots (a -> b, b > a) search: a lies in the lower part of b's sorted row,
+// [row_off[b], upper[b]); the slot t found there gets rev[t] = s, so every
+// slot is written once.
+__global__ void nl_reverse(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ upper,
+                           const int *__restrict__ nbr, int *__restrict__ rev, int *__restrict__ err) {
     int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int a = blockIdx.x * NL_WARPS + wid; a < n_atoms; a += gridDim.x * NL_WARPS) {
-        for (int s = row_off[a] + lane; s < row_off[a + 1]; s += 32) {
+        for (int s = upper[a] + lane; s < row_off[a + 1]; s += 32) {
             int b = nbr[s];
-            int lo = row_off[b], hi = row_off[b + 1] - 1, found = -1;
+            int lo = row_off[b], hi = upper[b] - 1, found = -1;
             while (lo <= hi) {
                 int mid = (lo + hi) >> 1;
                 int v = nbr[mid];
@@ -314,9 +406,11 @@ __global__ void nl_reverse(int n_atoms, const int *__restrict__ row_off, const i
             }
             if (found < 0) {
                 atomicOr(err, MBF_DEV_BAD_INDEX);
-                found = s;
+                rev[s] = s;
+                continue;
             }
             rev[s] = found;
+            rev[found] = s;
         }
     }
 }
@@ -505,7 +599,7 @@ static int nl_finish(const SysView &S, const int *grids, int n_cells_total, doub
     MBF_CHECK_LAUNCH();
     g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_reverse);
     PROF_BEGIN("nl_reverse", st);
-    nl_reverse<<<g, 32 * NL_WARPS, 0, st>>>(N, row_off, nbr, rev, err);
+    nl_reverse<<<g, 32 * NL_WARPS, 0, st>>>(N, row_off, upper, nbr, rev, err);
     PROF_END("nl_reverse", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;
@@ -529,7 +623,17 @@ int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total, dou
         return MBF_OK;
     }
     double rl2 = r_list * r_list;
-    int rc = nl_prepare(S, grids, n_cells_total, rl2, workspace, L, row_off, st);
+    // workspace beyond the layout holds staging rows at the stride it allows:
+    // if no row is longer, the search runs once (count and stage, then sort
+    // into the CSR), else the rows are searched again (fill)
+    int stride = 0;
+    if (workspace_bytes >= L.total + 256) {
+        size_t per = (workspace_bytes - L.total) / (sizeof(int) * (size_t)N);
+        stride = (int)(per < (size_t)NL_MAXROW ? per : (size_t)NL_MAXROW);
+        if ((long long)N * stride >= 0x7fffffffLL) stride = (int)(0x7ffffffeLL / N);
+    }
+    int *stage = stride > 0 ? ws_at<int>(workspace, L.total) : nullptr;
+    int rc = nl_prepare(S, grids, n_cells_total, rl2, workspace, L, row_off, st, stage, stride);
     if (rc != MBF_OK) return rc;
     int host[2];
     if (cudaMemcpyAsync(&host[0], row_off + N, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -542,7 +646,9 @@ int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total, dou
     if ((long long)host[0] > nbr_capacity || !nbr || !rev) return MBF_ERR_CAPACITY;
     if (!upper) return MBF_ERR_ARGUMENT;
     if (host[1] > NL_MAXROW) return MBF_ERR_ROW_TOO_LONG;
-    rc = nl_finish(S, grids, n_cells_total, rl2, workspace, L, row_off, nbr, rev, upper, st);
+    if (host[1] > stride) stage = nullptr;
+    rc = nl_finish(S, grids, n_cells_total, rl2, workspace, L, row_off, nbr, rev, upper, st, stage,
+                   stage ? stride : 0);
     if (rc != MBF_OK) return rc;
     int herr = 0;
     if (cudaMemcpyAsync(&herr, ws_at<int>(workspace, L.err), sizeof(int), cudaMemcpyDeviceToHost, st) !=

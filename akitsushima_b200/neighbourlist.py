@@ -15,9 +15,10 @@ import numpy as np
 import torch
 
 from . import _lib
-from .system import Batch, cell_grid, cell_metrics, check_min_image, default_device
+from .system import Batch, cell_grid, cell_widths, check_min_image, default_device
 
 _BACKENDS = ("auto", "cuda")
+NL_MAX_ROW = 1024   # the longest row the device row sort holds (mbf_nl.cu)
 
 
 class DeviceNeighbourList:
@@ -45,8 +46,9 @@ class DeviceNeighbourList:
     def _grid_table(self, batch):
         rows, first = [], 0
         for s in range(batch.n_struct):
-            check_min_image(batch.lattices[s], self.r_list)
-            nc, w = cell_grid(batch.lattices[s], self.r_list)
+            widths = cell_widths(batch.lattices[s])
+            check_min_image(batch.lattices[s], self.r_list, widths=widths)
+            nc, w = cell_grid(batch.lattices[s], self.r_list, widths=widths)
             rows.append([nc[0], nc[1], nc[2], first, w[0], w[1], w[2], 0])
             first += int(nc[0] * nc[1] * nc[2])
         return np.array(rows, np.int32), first
@@ -60,16 +62,21 @@ class DeviceNeighbourList:
         N = batch.n_atoms
         self.n_atoms = N
         L = _lib.lib()
-        need = int(L.mbf_nl_workspace_bytes(N, n_cells))
+        # the rows expected from each structure's number density (the sphere
+        # of radius r_list): the slot capacity 20 % over their sum, and the
+        # staging stride (the workspace beyond mbf_nl_workspace_bytes) 30 %
+        # over the longest, so one search usually suffices
+        cnt = np.asarray(batch.counts, float)
+        sphere = 4.0 / 3.0 * np.pi * self.r_list ** 3
+        rows = cnt / np.asarray(batch.volumes, float) * sphere if len(cnt) else np.zeros(1)
+        est = int(1.2 * float(np.sum(cnt * rows))) + 1024
+        stride = min(NL_MAX_ROW, int(1.3 * float(np.max(rows))) + 16)
+        need = int(L.mbf_nl_rebuild_workspace_bytes(N, n_cells, stride) if N else L.mbf_nl_workspace_bytes(N, n_cells))
         if self._ws is None or self._ws.numel() < need or self._ws.device != dev:
             self._ws = torch.empty(need, dtype=torch.uint8, device=dev)
         if self.row_off is None or self.row_off.numel() < N + 1 or self.row_off.device != dev:
             self.row_off = torch.empty(N + 1, dtype=torch.int32, device=dev)
             self.upper = torch.empty(max(N, 1), dtype=torch.int32, device=dev)
-        # the slots expected from each structure's number density (the sphere
-        # of radius r_list), 20 % over, so one search usually suffices
-        cnt = np.asarray(batch.counts, float)
-        est = int(1.2 * float(np.sum(cnt * cnt / batch.volumes)) * 4.0 / 3.0 * np.pi * self.r_list ** 3) + 1024
         if self.nbr is None or self.nbr.device != dev:
             self.nbr = torch.empty(est, dtype=torch.int32, device=dev)
             self.rev = torch.empty(est, dtype=torch.int32, device=dev)
@@ -79,7 +86,7 @@ class DeviceNeighbourList:
         max_row = _lib._i(0)
         for _ in range(3):
             rc = L.mbf_nl_build(sysd, _lib.ptr(self._grids), n_cells, self.r_list, _lib.ptr(self._ws),
-                                need, _lib.ptr(self.row_off), _lib.ptr(self.nbr), _lib.ptr(self.rev),
+                                self._ws.numel(), _lib.ptr(self.row_off), _lib.ptr(self.nbr), _lib.ptr(self.rev),
                                 _lib.ptr(self.upper), self.nbr.numel(), n_slots, max_row, stream)
             if rc == _lib.MBF_ERR_CAPACITY:
                 cap = int(n_slots.value * 1.25) + 1024
@@ -201,7 +208,7 @@ class NeighbourList:
         return self._dnl.n_atoms
 
     def _check_min_cell(self, lattice):
-        widths, _ = cell_metrics(lattice)
+        widths = cell_widths(lattice)
         if self.r_list >= float(np.min(widths)) / 2.0:
             check_min_image(lattice, self.r_list, "NeighbourList: r_cut + skin_width")
 
@@ -372,7 +379,7 @@ def owned_neighbour_list(lattice, positions, r_cut, device=None):
     ``check_and_rebuild`` finds the cached one still complete."""
     lattice = np.asarray(lattice, dtype=float)
     n = len(positions)
-    widths, _ = cell_metrics(lattice)
+    widths = cell_widths(lattice)
     half = float(np.min(widths)) / 2.0
     if r_cut + _OWNED_SKIN < half:
         skin = _OWNED_SKIN

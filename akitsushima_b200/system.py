@@ -20,6 +20,12 @@ def cell_metrics(lattice):
     (rows are lattice vectors); the reference's engine/neighborlist.py:170-267.
     Raises ValueError for a degenerate cell."""
     lat = np.asarray(lattice, dtype=float)
+    return cell_widths(lat), float(np.linalg.svd(lat, compute_uv=False)[-1])
+
+
+def cell_widths(lattice):
+    """The perpendicular widths of :func:`cell_metrics` alone."""
+    lat = np.asarray(lattice, dtype=float)
     if lat.shape != (3, 3):
         raise ValueError(f"NeighbourList: lattice must have shape (3, 3), got {lat.shape}.")
     volume = abs(float(np.linalg.det(lat)))
@@ -30,13 +36,15 @@ def cell_metrics(lattice):
             f"NeighbourList: degenerate (singular) lattice with volume {volume:.6g} A^3 -- "
             "the three lattice vectors must be linearly independent for a minimum-image "
             "convention to exist.")
-    return volume / cross, float(np.linalg.svd(lat, compute_uv=False)[-1])
+    return volume / cross
 
 
-def check_min_image(lattice, r_list, caller="NeighbourList"):
+def check_min_image(lattice, r_list, caller="NeighbourList", widths=None):
     """Refuse r_list >= half the smallest perpendicular width
-    (engine/neighborlist.py:98-132 and :489-572)."""
-    widths, _ = cell_metrics(lattice)
+    (engine/neighborlist.py:98-132 and :489-572); ``widths`` are the
+    lattice's from :func:`cell_widths` when the caller has them."""
+    if widths is None:
+        widths = cell_widths(lattice)
     if r_list >= float(np.min(widths)) / 2.0:
         lengths = np.linalg.norm(np.asarray(lattice, float), axis=1)
         raise ValueError(
@@ -47,10 +55,11 @@ def check_min_image(lattice, r_list, caller="NeighbourList"):
             f"lengths [{lengths[0]:.4f}, {lengths[1]:.4f}, {lengths[2]:.4f}] A.")
 
 
-def cell_grid(lattice, r_list):
+def cell_grid(lattice, r_list, widths=None):
     """Sub-cell counts nc_i = max(1, floor(d_i / r_list))
     (engine/neighborlist.py:976-978) and the stencil width per axis."""
-    widths, _ = cell_metrics(lattice)
+    if widths is None:
+        widths = cell_widths(lattice)
     nc = np.maximum(1, np.floor(widths / r_list).astype(int))
     w = np.where(nc == 1, 1, np.where(nc == 2, 2, 3))
     return nc, w
@@ -124,7 +133,7 @@ class Batch:
         self.offsets = off
         self.lattices = np.stack(lats)
         for lat in lats:
-            cell_metrics(lat)
+            cell_widths(lat)
         self.volumes = np.abs(np.linalg.det(self.lattices))
         invs = np.linalg.inv(self.lattices)
         cells = np.concatenate([self.lattices.reshape(-1, 9), invs.reshape(-1, 9)], axis=1)
@@ -222,7 +231,7 @@ class Batch:
         lat = np.asarray(lattice, np.float64).reshape(3, 3)
         if np.array_equal(lat, self.lattices[s]):
             return
-        cell_metrics(lat)
+        cell_widths(lat)
         self.lattices[s] = lat
         self.volumes[s] = abs(np.linalg.det(lat))
         row = np.concatenate([lat.reshape(9), np.linalg.inv(lat).reshape(9)])
@@ -251,7 +260,7 @@ def replicate_thin(lattice, positions, type_ids, r_list):
     forces of the first N atoms and the stress are unchanged (exact periodic
     physics)."""
     lat = np.asarray(lattice, float)
-    widths, _ = cell_metrics(lat)
+    widths = cell_widths(lat)
     reps = np.ones(3, int)
     for k in range(3):
         while widths[k] * reps[k] / 2.0 <= r_list:
@@ -266,5 +275,5 @@ def replicate_thin(lattice, positions, type_ids, r_list):
     return lat * reps[:, None], big, types, reps
 
 
-__all__ = ["Batch", "cell_metrics", "check_min_image", "cell_grid", "species_ids",
+__all__ = ["Batch", "cell_metrics", "cell_widths", "check_min_image", "cell_grid", "species_ids",
            "replicate_thin", "default_device"]

@@ -107,7 +107,11 @@ size_t mbf_nl_rebuild_workspace_bytes(int n_atoms, int n_cells_total, int max_ro
  * after the count, stores the need in *n_slots (host) and returns
  * MBF_ERR_CAPACITY; call again with a larger nbr/rev.  *n_slots and
  * *max_row are host outputs.  Synchronises `stream` once (to read the
- * count). */
+ * count).  Workspace beyond mbf_nl_workspace_bytes serves as staging rows
+ * (stride = the extra bytes / (4 n_atoms), at most 1024): when no row is
+ * longer than that stride the search runs once, as in
+ * mbf_nl_rebuild_async; size it with mbf_nl_rebuild_workspace_bytes and
+ * a row bound estimate.  The list is the same either way. */
 int mbf_nl_build(const mbf_system *sys, const int *grids, int n_cells_total,
                  double r_list, void *workspace, size_t workspace_bytes,
                  int *row_off, int *nbr, int *rev, int *upper, long long nbr_capacity,

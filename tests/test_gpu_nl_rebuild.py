@@ -3,7 +3,8 @@ the C ABI: with the staged workspace (one search: rows kept at the row
 bound's stride, then sorted into the CSR) and with the plain one (count,
 then fill) it gives exactly the general build's rows, reverse slots and
 upper offsets; a row bound below the longest row is reported, with every
-row left empty."""
+row left empty.  The general build (mbf_nl_build) gives one list with
+and without staging rows, whatever their stride."""
 import numpy as np
 import pytest
 import torch
@@ -26,7 +27,9 @@ def _cases():
     l2, p2 = strained(l2, p2, 0.03, 23)
     l3, p3, _ = cubic(DIAMOND, 5.431, 3, ["Si"] * 8, rattle=0.1, seed=24)
     many = ([l2, l3], [p2, p3], 6.1)
-    return {"si512": one, "batch_fcc_si": many}
+    l4, p4, _ = cubic(FCC, 3.58, 8, ["Cu"] * 4, rattle=0.08, seed=25)
+    long_rows = ([l4], [p4], 9.0)   # ~266 entries a row: the shared-memory sort
+    return {"si512": one, "batch_fcc_si": many, "fcc_long_rows": long_rows}
 
 
 def _rebuild(batch, ref, limit, staged):
@@ -53,7 +56,7 @@ def _rebuild(batch, ref, limit, staged):
     return row_off.cpu().numpy(), upper.cpu().numpy(), nbr.cpu().numpy(), rev.cpu().numpy(), int(status.item())
 
 
-@pytest.mark.parametrize("case", ["si512", "batch_fcc_si"])
+@pytest.mark.parametrize("case", ["si512", "batch_fcc_si", "fcc_long_rows"])
 @pytest.mark.parametrize("staged", [True, False])
 def test_rebuild_equals_general_build(cuda_device, case, staged):
     lats, poss, r_list = _cases()[case]
@@ -81,3 +84,48 @@ def test_row_bound_too_small_is_reported(cuda_device, staged):
     row_off, upper, _, _, status = _rebuild(batch, ref, ref.max_row - 2, staged)
     assert status & STATUS_ROW_TOO_LONG
     assert not row_off.any() and not upper.any()
+
+
+def _build(batch, r_list, grids_t, n_cells, ws_bytes, cap):
+    L = _lib.lib()
+    dev = batch.device
+    N = batch.n_atoms
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    row_off = torch.full((N + 1,), -7, dtype=torch.int32, device=dev)
+    upper = torch.full((N,), -7, dtype=torch.int32, device=dev)
+    nbr = torch.full((cap,), -7, dtype=torch.int32, device=dev)
+    rev = torch.full((cap,), -7, dtype=torch.int32, device=dev)
+    n_slots, max_row = _lib._ll(0), _lib._i(0)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    _lib.check(L.mbf_nl_build(batch.mbf_system(), _lib.ptr(grids_t), n_cells, r_list, _lib.ptr(ws), ws_bytes,
+                              _lib.ptr(row_off), _lib.ptr(nbr), _lib.ptr(rev), _lib.ptr(upper), cap, n_slots,
+                              max_row, st), "mbf_nl_build")
+    torch.cuda.synchronize(dev)
+    ns = int(n_slots.value)
+    return (row_off.cpu().numpy(), upper.cpu().numpy(), nbr[:ns].cpu().numpy(), rev[:ns].cpu().numpy(),
+            int(max_row.value))
+
+
+@pytest.mark.parametrize("case", ["si512", "batch_fcc_si", "fcc_long_rows"])
+def test_build_staging_widths_agree(cuda_device, case):
+    """mbf_nl_build with no staging rows (count, then fill), with a stride
+    below the longest row (the staged search falls back to the fill) and
+    with one above it (a single search) gives one list."""
+    lats, poss, r_list = _cases()[case]
+    batch = ak.Batch(lats, poss, [np.zeros(len(p), np.int32) for p in poss], device=cuda_device)
+    ref = DeviceNeighbourList(r_list).build(batch)
+    grids, n_cells = ref._grid_table(batch)
+    grids_t = torch.as_tensor(grids, device=cuda_device)
+    L = _lib.lib()
+    N = batch.n_atoms
+    plain = int(L.mbf_nl_workspace_bytes(N, n_cells))
+    cap = ref.n_slots + 64
+    outs = [_build(batch, r_list, grids_t, n_cells, plain, cap)]
+    for stride in (ref.max_row - 5, ref.max_row, ref.max_row + 40):
+        outs.append(_build(batch, r_list, grids_t, n_cells,
+                           int(L.mbf_nl_rebuild_workspace_bytes(N, n_cells, stride)), cap))
+    for o in outs:
+        assert o[4] == ref.max_row
+        for k in range(4):
+            np.testing.assert_array_equal(o[k], outs[0][k])
+    np.testing.assert_array_equal(outs[0][2], ref.nbr[:ref.n_slots].cpu().numpy())

@@ -68,6 +68,35 @@ def test_nl_large_matches_oracle():
     np.testing.assert_array_equal(j, oj)
 
 
+@pytest.mark.parametrize("rc", [6.75, 8.7])
+def test_nl_long_rows_match_oracle(rc):
+    """Rows near and above 128 entries, where the register sort gives way
+    to the shared-memory one (fcc Cu, r_list 7.05 A: a mean row of 128;
+    9.0 A: ~266): the oracle's pairs, rows ascending, the upper offsets,
+    rev an involution onto the row owners."""
+    lat, pos, _ = cubic(FCC, 3.58, 8, ["Cu"] * 4, rattle=0.08, seed=6)
+    nl = ak.NeighbourList(rc, skin_width=0.3)
+    nl.build(lat, pos)
+    i, j = nl.get_candidate_pairs()
+    oi, oj, _, _ = oracle.nl_build(lat, pos, rc, 0.3)
+    np.testing.assert_array_equal(i, oi)
+    np.testing.assert_array_equal(j, oj)
+    d = nl.device_list
+    ro = d.row_off.cpu().numpy()
+    nbr = d.nbr[:d.n_slots].cpu().numpy()
+    rev = d.rev[:d.n_slots].cpu().numpy()
+    up = d.upper[:len(ro) - 1].cpu().numpy()
+    lens = np.diff(ro)
+    assert lens.max() > 128
+    for a in range(len(ro) - 1):
+        row = nbr[ro[a]:ro[a + 1]]
+        assert np.all(np.diff(row) > 0)
+        assert up[a] - ro[a] == np.count_nonzero(row < a)
+    src = np.repeat(np.arange(len(ro) - 1), lens)
+    np.testing.assert_array_equal(nbr[rev], src)
+    np.testing.assert_array_equal(rev[rev], np.arange(d.n_slots))
+
+
 def test_nl_refuses_thin_cell():
     lat, pos, _ = cubic(DIAMOND, 5.431, 1, ["Si"] * 8)
     with pytest.raises(ValueError):
