@@ -275,10 +275,11 @@ __global__ void nl_cells(SysView S, const int *__restrict__ grids, const int *__
 
 // ---- row sorts -----------------------------------------------------------------
 // Rows come out of the search in traversal order; the CSR keeps them
-// ascending.  A row of at most 128 entries is sorted in registers by a
-// bitonic network over four entries per lane (entry e = 4 lane + j, padded
-// with INT_MAX, which sorts last since atom indices are smaller); a longer
-// one by rank in shared memory.  Entries of a row are distinct.
+// ascending.  By length n: up to 32 entries one per lane, ranked by
+// shuffles; up to 64 or 128 a bitonic network in registers over J = 2 or 4
+// entries a lane (entry e = J lane + j, padded with INT_MAX, which sorts
+// last since atom indices are smaller); longer rows by rank in shared
+// memory.  Entries of a row are distinct.
 constexpr int NL_PAD = 0x7fffffff;
 
 __device__ __forceinline__ void cmp_swap(int &lo, int &hi, bool asc) {
@@ -287,27 +288,48 @@ __device__ __forceinline__ void cmp_swap(int &lo, int &hi, bool asc) {
     hi = asc ? mx : mn;
 }
 
-__device__ __forceinline__ void bitonic128(int (&v)[4]) {
+template <int J>
+__device__ __forceinline__ void bitonic_sort(int (&v)[J]) {
     int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int k = 2; k <= 128; k <<= 1) {
+    for (int k = 2; k <= 32 * J; k <<= 1) {
 #pragma unroll
         for (int d = k >> 1; d > 0; d >>= 1) {
-            if (d >= 4) {  // partner in lane ^ (d / 4), same register
-                bool low = (lane & (d >> 2)) == 0;
+            if (d >= J) {  // partner in lane ^ (d / J), same register
+                bool low = (lane & (d / J)) == 0;
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    int o = __shfl_xor_sync(MBF_FULL, v[j], d >> 2);
-                    bool asc = ((4 * lane + j) & k) == 0;
+                for (int j = 0; j < J; ++j) {
+                    int o = __shfl_xor_sync(MBF_FULL, v[j], d / J);
+                    bool asc = ((J * lane + j) & k) == 0;
                     v[j] = (low == asc) ? min(v[j], o) : max(v[j], o);
                 }
             } else {  // partner in register j ^ d of this lane
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if ((j & d) == 0) cmp_swap(v[j], v[j ^ d], ((4 * lane + j) & k) == 0);
+                for (int j = 0; j < J; ++j)
+                    if ((j & d) == 0) cmp_swap(v[j], v[j ^ d], ((J * lane + j) & k) == 0);
             }
         }
     }
+}
+
+// Sorts n <= 32 J entries src[0..n) into out[0..n); returns this lane's
+// count of entries below `a`.
+template <int J>
+__device__ __forceinline__ int sort_row_bitonic(const int *src, int n, int *out, int a) {
+    int lane = threadIdx.x & 31;
+    int v[J];
+#pragma unroll
+    for (int j = 0; j < J; ++j) v[j] = J * lane + j < n ? src[J * lane + j] : NL_PAD;
+    __syncwarp();
+    bitonic_sort<J>(v);
+    int lower = 0;
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+        if (J * lane + j < n) {
+            out[J * lane + j] = v[j];
+            lower += v[j] < a ? 1 : 0;
+        }
+    return lower;
 }
 
 // Sorts the n entries src[0..n) (n <= NL_MAXROW) ascending into out[0..n)
@@ -317,18 +339,17 @@ __device__ __forceinline__ void bitonic128(int (&v)[4]) {
 __device__ __forceinline__ int sort_row(const int *src, int n, int *out, int a, int *row) {
     int lane = threadIdx.x & 31;
     int lower = 0;
-    if (n <= 128) {
-        int v[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) v[j] = 4 * lane + j < n ? src[4 * lane + j] : NL_PAD;
-        __syncwarp();
-        bitonic128(v);
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (4 * lane + j < n) {
-                out[4 * lane + j] = v[j];
-                lower += v[j] < a ? 1 : 0;
-            }
+    if (n <= 32) {
+        int v = lane < n ? src[lane] : NL_PAD, rank = 0;
+        for (int q = 0; q < n; ++q) rank += __shfl_sync(MBF_FULL, v, q) < v ? 1 : 0;
+        if (lane < n) {
+            out[rank] = v;
+            lower = v < a ? 1 : 0;
+        }
+    } else if (n <= 64) {
+        lower = sort_row_bitonic<2>(src, n, out, a);
+    } else if (n <= 128) {
+        lower = sort_row_bitonic<4>(src, n, out, a);
     } else {
         for (int k = lane; k < n; k += 32) row[k] = src[k];
         __syncwarp();
@@ -390,12 +411,16 @@ __global__ void nl_unstage_rows(int n_atoms, const int *__restrict__ row_off, co
 // Reverse slot of every slot.  rev is an involution, so only the upper
 // slots (a -> b, b > a) search: a lies in the lower part of b's sorted row,
 // [row_off[b], upper[b]); the slot t found there gets rev[t] = s, so every
-// slot is written once.
+// slot is written once.  Eight lanes per row: an upper part holds about
+// half a row, so short rows keep the lanes busy.
+constexpr int NL_REV_LANES = 8;
+
 __global__ void nl_reverse(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ upper,
                            const int *__restrict__ nbr, int *__restrict__ rev, int *__restrict__ err) {
-    int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int a = blockIdx.x * NL_WARPS + wid; a < n_atoms; a += gridDim.x * NL_WARPS) {
-        for (int s = upper[a] + lane; s < row_off[a + 1]; s += 32) {
+    const int grp = threadIdx.x / NL_REV_LANES, sub = threadIdx.x % NL_REV_LANES;
+    const int per_block = 32 * NL_WARPS / NL_REV_LANES;
+    for (int a = blockIdx.x * per_block + grp; a < n_atoms; a += gridDim.x * per_block) {
+        for (int s = upper[a] + sub; s < row_off[a + 1]; s += NL_REV_LANES) {
             int b = nbr[s];
             int lo = row_off[b], hi = upper[b] - 1, found = -1;
             while (lo <= hi) {
@@ -597,7 +622,8 @@ static int nl_finish(const SysView &S, const int *grids, int n_cells_total, doub
     }
     PROF_END("nl_fill", st);
     MBF_CHECK_LAUNCH();
-    g = persistent_grid(blocks, 32 * NL_WARPS, (const void *)nl_reverse);
+    g = persistent_grid((N + 32 * NL_WARPS / NL_REV_LANES - 1) / (32 * NL_WARPS / NL_REV_LANES), 32 * NL_WARPS,
+                        (const void *)nl_reverse);
     PROF_BEGIN("nl_reverse", st);
     nl_reverse<<<g, 32 * NL_WARPS, 0, st>>>(N, row_off, upper, nbr, rev, err);
     PROF_END("nl_reverse", st);
