@@ -41,15 +41,19 @@ struct EamDev {
 // compiled in: the float64 build of these kernels without them raised an
 // illegal-address fault on B200 whose cause was not found, while the checked
 // build, with the same indices, runs clean.
+// Every index and bound is an int (the entries refuse lists of more than
+// 0x7fffff00 slots, so a slot index plus its prefetch distance cannot
+// overflow), so lo <= idx < hi is one unsigned comparison: idx - lo taken
+// modulo 2^32 is below hi - lo exactly when idx is in range.
 struct Chk {
     int *err;
     int n_atoms;
-    long long n_slots;
+    int n_slots;
     int ns;
 };
-#define MBF_OK_IDX(ck, site, idx, lo, hi)                                          \
-    (((long long)(idx) >= (long long)(lo) && (long long)(idx) < (long long)(hi))    \
-         ? true                                                                    \
+#define MBF_OK_IDX(ck, site, idx, lo, hi)                                                          \
+    (((unsigned)(int)(idx) - (unsigned)(int)(lo) < (unsigned)max((int)(hi) - (int)(lo), 0))       \
+         ? true                                                                                    \
          : (atomicCAS((ck).err + 1, 0, (site)) == 0 ? ((ck).err[2] = (int)(idx), false) : false))
 
 // ---- generic function evaluation (engine/_eam_kernels.py:129-228) -------
@@ -762,7 +766,8 @@ static int eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
     Chk ck;
     ck.err = ws_at<int>(workspace, L.err);
     ck.n_atoms = sys->n_atoms;
-    ck.n_slots = nl->n_slots;
+    if (nl->n_slots < 0 || nl->n_slots > 0x7fffff00LL) return MBF_ERR_ARGUMENT;
+    ck.n_slots = (int)nl->n_slots;
     ck.ns = tab->ns;
     if (cudaMemsetAsync(ck.err, 0, ERR_CLEAR_BYTES, st) != cudaSuccess) return MBF_ERR_CUDA;
     double *f_local = ws_at<double>(workspace, L.f_local);
@@ -866,7 +871,8 @@ extern "C" int mbf_eam_eval_static(const mbf_system *sys, const mbf_nlist *nl, c
     Chk ck;
     ck.err = ws_at<int>(workspace, L.err);
     ck.n_atoms = sys->n_atoms;
-    ck.n_slots = nl->n_slots;
+    if (nl->n_slots < 0 || nl->n_slots > 0x7fffff00LL) return MBF_ERR_ARGUMENT;
+    ck.n_slots = (int)nl->n_slots;
     ck.ns = tab->ns;
     // the scratch keeps the previous call's contents: the error words must
     // start at zero (the reduction clears its own counters); every other
