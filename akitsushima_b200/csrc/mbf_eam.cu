@@ -575,34 +575,65 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1) 
 }
 
 // F_a = (pairs above a) + the forces its lower neighbours left in a's own
-// lower slots; lane group per atom, contiguous reads.
-template <typename V3, int LPA>
-__global__ void eam_gather(int n_atoms, const int *__restrict__ row_off, const int *__restrict__ upper,
-                           const V3 *__restrict__ slot_f, const double *__restrict__ f_local,
-                           double *__restrict__ forces, Chk ck) {
-    const int sub = threadIdx.x & (LPA - 1);
-    const int gpb = blockDim.x / LPA;
-    int a = blockIdx.x * gpb + threadIdx.x / LPA;
-    double fx = 0, fy = 0, fz = 0;
-    if (a < n_atoms) {
-        int up = upper[a];
-        if (!MBF_OK_IDX(ck, 31, up, row_off[a], row_off[a + 1] + 1)) up = row_off[a];
-        for (int s = row_off[a] + sub; s < up; s += LPA) {
-            if (!MBF_OK_IDX(ck, 32, s, 0, ck.n_slots)) break;
-            V3 w = slot_f[s];
-            fx += (double)w.x;
-            fy += (double)w.y;
-            fz += (double)w.z;
+// lower slots (contiguous reads), fused with the per-structure sums
+// (ChunkSums): a block per chunk of the reduction plan, 8 lanes per atom;
+// besides its atom's force each group adds the atom's record (entries sub
+// and sub + 8 of its 8 lanes), and the block finishes the chunk's and, if
+// last, the structure's sums.
+constexpr int GR_BLOCK = 512;
+
+template <typename V3>
+__global__ void __launch_bounds__(GR_BLOCK) eam_gather_reduce(const int *__restrict__ row_off,
+                                                              const int *__restrict__ upper,
+                                                              const V3 *__restrict__ slot_f,
+                                                              const double *__restrict__ f_local,
+                                                              double *__restrict__ forces, ChunkSums cs, Chk ck) {
+    constexpr int LPA = 8, G = GR_BLOCK / LPA;
+    const int c = blockIdx.x;
+    const int s = cs.chunk[3 * c], a0 = cs.chunk[3 * c + 1], a1 = cs.chunk[3 * c + 2];
+    const int sub = threadIdx.x & (LPA - 1), grp = threadIdx.x / LPA;
+    double r0 = 0.0, r1 = 0.0;
+    // the next atom's row bounds are loaded one iteration ahead
+    int nb = 0, nu = 0, ne = 0;
+    if (a0 + grp < a1) {
+        nb = row_off[a0 + grp];
+        ne = row_off[a0 + grp + 1];
+        nu = upper[a0 + grp];
+    }
+    for (int base = a0; base < a1; base += G) {  // uniform over the block
+        int a = base + grp;
+        const int beg = nb, rend = ne;
+        int up = nu;
+        if (a + G < a1) {
+            nb = row_off[a + G];
+            ne = row_off[a + G + 1];
+            nu = upper[a + G];
+        }
+        double fx = 0, fy = 0, fz = 0;
+        if (a < a1) {
+            if (!MBF_OK_IDX(ck, 31, up, beg, rend + 1)) up = beg;
+#pragma unroll 4
+            for (int q = beg + sub; q < up; q += LPA) {
+                if (!MBF_OK_IDX(ck, 32, q, 0, ck.n_slots)) break;
+                V3 w = slot_f[q];
+                fx += (double)w.x;
+                fy += (double)w.y;
+                fz += (double)w.z;
+            }
+            const double *pa = cs.per_atom + (size_t)a * ATOM_ACC;
+            r0 += pa[sub];
+            if (sub < ATOM_ACC - LPA) r1 += pa[LPA + sub];
+        }
+        fx = group_sum<LPA>(fx);
+        fy = group_sum<LPA>(fy);
+        fz = group_sum<LPA>(fz);
+        if (sub == 0 && a < a1) {
+            forces[3 * (size_t)a] = f_local[3 * (size_t)a] + fx;
+            forces[3 * (size_t)a + 1] = f_local[3 * (size_t)a + 1] + fy;
+            forces[3 * (size_t)a + 2] = f_local[3 * (size_t)a + 2] + fz;
         }
     }
-    fx = group_sum<LPA>(fx);
-    fy = group_sum<LPA>(fy);
-    fz = group_sum<LPA>(fz);
-    if (sub == 0 && a < n_atoms) {
-        forces[3 * (size_t)a] = f_local[3 * (size_t)a] + fx;
-        forces[3 * (size_t)a + 1] = f_local[3 * (size_t)a + 1] + fy;
-        forces[3 * (size_t)a + 2] = f_local[3 * (size_t)a + 2] + fz;
-    }
+    chunk_sums_finish<GR_BLOCK>(cs, c, s, r0, r1);
 }
 
 // Site terms (engine/site_terms.py:440-479): U_i = F_i(rho-bar_i) + 1/2
@@ -671,7 +702,7 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_site(SysView S, const int *__re
 template <typename T, int LPA, bool ZHOU, bool ORTHO>
 static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, double4 *pk, double *aux,
                       void *slot, double *f_local, double *forces, double *per_atom, Chk ck, const SiteOut &so,
-                      cudaStream_t st) {
+                      const ChunkSums &cs, int n_chunks, cudaStream_t st) {
     typedef typename SlotVec<T>::type V3;
     int gpb = EAM_BLOCK / LPA;
     int blocks = (S.n_atoms + gpb - 1) / gpb;
@@ -693,10 +724,10 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, do
                                                      aux, (V3 *)slot, f_local, per_atom, ck);
     PROF_END("eam_force", st);
     MBF_CHECK_LAUNCH();
-    PROF_BEGIN("eam_gather", st);
-    eam_gather<V3, 8><<<(S.n_atoms + 15) / 16, 128, 0, st>>>(S.n_atoms, nl->row_off, nl->upper,
-                                                             (const V3 *)slot, f_local, forces, ck);
-    PROF_END("eam_gather", st);
+    PROF_BEGIN("eam_gather_reduce", st);
+    eam_gather_reduce<V3><<<n_chunks, GR_BLOCK, 0, st>>>(nl->row_off, nl->upper, (const V3 *)slot, f_local,
+                                                          forces, cs, ck);
+    PROF_END("eam_gather_reduce", st);
     MBF_CHECK_LAUNCH();
     if (so.e) {
         g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_site<T, LPA, ZHOU, ORTHO>);
@@ -709,27 +740,31 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, do
 template <typename T, bool ZHOU, bool ORTHO>
 static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E, double4 *pk,
                             double *aux, void *slot, double *f_local, double *forces, double *per_atom,
-                            Chk ck, const SiteOut &so, cudaStream_t st) {
+                            Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks, cudaStream_t st) {
+#define MBF_EAM_LAUNCH(L) \
+    eam_launch<T, L, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, cs, n_chunks, st)
     switch (lpa) {
-        case 1: return eam_launch<T, 1, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
-        case 2: return eam_launch<T, 2, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
-        case 4: return eam_launch<T, 4, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
-        case 8: return eam_launch<T, 8, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
-        case 16: return eam_launch<T, 16, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
-        case 32: return eam_launch<T, 32, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
+        case 1: return MBF_EAM_LAUNCH(1);
+        case 2: return MBF_EAM_LAUNCH(2);
+        case 4: return MBF_EAM_LAUNCH(4);
+        case 8: return MBF_EAM_LAUNCH(8);
+        case 16: return MBF_EAM_LAUNCH(16);
+        case 32: return MBF_EAM_LAUNCH(32);
         default: return MBF_ERR_ARGUMENT;
     }
+#undef MBF_EAM_LAUNCH
 }
 
 template <typename T>
 static int eam_dispatch(bool zhou, int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E,
                         double4 *pk, double *aux, void *slot, double *f_local, double *forces,
-                        double *per_atom, Chk ck, const SiteOut &so, cudaStream_t st) {
+                        double *per_atom, Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks,
+                        cudaStream_t st) {
+#define MBF_EAM_ARGS lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, cs, n_chunks, st
     if (zhou)
-        return S.ortho ? eam_dispatch_lpa<T, true, true>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st)
-                       : eam_dispatch_lpa<T, true, false>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
-    return S.ortho ? eam_dispatch_lpa<T, false, true>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st)
-                   : eam_dispatch_lpa<T, false, false>(lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, st);
+        return S.ortho ? eam_dispatch_lpa<T, true, true>(MBF_EAM_ARGS) : eam_dispatch_lpa<T, true, false>(MBF_EAM_ARGS);
+    return S.ortho ? eam_dispatch_lpa<T, false, true>(MBF_EAM_ARGS) : eam_dispatch_lpa<T, false, false>(MBF_EAM_ARGS);
+#undef MBF_EAM_ARGS
 }
 
 }  // namespace mbf
@@ -774,14 +809,16 @@ static int eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
     double4 *pk = ws_at<double4>(workspace, L.pack);
     int lpa = lanes_per_atom > 0 ? lanes_per_atom : 8;
     bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
-    int rc;
+    ChunkSums cs = {plan->chunk, plan->chunk_first, per_atom, partial, energy, virial,
+                    ws_at<unsigned>(workspace, L.sdone)};
+    if (plan->n_chunks <= 0) return MBF_ERR_ARGUMENT;
+    if (cudaMemsetAsync(cs.sdone, 0, sizeof(unsigned) * (size_t)sys->n_struct, st) != cudaSuccess)
+        return MBF_ERR_CUDA;
     if (precision == MBF_FP64)
-        rc = eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, so, st);
-    else
-        rc = eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, so, st);
-    if (rc != MBF_OK) return rc;
-    return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial,
-                                ws_at<unsigned>(workspace, L.sdone), st);
+        return eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, so, cs,
+                                    plan->n_chunks, st);
+    return eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, so, cs,
+                               plan->n_chunks, st);
 }
 
 extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
@@ -882,11 +919,14 @@ extern "C" int mbf_eam_eval_static(const mbf_system *sys, const mbf_nlist *nl, c
     double4 *pk = ws_at<double4>(workspace, L.pack);
     int lpa = lanes_per_atom > 0 ? lanes_per_atom : 8;
     bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
+    ChunkSums cs = {plan->chunk, plan->chunk_first, per_atom, partial, energy, virial,
+                    ws_at<unsigned>(workspace, L.sdone)};
+    if (plan->n_chunks <= 0) return MBF_ERR_ARGUMENT;
+    if (cudaMemsetAsync(cs.sdone, 0, sizeof(unsigned) * (size_t)sys->n_struct, st) != cudaSuccess)
+        return MBF_ERR_CUDA;
     if (precision == MBF_FP64)
-        rc = eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, SiteOut{}, st);
-    else
-        rc = eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, SiteOut{}, st);
-    if (rc != MBF_OK) return rc;
-    return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial,
-                                ws_at<unsigned>(workspace, L.sdone), st);
+        return eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, SiteOut{},
+                                    cs, plan->n_chunks, st);
+    return eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, SiteOut{}, cs,
+                               plan->n_chunks, st);
 }

@@ -24,6 +24,71 @@ int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, in
 int gather_forces(int n_atoms, const int *row_off, const double *G, const double *f_local, double *forces,
                   cudaStream_t st);
 
+// The per-structure sums of reduce_per_structure done by the last kernel of
+// an evaluation instead: one block per chunk of the plan (a run of at most
+// REDUCE_CHUNK atoms of one structure) adds its atoms' records, writes the
+// chunk total to partial[c], and the block that completes a structure adds
+// that structure's chunk totals, each sum in a fixed order.
+struct ChunkSums {
+    const int *chunk;        // (n_chunks, 3): structure, first atom, end atom
+    const int *chunk_first;  // (n_struct + 1,): first chunk of each structure
+    const double *per_atom;  // (n_atoms, ATOM_ACC)
+    double *partial;         // (n_chunks, ATOM_ACC)
+    double *energy;          // (n_struct,)
+    double *virial;          // (n_struct, 9)
+    unsigned *sdone;         // (n_struct,) completion counters, zero at launch
+};
+
+// Block-wide end of a chunk's sums, called by every thread of an NT-thread
+// block.  r0 / r1: the thread's running sums of record entries q = t % 8 and
+// q = 8 + t % 8 (q < ATOM_ACC) over the atoms its 8-lane group visited.
+template <int NT>
+__device__ __forceinline__ void chunk_sums_finish(const ChunkSums &cs, int c, int s, double r0, double r1) {
+    static_assert(NT % 32 == 0 && NT >= 32 * 8, "chunk_sums_finish: 8 warps or more");
+    constexpr int NW = NT / 32;
+    constexpr int PER = NT / ATOM_ACC;   // chunk totals summed per value in the tail
+    __shared__ double sh[NW][16];
+    __shared__ double tail[PER * ATOM_ACC];
+    __shared__ bool last;
+    const int t = threadIdx.x, w = t >> 5, l = t & 31;
+    r0 += __shfl_xor_sync(MBF_FULL, r0, 8);
+    r1 += __shfl_xor_sync(MBF_FULL, r1, 8);
+    r0 += __shfl_xor_sync(MBF_FULL, r0, 16);
+    r1 += __shfl_xor_sync(MBF_FULL, r1, 16);
+    if (l < 8) {
+        sh[w][l] = r0;
+        sh[w][8 + l] = r1;
+    }
+    __syncthreads();
+    if (t < ATOM_ACC) {
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) v += sh[k][t];
+        cs.partial[(size_t)c * ATOM_ACC + t] = v;
+        __threadfence();
+    }
+    __syncthreads();
+    const int c0 = cs.chunk_first[s], c1 = cs.chunk_first[s + 1];
+    if (t == 0) last = atomicAdd(cs.sdone + s, 1u) == (unsigned)(c1 - c0 - 1);
+    __syncthreads();
+    if (!last) return;
+    const int q = t % ATOM_ACC, k0 = t / ATOM_ACC;
+    if (k0 < PER) {
+        double v = 0.0;
+        for (int k = c0 + k0; k < c1; k += PER) v += __ldcg(cs.partial + (size_t)k * ATOM_ACC + q);
+        tail[k0 * ATOM_ACC + q] = v;
+    }
+    __syncthreads();
+    if (t < ATOM_ACC) {
+        double v = 0.0;
+        for (int k = 0; k < PER; ++k) v += tail[k * ATOM_ACC + t];
+        sh[0][t] = v;
+    }
+    __syncthreads();
+    if (t == 0) cs.energy[s] = sh[0][10] > 0.0 ? sh[0][0] : 0.0;
+    if (t < 9) cs.virial[9 * (size_t)s + t] = sh[0][1 + t];
+}
+
 // Optional site-term outputs of an evaluation (all null: none): the site
 // energy U_i per atom and, per list slot, dU_centre/dv and v (the
 // minimum-image vector centre -> neighbour); slots outside the cutoff get
