@@ -580,15 +580,13 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1) 
 // besides its atom's force each group adds the atom's record (entries sub
 // and sub + 8 of its 8 lanes), and the block finishes the chunk's and, if
 // last, the structure's sums.
-constexpr int GR_BLOCK = 512;
-
-template <typename V3>
-__global__ void __launch_bounds__(GR_BLOCK) eam_gather_reduce(const int *__restrict__ row_off,
+template <typename V3, int NT>
+__global__ void __launch_bounds__(NT) eam_gather_reduce(const int *__restrict__ row_off,
                                                               const int *__restrict__ upper,
                                                               const V3 *__restrict__ slot_f,
                                                               const double *__restrict__ f_local,
                                                               double *__restrict__ forces, ChunkSums cs, Chk ck) {
-    constexpr int LPA = 8, G = GR_BLOCK / LPA;
+    constexpr int LPA = 8, G = NT / LPA;
     const int c = blockIdx.x;
     const int s = cs.chunk[3 * c], a0 = cs.chunk[3 * c + 1], a1 = cs.chunk[3 * c + 2];
     const int sub = threadIdx.x & (LPA - 1), grp = threadIdx.x / LPA;
@@ -633,7 +631,7 @@ __global__ void __launch_bounds__(GR_BLOCK) eam_gather_reduce(const int *__restr
             forces[3 * (size_t)a + 2] = f_local[3 * (size_t)a + 2] + fz;
         }
     }
-    chunk_sums_finish<GR_BLOCK>(cs, c, s, r0, r1);
+    chunk_sums_finish<NT>(cs, c, s, r0, r1);
 }
 
 // Site terms (engine/site_terms.py:440-479): U_i = F_i(rho-bar_i) + 1/2
@@ -725,8 +723,16 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, do
     PROF_END("eam_force", st);
     MBF_CHECK_LAUNCH();
     PROF_BEGIN("eam_gather_reduce", st);
-    eam_gather_reduce<V3><<<n_chunks, GR_BLOCK, 0, st>>>(nl->row_off, nl->upper, (const V3 *)slot, f_local,
-                                                          forces, cs, ck);
+    int nt = chunk_block(S.n_atoms, n_chunks);
+    if (nt == 128)
+        eam_gather_reduce<V3, 128><<<n_chunks, 128, 0, st>>>(nl->row_off, nl->upper, (const V3 *)slot, f_local,
+                                                              forces, cs, ck);
+    else if (nt == 256)
+        eam_gather_reduce<V3, 256><<<n_chunks, 256, 0, st>>>(nl->row_off, nl->upper, (const V3 *)slot, f_local,
+                                                              forces, cs, ck);
+    else
+        eam_gather_reduce<V3, 512><<<n_chunks, 512, 0, st>>>(nl->row_off, nl->upper, (const V3 *)slot, f_local,
+                                                              forces, cs, ck);
     PROF_END("eam_gather_reduce", st);
     MBF_CHECK_LAUNCH();
     if (so.e) {

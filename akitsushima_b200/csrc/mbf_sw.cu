@@ -272,7 +272,7 @@ static int sw_launch(const SysView &S, const mbf_nlist *nl, const SwDev &P, doub
                                                      so);
     PROF_END("sw_force", st);
     MBF_CHECK_LAUNCH();
-    return gather_forces(S.n_atoms, nl->row_off, slot_G, f_local, forces, st);
+    return MBF_OK;   // the eval's gather_reduce adds the slot forces
 }
 
 template <typename T, int MAXN, bool SYM>
@@ -339,8 +339,8 @@ static int sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tabl
         rc = sym ? sw_dispatch<float, true>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, so, st)
                  : sw_dispatch<float, false>(mr, lanes_per_atom, S, nl, P, slot_G, f_local, per_atom, forces, err, so, st);
     if (rc != MBF_OK) return rc;
-    return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial,
-                                ws_at<unsigned>(workspace, L.sdone), st);
+    return gather_reduce(sys->n_struct, sys->n_atoms, nl->row_off, slot_G, f_local, forces, per_atom, plan, partial,
+                         energy, virial, ws_at<unsigned>(workspace, L.sdone), st);
 }
 
 extern "C" int mbf_sw_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_sw_tables *tab,

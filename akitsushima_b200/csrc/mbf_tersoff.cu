@@ -9,7 +9,7 @@
 // Owner computes, no atomics: the lane group of centre i evaluates every
 // zeta-term gradient of its angles, keeps the force on i and writes the force
 // its angles put on neighbour x into x's own slot (x -> i); atom a later sums
-// its own row of slots (gather_forces).
+// its own row of slots (gather_reduce).
 #include "mbf_util.cuh"
 
 namespace mbf {
@@ -388,7 +388,7 @@ static int te_launch(const SysView &S, const mbf_nlist *nl, const TeDev &P, doub
                                          per_atom, err, so);
     PROF_END("te_force", st);
     MBF_CHECK_LAUNCH();
-    return gather_forces(S.n_atoms, nl->row_off, slot_G, f_local, forces, st);
+    return MBF_OK;   // the eval's gather_reduce adds the slot forces
 }
 
 template <typename T, int MAXN>
@@ -457,8 +457,8 @@ static int tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_te
     int rc = te_dispatch(precision, nl->max_row, lanes_per_atom, S, nl, P, slot_b, slot_G, f_local, per_atom,
                          forces, err, so, st);
     if (rc != MBF_OK) return rc;
-    return reduce_per_structure(per_atom, plan, sys->n_struct, partial, energy, virial,
-                                ws_at<unsigned>(workspace, L.sdone), st);
+    return gather_reduce(sys->n_struct, sys->n_atoms, nl->row_off, slot_G, f_local, forces, per_atom, plan, partial,
+                         energy, virial, ws_at<unsigned>(workspace, L.sdone), st);
 }
 
 extern "C" int mbf_tersoff_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_tersoff_tables *tab,

@@ -118,123 +118,74 @@ int exclusive_scan(const int *in, int *out, int n, int *ws, cudaStream_t st) {
     return MBF_OK;
 }
 
-// ---- per-structure reduction of per-atom (energy, virial[9]) -------------
-
-constexpr int RED_BLOCK = 128;
-
-// Per-structure sums of the per-atom accumulators in a fixed order, so every
-// evaluation of the same input gives the same bits.  Stage 1: one block per
-// chunk of atoms (chunks never straddle structures); each thread sums its
-// atoms' ATOM_ACC values in registers, then a shuffle tree per warp and the
-// warps in order.  Stage 2: one warp per structure sums its chunks the same
-// way, in the block that completes the structure.
-template <int NW>
-__device__ __forceinline__ void warp_sum_acc(double (&v)[ATOM_ACC]) {
-#pragma unroll
-    for (int q = 0; q < ATOM_ACC; ++q)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(MBF_FULL, v[q], o);
-}
-
-__global__ void __launch_bounds__(RED_BLOCK) reduce_chunks(const double *__restrict__ per_atom,
-                                                           const int *__restrict__ chunk, int n_chunks,
-                                                           double *__restrict__ partial,
-                                                           const int *__restrict__ chunk_first,
-                                                           double *__restrict__ energy, double *__restrict__ virial,
-                                                           unsigned *__restrict__ sdone) {
-    constexpr int NW = RED_BLOCK / 32;
-    __shared__ double sh[NW][ATOM_ACC];
-    __shared__ bool last;
-    int c = blockIdx.x;
-    int s = chunk[3 * c], a0 = chunk[3 * c + 1], a1 = chunk[3 * c + 2];
-    double v[ATOM_ACC];
-#pragma unroll
-    for (int q = 0; q < ATOM_ACC; ++q) v[q] = 0.0;
-    for (int a = a0 + threadIdx.x; a < a1; a += RED_BLOCK) {
-        const double *p = per_atom + (size_t)a * ATOM_ACC;
-#pragma unroll
-        for (int q = 0; q < ATOM_ACC; ++q) v[q] += p[q];
-    }
-    warp_sum_acc<NW>(v);
-    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) {
-#pragma unroll
-        for (int q = 0; q < ATOM_ACC; ++q) sh[w][q] = v[q];
-    }
-    __syncthreads();
-    if (threadIdx.x < ATOM_ACC) {
-        double t = 0.0;
-#pragma unroll
-        for (int k = 0; k < NW; ++k) t += sh[k][threadIdx.x];
-        partial[(size_t)c * ATOM_ACC + threadIdx.x] = t;
-        __threadfence();
-    }
-    __syncthreads();
-    // Stage 2 in the block that finishes its structure's last chunk (a
-    // completion counter per structure): its first warp sums the
-    // structure's chunks (lane-strided, then the shuffle tree).
-    int c0 = chunk_first[s], c1 = chunk_first[s + 1];
-    if (threadIdx.x == 0) last = atomicAdd(sdone + s, 1u) == (unsigned)(c1 - c0 - 1);
-    __syncthreads();
-    if (!last || w != 0) return;
-#pragma unroll
-    for (int q = 0; q < ATOM_ACC; ++q) v[q] = 0.0;
-    for (int k = c0 + l; k < c1; k += 32) {
-        const double *p = partial + (size_t)k * ATOM_ACC;
-#pragma unroll
-        for (int q = 0; q < ATOM_ACC; ++q) v[q] += __ldcg(p + q);
-    }
-    warp_sum_acc<1>(v);
-    if (l == 0) {
-        energy[s] = v[10] > 0.0 ? v[0] : 0.0;
-#pragma unroll
-        for (int q = 0; q < 9; ++q) virial[9 * s + q] = v[1 + q];
-    }
-}
-
-int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, int n_struct,
-                         double *partial, double *energy, double *virial, unsigned *sdone, cudaStream_t st) {
-    if (plan->n_chunks <= 0 || n_struct <= 0 || !sdone) return MBF_ERR_ARGUMENT;
-    if (cudaMemsetAsync(sdone, 0, sizeof(unsigned) * (size_t)n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
-    PROF_BEGIN("reduce_chunks", st);
-    reduce_chunks<<<plan->n_chunks, RED_BLOCK, 0, st>>>(per_atom, plan->chunk, plan->n_chunks, partial,
-                                                        plan->chunk_first, energy, virial, sdone);
-    PROF_END("reduce_chunks", st);
-    MBF_CHECK_LAUNCH();
-    return MBF_OK;
-}
+// ---- force gather and per-structure sums -----------------------------------
 
 // Gather the three-body forces the centres left on atom a: every centre x
 // wrote the force its angles put on a into a's own slot (a -> x), so the
-// row is read contiguously, lane group per atom.
-__global__ void gather_slot_forces(int n_atoms, const int *__restrict__ row_off, const double *__restrict__ G,
-                                   const double *__restrict__ f_local, double *__restrict__ forces) {
-    constexpr int LPA = 8;
-    const int sub = threadIdx.x & (LPA - 1);
-    int a = blockIdx.x * (blockDim.x / LPA) + threadIdx.x / LPA;
-    double fx = 0, fy = 0, fz = 0;
-    if (a < n_atoms) {
-        for (int s = row_off[a] + sub; s < row_off[a + 1]; s += LPA) {
-            fx += G[3 * (size_t)s];
-            fy += G[3 * (size_t)s + 1];
-            fz += G[3 * (size_t)s + 2];
+// row is read contiguously, 8 lanes per atom; fused with the per-structure
+// sums (ChunkSums): a block per chunk of the reduction plan, each group also
+// adding its atom's record (entries sub and sub + 8), the next atom's row
+// bounds loaded one iteration ahead.
+template <int NT>
+__global__ void __launch_bounds__(NT) gather_reduce_rows(const int *__restrict__ row_off,
+                                                         const double *__restrict__ G,
+                                                         const double *__restrict__ f_local,
+                                                         double *__restrict__ forces, ChunkSums cs) {
+    constexpr int LPA = 8, NG = NT / LPA;
+    const int c = blockIdx.x;
+    const int s = cs.chunk[3 * c], a0 = cs.chunk[3 * c + 1], a1 = cs.chunk[3 * c + 2];
+    const int sub = threadIdx.x & (LPA - 1), grp = threadIdx.x / LPA;
+    double r0 = 0.0, r1 = 0.0;
+    int nb = 0, ne = 0;
+    if (a0 + grp < a1) {
+        nb = row_off[a0 + grp];
+        ne = row_off[a0 + grp + 1];
+    }
+    for (int base = a0; base < a1; base += NG) {  // uniform over the block
+        const int a = base + grp, beg = nb, end = ne;
+        if (a + NG < a1) {
+            nb = row_off[a + NG];
+            ne = row_off[a + NG + 1];
+        }
+        double fx = 0, fy = 0, fz = 0;
+        if (a < a1) {
+#pragma unroll 4
+            for (int q = beg + sub; q < end; q += LPA) {
+                fx += G[3 * (size_t)q];
+                fy += G[3 * (size_t)q + 1];
+                fz += G[3 * (size_t)q + 2];
+            }
+            const double *pa = cs.per_atom + (size_t)a * ATOM_ACC;
+            r0 += pa[sub];
+            if (sub < ATOM_ACC - LPA) r1 += pa[LPA + sub];
+        }
+        fx = group_sum<LPA>(fx);
+        fy = group_sum<LPA>(fy);
+        fz = group_sum<LPA>(fz);
+        if (sub == 0 && a < a1) {
+            forces[3 * (size_t)a] = f_local[3 * (size_t)a] + fx;
+            forces[3 * (size_t)a + 1] = f_local[3 * (size_t)a + 1] + fy;
+            forces[3 * (size_t)a + 2] = f_local[3 * (size_t)a + 2] + fz;
         }
     }
-    fx = group_sum<LPA>(fx);
-    fy = group_sum<LPA>(fy);
-    fz = group_sum<LPA>(fz);
-    if (sub == 0 && a < n_atoms) {
-        forces[3 * (size_t)a] = f_local[3 * (size_t)a] + fx;
-        forces[3 * (size_t)a + 1] = f_local[3 * (size_t)a + 1] + fy;
-        forces[3 * (size_t)a + 2] = f_local[3 * (size_t)a + 2] + fz;
-    }
+    chunk_sums_finish<NT>(cs, c, s, r0, r1);
 }
 
-int gather_forces(int n_atoms, const int *row_off, const double *G, const double *f_local, double *forces,
-                  cudaStream_t st) {
-    PROF_BEGIN("gather_forces", st);
-    gather_slot_forces<<<(n_atoms + 15) / 16, 128, 0, st>>>(n_atoms, row_off, G, f_local, forces);
-    PROF_END("gather_forces", st);
+int gather_reduce(int n_struct, int n_atoms, const int *row_off, const double *G, const double *f_local,
+                  double *forces, const double *per_atom, const mbf_reduce_plan *plan, double *partial,
+                  double *energy, double *virial, unsigned *sdone, cudaStream_t st) {
+    if (plan->n_chunks <= 0 || n_struct <= 0 || !sdone) return MBF_ERR_ARGUMENT;
+    if (cudaMemsetAsync(sdone, 0, sizeof(unsigned) * (size_t)n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
+    ChunkSums cs = {plan->chunk, plan->chunk_first, per_atom, partial, energy, virial, sdone};
+    PROF_BEGIN("gather_reduce", st);
+    int nt = chunk_block(n_atoms, plan->n_chunks);
+    if (nt == 128)
+        gather_reduce_rows<128><<<plan->n_chunks, 128, 0, st>>>(row_off, G, f_local, forces, cs);
+    else if (nt == 256)
+        gather_reduce_rows<256><<<plan->n_chunks, 256, 0, st>>>(row_off, G, f_local, forces, cs);
+    else
+        gather_reduce_rows<512><<<plan->n_chunks, 512, 0, st>>>(row_off, G, f_local, forces, cs);
+    PROF_END("gather_reduce", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;
 }

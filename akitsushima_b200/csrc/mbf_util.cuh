@@ -16,19 +16,28 @@ size_t scan_workspace_ints(int n);
 // scan_workspace_ints(n) ints.
 int exclusive_scan(const int *in, int *out, int n, int *ws, cudaStream_t st);
 
-// `sdone` (n_struct words, the workspace's sdone region) holds the
-// per-structure completion counters; the call clears it.
-int reduce_per_structure(const double *per_atom, const mbf_reduce_plan *plan, int n_struct,
-                         double *partial, double *energy, double *virial, unsigned *sdone, cudaStream_t st);
+// The last step of the three-body evaluations: F_a = f_local[a] + the slot
+// forces in a's row of G (n_slots x 3), with the per-structure sums of
+// per_atom into energy / virial (ChunkSums below).  `sdone` (n_struct
+// words, the workspace's sdone region) is cleared by the call.
+int gather_reduce(int n_struct, int n_atoms, const int *row_off, const double *G, const double *f_local,
+                  double *forces, const double *per_atom, const mbf_reduce_plan *plan, double *partial,
+                  double *energy, double *virial, unsigned *sdone, cudaStream_t st);
 
-int gather_forces(int n_atoms, const int *row_off, const double *G, const double *f_local, double *forces,
-                  cudaStream_t st);
+// Threads per block of the fused gather kernels: 8 lanes per atom of the
+// plan's mean chunk, at least 128 and at most 512.
+static inline int chunk_block(int n_atoms, int n_chunks) {
+    int per = n_chunks > 0 ? (n_atoms + n_chunks - 1) / n_chunks : 1;
+    return per <= 16 ? 128 : (per <= 32 ? 256 : 512);
+}
 
-// The per-structure sums of reduce_per_structure done by the last kernel of
-// an evaluation instead: one block per chunk of the plan (a run of at most
-// REDUCE_CHUNK atoms of one structure) adds its atoms' records, writes the
-// chunk total to partial[c], and the block that completes a structure adds
-// that structure's chunk totals, each sum in a fixed order.
+// The per-structure sums of the per-atom records (energy, virial, pair
+// count), done by the last kernel of an evaluation: one block per chunk of
+// the reduction plan (a run of atoms of one structure; 512 in the plans the
+// Python Batch makes) adds its atoms' records, writes the chunk total to
+// partial[c], and the block that completes a structure (a completion
+// counter per structure) adds that structure's chunk totals; every sum in
+// a fixed order, so the same input gives the same bits.
 struct ChunkSums {
     const int *chunk;        // (n_chunks, 3): structure, first atom, end atom
     const int *chunk_first;  // (n_struct + 1,): first chunk of each structure
@@ -44,7 +53,7 @@ struct ChunkSums {
 // q = 8 + t % 8 (q < ATOM_ACC) over the atoms its 8-lane group visited.
 template <int NT>
 __device__ __forceinline__ void chunk_sums_finish(const ChunkSums &cs, int c, int s, double r0, double r1) {
-    static_assert(NT % 32 == 0 && NT >= 32 * 8, "chunk_sums_finish: 8 warps or more");
+    static_assert(NT % 32 == 0 && NT >= 64, "chunk_sums_finish: whole warps, two or more");
     constexpr int NW = NT / 32;
     constexpr int PER = NT / ATOM_ACC;   // chunk totals summed per value in the tail
     __shared__ double sh[NW][16];

@@ -148,19 +148,37 @@ class DevicePotential:
     def autotune_lanes(self, batch, dlist, candidates=None, reps=3, ws=None, out=None):
         """Time every lanes-per-atom candidate on this batch (CUDA events,
         after one untimed call each), keep the fastest and return
-        {"lanes_per_atom": best, "ms": {candidate: ms}}."""
+        {"lanes_per_atom": best, "ms": {candidate: ms}}.  With ``out`` and
+        ``ws`` given, each candidate is captured in a CUDA graph and the
+        replays are timed, so the host's launch cost (which can exceed a
+        small batch's device time) does not decide the choice."""
         cands = tuple(candidates or self.lane_choices)
         timings = {}
+        dev = batch.device
         for c in cands:
             self.lanes_per_atom = c
             self.evaluate(batch, dlist, out=out, ws=ws)
+            run = lambda: self.evaluate(batch, dlist, out=out, ws=ws)  # noqa: E731
+            graph = None
+            if out is not None and ws is not None:
+                side = torch.cuda.Stream(dev)
+                side.wait_stream(torch.cuda.current_stream(dev))
+                with torch.cuda.stream(side):
+                    run()
+                torch.cuda.current_stream(dev).wait_stream(side)
+                graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(graph):
+                    run()
+                graph.replay()
+                run = graph.replay
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
             for _ in range(reps):
-                self.evaluate(batch, dlist, out=out, ws=ws)
+                run()
             b.record()
             b.synchronize()
             timings[c] = a.elapsed_time(b) / reps
+            del graph
         best = min(cands, key=lambda c: (timings[c], c))
         self.lanes_per_atom = best
         return {"lanes_per_atom": best, "ms": timings}

@@ -11,8 +11,19 @@ import torch
 
 from . import _lib
 
-# Atoms per reduction chunk (the per-structure energy/virial sums).
+# Atoms per reduction chunk (the per-structure energy/virial sums, one
+# block of the last kernel of an evaluation per chunk): enough chunks for
+# about two blocks per SM of a B200, 32 to 512 atoms each.
 REDUCE_CHUNK = 512
+REDUCE_CHUNK_MIN = 32
+REDUCE_TARGET_CHUNKS = 296
+
+
+def reduce_chunk_size(n_atoms):
+    size = REDUCE_CHUNK_MIN
+    while size < REDUCE_CHUNK and size * REDUCE_TARGET_CHUNKS < n_atoms:
+        size *= 2
+    return size
 
 
 def cell_metrics(lattice):
@@ -147,12 +158,13 @@ class Batch:
         self._types_host = None
         self.set_positions(positions)
         self.set_types(type_ids)
-        # reduction plan: chunks of REDUCE_CHUNK atoms inside one structure
+        # reduction plan: chunks of reduce_chunk_size atoms inside one structure
+        size = reduce_chunk_size(self.n_atoms)
         chunk, first = [], [0]
         for s in range(self.n_struct):
             a0, a1 = int(off[s]), int(off[s + 1])
-            for c0 in range(a0, a1, REDUCE_CHUNK):
-                chunk.append((s, c0, min(a1, c0 + REDUCE_CHUNK)))
+            for c0 in range(a0, a1, size):
+                chunk.append((s, c0, min(a1, c0 + size)))
             if a1 == a0:
                 chunk.append((s, a0, a0))
             first.append(len(chunk))

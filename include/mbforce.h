@@ -76,7 +76,10 @@ typedef struct mbf_nlist {
 /* Per-structure reduction table: chunks of atoms that lie in one structure.
  * chunk (n_chunks, 3) int32 rows (struct id, first atom, end atom);
  * chunk_first (n_struct + 1) int32: chunks of structure s are
- * chunk_first[s] .. chunk_first[s+1]-1. */
+ * chunk_first[s] .. chunk_first[s+1]-1; a structure without atoms has one
+ * empty chunk.  Any chunk length works; the last kernel of an evaluation runs
+ * one block per chunk (8 threads per atom of the mean chunk, 128 to 512),
+ * so chunks of 32-512 atoms, about two per SM, keep it busy. */
 typedef struct mbf_reduce_plan {
     int n_chunks;
     const int *chunk;
