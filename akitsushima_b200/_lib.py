@@ -86,6 +86,8 @@ _SIGS = {
     "mbf_md_kick": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _d, _vp, _vp, _vp, _i, _vp, _vp, _vp]),
     "mbf_md_kick_drift_check": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _vp, _d, _vp, _d, _d, _vp, _vp,
                                      _vp, _i, _vp, _vp, ctypes.c_ulonglong, _vp]),
+    "mbf_md_kick_kick_drift_check": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp, _i,
+                                          _vp, _vp, _d, _d, _vp, _vp, _i, _vp, _vp, ctypes.c_ulonglong, _vp, _vp]),
     "mbf_md_skin_check": (_i, [ctypes.POINTER(MbfSystem), _vp, _d, _d, _vp, _vp, _i, _vp, _vp, _vp,
                                ctypes.c_ulonglong, _vp]),
     "mbf_md_rebuild_done": (_i, [ctypes.POINTER(MbfSystem), _vp, _vp, _vp]),

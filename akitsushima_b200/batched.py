@@ -20,7 +20,7 @@ import torch
 from .neighbourlist import DeviceNeighbourList
 from . import _lib
 from .potential import EvalResult
-from .system import Batch, default_device, species_ids
+from .system import Batch, capture_graph, default_device, species_ids
 from .system import replicate_thin as _replicate
 
 
@@ -98,17 +98,8 @@ class BatchedEvaluator:
         it (positions, lattices and species are read from the batch's device
         arrays, so updating those in place keeps the graph valid)."""
         self._eval()
+        self._graph = capture_graph(self._eval, self.device)
         torch.cuda.synchronize(self.device)
-        g = torch.cuda.CUDAGraph()
-        s = torch.cuda.Stream(self.device)
-        s.wait_stream(torch.cuda.current_stream(self.device))
-        with torch.cuda.stream(s):
-            self._eval()
-        torch.cuda.current_stream(self.device).wait_stream(s)
-        torch.cuda.synchronize(self.device)
-        with torch.cuda.graph(g):
-            self._eval()
-        self._graph = g
         return self
 
     def results(self):

@@ -187,6 +187,97 @@ __global__ void __launch_bounds__(MD_BLOCK) md_kick(SysView S, double *__restric
     if (threadIdx.x == 0) *done = 0u;
 }
 
+// The second half kick of one step and the first half kick, drift and
+// list-validity check of the next, in one launch (the two kicks use the same
+// forces): per atom md_kick's arithmetic, its kinetic-energy term from the
+// mid-step velocity, then md_kick_drift_check's arithmetic on that velocity,
+// so every stored value has the bits of the two separate launches.  Grid and
+// partial sums as md_kick (blocks of one structure, blockIdx.y = s, so the
+// displacement maximum of a warp belongs to one structure); the block that
+// finishes last writes the thermo row of the step that ended and then takes
+// the rebuild decision of the next (md_kick_drift_check's tail).
+__global__ void __launch_bounds__(MD_BLOCK) md_kick_kick_drift_check(
+    SysView S, double *__restrict__ pos, double *__restrict__ vel, const double *__restrict__ F,
+    const double *__restrict__ im, double dt, int P, double *__restrict__ partial,
+    const double *__restrict__ energy, double *__restrict__ thermo, int rows, int *__restrict__ tcounter,
+    const double *__restrict__ ref, unsigned long long *__restrict__ dmax, double r_list, double r_cut,
+    double *__restrict__ d_log, int *__restrict__ scounter, int *__restrict__ gate, unsigned long long cond,
+    unsigned *__restrict__ done) {
+    __shared__ double sh[MD_BLOCK / 32];
+    __shared__ bool last;
+    int s = blockIdx.y;
+    int beg = S.n_struct > 1 ? S.struct_off[s] : 0;
+    int end = S.n_struct > 1 ? S.struct_off[s + 1] : S.n_atoms;
+    const double *c = S.cells + 18 * (size_t)s;
+    double acc = 0.0;
+    unsigned long long bits = 0ull;
+    int first = beg + blockIdx.x * MD_CHUNK;
+#pragma unroll
+    for (int k = 0; k < MD_ITEMS; ++k) {
+        int a = first + k * MD_BLOCK + threadIdx.x;
+        if (a < end) {
+            size_t o = 3 * (size_t)a;
+            double w = im[a];
+            double h = 0.5 * dt * w;
+            double fx = F[o], fy = F[o + 1], fz = F[o + 2];
+            double vx = vel[o] + h * fx, vy = vel[o + 1] + h * fy, vz = vel[o + 2] + h * fz;
+            acc += (vx * vx + vy * vy + vz * vz) / w;
+            vx = vx + h * fx;
+            vy = vy + h * fy;
+            vz = vz + h * fz;
+            double x = pos[o] + dt * vx, y = pos[o + 1] + dt * vy, z = pos[o + 2] + dt * vz;
+            double s0 = x * c[9] + y * c[12] + z * c[15];
+            double s1 = x * c[10] + y * c[13] + z * c[16];
+            double s2 = x * c[11] + y * c[14] + z * c[17];
+            s0 -= floor(s0);
+            s1 -= floor(s1);
+            s2 -= floor(s2);
+            if (s0 >= 1.0) s0 = 0.0;
+            if (s1 >= 1.0) s1 = 0.0;
+            if (s2 >= 1.0) s2 = 0.0;
+            double px = s0 * c[0] + s1 * c[3] + s2 * c[6];
+            double py = s0 * c[1] + s1 * c[4] + s2 * c[7];
+            double pz = s0 * c[2] + s1 * c[5] + s2 * c[8];
+            pos[o] = px;
+            pos[o + 1] = py;
+            pos[o + 2] = pz;
+            vel[o] = vx;
+            vel[o + 1] = vy;
+            vel[o + 2] = vz;
+            double dx, dy, dz;
+            mic_exact(c, px - ref[o], py - ref[o + 1], pz - ref[o + 2], dx, dy, dz);
+            unsigned long long b = (unsigned long long)__double_as_longlong(sqrt(dx * dx + dy * dy + dz * dz));
+            bits = b > bits ? b : bits;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long b = __shfl_xor_sync(MBF_FULL, bits, o);
+        bits = b > bits ? b : bits;
+    }
+    if ((threadIdx.x & 31) == 0 && bits) atomicMax(dmax + s, bits);
+    acc = block_sum<MD_BLOCK>(acc, sh);
+    if (threadIdx.x == 0) partial[(size_t)s * P + blockIdx.x] = acc;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(done, 1u) == gridDim.x * gridDim.y - 1;
+    __syncthreads();
+    if (!last) return;
+    md_thermo_body(S.n_struct, P, partial, energy, thermo, rows, tcounter, sh);
+    if (threadIdx.x != 0) return;
+    int row = *scounter % rows;
+    int need = 0;
+    for (int q = 0; q < S.n_struct; ++q) {
+        double d = __longlong_as_double((long long)atomicExch(dmax + q, 0ull));
+        d_log[(size_t)row * S.n_struct + q] = d;
+        if (r_list - 2.0 * d <= r_cut) need = 1;
+    }
+    *gate = need;
+    if (cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, need ? 1u : 0u);
+    *scounter += 1;
+    *done = 0u;
+}
+
 // With inv_mass = conv / m the partials hold sum m v^2 / conv, so the
 // kinetic energy is half their sum, in eV (the reference's
 // 0.5 sum m v^2 / EV_ANG_TO_AMU_ANG_FS2, :243-244).
@@ -263,6 +354,29 @@ int mbf_md_kick_drift_check(const mbf_system *sys, double *positions, double *ve
         S, positions, velocities, forces, inv_mass, dt, ref_positions, d_max, done, r_list, r_cut, d_log, rows,
         counter, gate, cond_handle);
     PROF_END("md_kick_drift", st);
+    MBF_CHECK_LAUNCH();
+    return MBF_OK;
+}
+
+int mbf_md_kick_kick_drift_check(const mbf_system *sys, double *positions, double *velocities,
+                                 const double *forces, const double *inv_mass, double dt, const double *energy,
+                                 double *partial, double *thermo, int thermo_rows, int *thermo_counter,
+                                 const double *ref_positions, double r_list, double r_cut,
+                                 unsigned long long *d_max, double *d_log, int rows, int *skin_counter, int *gate,
+                                 unsigned long long cond_handle, unsigned *done, void *stream) {
+    if (!sys || !positions || !velocities || !forces || !inv_mass || positions != sys->positions || !energy ||
+        !partial || !thermo || thermo_rows <= 0 || !thermo_counter || !ref_positions || !d_max || !d_log ||
+        rows <= 0 || !skin_counter || !gate || !done || !(r_list > r_cut) || !(r_cut > 0.0) ||
+        sys->n_struct <= 0 || sys->n_struct > 65535 || sys->n_atoms <= 0)
+        return MBF_ERR_ARGUMENT;
+    SysView S = make_view(sys);
+    cudaStream_t st = (cudaStream_t)stream;
+    int P = mbf_md_partial_count(sys->n_atoms);
+    PROF_BEGIN("md_kick_kick_drift", st);
+    md_kick_kick_drift_check<<<dim3(P, sys->n_struct), MD_BLOCK, 0, st>>>(
+        S, positions, velocities, forces, inv_mass, dt, P, partial, energy, thermo, thermo_rows, thermo_counter,
+        ref_positions, d_max, r_list, r_cut, d_log, skin_counter, gate, cond_handle, done);
+    PROF_END("md_kick_kick_drift", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;
 }

@@ -24,7 +24,7 @@ import torch
 from . import _lib
 from .neighbourlist import DeviceNeighbourList
 from .potential import EvalResult
-from .system import Batch, default_device, species_ids
+from .system import Batch, capture_graph, default_device, species_ids
 
 # solvers/../constants.py:8-20 of the reference (CODATA values it uses).
 EV_ANG_TO_AMU_ANG_FS2 = (1.60217663e-19 / 1.0e-10) / (1.66053906660e-27) * 1.0e-20
@@ -202,6 +202,7 @@ class NVE:
         saved = [t.clone() for t in (self.batch.pos, self.vel, self.out.forces, self.out.energy, self._ref)]
         st = torch.cuda.current_stream(self.device).cuda_stream
         self._step(0, capturing=False)
+        self._kick_kick(st)
         self._skin_check(st, assert_only=False)
         self._rebuild(st)
         for dst, src in zip((self.batch.pos, self.vel, self.out.forces, self.out.energy, self._ref), saved):
@@ -244,6 +245,37 @@ class NVE:
             _lib.ptr(self._dmax), self._word(5), _lib.ptr(self.skin_log), self.thermo_rows, self._word(1),
             self._word(4), cond, stream), "mbf_md_kick_drift_check")
 
+    def _kick_kick(self, stream, cond=0):
+        """The second half kick (and thermo row) of a step and the first
+        half kick, drift and criterion check of the next in one launch."""
+        _lib.check(_lib.lib().mbf_md_kick_kick_drift_check(
+            self.batch.mbf_system(), _lib.ptr(self.batch.pos), _lib.ptr(self.vel), _lib.ptr(self.out.forces),
+            _lib.ptr(self.inv_mass), self.dt, _lib.ptr(self.out.energy), _lib.ptr(self._partial),
+            _lib.ptr(self.thermo), self.thermo_rows, self._word(0), _lib.ptr(self._ref), self.dlist.r_list,
+            float(self.pot.r_cut), _lib.ptr(self._dmax), _lib.ptr(self.skin_log), self.thermo_rows, self._word(1),
+            self._word(4), cond, self._word(5), stream), "mbf_md_kick_kick_drift_check")
+
+    def _check_then_rebuild(self, launch, capturing):
+        """`launch` (a kick ending in the criterion check), then the list
+        rebuild it asks for: an IF branch in a capture, else decided on the
+        host from the gate word."""
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        if capturing:
+            L = _lib.lib()
+            h = ctypes.c_ulonglong(0)
+            _lib.check(L.mbf_capture_cond_create(st, ctypes.byref(h)), "mbf_capture_cond_create")
+            launch(st, cond=h.value)
+            body = self._body.cuda_stream
+            _lib.check(L.mbf_capture_if_begin(st, body, h.value), "mbf_capture_if_begin")
+            try:
+                self._rebuild(body)
+            finally:
+                _lib.check(L.mbf_capture_if_end(body), "mbf_capture_if_end")
+        else:
+            launch(st)
+            if int(self._counters[4].item()):
+                self._rebuild(st)
+
     def _step(self, k, capturing):
         """MD step number k of a block (k counts from 0)."""
         L = _lib.lib()
@@ -256,40 +288,44 @@ class NVE:
             if k % self.rebuild_every == 0:
                 self._skin_check(st, assert_only=True)
                 self._rebuild(st)
-        elif capturing:
-            h = ctypes.c_ulonglong(0)
-            _lib.check(L.mbf_capture_cond_create(st, ctypes.byref(h)), "mbf_capture_cond_create")
-            self._kick_drift_check(st, cond=h.value)
-            body = self._body.cuda_stream
-            _lib.check(L.mbf_capture_if_begin(st, body, h.value), "mbf_capture_if_begin")
-            try:
-                self._rebuild(body)
-            finally:
-                _lib.check(L.mbf_capture_if_end(body), "mbf_capture_if_end")
         else:
-            self._kick_drift_check(st)
-            if int(self._counters[4].item()):
-                self._rebuild(st)
+            self._check_then_rebuild(self._kick_drift_check, capturing)
         self._eval()
-        _lib.check(L.mbf_md_kick(sysd, _lib.ptr(self.vel), _lib.ptr(self.out.forces), _lib.ptr(self.inv_mass),
-                                 self.dt, _lib.ptr(self.out.energy), _lib.ptr(self._partial),
-                                 _lib.ptr(self.thermo), self.thermo_rows, self._word(0), self._word(6), st),
-                   "mbf_md_kick")
+        self._kick(st)
+
+    def _kick(self, stream):
+        """Second half kick and the thermo row of the step."""
+        L = _lib.lib()
+        _lib.check(L.mbf_md_kick(self.batch.mbf_system(), _lib.ptr(self.vel), _lib.ptr(self.out.forces),
+                                 _lib.ptr(self.inv_mass), self.dt, _lib.ptr(self.out.energy),
+                                 _lib.ptr(self._partial), _lib.ptr(self.thermo), self.thermo_rows, self._word(0),
+                                 self._word(6), stream), "mbf_md_kick")
 
     def _run_block(self, capturing=False):
+        """A block of MD steps.  Under the criterion policy the second half
+        kick of every step but the last shares a launch with the first half
+        kick, drift and check of the next (the same arithmetic); the block
+        still ends on a whole step, so positions, velocities and thermo
+        between blocks are those of separate launches."""
+        if self.rebuild_every is not None:
+            for k in range(self.block):
+                self._step(k, capturing)
+            return
+        self._check_then_rebuild(self._kick_drift_check, capturing)
         for k in range(self.block):
-            self._step(k, capturing)
+            self._eval()
+            if k + 1 < self.block:
+                self._check_then_rebuild(self._kick_kick, capturing)
+            else:
+                self._kick(torch.cuda.current_stream(self.device).cuda_stream)
 
     # -- public ---------------------------------------------------------------
     def capture(self):
         """Capture one block of MD steps (criterion checks and the gated
         rebuild branches included) as a CUDA graph; run() replays it."""
         torch.cuda.synchronize(self.device)
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            self._run_block(capturing=True)
+        self._graph = capture_graph(lambda: self._run_block(capturing=True), self.device, warm=False)
         torch.cuda.synchronize(self.device)
-        self._graph = g
         return self
 
     def run(self, n_steps, graph=True):

@@ -18,7 +18,7 @@ import torch
 
 from . import _lib
 from .neighbourlist import DeviceNeighbourList, NeighbourList, owned_neighbour_list
-from .system import Batch, species_ids
+from .system import Batch, capture_graph, species_ids
 
 PRECISIONS = {"fp64": _lib.MBF_FP64, "mixed": _lib.MBF_MIXED}
 
@@ -161,14 +161,7 @@ class DevicePotential:
             run = lambda: self.evaluate(batch, dlist, out=out, ws=ws)  # noqa: E731
             graph = None
             if out is not None and ws is not None:
-                side = torch.cuda.Stream(dev)
-                side.wait_stream(torch.cuda.current_stream(dev))
-                with torch.cuda.stream(side):
-                    run()
-                torch.cuda.current_stream(dev).wait_stream(side)
-                graph = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(graph):
-                    run()
+                graph = capture_graph(run, dev)
                 graph.replay()
                 run = graph.replay
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

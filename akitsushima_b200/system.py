@@ -76,6 +76,26 @@ def cell_grid(lattice, r_list, widths=None):
     return nc, w
 
 
+def capture_graph(fn, device, warm=True):
+    """A CUDA graph of fn()'s launches, captured on a side stream (after one
+    eager call there when ``warm``).  capture_begin / capture_end directly:
+    torch.cuda.graph() would also run the garbage collector and empty the
+    allocator's cache, costing more than a small capture."""
+    side = torch.cuda.Stream(device)
+    side.wait_stream(torch.cuda.current_stream(device))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        if warm:
+            fn()
+        g.capture_begin()
+        try:
+            fn()
+        finally:
+            g.capture_end()
+    torch.cuda.current_stream(device).wait_stream(side)
+    return g
+
+
 def default_device():
     if not torch.cuda.is_available():
         raise RuntimeError("akitsushima_b200 needs a CUDA device (B200); none is visible.")
@@ -287,5 +307,5 @@ def replicate_thin(lattice, positions, type_ids, r_list):
     return lat * reps[:, None], big, types, reps
 
 
-__all__ = ["Batch", "cell_metrics", "cell_widths", "check_min_image", "cell_grid", "species_ids",
+__all__ = ["Batch", "capture_graph", "cell_metrics", "cell_widths", "check_min_image", "cell_grid", "species_ids",
            "replicate_thin", "default_device"]

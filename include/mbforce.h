@@ -429,6 +429,20 @@ int mbf_md_kick_drift_check(const mbf_system *sys, double *positions, double *ve
                             unsigned long long *d_max, unsigned *done, double *d_log, int rows,
                             int *counter, int *gate, unsigned long long cond_handle, void *stream);
 
+/* mbf_md_kick of one step followed by mbf_md_kick_drift_check of the
+ * next, in one launch (both half kicks use the forces of the step that
+ * ended; every stored value, the thermo row and the decision equal those of
+ * the two launches).  thermo_counter / skin_counter are the two entries'
+ * counters; d_max (n_struct device words) and *done must be 0 and are left
+ * at 0.                                                                   */
+int mbf_md_kick_kick_drift_check(const mbf_system *sys, double *positions, double *velocities,
+                                 const double *forces, const double *inv_mass, double dt,
+                                 const double *energy, double *partial, double *thermo,
+                                 int thermo_rows, int *thermo_counter, const double *ref_positions,
+                                 double r_list, double r_cut, unsigned long long *d_max,
+                                 double *d_log, int rows, int *skin_counter, int *gate,
+                                 unsigned long long cond_handle, unsigned *done, void *stream);
+
 /* The reference's rebuild decision (engine/neighborlist.py:613-673 with
  * the lattice fixed: rebuild iff r_list - 2 d <= r_cut, d = max_a |MIC(r_a -
  * r_ref_a)| since the last rebuild) evaluated on the device every step:
