@@ -144,3 +144,23 @@ def test_criterion_graph_equals_eager(cuda_device):
     d = r1["skin_displacement"]
     # a rebuild resets the displacement: it never stays above the trigger
     assert np.all(2 * d < 0.2 + 2 * 0.1)
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_fused_kicks_equal_separate_launches(cuda_device, graph):
+    """A block of steps (the second half kick of each step but the last
+    fused with the first half kick, drift and check of the next) gives the
+    bits of the same steps run one by one as separate launches."""
+    lat, pos, types = cubic(DIAMOND, 5.431, 3, ["Si"] * 8, rattle=0.1, seed=41)
+    pot = ak.StillingerWeberPotential(SW_SI, species=["Si"], precision="fp64")
+    args = dict(temperature=900.0, seed=5, skin=0.3, autotune=False)
+    blocked = md.NVE(pot, lat, pos, types, steps_per_graph=12, **args)
+    single = md.NVE(pot, lat, pos, types, steps_per_graph=100, **args)
+    blocked.run(24, graph=graph)    # two whole blocks
+    single.run(24, graph=graph)     # no whole block: 24 single steps
+    np.testing.assert_array_equal(blocked.positions, single.positions)
+    np.testing.assert_array_equal(blocked.velocities, single.velocities)
+    rb, rs = blocked.results(), single.results()
+    for key in ("e_pot", "e_kin", "skin_displacement"):
+        np.testing.assert_array_equal(rb[key], rs[key])
+    assert rb["rebuilds"] == rs["rebuilds"]
