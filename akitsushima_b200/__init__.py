@@ -15,6 +15,7 @@ from .neighbourlist import (DeviceNeighbourList, NeighbourList, NullNeighbourLis
                             clear_owned_neighbour_lists, neighbour_list_for,
                             owned_neighbour_list, uses_neighbour_list)
 from .published_parameters import SW_SI_1985, TERSOFF_1989, TERSOFF_SI_1988, ZHOU_2004
+from .spatial import SpatialForceFn, slab_partition
 from .stillinger_weber import StillingerWeberPotential
 from .system import Batch
 from .tersoff import TersoffPotential, tersoff1989_to_triplets
@@ -23,9 +24,9 @@ __version__ = "0.1.0"
 
 __all__ = [
     "Batch", "BatchedEvaluator", "DeviceNeighbourList", "EAMPotential", "NeighbourList", "NullNeighbourList",
-    "PotentialEngine", "StillingerWeberPotential", "TersoffPotential", "accepts_need_stress",
+    "PotentialEngine", "SpatialForceFn", "StillingerWeberPotential", "TersoffPotential", "accepts_need_stress",
     "call_force_fn", "clear_owned_neighbour_lists", "continuous", "force_fn_from_config",
-    "make_force_fn", "neighbour_list_for", "owned_neighbour_list", "read_setfl",
+    "make_force_fn", "neighbour_list_for", "owned_neighbour_list", "read_setfl", "slab_partition",
     "tersoff1989_to_triplets", "uses_neighbour_list", "zhou_cutoff", "zhou_eam",
     "SW_SI_1985", "TERSOFF_1989", "TERSOFF_SI_1988", "ZHOU_2004",
 ]

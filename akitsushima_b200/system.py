@@ -138,6 +138,13 @@ def species_ids(atom_types, species):
     return ids
 
 
+def _runs(mask, a0, a1):
+    """Maximal runs [r0, r1) of True in mask[a0:a1] (absolute indices)."""
+    m = np.concatenate([[False], mask[a0:a1], [False]]).astype(np.int8)
+    d = np.flatnonzero(np.diff(m))
+    return [(a0 + int(d[k]), a0 + int(d[k + 1])) for k in range(0, len(d), 2)]
+
+
 class Batch:
     """``n_struct`` periodic structures flattened on one device.
 
@@ -146,9 +153,13 @@ class Batch:
     lattices  : sequence of (3, 3) row-vector lattices [A].
     positions : sequence of (N_s, 3) Cartesian positions [A] (numpy or torch).
     type_ids  : sequence of (N_s,) integer species ids.
+    owned     : optional (n_atoms,) bool mask: the per-structure energy and
+                virial sum only the records of these atoms (the others are
+                halo atoms of a spatial slab, evaluated so that the owned
+                atoms' neighbourhoods are complete).  Default: every atom.
     """
 
-    def __init__(self, lattices, positions, type_ids, device=None):
+    def __init__(self, lattices, positions, type_ids, device=None, owned=None):
         self.device = torch.device(device) if device is not None else default_device()
         lats = [np.asarray(l, dtype=np.float64).reshape(3, 3) for l in lattices]
         if len(lats) == 0:
@@ -178,14 +189,21 @@ class Batch:
         self._types_host = None
         self.set_positions(positions)
         self.set_types(type_ids)
-        # reduction plan: chunks of reduce_chunk_size atoms inside one structure
-        size = reduce_chunk_size(self.n_atoms)
+        # reduction plan: chunks of reduce_chunk_size atoms inside one
+        # structure, over the runs of owned atoms (all atoms by default)
+        if owned is not None:
+            owned = np.asarray(owned, bool).reshape(-1)
+            if owned.shape != (self.n_atoms,):
+                raise ValueError("Batch: owned must have one entry per atom")
+        size = reduce_chunk_size(self.n_atoms if owned is None else int(owned.sum()))
         chunk, first = [], [0]
         for s in range(self.n_struct):
             a0, a1 = int(off[s]), int(off[s + 1])
-            for c0 in range(a0, a1, size):
-                chunk.append((s, c0, min(a1, c0 + size)))
-            if a1 == a0:
+            n0 = len(chunk)
+            for r0, r1 in ([(a0, a1)] if owned is None else _runs(owned, a0, a1)):
+                for c0 in range(r0, r1, size):
+                    chunk.append((s, c0, min(r1, c0 + size)))
+            if len(chunk) == n0:
                 chunk.append((s, a0, a0))
             first.append(len(chunk))
         self.chunk = torch.as_tensor(np.array(chunk, np.int32).reshape(-1, 3), device=dev)
