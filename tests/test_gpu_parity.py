@@ -202,6 +202,28 @@ def test_fp64_matches_oracle_same_pairs(name):
     _assert_rel(res, ref, 1e-10)
 
 
+@pytest.mark.parametrize("name", ["tersoff_si512", "tersoff_xy512", "sw_si512", "sw_gesn512"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_every_lane_group_width_matches_oracle(name, precision):
+    """Each lanes-per-atom tile shape the autotuner may pick (4, 8 and 16
+    lanes per centre) gives the oracle's result on the same pairs."""
+    cfg, orc = CASES[name]
+    g = golden(name)
+    fn = _fn(cfg, precision)
+    pot = fn.engine.potentials[0]
+    nl = ak.NeighbourList(float(fn.r_cut), skin_width=float(g["skin"]))
+    nl.build(g["lattice"], g["positions"])
+    ref = orc(g, nl.get_candidate_pairs())
+    assert tuple(pot.lane_choices) == (4, 8, 16)
+    for lpa in pot.lane_choices:
+        pot.lanes_per_atom = lpa
+        res = fn(g["lattice"], g["positions"], list(g["atom_types"]), nl)
+        if precision == "fp64":
+            _assert_rel(res, ref, 1e-10)
+        else:
+            _assert_close(res, ref, len(g["positions"]), MIX_E, MIX_F, MIX_S)
+
+
 @pytest.mark.parametrize("name", ["tersoff1989_sic64", "tersoff1989_sic216"])
 def test_fp64_tersoff1989_sic(name):
     g = golden(name)
