@@ -17,6 +17,7 @@ fixed interval instead, the criterion is asserted at each rebuild.  A block
 of steps is captured as one CUDA graph and replayed.
 """
 import ctypes
+import weakref
 
 import numpy as np
 import torch
@@ -103,6 +104,10 @@ def _row_bound(max_row):
     return max(need, 128)
 
 
+# lanes-per-atom choices per potential (weakly held) and system shape
+_TUNED = weakref.WeakKeyDictionary()
+
+
 class NVE:
     """Velocity-Verlet NVE of one structure on the GPU.
 
@@ -125,7 +130,9 @@ class NVE:
     masses        : per-atom amu or {species: amu} (default: the table).
     precision     : 'fp64' or 'mixed' (default: the potential's).
     autotune      : time the potential's lanes-per-atom tile shapes on this
-                    structure once and keep the fastest.
+                    structure once and keep the fastest (remembered for
+                    later NVEs of the same potential, atom count, row bound
+                    and precision).
     """
 
     def __init__(self, potential, lattice, positions, atom_types, temperature=300.0, dt=1.0, seed=None,
@@ -187,10 +194,19 @@ class NVE:
         self._graph = None
         self.steps_done = 0
         if autotune:
-            saved_precision = self.pot.precision
-            self.pot.precision = self.precision
-            self.tuned = self.pot.autotune_lanes(self.batch, self.view, ws=self._ws, out=self.out)
-            self.pot.precision = saved_precision
+            # one tuning per potential, atom count, row bound and precision:
+            # a later NVE of the same system shape reuses the choice
+            key = (self.n_atoms, self.view.max_row, self.precision, str(dev))
+            cache = _TUNED.setdefault(self.pot, {})
+            if key in cache:
+                self.tuned = cache[key]
+                self.pot.lanes_per_atom = self.tuned["lanes_per_atom"]
+            else:
+                saved_precision = self.pot.precision
+                self.pot.precision = self.precision
+                self.tuned = self.pot.autotune_lanes(self.batch, self.view, ws=self._ws, out=self.out)
+                self.pot.precision = saved_precision
+                cache[key] = self.tuned
         self._eval()
         self.e_pot0 = float(self.out.energy[0].item())
         self.e_kin0 = self.kinetic_energy()
