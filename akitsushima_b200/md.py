@@ -157,11 +157,17 @@ class NVE:
         self.masses = masses_for(atom_types, masses)
         ids = species_ids(atom_types, potential.species)
         self.batch = Batch.single(lattice, pos, ids, device=dev)
-        self.dlist = DeviceNeighbourList(float(potential.r_cut) + self.skin).build(self.batch)
+        # list buffers with room for the rows to grow: 1.5 x the slots, from
+        # the density's estimate first and, if the list came out larger,
+        # from its own count (then built once more)
+        self.dlist = DeviceNeighbourList(float(potential.r_cut) + self.skin)
+        self.dlist.build(self.batch, capacity=int(1.5 * self.dlist.expected_rows(self.batch)[0]) + 4096)
         cap = int(self.dlist.n_slots * 1.5) + 4096
-        self.dlist.nbr = torch.empty(cap, dtype=torch.int32, device=dev)
-        self.dlist.rev = torch.empty(cap, dtype=torch.int32, device=dev)
-        self.dlist.build(self.batch)
+        if self.dlist.nbr.numel() < cap:
+            self.dlist.nbr = torch.empty(cap, dtype=torch.int32, device=dev)
+            self.dlist.rev = torch.empty(cap, dtype=torch.int32, device=dev)
+            self.dlist.build(self.batch)
+        cap = self.dlist.nbr.numel()
         self.view = _FixedList(self.dlist, cap, _row_bound(self.dlist.max_row))
         L = _lib.lib()
         nbytes = int(L.mbf_eval_workspace_bytes(self.n_atoms, cap, self.batch.n_chunks))
@@ -215,18 +221,20 @@ class NVE:
     def _warm(self):
         """One eager step and one rebuild, then the state put back: every
         kernel is loaded before a graph capture needs it."""
-        saved = [t.clone() for t in (self.batch.pos, self.vel, self.out.forces, self.out.energy, self._ref)]
+        d = self.dlist
+        state = (self.batch.pos, self.vel, self.out.forces, self.out.energy, self._ref, d.row_off, d.upper,
+                 d.nbr, d.rev)
+        saved = [t.clone() for t in state]
         st = torch.cuda.current_stream(self.device).cuda_stream
         self._step(0, capturing=False)
         self._kick_kick(st)
         self._skin_check(st, assert_only=False)
         self._rebuild(st)
-        for dst, src in zip((self.batch.pos, self.vel, self.out.forces, self.out.energy, self._ref), saved):
+        for dst, src in zip(state, saved):
             dst.copy_(src)
         self._counters.zero_()
         self.thermo.zero_()
         self.skin_log.zero_()
-        self.dlist.build(self.batch)
         torch.cuda.synchronize(self.device)
 
     # -- launch pieces --------------------------------------------------------

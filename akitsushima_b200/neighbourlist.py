@@ -53,8 +53,19 @@ class DeviceNeighbourList:
             first += int(nc[0] * nc[1] * nc[2])
         return np.array(rows, np.int32), first
 
-    def build(self, batch):
-        """(Re)build from the batch's current positions and lattices."""
+    def expected_rows(self, batch):
+        """(total slots, longest mean row) expected from each structure's
+        number density and the sphere of radius r_list."""
+        cnt = np.asarray(batch.counts, float)
+        if not len(cnt):
+            return 0.0, 0.0
+        rows = cnt / np.asarray(batch.volumes, float) * (4.0 / 3.0 * np.pi * self.r_list ** 3)
+        return float(np.sum(cnt * rows)), float(np.max(rows))
+
+    def build(self, batch, capacity=None):
+        """(Re)build from the batch's current positions and lattices.
+        ``capacity``: slots to reserve in nbr / rev before the first build
+        (grown as needed either way)."""
         dev = batch.device
         self.device = dev
         grids, n_cells = self._grid_table(batch)
@@ -62,22 +73,22 @@ class DeviceNeighbourList:
         N = batch.n_atoms
         self.n_atoms = N
         L = _lib.lib()
-        # the rows expected from each structure's number density (the sphere
-        # of radius r_list): the slot capacity 20 % over their sum, and the
-        # staging stride (the workspace beyond mbf_nl_workspace_bytes) 30 %
-        # over the longest, so one search usually suffices
-        cnt = np.asarray(batch.counts, float)
-        sphere = 4.0 / 3.0 * np.pi * self.r_list ** 3
-        rows = cnt / np.asarray(batch.volumes, float) * sphere if len(cnt) else np.zeros(1)
-        est = int(1.2 * float(np.sum(cnt * rows))) + 1024
-        stride = min(NL_MAX_ROW, int(1.3 * float(np.max(rows))) + 16)
+        # the rows expected from each structure's number density: the slot
+        # capacity 20 % over their sum, and the staging stride (the workspace
+        # beyond mbf_nl_workspace_bytes) 30 % over the longest, so one
+        # search usually suffices
+        slots, longest = self.expected_rows(batch)
+        est = int(1.2 * slots) + 1024
+        stride = min(NL_MAX_ROW, int(1.3 * longest) + 16)
         need = int(L.mbf_nl_rebuild_workspace_bytes(N, n_cells, stride) if N else L.mbf_nl_workspace_bytes(N, n_cells))
         if self._ws is None or self._ws.numel() < need or self._ws.device != dev:
             self._ws = torch.empty(need, dtype=torch.uint8, device=dev)
         if self.row_off is None or self.row_off.numel() < N + 1 or self.row_off.device != dev:
             self.row_off = torch.empty(N + 1, dtype=torch.int32, device=dev)
             self.upper = torch.empty(max(N, 1), dtype=torch.int32, device=dev)
-        if self.nbr is None or self.nbr.device != dev:
+        if capacity is not None:
+            est = max(est, int(capacity))
+        if self.nbr is None or self.nbr.device != dev or self.nbr.numel() < est and capacity is not None:
             self.nbr = torch.empty(est, dtype=torch.int32, device=dev)
             self.rev = torch.empty(est, dtype=torch.int32, device=dev)
         sysd = batch.mbf_system()
