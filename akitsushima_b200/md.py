@@ -89,11 +89,14 @@ class _FixedList:
         self.d = dlist
         self.n_slots = int(capacity)
         self.max_row = int(max_row)
+        self._nl = None   # the C view, built once (the buffers never move)
 
     def mbf_nlist(self):
-        d = self.d
-        return _lib.MbfNlist(d.n_atoms, self.n_slots, self.max_row, _lib.ptr(d.row_off), _lib.ptr(d.nbr),
-                             _lib.ptr(d.rev), _lib.ptr(d.upper))
+        if self._nl is None:
+            d = self.d
+            self._nl = _lib.MbfNlist(d.n_atoms, self.n_slots, self.max_row, _lib.ptr(d.row_off),
+                                     _lib.ptr(d.nbr), _lib.ptr(d.rev), _lib.ptr(d.upper))
+        return self._nl
 
 
 def _row_bound(max_row):

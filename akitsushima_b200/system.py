@@ -282,21 +282,32 @@ class Batch:
         if np.array_equal(lat, self.lattices[s]):
             return
         cell_widths(lat)
+        self._sysd = None
         self.lattices[s] = lat
         self.volumes[s] = abs(np.linalg.det(lat))
         row = np.concatenate([lat.reshape(9), np.linalg.inv(lat).reshape(9)])
         self.cells[s].copy_(torch.from_numpy(row))
 
     def mbf_system(self):
-        off = self.lattices - np.einsum("sij,ij->sij", self.lattices, np.eye(3))
-        ortho = 1 if not np.any(off) else 0
-        return _lib.MbfSystem(self.n_atoms, self.n_struct, _lib.ptr(self.pos), _lib.ptr(self.types),
-                              _lib.ptr(self.atom_struct), _lib.ptr(self.struct_off),
-                              _lib.ptr(self.cells), ortho)
+        """The C ABI's view of the batch (device pointers and the diagonal
+        cell flag), built once and again only after a lattice change: the
+        device arrays keep their addresses."""
+        sysd = getattr(self, "_sysd", None)
+        if sysd is None:
+            off = self.lattices - np.einsum("sij,ij->sij", self.lattices, np.eye(3))
+            ortho = 1 if not np.any(off) else 0
+            sysd = _lib.MbfSystem(self.n_atoms, self.n_struct, _lib.ptr(self.pos), _lib.ptr(self.types),
+                                  _lib.ptr(self.atom_struct), _lib.ptr(self.struct_off),
+                                  _lib.ptr(self.cells), ortho)
+            self._sysd = sysd
+        return sysd
 
     def reduce_plan(self):
-        return _lib.MbfReducePlan(int(self.chunk.shape[0]), _lib.ptr(self.chunk),
-                                  _lib.ptr(self.chunk_first))
+        plan = getattr(self, "_plan", None)
+        if plan is None:
+            plan = self._plan = _lib.MbfReducePlan(int(self.chunk.shape[0]), _lib.ptr(self.chunk),
+                                                   _lib.ptr(self.chunk_first))
+        return plan
 
     @property
     def n_chunks(self):
