@@ -81,23 +81,6 @@ __global__ void nl_fill_cells(int n_atoms, const int *__restrict__ atom_cell, in
     cell_atoms[p] = a;
 }
 
-// Each cell's atoms in ascending index order, so the traversal below (and
-// the rows it produces) do not depend on the order of the atomics above.
-__global__ void nl_sort_cells(int n_cells, const int *__restrict__ cell_start, int *__restrict__ cell_atoms) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n_cells) return;
-    int b = cell_start[c], e = cell_start[c + 1];
-    for (int i = b + 1; i < e; ++i) {
-        int v = cell_atoms[i];
-        int j = i - 1;
-        while (j >= b && cell_atoms[j] > v) {
-            cell_atoms[j + 1] = cell_atoms[j];
-            --j;
-        }
-        cell_atoms[j + 1] = v;
-    }
-}
-
 // Stencil of atom a's cell: up to 27 neighbour cells (per-axis offsets
 // {0} for nc = 1, {0, 1} for nc = 2, {-1, 0, 1} otherwise -- the reference's
 // _axis_offsets, engine/neighborlist.py:270-299), visited in (da, db, dc)
@@ -366,6 +349,32 @@ __device__ __forceinline__ int sort_row(const int *src, int n, int *out, int a, 
     return lower;
 }
 
+// Each cell's atoms in ascending index order, so the traversal (and the
+// rows it produces) do not depend on the order of nl_fill_cells's atomics:
+// a warp per cell, the row sort above (a cell beyond NL_MAXROW atoms, which
+// no physical density reaches, by insertion on one lane).
+__global__ void nl_sort_cells(int n_cells, const int *__restrict__ cell_start, int *__restrict__ cell_atoms) {
+    __shared__ int srow[NL_WARPS][NL_MAXROW];
+    int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int c = blockIdx.x * NL_WARPS + wid; c < n_cells; c += gridDim.x * NL_WARPS) {
+        int b = cell_start[c], n = cell_start[c + 1] - b;
+        if (n <= NL_MAXROW) {
+            sort_row(cell_atoms + b, n, cell_atoms + b, NL_PAD, srow[wid]);
+        } else if (lane == 0) {
+            for (int i = b + 1; i < b + n; ++i) {
+                int v = cell_atoms[i];
+                int j = i - 1;
+                while (j >= b && cell_atoms[j] > v) {
+                    cell_atoms[j + 1] = cell_atoms[j];
+                    --j;
+                }
+                cell_atoms[j + 1] = v;
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // Rows written in traversal order by nl_cells<1>: sorted in place, and
 // each row's first upper slot recorded.
 __global__ void nl_sort_rows(int n_atoms, const int *__restrict__ row_off, int *__restrict__ nbr,
@@ -583,7 +592,9 @@ static int nl_prepare(const SysView &S, const int *grids, int n_cells_total, dou
                         cudaMemcpyDeviceToDevice, st) != cudaSuccess)
         return MBF_ERR_CUDA;
     nl_fill_cells<<<(N + 255) / 256, 256, 0, st>>>(N, atom_cell, cursor, cell_atoms);
-    nl_sort_cells<<<(n_cells_total + 127) / 128, 128, 0, st>>>(n_cells_total, cell_start, cell_atoms);
+    nl_sort_cells<<<persistent_grid((n_cells_total + NL_WARPS - 1) / NL_WARPS, 32 * NL_WARPS,
+                                    (const void *)nl_sort_cells),
+                    32 * NL_WARPS, 0, st>>>(n_cells_total, cell_start, cell_atoms);
     MBF_CHECK_LAUNCH();
     int cblocks = (n_cells_total + NL_WARPS - 1) / NL_WARPS;
     int g = persistent_grid(cblocks, 32 * NL_WARPS, (const void *)nl_cells<0>);
