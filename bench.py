@@ -92,6 +92,23 @@ def _ncu_traffic(kernel, workload, precision):
     return {"bytes_per_launch": rec["dram_bytes_per_launch"], "source": rec["source"]}
 
 
+def _ncu_issue(kernel, workload, precision):
+    """The instruction-issue view of `kernel` from the same committed ncu
+    capture: the fraction of issue slots used (the bound of an issue-limited
+    kernel) and the warp instructions per launch, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            rec = json.load(f).get(kernel)
+    except (OSError, ValueError):
+        return None
+    if not rec or rec.get("workload") != workload or rec.get("precision") != precision \
+            or "issue_active_pct" not in rec:
+        return None
+    return {"frac": rec["issue_active_pct"] / 100.0, "metric": "smsp__issue_active.avg.pct_of_peak_sustained_active",
+            "warp_inst_per_launch": rec["warp_inst_per_launch"],
+            "threads_per_warp_inst": rec["threads_per_warp_inst"], "source": rec["source"]}
+
+
 def cpu_count():
     try:
         return len(os.sched_getaffinity(0))
@@ -1181,6 +1198,7 @@ def main():
             "peak_source": "measured live on this GPU: mbf_peak_probe FMA chains",
             "algorithmic_flops_per_launch": force_flops, "launch_ms": t_dom * 1e3,
             "traffic": _ncu_traffic(dom, workload, args.precision),
+            "issue_view": _ncu_issue(dom, workload, args.precision),
             "hbm_view": {"achieved": ach_gbs, "peak": hbm_peak, "unit": "GB/s",
                          "frac": ach_gbs / hbm_peak, "peak_source": hbm_src,
                          "algorithmic_bytes_per_launch": force_bytes},
