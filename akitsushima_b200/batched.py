@@ -62,6 +62,8 @@ class BatchedEvaluator:
             if self.n_orig else np.zeros(0, np.int64)
         self._orig_index = torch.as_tensor(idx, device=self.device)
         self._inv_reps = torch.as_tensor(1.0 / np.array(self.reps, float), device=self.device)
+        ends = np.cumsum(self.n_orig)
+        self._slices = [slice(int(b - n), int(b)) for b, n in zip(ends, self.n_orig)]
         self._vol = torch.as_tensor(self.batch.volumes, device=self.device)
         dev = self.device
         self.out = EvalResult(torch.empty(self.batch.n_struct, dtype=torch.float64, device=dev),
@@ -104,16 +106,22 @@ class BatchedEvaluator:
 
     def results(self):
         """Per-structure (energies (S,), forces list of (N_s, 3), stresses
-        (S, 3, 3)) of the ORIGINAL structures, on the host."""
+        (S, 3, 3)) of the ORIGINAL structures, on the host: one device-side
+        gather into a fresh pinned block and one copy (the arrays returned
+        are views of that block, which the caller's references keep)."""
         out = self.run()
-        e = (out.energy * self._inv_reps).cpu().numpy()
-        f = out.forces.index_select(0, self._orig_index).cpu().numpy()
-        s = (out.virial / self._vol[:, None]).cpu().numpy().reshape(-1, 3, 3)
-        forces, o = [], 0
-        for n in self.n_orig:
-            forces.append(f[o:o + n])
-            o += n
-        return e, forces, s
+        S, n0 = self.batch.n_struct, int(sum(self.n_orig))
+        dev_buf = torch.cat([(out.energy * self._inv_reps),
+                             (out.virial / self._vol[:, None]).reshape(-1),
+                             out.forces.index_select(0, self._orig_index).reshape(-1)])
+        host = torch.empty(dev_buf.numel(), dtype=torch.float64, pin_memory=True)
+        host.copy_(dev_buf, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        h = host.numpy()
+        e = h[:S]
+        s = h[S:10 * S].reshape(-1, 3, 3)
+        f = h[10 * S:10 * S + 3 * n0].reshape(-1, 3)
+        return e, [f[sl] for sl in self._slices], s
 
     def autotune(self, candidates=None, reps=5):
         """Time every lanes-per-atom candidate on this batch and keep the
