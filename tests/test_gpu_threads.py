@@ -32,3 +32,24 @@ def test_concurrent_calls_equal_serial(cuda_device, case):
         assert e1 == pytest.approx(e0, rel=1e-12, abs=1e-12)
         np.testing.assert_allclose(f1, f0, rtol=0, atol=1e-11)
         np.testing.assert_allclose(s1, s0, rtol=0, atol=1e-13)
+
+
+def test_returned_forces_are_not_overwritten_by_later_calls(cuda_device):
+    """The force arrays live in pinned host blocks that are recycled: a
+    block is reused only when no array of it is alive, so results the caller
+    keeps (or a view of them) survive later calls, and dropped ones give
+    their blocks back."""
+    fn = ak.force_fn_from_config({"type": "Tersoff", "species": ["Si"], "params": TERSOFF_SI})
+    lat, pos, types = cubic(DIAMOND, 5.431, 3, ["Si"] * 8, rattle=0.05, seed=34)
+    rng = np.random.default_rng(35)
+    confs = [pos + rng.normal(0.0, 0.01, pos.shape) for _ in range(7)]
+    want = [fn(lat, p, list(types))[1].copy() for p in confs]
+    kept = []
+    for k, p in enumerate(confs):
+        f = fn(lat, p, list(types))[1]
+        kept.append(f[1:] if k % 2 else f)      # keep a view of some, the array of others
+        for j, g in enumerate(kept):
+            np.testing.assert_array_equal(g, want[j][1:] if j % 2 else want[j])
+    kept.clear()
+    for p, w in zip(confs, want):                # blocks recycled once dropped
+        np.testing.assert_array_equal(fn(lat, p, list(types))[1], w)
