@@ -22,6 +22,10 @@ constexpr int EAM_BLOCK = 128;
 #ifndef MBF_EAM_MINB
 #define MBF_EAM_MINB 5
 #endif
+// The same for the float32 density kernel (48 registers, no spills).
+#ifndef MBF_EAM_DENS_MINB
+#define MBF_EAM_DENS_MINB 10
+#endif
 
 enum { F_SPLINE = 1, F_SPLINE_R = 2, F_Z_DENS = 3, F_Z_PAIR = 4, F_Z_CROSS = 5, F_Z_EMB = 6 };
 
@@ -365,7 +369,7 @@ __device__ __forceinline__ double4 ld_pack(const double4 *__restrict__ pk, int j
 // The next neighbour's index, record and species are loaded one iteration
 // ahead of their use.
 template <typename T, int LPA, bool ZHOU, bool ORTHO>
-__global__ void __launch_bounds__(EAM_BLOCK) eam_density(SysView S, const int *__restrict__ row_off,
+__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB : 1) eam_density(SysView S, const int *__restrict__ row_off,
                                                          const int *__restrict__ nbr, EamDev E,
                                                          double4 *__restrict__ pk,
                                                          double *__restrict__ aux, Chk ck) {
