@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB 
 // F(rho-bar) and F'(rho-bar) in float64, rho-bar clamped at 0
 // (engine/_eam_kernels.py:268-274); kept out of the density loop so the
 // float64 pow/log of the embedding does not set that kernel's register count.
-__global__ void eam_embed(int n_atoms, const int *__restrict__ types, EamDev E, double4 *__restrict__ pk,
+__global__ void __launch_bounds__(256, 4) eam_embed(int n_atoms, const int *__restrict__ types, EamDev E, double4 *__restrict__ pk,
                           double *__restrict__ aux, Chk ck) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_atoms) return;
