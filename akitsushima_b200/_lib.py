@@ -41,7 +41,8 @@ class MbfReducePlan(ctypes.Structure):
 class MbfEamTables(ctypes.Structure):
     _fields_ = [("ns", _i), ("nf", _i), ("nX", _i), ("codes", _vp), ("P", _vp), ("xo", _vp),
                 ("nx", _vp), ("X", _vp), ("C", _vp), ("rho_f", _vp), ("F_f", _vp),
-                ("phi_f", _vp), ("r_cut", _d), ("zhou_fused", _i)]
+                ("phi_f", _vp), ("r_cut", _d), ("zhou_fused", _i),
+                ("P_host", _vp), ("rho_f_host", _vp), ("phi_f_host", _vp)]
 
 
 class MbfFitSet(ctypes.Structure):
@@ -104,6 +105,7 @@ _SIGS = {
     "mbf_eam_eval_static": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                                  ctypes.POINTER(MbfEamTables), ctypes.POINTER(MbfReducePlan), _i, _i,
                                  _vp, _vp, _vp, _vp]),
+    "mbf_eam_eval_static_status": (_i, [ctypes.POINTER(_i), _vp]),
     "mbf_tersoff_eval": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                               ctypes.POINTER(MbfTersoffTables), ctypes.POINTER(MbfReducePlan), _i, _i,
                               _vp, _sz, _vp, _vp, _vp, _vp]),

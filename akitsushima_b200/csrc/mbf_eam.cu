@@ -1,12 +1,26 @@
-// Alloy EAM: density kernel (rho-bar, F, F') and force kernel, lane group
-// per atom over the two-way CSR, no atomics.
+// Alloy EAM: energy, forces and virial of the DYNAMO / setfl alloy form over
+// the two-way CSR neighbour list, in four passes, with no float atomics.
 //
 // Replaces engine/eam.py:174-256 and engine/_eam_kernels.py:231-307.  The
-// reference evaluates each half pair once and scatters through a serial
-// two-way CSR; here each atom gathers over its own row (owner computes), so
-// a pair's functions are evaluated from both sides and nothing is written
-// twice.  rho-bar is accumulated and clamped in float64 and F(rho-bar) is
-// evaluated in float64 in both precisions.
+// reference visits each half pair once per phase in four serial phases
+// (density, embedding, pair forces, scatter).  Here every pass is a lane
+// group per atom over its own row:
+//   eam_density   each unordered pair once (the upper half of every row):
+//                 rho_{s_j}(r) is added to atom i's sum and rho_{s_i}(r) is
+//                 left in j's own slot (j -> i) = rev(i -> j);
+//   eam_embed     rho-bar_i = i's own sum + the shares in i's lower slots
+//                 (contiguous), clamped at 0; F and F' in float64; the record
+//                 {x, y, z, F'} every neighbour gathers in the force pass;
+//   eam_force     each unordered pair once: the pair's force coefficient
+//                 c / r, c = phi' + F'_i rho'_{s_j} + F'_j rho'_{s_i}; its force,
+//                 energy and virial go to i, the coefficient to j's slot;
+//   eam_gather_reduce  F_j = j's own upper-pair sum + coefficient x
+//                 minimum-image vector over j's lower slots, fused with the
+//                 per-structure energy / virial sums.
+// The minimum image used here is odd in the displacement (round half to even
+// and every product are), so the product j adds is the exact negative of the
+// one i added for the same pair.  rho-bar and F(rho-bar) are float64 in both
+// precisions.
 #include <mutex>
 
 #include "mbf_util.cuh"
@@ -22,9 +36,9 @@ constexpr int EAM_BLOCK = 128;
 #ifndef MBF_EAM_MINB
 #define MBF_EAM_MINB 5
 #endif
-// The same for the float32 density kernel (48 registers, no spills).
+// The same for the float32 density kernel.
 #ifndef MBF_EAM_DENS_MINB
-#define MBF_EAM_DENS_MINB 10
+#define MBF_EAM_DENS_MINB 8
 #endif
 
 enum { F_SPLINE = 1, F_SPLINE_R = 2, F_Z_DENS = 3, F_Z_PAIR = 4, F_Z_CROSS = 5, F_Z_EMB = 6 };
@@ -39,26 +53,34 @@ struct EamDev {
     double r_cut;
 };
 
-// Bounds checks on every neighbour-list index the kernels dereference: a
-// failed check records (site, index) in the workspace error words and skips
-// the access; mbf_eval_status() returns them to the host.  They are always
-// compiled in: the float64 build of these kernels without them raised an
-// illegal-address fault on B200 whose cause was not found, while the checked
-// build, with the same indices, runs clean.
-// Every index and bound is an int (the entries refuse lists of more than
-// 0x7fffff00 slots, so a slot index plus its prefetch distance cannot
-// overflow), so lo <= idx < hi is one unsigned comparison: idx - lo taken
-// modulo 2^32 is below hi - lo exactly when idx is in range.
+// Checks on every index the kernels read from the list or the species array
+// before they dereference it.  A failed check substitutes an in-range index
+// (or skips the store), sets the lane's flag, and the row's end records
+// (site, atom) in the workspace error words 1 and 2 once; mbf_eval_status()
+// returns them to the host.  They are always compiled in.  Each is one
+// unsigned comparison: the entries refuse lists of more than 0x7fffff00
+// slots, so every index and bound fits an int.
 struct Chk {
     int *err;
     int n_atoms;
     int n_slots;
     int ns;
 };
-#define MBF_OK_IDX(ck, site, idx, lo, hi)                                                          \
-    (((unsigned)(int)(idx) - (unsigned)(int)(lo) < (unsigned)max((int)(hi) - (int)(lo), 0))       \
-         ? true                                                                                    \
-         : (atomicCAS((ck).err + 1, 0, (site)) == 0 ? ((ck).err[2] = (int)(idx), false) : false))
+
+__device__ __forceinline__ int chk_idx(int v, int n, int fallback, int &flag) {
+    const bool ok = (unsigned)v < (unsigned)n;
+    flag |= ok ? 0 : 1;
+    return ok ? v : fallback;
+}
+
+// 0 <= beg <= up <= end <= n_slots, each step one unsigned comparison.
+__device__ __forceinline__ bool row_ok(int beg, int up, int end, int n_slots) {
+    return (unsigned)beg <= (unsigned)up && (unsigned)up <= (unsigned)end && (unsigned)end <= (unsigned)n_slots;
+}
+
+__device__ __forceinline__ void chk_flush(const Chk &ck, int flag, int site, int atom) {
+    if (flag && atomicCAS(ck.err + 1, 0, site) == 0) ck.err[2] = atom;
+}
 
 // ---- generic function evaluation (engine/_eam_kernels.py:129-228) -------
 
@@ -199,7 +221,7 @@ __device__ __forceinline__ void embed64(const EamDev &E, int f, double rho, doub
     }
 }
 
-// ---- fused Zhou alloy path ----------------------------------------------
+// ---- fused Zhou alloy path, up to EAM_MAXSP elements (shared memory) --------
 // One element's density f and pair phi_aa share exp(-beta (x - 1)) and the
 // denominator 1 + (x - lambda)^20, so a species costs two exponentials.
 
@@ -273,7 +295,6 @@ __device__ void load_ztab(const EamDev &E, ZTab<T> &Z) {
     __syncthreads();
 }
 
-// phi_{si,sj}, rho'_{sj}, rho'_{si} at r (fused Zhou path).
 // phi_{si,sj}, rho'_{sj}, rho'_{si} at r (fused Zhou path), without a
 // branch on the species: both species' functions are evaluated and combined
 // by the cross-pair rule phi_ab = 1/2 k (q phi_aa + phi_bb / q), q = f_b/f_a
@@ -302,6 +323,224 @@ __device__ __forceinline__ void zhou_pair_terms(const ZTab<T> &Z, int si, int sj
     drho_j = sj == a ? dra : drb;
     drho_i = si == a ? dra : drb;
 }
+
+// ---- one- and two-element Zhou path: constants as kernel arguments ---------
+// For the common alloy sizes the element constants travel in the kernel's
+// parameter block, so every use is an operand of the instruction itself (no
+// load, no shared memory), and both elements are evaluated for every pair
+// without a branch on the species.  In float32 the exponentials, reciprocals
+// and the root are the PTX approximations (ex2 / rcp / rsqrt .approx, about
+// 2^-22 relative); float64 keeps exp and IEEE division.
+
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// One element's constants (x = r / r_e).  exp(-beta (x - 1)) is
+// 2^(eb0 + eb1 r) with eb0 = beta log2(e), eb1 = -beta log2(e) / r_e (the
+// float32 form); likewise alpha.
+template <typename T>
+struct ZEl {
+    T ire, lam, kap, beta, alpha, eb0, eb1, ea0, ea1, fe, fe_ire, A, B;
+};
+
+template <typename T>
+struct ZK {
+    ZEl<T> el[2];
+    T half_chi;       // chi / 2 of the cross pair
+    T r0, iw, m30iw;  // switch: s = (r - (r_c - w)) / w; dS factor -30 / w
+};
+
+// g = exp(-expo (x - 1)) / (1 + (x - shift)^20) and h with dg/dr = -g h / r_e,
+// h = expo + 20 (x - shift)^19 / (1 + (x - shift)^20) (engine/eam_zhou.py's
+// decay and its derivative).
+__device__ __forceinline__ void zdec(float r, float ire, float shift, float e0, float e1, float expo,
+                                     float &g, float &h) {
+    float u = fmaf(r, ire, -shift);
+    float u2 = u * u, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8;
+    float u19 = u16 * u2 * u;
+    float rd = rcp_approx(fmaf(u16, u4, 1.0f));
+    g = ex2_approx(fmaf(e1, r, e0)) * rd;
+    h = fmaf(20.0f * u19, rd, expo);
+}
+__device__ __forceinline__ void zdec(double r, double ire, double shift, double, double, double expo,
+                                     double &g, double &h) {
+    double x = r * ire, u = x - shift;
+    double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8;
+    double u19 = u16 * u2 * u;
+    double rd = 1.0 / (1.0 + u16 * u4);
+    g = exp(-expo * (x - 1.0)) * rd;
+    h = expo + 20.0 * u19 * rd;
+}
+__device__ __forceinline__ float zval(float r, float ire, float shift, float e0, float e1, float) {
+    float u = fmaf(r, ire, -shift);
+    float u2 = u * u, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8;
+    return ex2_approx(fmaf(e1, r, e0)) * rcp_approx(fmaf(u16, u4, 1.0f));
+}
+__device__ __forceinline__ double zval(double r, double ire, double shift, double, double, double expo) {
+    double x = r * ire, u = x - shift;
+    double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8;
+    return exp(-expo * (x - 1.0)) / (1.0 + u16 * u4);
+}
+
+__device__ __forceinline__ void dist_ir(double r2, float &r, float &ir) {
+    float q = (float)r2;
+    ir = rsqrt_approx(q);
+    r = q * ir;
+}
+__device__ __forceinline__ void dist_ir(double r2, double &r, double &ir) {
+    r = sqrt(r2);
+    ir = 1.0 / r;
+}
+
+// ---- evaluation policies ----------------------------------------------------
+// A policy gives, for a pair inside the cutoff at squared distance r2 of
+// species (si, sj):
+//   dens: the switched densities the pair puts on atom i, rho_{s_j}(r), and on
+//         atom j, rho_{s_i}(r);
+//   pair: the switched pair function phi_{s_i s_j}(r) and its r-derivative,
+//         the r-derivatives of the switched rho_{s_j} and rho_{s_i}, and 1 / r.
+// PolGeneric reads any table (splines and every Zhou form, per call);
+// PolZSmem the fused Zhou path for up to EAM_MAXSP elements (parameters in
+// shared memory); PolZ2<NS> the one- or two-element Zhou path with its
+// constants as kernel arguments.
+
+template <typename T>
+struct PolGeneric {
+    EamDev E;
+    __device__ __forceinline__ void setup(ZTab<T> &) const {}
+    __device__ __forceinline__ void dens(const ZTab<T> &, int si, int sj, double r2, T &to_i, T &to_j) const {
+        double rr = sqrt(r2);
+        T v, dv;
+        feval<T>(E, E.rho_f[sj], rr, v, dv);
+        to_i = v;
+        if (si != sj) feval<T>(E, E.rho_f[si], rr, v, dv);
+        to_j = v;
+    }
+    __device__ __forceinline__ void pair(const ZTab<T> &, int si, int sj, double r2, T &phi, T &dphi, T &drj,
+                                         T &dri, T &ir) const {
+        double rr = sqrt(r2);
+        T v;
+        feval<T>(E, E.phi_f[si * E.ns + sj], rr, phi, dphi);
+        feval<T>(E, E.rho_f[sj], rr, v, drj);
+        dri = drj;
+        if (si != sj) feval<T>(E, E.rho_f[si], rr, v, dri);
+        ir = (T)(1.0 / rr);
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ T pair_dist(double r2);
+template <> __device__ __forceinline__ double pair_dist<double>(double r2) { return sqrt(r2); }
+template <> __device__ __forceinline__ float pair_dist<float>(double r2) { return sqrtf((float)r2); }
+
+template <typename T>
+struct PolZSmem {
+    EamDev E;
+    __device__ __forceinline__ void setup(ZTab<T> &Z) const { load_ztab<T>(E, Z); }
+    __device__ __forceinline__ void dens(const ZTab<T> &Z, int si, int sj, double r2, T &to_i, T &to_j) const {
+        T r = pair_dist<T>(r2);
+        T S, dS;
+        zswitch_fast<T>(r, Z, S, dS);
+        to_i = zdens_only<T>(Z.sp[sj], r) * S;
+        to_j = si == sj ? to_i : zdens_only<T>(Z.sp[si], r) * S;
+    }
+    __device__ __forceinline__ void pair(const ZTab<T> &Z, int si, int sj, double r2, T &phi, T &dphi, T &drj,
+                                         T &dri, T &ir) const {
+        T r = pair_dist<T>(r2);
+        zhou_pair_terms<T>(Z, si, sj, r, phi, dphi, drj, dri);
+        ir = fdiv<T>(T(1), r);
+    }
+};
+
+template <typename T, int NS>
+struct PolZ2 {
+    ZK<T> K;
+    __device__ __forceinline__ void setup(ZTab<T> &) const {}
+
+    __device__ __forceinline__ T sw_val(T r) const {
+        T s = (r - K.r0) * K.iw;
+        s = s < T(0) ? T(0) : (s > T(1) ? T(1) : s);
+        return T(1) - s * s * s * (T(10) - T(15) * s + T(6) * s * s);
+    }
+    __device__ __forceinline__ void sw(T r, T &S, T &dS) const {
+        T s = (r - K.r0) * K.iw;
+        s = s < T(0) ? T(0) : (s > T(1) ? T(1) : s);
+        T s2 = s * s, om = T(1) - s;
+        S = T(1) - s2 * s * (T(10) - T(15) * s + T(6) * s2);
+        dS = K.m30iw * s2 * om * om;
+    }
+    // f = f_e gB, phi_aa = A gA - B gB and their r-derivatives, unswitched.
+    __device__ __forceinline__ void element(const ZEl<T> &p, T r, T &f, T &df, T &ph, T &dph) const {
+        T gB, hB, gA, hA;
+        zdec(r, p.ire, p.lam, p.eb0, p.eb1, p.beta, gB, hB);
+        zdec(r, p.ire, p.kap, p.ea0, p.ea1, p.alpha, gA, hA);
+        f = p.fe * gB;
+        df = -p.fe_ire * gB * hB;
+        T a = p.A * gA, b = p.B * gB;
+        ph = a - b;
+        dph = -p.ire * (a * hA - b * hB);
+    }
+    __device__ __forceinline__ void dens(const ZTab<T> &, int si, int sj, double r2, T &to_i, T &to_j) const {
+        T r, ir;
+        dist_ir(r2, r, ir);
+        T S = sw_val(r);
+        const ZEl<T> &a = K.el[0];
+        T f0 = a.fe * S * zval(r, a.ire, a.lam, a.eb0, a.eb1, a.beta);
+        if (NS == 1) {
+            to_i = to_j = f0;
+            return;
+        }
+        const ZEl<T> &b = K.el[1];
+        T f1 = b.fe * S * zval(r, b.ire, b.lam, b.eb0, b.eb1, b.beta);
+        to_i = sj == 0 ? f0 : f1;
+        to_j = si == 0 ? f0 : f1;
+    }
+    __device__ __forceinline__ void pair(const ZTab<T> &, int si, int sj, double r2, T &phi, T &dphi, T &drj,
+                                         T &dri, T &ir) const {
+        T r;
+        dist_ir(r2, r, ir);
+        T S, dS;
+        sw(r, S, dS);
+        T f0, df0, p0, dp0;
+        element(K.el[0], r, f0, df0, p0, dp0);
+        if (NS == 1) {
+            phi = p0 * S;
+            dphi = dp0 * S + p0 * dS;
+            drj = dri = df0 * S + f0 * dS;
+            return;
+        }
+        T f1, df1, p1, dp1;
+        element(K.el[1], r, f1, df1, p1, dp1);
+        // cross pair phi_01 = chi / 2 (q phi_00 + phi_11 / q), q = f_1 / f_0,
+        // from the unswitched functions (engine/eam_zhou.py:128-207)
+        T inv = fdiv<T>(T(1), f0 * f1);
+        T q = f1 * f1 * inv, rq = f0 * f0 * inv, rf0 = f1 * inv;
+        T dq = (df1 - q * df0) * rf0;
+        T v = K.half_chi * (q * p0 + p1 * rq);
+        T dv = K.half_chi * (dq * p0 + q * dp0 + (dp1 - p1 * dq * rq) * rq);
+        const bool cross = si != sj;
+        T pv = cross ? v : (si == 0 ? p0 : p1);
+        T pdv = cross ? dv : (si == 0 ? dp0 : dp1);
+        phi = pv * S;
+        dphi = pdv * S + pv * dS;
+        T d0 = df0 * S + f0 * dS, d1 = df1 * S + f1 * dS;
+        drj = sj == 0 ? d0 : d1;
+        dri = si == 0 ? d0 : d1;
+    }
+};
 
 // Minimum image for the force kernels (fused multiply-add allowed).
 __device__ __forceinline__ void mic_fast(const double *__restrict__ c, double rx, double ry, double rz,
@@ -342,22 +581,7 @@ struct CellView {
     }
 };
 
-// Distance of a minimum-imaged displacement in the working precision: the
-// wrap and the square stay float64; the root is taken in T.
-template <typename T>
-__device__ __forceinline__ T pair_dist(double r2);
-template <> __device__ __forceinline__ double pair_dist<double>(double r2) { return sqrt(r2); }
-template <> __device__ __forceinline__ float pair_dist<float>(double r2) { return sqrtf((float)r2); }
-
 // ---- kernels --------------------------------------------------------------
-
-// Per-atom record read by every neighbour: position and, once the density
-// pass has run, F'(rho-bar) -- one 32-byte sector per neighbour gather.
-__global__ void eam_pack(SysView S, double4 *__restrict__ pk) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= S.n_atoms) return;
-    pk[i] = make_double4(S.pos[3 * (size_t)i], S.pos[3 * (size_t)i + 1], S.pos[3 * (size_t)i + 2], 0.0);
-}
 
 __device__ __forceinline__ double4 ld_pack(const double4 *__restrict__ pk, int j) {
     const double2 *p = reinterpret_cast<const double2 *>(pk + j);
@@ -365,176 +589,194 @@ __device__ __forceinline__ double4 ld_pack(const double4 *__restrict__ pk, int j
     return make_double4(a.x, a.y, b.x, b.y);
 }
 
-// rho-bar_i over the full row, F(rho-bar_i) and F'(rho-bar_i) in float64.
-// The next neighbour's index, record and species are loaded one iteration
-// ahead of their use.
-template <typename T, int LPA, bool ZHOU, bool ORTHO>
-__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB : 1) eam_density(SysView S, const int *__restrict__ row_off,
-                                                         const int *__restrict__ nbr, EamDev E,
-                                                         double4 *__restrict__ pk,
-                                                         double *__restrict__ aux, Chk ck) {
+__device__ __forceinline__ double3 ld_pos(const double *__restrict__ pos, int j) {
+    const double *p = pos + 3 * (size_t)j;
+    return make_double3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
+}
+
+// Density over the upper half of every row: each unordered pair once.  Atom
+// i sums rho_{s_j}(r) over its upper pairs (into aux[2 i]); rho_{s_i}(r), the
+// pair's share of j's density, goes to j's own slot (j -> i) = rev(i -> j), so
+// j's embedding pass reads its lower slots contiguously.  Every upper slot
+// writes its reverse slot (0 beyond the cutoff), so every lower slot of the
+// list is written.  Slot indices are loaded two iterations ahead, the
+// neighbour's position and species one ahead.
+template <typename T, int LPA, class Pol, bool ORTHO>
+__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB : 1)
+    eam_density(SysView S, const int *__restrict__ row_off, const int *__restrict__ upper,
+                const int *__restrict__ nbr, const int *__restrict__ rev, Pol P, double rc2,
+                T *__restrict__ share, double *__restrict__ aux, Chk ck) {
     __shared__ ZTab<T> Z;
-    if (ZHOU) load_ztab<T>(E, Z);
+    P.setup(Z);
     const int sub = threadIdx.x & (LPA - 1);
     const int gpb = EAM_BLOCK / LPA;
-    const double rc = E.r_cut, rc2 = rc * rc;
     for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
-        int i = base + threadIdx.x / LPA;
+        const int i = base + threadIdx.x / LPA;
         double acc = 0.0;
         if (i < S.n_atoms) {
+            int flag = 0;
+            int up = upper[i], end = row_off[i + 1];
+            if (!row_ok(row_off[i], up, end, ck.n_slots)) {
+                flag = 1;
+                up = end = 0;
+            }
+            const int si = chk_idx(__ldg(S.types + i), ck.ns, 0, flag);
             CellView<ORTHO> cv;
             cv.load(S, i);
-            double4 pi = ld_pack(pk, i);
-            int end = row_off[i + 1];
-            int s = row_off[i] + sub;
-            if (!MBF_OK_IDX(ck, 11, end, 0, ck.n_slots + 1)) end = s;
-            // two-stage prefetch, as in eam_force
-            int j0 = i, j1 = i;
-            if (s < end && MBF_OK_IDX(ck, 12, s, 0, ck.n_slots)) j0 = nbr[s];
-            if (s + LPA < end && MBF_OK_IDX(ck, 15, s + LPA, 0, ck.n_slots)) j1 = nbr[s + LPA];
-            if (!MBF_OK_IDX(ck, 13, j0, 0, ck.n_atoms)) j0 = i;
-            double4 pn = ld_pack(pk, j0);
+            const double3 pi = ld_pos(S.pos, i);
+            int s = up + sub;
+            int j0 = i, v0 = 0, j1 = i, v1 = 0;
+            if (s < end) {
+                j0 = nbr[s];
+                v0 = rev[s];
+            }
+            if (s + LPA < end) {
+                j1 = nbr[s + LPA];
+                v1 = rev[s + LPA];
+            }
+            j0 = chk_idx(j0, ck.n_atoms, i, flag);
+            double3 pn = ld_pos(S.pos, j0);
             int tn = __ldg(S.types + j0);
             for (; s < end; s += LPA) {
-                double4 pj = pn;
-                int sj = tn;
-                if (!MBF_OK_IDX(ck, 14, sj, 0, ck.ns)) sj = 0;
+                const double3 pj = pn;
+                const int sj = chk_idx(tn, ck.ns, 0, flag);
+                const int rs = v0;
                 if (s + LPA < end) {
-                    if (!MBF_OK_IDX(ck, 16, j1, 0, ck.n_atoms)) j1 = i;
-                    pn = ld_pack(pk, j1);
+                    j1 = chk_idx(j1, ck.n_atoms, i, flag);
+                    pn = ld_pos(S.pos, j1);
                     tn = __ldg(S.types + j1);
                 }
-                if (s + 2 * LPA < end && MBF_OK_IDX(ck, 15, s + 2 * LPA, 0, ck.n_slots)) j1 = nbr[s + 2 * LPA];
+                v0 = v1;
+                if (s + 2 * LPA < end) {
+                    j1 = nbr[s + 2 * LPA];
+                    v1 = rev[s + 2 * LPA];
+                }
                 double dx, dy, dz;
                 cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
-                double r2 = dx * dx + dy * dy + dz * dz;
-                if (!(r2 < rc2 && r2 > 1e-24)) continue;
-                if (ZHOU) {
-                    T r = pair_dist<T>(r2);
-                    T Sw, dSw;
-                    zswitch_fast<T>(r, Z, Sw, dSw);
-                    acc += (double)(zdens_only<T>(Z.sp[sj], r) * Sw);
-                } else {
-                    T v, dv;
-                    feval<T>(E, E.rho_f[sj], sqrt(r2), v, dv);
-                    acc += (double)v;
-                }
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                T to_i = T(0), to_j = T(0);
+                if (r2 < rc2 && r2 > 1e-24) P.dens(Z, si, sj, r2, to_i, to_j);
+                acc += (double)to_i;
+                if ((unsigned)rs < (unsigned)ck.n_slots) share[rs] = to_j;
+                else flag = 1;
             }
+            chk_flush(ck, flag, 11, i);
         }
         acc = group_sum<LPA>(acc);
         if (sub == 0 && i < S.n_atoms) aux[2 * (size_t)i] = acc;
     }
 }
 
-// F(rho-bar) and F'(rho-bar) in float64, rho-bar clamped at 0
-// (engine/_eam_kernels.py:268-274); kept out of the density loop so the
-// float64 pow/log of the embedding does not set that kernel's register count.
-__global__ void __launch_bounds__(256, 4) eam_embed(int n_atoms, const int *__restrict__ types, EamDev E, double4 *__restrict__ pk,
-                          double *__restrict__ aux, Chk ck) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_atoms) return;
-    if (!MBF_OK_IDX(ck, 41, types[i], 0, ck.ns)) return;
-    double acc = aux[2 * (size_t)i];
-    double rb = acc > 0.0 ? acc : 0.0;
+// rho-bar_a = a's upper-pair sum + the shares in a's lower slots, clamped at
+// 0 (engine/_eam_kernels.py:268-274); F(rho-bar) and F'(rho-bar) in float64;
+// the record {x, y, z, F'} every neighbour reads in the force pass.  A thread
+// per atom: its lower slots are one contiguous run, so the shares arrive
+// sector by sector, and the embedding's branches run on full warps.
+template <typename T>
+__global__ void __launch_bounds__(256, 4) eam_embed(SysView S, const int *__restrict__ row_off,
+                                                    const int *__restrict__ upper, EamDev E,
+                                                    const T *__restrict__ share, double4 *__restrict__ pk,
+                                                    double *__restrict__ aux, Chk ck) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= S.n_atoms) return;
+    int flag = 0;
+    int beg = row_off[a], up = upper[a];
+    if (!row_ok(beg, up, row_off[a + 1], ck.n_slots)) {
+        flag = 1;
+        beg = up = 0;
+    }
+    double s0 = 0.0, s1 = 0.0;
+    int q = beg;
+    for (; q + 1 < up; q += 2) {
+        s0 += (double)share[q];
+        s1 += (double)share[q + 1];
+    }
+    if (q < up) s0 += (double)share[q];
+    const int t = chk_idx(__ldg(S.types + a), ck.ns, 0, flag);
+    double rb = aux[2 * (size_t)a] + (s0 + s1);
+    rb = rb > 0.0 ? rb : 0.0;
     double F, dF;
-    embed64(E, E.F_f[types[i]], rb, F, dF);
-    pk[i].w = dF;
-    aux[2 * (size_t)i] = dF;
-    aux[2 * (size_t)i + 1] = F;
+    embed64(E, E.F_f[t], rb, F, dF);
+    const double3 p = ld_pos(S.pos, a);
+    pk[a] = make_double4(p.x, p.y, p.z, dF);
+    aux[2 * (size_t)a] = dF;
+    aux[2 * (size_t)a + 1] = F;
+    chk_flush(ck, flag, 41, a);
 }
 
 // Force pass over the upper half of every row: each unordered pair once.
-// The pair force on i is accumulated here; the one on j (its negative) is
-// written to j's own slot (j -> i) = rev(i -> j), so j's gather reads its row
-// contiguously.  Energy phi and the virial of the pair go to i, the lower
-// index.  SlotT is float in the mixed path (a per-pair term, accumulated in
-// float64 by the gather) and double in the float64 path.
-template <typename T> struct SlotVec;
-template <> struct SlotVec<double> { typedef double3 type; };
-template <> struct SlotVec<float> { typedef float3 type; };
-
-template <typename T, int LPA, bool ZHOU, bool ORTHO>
-__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1) eam_force(SysView S, const int *__restrict__ row_off,
-                                                       const int *__restrict__ upper,
-                                                       const int *__restrict__ nbr,
-                                                       const int *__restrict__ rev, EamDev E,
-                                                       const double4 *__restrict__ pk,
-                                                       const double *__restrict__ aux,
-                                                       typename SlotVec<T>::type *__restrict__ slot_f,
-                                                       double *__restrict__ f_local,
-                                                       double *__restrict__ per_atom, Chk ck) {
-    typedef typename SlotVec<T>::type V3;
+// The pair's force coefficient sc = c / r (c = phi' + F'_i rho'_{s_j} +
+// F'_j rho'_{s_i}) gives i the force sc d (d = r_j - r_i, minimum image), the
+// pair energy and the virial -sc d (x) d; sc goes to j's own slot (j -> i) =
+// rev(i -> j) (0 beyond the cutoff), from which j's gather rebuilds its share.
+// T is float in the mixed path (a per-pair term, accumulated in float64) and
+// double in the float64 path.
+template <typename T, int LPA, class Pol, bool ORTHO>
+__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
+    eam_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ upper,
+              const int *__restrict__ nbr, const int *__restrict__ rev, Pol P, double rc2,
+              const double4 *__restrict__ pk, const double *__restrict__ aux, T *__restrict__ coef,
+              double *__restrict__ f_local, double *__restrict__ per_atom, Chk ck) {
     __shared__ ZTab<T> Z;
-    if (ZHOU) load_ztab<T>(E, Z);
+    P.setup(Z);
     const int sub = threadIdx.x & (LPA - 1);
     const int gpb = EAM_BLOCK / LPA;
-    const double rc = E.r_cut, rc2 = rc * rc;
     for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
-        int i = base + threadIdx.x / LPA;
+        const int i = base + threadIdx.x / LPA;
         double fx = 0, fy = 0, fz = 0, e = 0;
         int npair = 0;
         double vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
         if (i < S.n_atoms) {
-            int si = S.types[i];
-            double4 pi = ld_pack(pk, i);
-            T Fp_i = (T)pi.w;
+            int flag = 0;
+            int up = upper[i], end = row_off[i + 1];
+            if (!row_ok(row_off[i], up, end, ck.n_slots)) {
+                flag = 1;
+                up = end = 0;
+            }
+            const int si = chk_idx(__ldg(S.types + i), ck.ns, 0, flag);
+            const double4 pi = ld_pack(pk, i);
+            const T Fp_i = (T)pi.w;
             CellView<ORTHO> cv;
             cv.load(S, i);
-            int end = row_off[i + 1];
-            int up = upper[i];
-            if (!MBF_OK_IDX(ck, 21, up, row_off[i], end + 1)) up = end;
-            // two-stage prefetch: slot indices two iterations ahead, the
-            // neighbour's record and species one ahead, so the record load
-            // never waits on the index load of the same iteration
             int s = up + sub;
-            int j0 = i, r0 = 0, j1 = i, r1 = 0;
-            if (s < end && MBF_OK_IDX(ck, 22, s, 0, ck.n_slots)) {
+            int j0 = i, v0 = 0, j1 = i, v1 = 0;
+            if (s < end) {
                 j0 = nbr[s];
-                r0 = rev[s];
+                v0 = rev[s];
             }
-            if (s + LPA < end && MBF_OK_IDX(ck, 25, s + LPA, 0, ck.n_slots)) {
+            if (s + LPA < end) {
                 j1 = nbr[s + LPA];
-                r1 = rev[s + LPA];
+                v1 = rev[s + LPA];
             }
-            if (!MBF_OK_IDX(ck, 23, j0, 0, ck.n_atoms)) j0 = i;
+            j0 = chk_idx(j0, ck.n_atoms, i, flag);
             double4 pn = ld_pack(pk, j0);
             int tn = __ldg(S.types + j0);
             for (; s < end; s += LPA) {
-                double4 pj = pn;
-                int sj = tn, rs = r0;
-                if (!MBF_OK_IDX(ck, 24, sj, 0, ck.ns)) sj = 0;
+                const double4 pj = pn;
+                const int sj = chk_idx(tn, ck.ns, 0, flag);
+                const int rs = v0;
                 if (s + LPA < end) {
-                    if (!MBF_OK_IDX(ck, 26, j1, 0, ck.n_atoms)) j1 = i;
+                    j1 = chk_idx(j1, ck.n_atoms, i, flag);
                     pn = ld_pack(pk, j1);
                     tn = __ldg(S.types + j1);
                 }
-                r0 = r1;
-                if (s + 2 * LPA < end && MBF_OK_IDX(ck, 25, s + 2 * LPA, 0, ck.n_slots)) {
+                v0 = v1;
+                if (s + 2 * LPA < end) {
                     j1 = nbr[s + 2 * LPA];
-                    r1 = rev[s + 2 * LPA];
+                    v1 = rev[s + 2 * LPA];
                 }
                 double dx, dy, dz;
                 cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
-                double r2 = dx * dx + dy * dy + dz * dz;
-                double px = 0, py = 0, pz = 0;
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                T sc = T(0);
                 if (r2 < rc2 && r2 > 1e-24) {
                     npair += 1;
-                    T r = pair_dist<T>(r2);
-                    T phi, dphi, drho_j, drho_i;
-                    if (ZHOU) {
-                        zhou_pair_terms<T>(Z, si, sj, r, phi, dphi, drho_j, drho_i);
-                    } else {
-                        double rr = sqrt(r2);
-                        T rj, ri;
-                        feval<T>(E, E.phi_f[si * E.ns + sj], rr, phi, dphi);
-                        feval<T>(E, E.rho_f[sj], rr, rj, drho_j);
-                        feval<T>(E, E.rho_f[si], rr, ri, drho_i);
-                    }
-                    T c = dphi + Fp_i * drho_j + (T)pj.w * drho_i;
-                    double sc = (double)fdiv<T>(c, r);
-                    px = sc * dx;
-                    py = sc * dy;
-                    pz = sc * dz;
+                    T phi, dphi, drj, dri, ir;
+                    P.pair(Z, si, sj, r2, phi, dphi, drj, dri, ir);
+                    const T c = dphi + Fp_i * drj + (T)pj.w * dri;
+                    sc = c * ir;
+                    const double scd = (double)sc;
+                    const double px = scd * dx, py = scd * dy, pz = scd * dz;
                     fx += px;
                     fy += py;
                     fz += pz;
@@ -546,12 +788,10 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1) 
                     vxz -= px * dz;
                     vyz -= py * dz;
                 }
-                V3 w;
-                w.x = (T)(-px);
-                w.y = (T)(-py);
-                w.z = (T)(-pz);
-                if (MBF_OK_IDX(ck, 27, rs, 0, ck.n_slots)) slot_f[rs] = w;
+                if ((unsigned)rs < (unsigned)ck.n_slots) coef[rs] = sc;
+                else flag = 1;
             }
+            chk_flush(ck, flag, 21, i);
         }
         fx = group_sum<LPA>(fx);
         fy = group_sum<LPA>(fy);
@@ -578,18 +818,18 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1) 
     }
 }
 
-// F_a = (pairs above a) + the forces its lower neighbours left in a's own
-// lower slots (contiguous reads), fused with the per-structure sums
-// (ChunkSums): a block per chunk of the reduction plan, 8 lanes per atom;
-// besides its atom's force each group adds the atom's record (entries sub
-// and sub + 8 of its 8 lanes), and the block finishes the chunk's and, if
-// last, the structure's sums.
-template <typename V3, int NT>
-__global__ void __launch_bounds__(NT) eam_gather_reduce(const int *__restrict__ row_off,
-                                                              const int *__restrict__ upper,
-                                                              const V3 *__restrict__ slot_f,
-                                                              const double *__restrict__ f_local,
-                                                              double *__restrict__ forces, ChunkSums cs, Chk ck) {
+// F_a = (pairs above a, from the force pass) + sum over a's lower slots of
+// coefficient x minimum-image vector to that neighbour (contiguous reads of
+// the row), fused with the per-structure sums (ChunkSums): a block per chunk
+// of the reduction plan, 8 lanes per atom; besides its atom's force each
+// group adds the atom's record (entries sub and sub + 8 of its 8 lanes), and
+// the block finishes the chunk's and, if last, the structure's sums.
+template <typename T, int NT, bool ORTHO>
+__global__ void __launch_bounds__(NT) eam_gather_reduce(SysView S, const int *__restrict__ row_off,
+                                                        const int *__restrict__ upper, const int *__restrict__ nbr,
+                                                        const T *__restrict__ coef, const double4 *__restrict__ pk,
+                                                        const double *__restrict__ f_local,
+                                                        double *__restrict__ forces, ChunkSums cs, Chk ck) {
     constexpr int LPA = 8, G = NT / LPA;
     const int c = blockIdx.x;
     const int s = cs.chunk[3 * c], a0 = cs.chunk[3 * c + 1], a1 = cs.chunk[3 * c + 2];
@@ -603,9 +843,9 @@ __global__ void __launch_bounds__(NT) eam_gather_reduce(const int *__restrict__ 
         nu = upper[a0 + grp];
     }
     for (int base = a0; base < a1; base += G) {  // uniform over the block
-        int a = base + grp;
-        const int beg = nb, rend = ne;
-        int up = nu;
+        const int a = base + grp;
+        int beg = nb, up = nu;
+        const int rend = ne;
         if (a + G < a1) {
             nb = row_off[a + G];
             ne = row_off[a + G + 1];
@@ -613,18 +853,29 @@ __global__ void __launch_bounds__(NT) eam_gather_reduce(const int *__restrict__ 
         }
         double fx = 0, fy = 0, fz = 0;
         if (a < a1) {
-            if (!MBF_OK_IDX(ck, 31, up, beg, rend + 1)) up = beg;
+            int flag = 0;
+            if (!row_ok(beg, up, rend, ck.n_slots)) {
+                flag = 1;
+                beg = up = 0;
+            }
+            CellView<ORTHO> cv;
+            cv.load(S, a);
+            const double4 pa = ld_pack(pk, a);
 #pragma unroll 4
             for (int q = beg + sub; q < up; q += LPA) {
-                if (!MBF_OK_IDX(ck, 32, q, 0, ck.n_slots)) break;
-                V3 w = slot_f[q];
-                fx += (double)w.x;
-                fy += (double)w.y;
-                fz += (double)w.z;
+                const int j = chk_idx(nbr[q], ck.n_atoms, a, flag);
+                const double cq = (double)coef[q];
+                const double4 pj = ld_pack(pk, j);
+                double dx, dy, dz;
+                cv.mic(pj.x - pa.x, pj.y - pa.y, pj.z - pa.z, dx, dy, dz);
+                fx += cq * dx;
+                fy += cq * dy;
+                fz += cq * dz;
             }
-            const double *pa = cs.per_atom + (size_t)a * ATOM_ACC;
-            r0 += pa[sub];
-            if (sub < ATOM_ACC - LPA) r1 += pa[LPA + sub];
+            chk_flush(ck, flag, 31, a);
+            const double *rec = cs.per_atom + (size_t)a * ATOM_ACC;
+            r0 += rec[sub];
+            if (sub < ATOM_ACC - LPA) r1 += rec[LPA + sub];
         }
         fx = group_sum<LPA>(fx);
         fy = group_sum<LPA>(fy);
@@ -641,140 +892,190 @@ __global__ void __launch_bounds__(NT) eam_gather_reduce(const int *__restrict__ 
 // Site terms (engine/site_terms.py:440-479): U_i = F_i(rho-bar_i) + 1/2
 // sum_j phi_ij and dU_i/dv_ij = (F'_i rho'_{s_j}(r) + 1/2 phi'(r)) v / r over
 // the full row, after the density and embedding passes; v for every slot.
-template <typename T, int LPA, bool ZHOU, bool ORTHO>
+template <typename T, class Pol, bool ORTHO>
 __global__ void __launch_bounds__(EAM_BLOCK) eam_site(SysView S, const int *__restrict__ row_off,
-                                                      const int *__restrict__ nbr, EamDev E,
+                                                      const int *__restrict__ nbr, Pol P, double rc2,
                                                       const double4 *__restrict__ pk,
                                                       const double *__restrict__ aux, SiteOut so, Chk ck) {
+    constexpr int LPA = 8;
     __shared__ ZTab<T> Z;
-    if (ZHOU) load_ztab<T>(E, Z);
+    P.setup(Z);
     const int sub = threadIdx.x & (LPA - 1);
     const int gpb = EAM_BLOCK / LPA;
-    const double rc = E.r_cut, rc2 = rc * rc;
     for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
-        int i = base + threadIdx.x / LPA;
+        const int i = base + threadIdx.x / LPA;
         double e = 0.0;
         if (i < S.n_atoms) {
-            int si = S.types[i];
-            if (!MBF_OK_IDX(ck, 51, si, 0, ck.ns)) si = 0;
+            int flag = 0;
+            int beg = row_off[i], end = row_off[i + 1];
+            if (!row_ok(beg, beg, end, ck.n_slots)) {
+                flag = 1;
+                beg = end = 0;
+            }
+            const int si = chk_idx(__ldg(S.types + i), ck.ns, 0, flag);
             CellView<ORTHO> cv;
             cv.load(S, i);
-            double4 pi = ld_pack(pk, i);
-            double Fp = aux[2 * (size_t)i];
-            int end = row_off[i + 1];
-            if (!MBF_OK_IDX(ck, 52, end, 0, ck.n_slots + 1)) end = row_off[i];
-            for (int s = row_off[i] + sub; s < end; s += LPA) {
-                int j = nbr[s];
-                if (!MBF_OK_IDX(ck, 53, j, 0, ck.n_atoms)) continue;
-                int sj = __ldg(S.types + j);
-                if (!MBF_OK_IDX(ck, 54, sj, 0, ck.ns)) sj = 0;
-                double4 pj = ld_pack(pk, j);
+            const double4 pi = ld_pack(pk, i);
+            const double Fp = aux[2 * (size_t)i];
+            for (int s = beg + sub; s < end; s += LPA) {
+                const int j = chk_idx(nbr[s], ck.n_atoms, i, flag);
+                const int sj = chk_idx(__ldg(S.types + j), ck.ns, 0, flag);
+                const double4 pj = ld_pack(pk, j);
                 double dx, dy, dz;
                 cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
-                double r2 = dx * dx + dy * dy + dz * dz;
-                size_t o = 3 * (size_t)s;
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                const size_t o = 3 * (size_t)s;
                 so.vec[o] = dx;
                 so.vec[o + 1] = dy;
                 so.vec[o + 2] = dz;
                 double c = 0.0;
                 if (r2 < rc2 && r2 > 1e-24) {
-                    T phi, dphi, drho_j, drho_i;
-                    if (ZHOU) {
-                        zhou_pair_terms<T>(Z, si, sj, pair_dist<T>(r2), phi, dphi, drho_j, drho_i);
-                    } else {
-                        double rr = sqrt(r2);
-                        T rj;
-                        feval<T>(E, E.phi_f[si * E.ns + sj], rr, phi, dphi);
-                        feval<T>(E, E.rho_f[sj], rr, rj, drho_j);
-                    }
-                    double r = sqrt(r2);
+                    T phi, dphi, drj, dri, ir;
+                    P.pair(Z, si, sj, r2, phi, dphi, drj, dri, ir);
                     e += 0.5 * (double)phi;
-                    c = (Fp * (double)drho_j + 0.5 * (double)dphi) / r;
+                    c = (Fp * (double)drj + 0.5 * (double)dphi) / sqrt(r2);
                 }
                 so.dudv[o] = c * dx;
                 so.dudv[o + 1] = c * dy;
                 so.dudv[o + 2] = c * dz;
             }
+            chk_flush(ck, flag, 51, i);
         }
         e = group_sum<LPA>(e);
         if (sub == 0 && i < S.n_atoms) so.e[i] = e + aux[2 * (size_t)i + 1];
     }
 }
 
-template <typename T, int LPA, bool ZHOU, bool ORTHO>
-static int eam_launch(const SysView &S, const mbf_nlist *nl, const EamDev &E, double4 *pk, double *aux,
-                      void *slot, double *f_local, double *forces, double *per_atom, Chk ck, const SiteOut &so,
-                      const ChunkSums &cs, int n_chunks, cudaStream_t st) {
-    typedef typename SlotVec<T>::type V3;
-    int gpb = EAM_BLOCK / LPA;
-    int blocks = (S.n_atoms + gpb - 1) / gpb;
-    PROF_BEGIN("eam_pack", st);
-    eam_pack<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S, pk);
-    PROF_END("eam_pack", st);
-    int g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_density<T, LPA, ZHOU, ORTHO>);
+// ---- host side ----------------------------------------------------------------
+
+struct EamBufs {
+    double4 *pk;
+    double *aux;
+    void *slot;  // per-slot density shares, then force coefficients (T each)
+    double *f_local;
+    double *forces;
+    double *per_atom;
+};
+
+template <typename T, int LPA, class Pol, bool ORTHO>
+static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const EamDev &E, double rc2,
+                      const EamBufs &B, Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks,
+                      cudaStream_t st) {
+    T *slot = static_cast<T *>(B.slot);
+    const int gpb = EAM_BLOCK / LPA;
+    const int blocks = (S.n_atoms + gpb - 1) / gpb;
+    int g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_density<T, LPA, Pol, ORTHO>);
     PROF_BEGIN("eam_density", st);
-    eam_density<T, LPA, ZHOU, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, E, pk, aux, ck);
+    eam_density<T, LPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, P, rc2,
+                                                             slot, B.aux, ck);
     PROF_END("eam_density", st);
     MBF_CHECK_LAUNCH();
     PROF_BEGIN("eam_embed", st);
-    eam_embed<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S.n_atoms, S.types, E, pk, aux, ck);
+    eam_embed<T><<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S, nl->row_off, nl->upper, E, slot, B.pk, B.aux, ck);
     PROF_END("eam_embed", st);
     MBF_CHECK_LAUNCH();
-    g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_force<T, LPA, ZHOU, ORTHO>);
+    g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_force<T, LPA, Pol, ORTHO>);
     PROF_BEGIN("eam_force", st);
-    eam_force<T, LPA, ZHOU, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, E, pk,
-                                                     aux, (V3 *)slot, f_local, per_atom, ck);
+    eam_force<T, LPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, P, rc2,
+                                                           B.pk, B.aux, slot, B.f_local, B.per_atom, ck);
     PROF_END("eam_force", st);
     MBF_CHECK_LAUNCH();
     PROF_BEGIN("eam_gather_reduce", st);
-    int nt = chunk_block(S.n_atoms, n_chunks);
+    const int nt = chunk_block(S.n_atoms, n_chunks);
     if (nt == 128)
-        eam_gather_reduce<V3, 128><<<n_chunks, 128, 0, st>>>(nl->row_off, nl->upper, (const V3 *)slot, f_local,
-                                                              forces, cs, ck);
+        eam_gather_reduce<T, 128, ORTHO><<<n_chunks, 128, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, slot, B.pk,
+                                                                   B.f_local, B.forces, cs, ck);
     else if (nt == 256)
-        eam_gather_reduce<V3, 256><<<n_chunks, 256, 0, st>>>(nl->row_off, nl->upper, (const V3 *)slot, f_local,
-                                                              forces, cs, ck);
+        eam_gather_reduce<T, 256, ORTHO><<<n_chunks, 256, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, slot, B.pk,
+                                                                   B.f_local, B.forces, cs, ck);
     else
-        eam_gather_reduce<V3, 512><<<n_chunks, 512, 0, st>>>(nl->row_off, nl->upper, (const V3 *)slot, f_local,
-                                                              forces, cs, ck);
+        eam_gather_reduce<T, 512, ORTHO><<<n_chunks, 512, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, slot, B.pk,
+                                                                   B.f_local, B.forces, cs, ck);
     PROF_END("eam_gather_reduce", st);
     MBF_CHECK_LAUNCH();
     if (so.e) {
-        g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_site<T, LPA, ZHOU, ORTHO>);
-        eam_site<T, LPA, ZHOU, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, E, pk, aux, so, ck);
+        g = persistent_grid((S.n_atoms + 15) / 16, EAM_BLOCK, (const void *)eam_site<T, Pol, ORTHO>);
+        eam_site<T, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, rc2, B.pk, B.aux, so, ck);
         MBF_CHECK_LAUNCH();
     }
     return MBF_OK;
 }
 
-template <typename T, bool ZHOU, bool ORTHO>
-static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E, double4 *pk,
-                            double *aux, void *slot, double *f_local, double *forces, double *per_atom,
-                            Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks, cudaStream_t st) {
-#define MBF_EAM_LAUNCH(L) \
-    eam_launch<T, L, ZHOU, ORTHO>(S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, cs, n_chunks, st)
+template <typename T, class Pol, bool ORTHO>
+static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const Pol &P, const EamDev &E,
+                            double rc2, const EamBufs &B, Chk ck, const SiteOut &so, const ChunkSums &cs,
+                            int n_chunks, cudaStream_t st) {
+#define MBF_EAM_LAUNCH(L) eam_launch<T, L, Pol, ORTHO>(S, nl, P, E, rc2, B, ck, so, cs, n_chunks, st)
     switch (lpa) {
         case 1: return MBF_EAM_LAUNCH(1);
         case 2: return MBF_EAM_LAUNCH(2);
         case 4: return MBF_EAM_LAUNCH(4);
         case 8: return MBF_EAM_LAUNCH(8);
-        case 16: return MBF_EAM_LAUNCH(16);
-        case 32: return MBF_EAM_LAUNCH(32);
         default: return MBF_ERR_ARGUMENT;
     }
 #undef MBF_EAM_LAUNCH
 }
 
-template <typename T>
-static int eam_dispatch(bool zhou, int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E,
-                        double4 *pk, double *aux, void *slot, double *f_local, double *forces,
-                        double *per_atom, Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks,
+template <typename T, class Pol>
+static int eam_dispatch(const Pol &P, int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E, double rc2,
+                        const EamBufs &B, Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks,
                         cudaStream_t st) {
-#define MBF_EAM_ARGS lpa, S, nl, E, pk, aux, slot, f_local, forces, per_atom, ck, so, cs, n_chunks, st
-    if (zhou)
-        return S.ortho ? eam_dispatch_lpa<T, true, true>(MBF_EAM_ARGS) : eam_dispatch_lpa<T, true, false>(MBF_EAM_ARGS);
-    return S.ortho ? eam_dispatch_lpa<T, false, true>(MBF_EAM_ARGS) : eam_dispatch_lpa<T, false, false>(MBF_EAM_ARGS);
-#undef MBF_EAM_ARGS
+    return S.ortho ? eam_dispatch_lpa<T, Pol, true>(lpa, S, nl, P, E, rc2, B, ck, so, cs, n_chunks, st)
+                   : eam_dispatch_lpa<T, Pol, false>(lpa, S, nl, P, E, rc2, B, ck, so, cs, n_chunks, st);
+}
+
+// The constants of the one- and two-element Zhou path from the host copies
+// of the tables; false when the tables have none, are not a fused Zhou set
+// or have more than two elements.  The element parameters are those of each
+// density row (ZHOU_KEYS order: r_e f_e rho_e rho_s alpha beta A B kappa
+// lambda ...); the switch is the shared one of the table.
+template <typename T>
+static bool make_zk(const mbf_eam_tables *tab, ZK<T> &K) {
+    if (!tab->zhou_fused || tab->ns < 1 || tab->ns > 2 || !tab->P_host || !tab->rho_f_host || !tab->phi_f_host)
+        return false;
+    const double LOG2E = 1.4426950408889634074;
+    for (int s = 0; s < 2; ++s) {
+        const double *p = tab->P_host + (size_t)tab->rho_f_host[s < tab->ns ? s : 0] * EAM_NCOL;
+        const double re = p[0], fe = p[1], alpha = p[4], beta = p[5];
+        ZEl<T> &q = K.el[s];
+        q.ire = (T)(1.0 / re);
+        q.lam = (T)p[9];
+        q.kap = (T)p[8];
+        q.beta = (T)beta;
+        q.alpha = (T)alpha;
+        q.eb0 = (T)(beta * LOG2E);
+        q.eb1 = (T)(-beta * LOG2E / re);
+        q.ea0 = (T)(alpha * LOG2E);
+        q.ea1 = (T)(-alpha * LOG2E / re);
+        q.fe = (T)fe;
+        q.fe_ire = (T)(fe / re);
+        q.A = (T)p[6];
+        q.B = (T)p[7];
+    }
+    const double *p0 = tab->P_host + (size_t)tab->rho_f_host[0] * EAM_NCOL;
+    const double rc = p0[2 * EAM_NZ], w = p0[2 * EAM_NZ + 1];
+    if (!(w > 0.0)) return false;
+    K.r0 = (T)(rc - w);
+    K.iw = (T)(1.0 / w);
+    K.m30iw = (T)(-30.0 / w);
+    double chi = 1.0;
+    if (tab->ns == 2) chi = tab->P_host[(size_t)tab->phi_f_host[1] * EAM_NCOL + 2 * EAM_NZ + 2];
+    K.half_chi = (T)(0.5 * chi);
+    return true;
+}
+
+template <typename T>
+static int eam_select(const mbf_eam_tables *tab, int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E,
+                      double rc2, const EamBufs &B, Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks,
+                      cudaStream_t st) {
+    ZK<T> K;
+    if (make_zk<T>(tab, K)) {
+        if (tab->ns == 1) return eam_dispatch<T>(PolZ2<T, 1>{K}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, st);
+        return eam_dispatch<T>(PolZ2<T, 2>{K}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, st);
+    }
+    if (tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP)
+        return eam_dispatch<T>(PolZSmem<T>{E}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, st);
+    return eam_dispatch<T>(PolGeneric<T>{E}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, st);
 }
 
 }  // namespace mbf
@@ -787,15 +1088,28 @@ static int eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
                     void *stream) {
     if (!sys || !nl || !tab || !plan || !workspace || !forces || !energy || !virial) return MBF_ERR_ARGUMENT;
     if (precision != MBF_FP64 && precision != MBF_MIXED) return MBF_ERR_ARGUMENT;
-    if (nl->n_atoms != sys->n_atoms || tab->ns <= 0) return MBF_ERR_ARGUMENT;
+    if (nl->n_atoms != sys->n_atoms || tab->ns <= 0 || sys->n_struct <= 0) return MBF_ERR_ARGUMENT;
+    if (nl->n_slots < 0 || nl->n_slots > 0x7fffff00LL) return MBF_ERR_ARGUMENT;
+    // the per-structure completion counters live in a region of n_chunks
+    // words; every structure owns at least one chunk
+    if (plan->n_chunks <= 0 || plan->n_chunks < sys->n_struct) return MBF_ERR_ARGUMENT;
+    const int lpa = lanes_per_atom > 0 ? lanes_per_atom : 8;
+    if (lpa != 1 && lpa != 2 && lpa != 4 && lpa != 8) return MBF_ERR_ARGUMENT;
     EvalLayout L = eval_layout(sys->n_atoms, nl->n_slots, plan->n_chunks);
     if (workspace_bytes < L.total) return MBF_ERR_WORKSPACE;
     cudaStream_t st = (cudaStream_t)stream;
+    Chk ck;
+    ck.err = ws_at<int>(workspace, L.err);
+    ck.n_atoms = sys->n_atoms;
+    ck.n_slots = (int)nl->n_slots;
+    ck.ns = tab->ns;
+    if (cudaMemsetAsync(ck.err, 0, ERR_CLEAR_BYTES, st) != cudaSuccess) return MBF_ERR_CUDA;
     if (sys->n_atoms == 0) {
         if (cudaMemsetAsync(energy, 0, sizeof(double) * sys->n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
         if (cudaMemsetAsync(virial, 0, sizeof(double) * 9 * sys->n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
         return MBF_OK;
     }
+    if (!nl->upper || !nl->row_off || !nl->nbr || !nl->rev) return MBF_ERR_ARGUMENT;
     SysView S = make_view(sys);
     EamDev E;
     E.ns = tab->ns; E.nf = tab->nf; E.nX = tab->nX;
@@ -803,32 +1117,21 @@ static int eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
     E.X = tab->X; E.C = tab->C;
     E.rho_f = tab->rho_f; E.F_f = tab->F_f; E.phi_f = tab->phi_f;
     E.r_cut = tab->r_cut;
-    if (!nl->upper) return MBF_ERR_ARGUMENT;
-    double *aux = ws_at<double>(workspace, L.atom_aux);
-    double *per_atom = ws_at<double>(workspace, L.per_atom);
-    double *partial = ws_at<double>(workspace, L.partial);
-    void *slot_f = ws_at<char>(workspace, L.slot);
-    Chk ck;
-    ck.err = ws_at<int>(workspace, L.err);
-    ck.n_atoms = sys->n_atoms;
-    if (nl->n_slots < 0 || nl->n_slots > 0x7fffff00LL) return MBF_ERR_ARGUMENT;
-    ck.n_slots = (int)nl->n_slots;
-    ck.ns = tab->ns;
-    if (cudaMemsetAsync(ck.err, 0, ERR_CLEAR_BYTES, st) != cudaSuccess) return MBF_ERR_CUDA;
-    double *f_local = ws_at<double>(workspace, L.f_local);
-    double4 *pk = ws_at<double4>(workspace, L.pack);
-    int lpa = lanes_per_atom > 0 ? lanes_per_atom : 8;
-    bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
-    ChunkSums cs = {plan->chunk, plan->chunk_first, per_atom, partial, energy, virial,
+    EamBufs B;
+    B.pk = ws_at<double4>(workspace, L.pack);
+    B.aux = ws_at<double>(workspace, L.atom_aux);
+    B.slot = ws_at<char>(workspace, L.slot);
+    B.f_local = ws_at<double>(workspace, L.f_local);
+    B.forces = forces;
+    B.per_atom = ws_at<double>(workspace, L.per_atom);
+    ChunkSums cs = {plan->chunk, plan->chunk_first, B.per_atom, ws_at<double>(workspace, L.partial), energy, virial,
                     ws_at<unsigned>(workspace, L.sdone)};
-    if (plan->n_chunks <= 0) return MBF_ERR_ARGUMENT;
     if (cudaMemsetAsync(cs.sdone, 0, sizeof(unsigned) * (size_t)sys->n_struct, st) != cudaSuccess)
         return MBF_ERR_CUDA;
+    const double rc2 = tab->r_cut * tab->r_cut;
     if (precision == MBF_FP64)
-        return eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, so, cs,
-                                    plan->n_chunks, st);
-    return eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, so, cs,
-                               plan->n_chunks, st);
+        return eam_select<double>(tab, lpa, S, nl, E, rc2, B, ck, so, cs, plan->n_chunks, st);
+    return eam_select<float>(tab, lpa, S, nl, E, rc2, B, ck, so, cs, plan->n_chunks, st);
 }
 
 extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
@@ -865,9 +1168,12 @@ static __device__ __align__(256) unsigned char g_eam_scratch[MBF_STATIC_SCRATCH_
 
 namespace mbf {
 
-// Device address of g_eam_scratch, looked up once per device.  Host code
-// must not use the array's name as a pointer: on the host it is only a
-// stand-in symbol, not a device address.
+// Device address of g_eam_scratch, looked up once per device (with that
+// device current) and kept for the life of the process.  Host code must not
+// use the array's name as a pointer: on the host it is only a stand-in
+// symbol, not a device address.  The cached address belongs to the device's
+// primary context, so a cudaDeviceReset() in the process invalidates it:
+// callers of the no-allocation entry must not reset the device.
 static std::mutex g_scratch_mu;
 static void *g_scratch_ptr[64];
 
@@ -889,54 +1195,29 @@ static int scratch_address(void **out) {
 extern "C" int mbf_eam_eval_static(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
                                    const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
                                    double *forces, double *energy, double *virial, void *stream) {
-    if (!sys || !nl || !tab || !plan || !forces || !energy || !virial) return MBF_ERR_ARGUMENT;
-    if (precision != MBF_FP64 && precision != MBF_MIXED) return MBF_ERR_ARGUMENT;
-    if (nl->n_atoms != sys->n_atoms || tab->ns <= 0) return MBF_ERR_ARGUMENT;
-    EvalLayout L = eval_layout(sys->n_atoms, nl->n_slots, plan->n_chunks);
-    if (L.total > (size_t)MBF_STATIC_SCRATCH_BYTES) return MBF_ERR_SCRATCH_LIMIT;
+    if (!sys || !nl || !plan) return MBF_ERR_ARGUMENT;
+    if (nl->n_slots < 0 || plan->n_chunks <= 0) return MBF_ERR_ARGUMENT;
+    if (eval_layout(sys->n_atoms, nl->n_slots, plan->n_chunks).total > (size_t)MBF_STATIC_SCRATCH_BYTES)
+        return MBF_ERR_SCRATCH_LIMIT;
+    void *workspace = nullptr;
+    int rc = scratch_address(&workspace);
+    if (rc != MBF_OK) return rc;
+    // the array keeps the previous call's contents: eam_eval clears the
+    // error words and the completion counters at its start; every other
+    // region is written before it is read
+    SiteOut none = {nullptr, nullptr, nullptr};
+    return eam_eval(sys, nl, tab, plan, precision, lanes_per_atom, workspace, MBF_STATIC_SCRATCH_BYTES, forces,
+                    energy, virial, none, stream);
+}
+
+extern "C" int mbf_eam_eval_static_status(int *host_words, void *stream) {
+    if (!host_words) return MBF_ERR_ARGUMENT;
     void *workspace = nullptr;
     int rc = scratch_address(&workspace);
     if (rc != MBF_OK) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    if (sys->n_atoms == 0) {
-        if (cudaMemsetAsync(energy, 0, sizeof(double) * sys->n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
-        if (cudaMemsetAsync(virial, 0, sizeof(double) * 9 * sys->n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
-        return MBF_OK;
-    }
-    SysView S = make_view(sys);
-    EamDev E;
-    E.ns = tab->ns; E.nf = tab->nf; E.nX = tab->nX;
-    E.codes = tab->codes; E.P = tab->P; E.xo = tab->xo; E.nx = tab->nx;
-    E.X = tab->X; E.C = tab->C;
-    E.rho_f = tab->rho_f; E.F_f = tab->F_f; E.phi_f = tab->phi_f;
-    E.r_cut = tab->r_cut;
-    if (!nl->upper) return MBF_ERR_ARGUMENT;
-    double *aux = ws_at<double>(workspace, L.atom_aux);
-    double *per_atom = ws_at<double>(workspace, L.per_atom);
-    double *partial = ws_at<double>(workspace, L.partial);
-    void *slot_f = ws_at<char>(workspace, L.slot);
-    Chk ck;
-    ck.err = ws_at<int>(workspace, L.err);
-    ck.n_atoms = sys->n_atoms;
-    if (nl->n_slots < 0 || nl->n_slots > 0x7fffff00LL) return MBF_ERR_ARGUMENT;
-    ck.n_slots = (int)nl->n_slots;
-    ck.ns = tab->ns;
-    // the scratch keeps the previous call's contents: the error words must
-    // start at zero (the reduction clears its own counters); every other
-    // region is fully written before it is read
-    if (cudaMemsetAsync(ck.err, 0, ERR_CLEAR_BYTES, st) != cudaSuccess) return MBF_ERR_CUDA;
-    double *f_local = ws_at<double>(workspace, L.f_local);
-    double4 *pk = ws_at<double4>(workspace, L.pack);
-    int lpa = lanes_per_atom > 0 ? lanes_per_atom : 8;
-    bool zhou = tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP;
-    ChunkSums cs = {plan->chunk, plan->chunk_first, per_atom, partial, energy, virial,
-                    ws_at<unsigned>(workspace, L.sdone)};
-    if (plan->n_chunks <= 0) return MBF_ERR_ARGUMENT;
-    if (cudaMemsetAsync(cs.sdone, 0, sizeof(unsigned) * (size_t)sys->n_struct, st) != cudaSuccess)
+    if (cudaMemcpyAsync(host_words, workspace, 4 * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
         return MBF_ERR_CUDA;
-    if (precision == MBF_FP64)
-        return eam_dispatch<double>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, SiteOut{},
-                                    cs, plan->n_chunks, st);
-    return eam_dispatch<float>(zhou, lpa, S, nl, E, pk, aux, slot_f, f_local, forces, per_atom, ck, SiteOut{}, cs,
-                               plan->n_chunks, st);
+    return MBF_OK;
 }

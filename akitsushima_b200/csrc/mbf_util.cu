@@ -174,7 +174,9 @@ __global__ void __launch_bounds__(NT) gather_reduce_rows(const int *__restrict__
 int gather_reduce(int n_struct, int n_atoms, const int *row_off, const double *G, const double *f_local,
                   double *forces, const double *per_atom, const mbf_reduce_plan *plan, double *partial,
                   double *energy, double *virial, unsigned *sdone, cudaStream_t st) {
-    if (plan->n_chunks <= 0 || n_struct <= 0 || !sdone) return MBF_ERR_ARGUMENT;
+    // the completion counters live in a region of n_chunks words; every
+    // structure owns at least one chunk
+    if (plan->n_chunks <= 0 || n_struct <= 0 || plan->n_chunks < n_struct || !sdone) return MBF_ERR_ARGUMENT;
     if (cudaMemsetAsync(sdone, 0, sizeof(unsigned) * (size_t)n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
     ChunkSums cs = {plan->chunk, plan->chunk_first, per_atom, partial, energy, virial, sdone};
     PROF_BEGIN("gather_reduce", st);

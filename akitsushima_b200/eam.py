@@ -252,10 +252,16 @@ class EAMPotential(DevicePotential):
                 switches.add((float(rc), float(w)))
         X = np.concatenate(Xs) if Xs else np.zeros(1)
         C = np.concatenate(Cs, axis=1) if Cs else np.zeros((4, 1))
+        # the fused kernels take each element's parameters from its density
+        # row, so every pair row must carry the same element parameters
         fused = (ns <= 8 and len(switches) == 1
                  and all(codes[rho_f[a]] == 3 and codes[F_f[a]] == 6 for a in range(ns))
                  and all(codes[phi_f[a, b]] == (4 if a == b else 5)
-                         for a in range(ns) for b in range(ns)))
+                         for a in range(ns) for b in range(ns))
+                 and all(np.array_equal(P[phi_f[a, a], :_NZ], P[rho_f[a], :_NZ]) for a in range(ns))
+                 and all(np.array_equal(P[phi_f[a, b], :_NZ], P[rho_f[a], :_NZ])
+                         and np.array_equal(P[phi_f[a, b], _NZ:2 * _NZ], P[rho_f[b], :_NZ])
+                         for a in range(ns) for b in range(a + 1, ns)))
         return dict(codes=codes, P=P, xo=xo, nx=nx, X=X, C=np.ascontiguousarray(C),
                     rho_f=np.array(rho_f, np.int32), F_f=np.array(F_f, np.int32),
                     phi_f=phi_f, fused=fused)
@@ -264,14 +270,20 @@ class EAMPotential(DevicePotential):
         t = self.function_table()
         keep = {k: torch.as_tensor(np.ascontiguousarray(v), device=device)
                 for k, v in t.items() if k != "fused"}
+        # host copies of P, rho_f, phi_f: with them a one- or two-element
+        # Zhou table runs with its constants as kernel arguments
+        host = {k: np.ascontiguousarray(t[k], dtype=np.float64 if k == "P" else np.int32)
+                for k in ("P", "rho_f", "phi_f")}
+        keep.update({k + "_host": v for k, v in host.items()})
         st = _lib.MbfEamTables(len(self.species), int(len(t["codes"])), int(t["X"].shape[0]),
                                *[_lib.ptr(keep[k]) for k in ("codes", "P", "xo", "nx", "X", "C",
                                                              "rho_f", "F_f", "phi_f")],
-                               self.r_cut, 1 if t["fused"] else 0)
+                               self.r_cut, 1 if t["fused"] else 0,
+                               *[host[k].ctypes.data for k in ("P", "rho_f", "phi_f")])
         return (st, keep)
 
     sites_entry = "mbf_eam_eval_sites"
-    lane_choices = (1, 2, 4, 8, 16, 32)
+    lane_choices = (1, 2, 4, 8)
     # lanes of one atom's group: 2 measured fastest on B200 (256k Cu-Ni, both precisions)
     lanes_per_atom = 2
 

@@ -41,42 +41,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-FCC = np.array([[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0]], float)
 METRIC = "atom-force-evals/s"
 
-
-def make_cuni(n_cells=40, a=3.58, sigma=0.08, seed=0):
-    rng = np.random.default_rng(seed)
-    g = np.arange(n_cells)
-    cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
-    frac = (FCC[None] + cells[:, None]).reshape(-1, 3)
-    pos = frac * a + rng.normal(0.0, sigma, frac.shape)
-    ids = np.random.default_rng(seed + 1).integers(0, 2, len(pos)).astype(np.int32)
-    return np.eye(3) * a * n_cells, pos, ids
-
-
-DIAMOND = np.array([[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0],
-                    [0.25, 0.25, 0.25], [0.25, 0.75, 0.75], [0.75, 0.25, 0.75],
-                    [0.75, 0.75, 0.25]], float)
-
-
-def make_si_set(n=512, a=5.431, strain=0.03, sigma=0.1, seed=0):
-    """Uneven strained Si diamond supercells: (lattice, positions, types)."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for _ in range(n):
-        reps = rng.integers(1, 5, size=3)
-        g = [np.arange(r) for r in reps]
-        cells = np.stack(np.meshgrid(*g, indexing="ij"), -1).reshape(-1, 3)
-        frac = (DIAMOND[None] + cells[:, None]).reshape(-1, 3)
-        lat = np.diag(reps.astype(float)) * a
-        pos = frac * a
-        e = rng.uniform(-strain, strain, (3, 3))
-        m = np.eye(3) + 0.5 * (e + e.T)
-        lat, pos = lat @ m, pos @ m
-        pos = pos + rng.normal(0.0, sigma, pos.shape)
-        out.append((lat, pos, ["Si"] * len(pos)))
-    return out
+from akitsushima_b200.workloads import (make_cuni, make_gesn, make_ni3al_set, make_si,  # noqa: E402
+                                        make_si_set, make_sic_set)
 
 
 def _ncu_traffic(kernel, workload, precision):
@@ -174,9 +142,18 @@ class ClockSampler:
         return out
 
 
-def time_reference(lat, pos, ids, steps, warmup):
+def emit(args, line):
+    """Print the JSON line, or keep it when the caller collects sub-records."""
+    if getattr(args, "collect", None) is not None:
+        args.collect.append(line)
+    else:
+        print(json.dumps(line), flush=True)
+
+
+def time_reference(lat, pos, ids, steps, warmup, result=None):
     """The CPU port of the reference's numba path (oracle/): numpy prep and
-    C kernels under OpenMP with every host thread, prebuilt neighbour list."""
+    C kernels under OpenMP with every host thread, prebuilt neighbour list.
+    ``result`` (a list) receives the last call's (E, F, S)."""
     import oracle
     from akitsushima_b200.published_parameters import ZHOU_2004
     threads = cpu_count()
@@ -189,8 +166,10 @@ def time_reference(lat, pos, ids, steps, warmup):
     ts = []
     for _ in range(steps):
         t0 = time.perf_counter()
-        oracle.eam(spec, lat, pos, types, (i, j))
+        out = oracle.eam(spec, lat, pos, types, (i, j))
         ts.append(time.perf_counter() - t0)
+    if result is not None:
+        result.append(out)
     return float(np.mean(ts)), threads
 
 def time_reference_batched(structs, n_sample):
@@ -390,17 +369,8 @@ def run_batched(args, world, rank, local):
              "speedup_of_batched": ms_single / ms},
             "kernels": {k: {"launches": c, "ms_per_launch": t / c} for k, (c, t) in prof.items()},
             "e2e": e2e, "cpu_baseline": cpu, "roofline": None}
-    print(json.dumps(line), flush=True)
+    emit(args, line)
     return 0
-
-def make_si(n_cells, a=5.431, sigma=0.05, seed=0):
-    rng = np.random.default_rng(seed)
-    g = np.arange(n_cells)
-    cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
-    frac = (DIAMOND[None] + cells[:, None]).reshape(-1, 3)
-    pos = frac * a + rng.normal(0.0, sigma, frac.shape)
-    return np.eye(3) * a * n_cells, pos, ["Si"] * len(pos)
-
 
 MD_WORKLOADS = {
     # name: (potential, cells, sigma, precision, MD steps per bench step)
@@ -574,34 +544,8 @@ def run_md(args, world, rank, local):
                        "max_skin_displacement": float(res["skin_displacement"].max()),
                        "rebuilds": int(res["rebuilds"])},
             "e2e": e2e, "cpu_baseline": cpu, "roofline": None}
-    print(json.dumps(line), flush=True)
+    emit(args, line)
     return 0
-
-
-SIC_ZB = np.array([[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0],
-                   [0.25, 0.25, 0.25], [0.25, 0.75, 0.75], [0.75, 0.25, 0.75],
-                   [0.75, 0.75, 0.25]], float)
-
-
-def make_sic_set(n=256, a=4.36, strain=0.02, sigma=0.1, seed=0):
-    """Zincblende SiC, 2^3 or 3^3 conventional cells (64 or 216 atoms),
-    symmetric strain entries uniform +-2 %, Gaussian displacements."""
-    rng = np.random.default_rng(seed)
-    types8 = ["Si"] * 4 + ["C"] * 4
-    out = []
-    for _ in range(n):
-        m = int(rng.integers(2, 4))
-        g = np.arange(m)
-        cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
-        frac = (SIC_ZB[None] + cells[:, None]).reshape(-1, 3)
-        lat = np.eye(3) * a * m
-        pos = frac * a
-        e = rng.uniform(-strain, strain, (3, 3))
-        M = np.eye(3) + 0.5 * (e + e.T)
-        lat, pos = lat @ M, pos @ M
-        pos = pos + rng.normal(0.0, sigma, pos.shape)
-        out.append((lat, pos, types8 * len(cells)))
-    return out
 
 
 def _fit_setup():
@@ -617,29 +561,6 @@ def _fit_setup():
     xt = np.array([np.log(np.exp(x) * f) if key in ps._LOG_KEYS else x * f
                    for x, f, (_, key, _) in zip(x0, u, ps.variables)])
     return ps, x0, xt
-
-
-def make_ni3al_set(n=256, a=3.57, strain=0.02, sigma=0.08, seed=0):
-    """L1_2 Ni3Al (Al on the cube corners), 4^3 or 5^3 conventional cells
-    (256 or 500 atoms), symmetric strain entries uniform +-2 %, Gaussian
-    displacements."""
-    rng = np.random.default_rng(seed)
-    fcc = np.array([[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0]], float)
-    types4 = ["Al", "Ni", "Ni", "Ni"]
-    out = []
-    for _ in range(n):
-        m = int(rng.integers(4, 6))
-        g = np.arange(m)
-        cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
-        frac = (fcc[None] + cells[:, None]).reshape(-1, 3)
-        lat = np.eye(3) * a * m
-        pos = frac * a
-        e = rng.uniform(-strain, strain, (3, 3))
-        M = np.eye(3) + 0.5 * (e + e.T)
-        lat, pos = lat @ M, pos @ M
-        pos = pos + rng.normal(0.0, sigma, pos.shape)
-        out.append((lat, pos, types4 * len(cells)))
-    return out
 
 
 def _fit_setup_multi():
@@ -869,15 +790,8 @@ def run_fit(args, world, rank, local):
                     "path": "PotentialFit.loss_and_grad(numpy x) -> (loss, numpy gradient)"},
             "check": {"loss": float(loss), "grad_norm": float(np.linalg.norm(grad))},
             "cpu_baseline": cpu, "roofline": None}
-    print(json.dumps(line), flush=True)
+    emit(args, line)
     return 0
-
-
-def _gesn(n_cells=20, a=5.762, sigma=0.1, seed=0, frac_sn=0.25):
-    lat, pos, _ = make_si(n_cells, a=a, sigma=sigma, seed=seed)
-    types = [str(t) for t in np.random.default_rng(seed + 1).choice(["Ge", "Sn"], len(pos),
-                                                                    p=[1 - frac_sn, frac_sn])]
-    return lat, pos, types
 
 
 def _perf_case(name, precision):
@@ -901,7 +815,7 @@ def _perf_case(name, precision):
             return oracle.eam(ospec, L, P, T, pairs)
         desc = "Zhou 2004 Cu-Ni as setfl cubic splines (2000 r and rho knots), fcc 40^3"
     else:
-        lat, pos, types = _gesn()
+        lat, pos, types = make_gesn()
         pot = ak.StillingerWeberPotential(SW_GESN_TOMITA_2018, species=["Ge", "Sn"], precision=precision)
         recs = {(r["i"], r["j"], r["k"]): {k: v for k, v in r.items() if k not in "ijk"}
                 for r in SW_GESN_TOMITA_2018}
@@ -1021,7 +935,7 @@ def run_perf_path(args, world, rank, local):
                     "d2h_bytes_per_step": n_atoms * 24 + 80, "ms_per_step": t_e2e * 1e3,
                     "path": "force_fn(lattice, numpy positions, species names, NeighbourList) -> numpy"},
             "cpu_baseline": cpu, "roofline": None}
-    print(json.dumps(line), flush=True)
+    emit(args, line)
     return 0
 
 
@@ -1039,7 +953,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--cells", type=int, default=40)
-    ap.add_argument("--lanes", type=int, default=2, help="EAM lanes per atom (1, 2, 4, 8, 16, 32)")
+    ap.add_argument("--lanes", type=int, default=2, help="EAM lanes per atom (1, 2, 4 or 8)")
+    ap.add_argument("--no-sub-records", action="store_true",
+                    help="default workload: skip the other configurations' sub-records")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=200)
     ap.add_argument("--skip-singles", action="store_true",
@@ -1135,6 +1051,25 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = world * n_atoms / (ms * 1e-3)
+    res_main = (float(out.energy[0]), out.forces.cpu().numpy(), out.virial[0].cpu().numpy())
+
+    # the other precision on the same inputs and list (the float64 GPU path
+    # the mixed one is measured against), timed the same way after the
+    # timed region
+    other = "fp64" if args.precision == "mixed" else "mixed"
+    out_o = pot.evaluate(batch, dnl, precision=other)
+    for _ in range(3):
+        pot.evaluate(batch, dnl, precision=other, out=out_o)
+    n_o = max(3, min(args.steps, 10))
+    ev_o = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n_o)]
+    for k in range(n_o):
+        flush.zero_()
+        ev_o[k][0].record()
+        pot.evaluate(batch, dnl, precision=other, out=out_o)
+        ev_o[k][1].record()
+    torch.cuda.synchronize()
+    ms_o = sum(a.elapsed_time(b) for a, b in ev_o) / n_o
+    res_other = (float(out_o.energy[0]), out_o.forces.cpu().numpy(), out_o.virial[0].cpu().numpy())
 
     # per-kernel breakdown: a second identical pass under the launch profiler
     _lib.profile_begin()
@@ -1174,6 +1109,7 @@ def main():
     cross = (tp[pi] != tp[pj]) & inside
     n_in = int(inside.sum().item())
     n_cross = int(cross.sum().item())
+    del pi, pj, d, s, r, inside, cross
     force_flops = roofline.eam_force_flops(n_in - n_cross, n_cross)
     force_bytes = roofline.eam_force_bytes(n_atoms, dnl.n_slots)
     dom = "eam_force"
@@ -1193,6 +1129,8 @@ def main():
     except (OSError, KeyError, ValueError):
         hbm_peak, hbm_src = 6650.0, "fallback"
     ach_gbs = force_bytes / t_dom / 1e9
+    dens_flops = roofline.eam_density_flops(n_in, n_atoms)
+    t_all = sum(t for _, t in prof.values()) / args.steps * 1e-3
     roof = {"kernel": dom, "bound": "fp32" if args.precision == "mixed" else "fp64",
             "achieved": ach_tf, "peak": peak_tf, "unit": "TFLOP/s", "frac": ach_tf / peak_tf,
             "peak_source": "measured live on this GPU: mbf_peak_probe FMA chains",
@@ -1202,42 +1140,92 @@ def main():
             "hbm_view": {"achieved": ach_gbs, "peak": hbm_peak, "unit": "GB/s",
                          "frac": ach_gbs / hbm_peak, "peak_source": hbm_src,
                          "algorithmic_bytes_per_launch": force_bytes},
+            "whole_step": {"algorithmic_flops": force_flops + dens_flops,
+                           "kernels_ms": t_all * 1e3,
+                           "frac": (force_flops + dens_flops) / t_all / 1e12 / peak_tf,
+                           "note": "density + force algorithmic FLOPs over the sum of the step's kernel "
+                                   "times, against the same FMA peak"},
             "kernels": {k: {"launches": c, "ms_per_launch": t / c} for k, (c, t) in prof.items()}}
 
-    # end to end through the public API, host arrays in and out
-    nl = ak.NeighbourList(fn.r_cut, skin_width=0.3, device=dev)
+    # end to end through the public API in the reference's call form: host
+    # lattice and positions, atom_types a list of species names (the same
+    # list object every call, as the reference's solvers pass it), host
+    # (E, F (N, 3), stress) back
+    nl = ak.NeighbourList(fn.r_cut, skin_width=0.3)
     nl.build_batch(batch)
     pos_host = np.ascontiguousarray(pos)
-    for _ in range(args.warmup):   # the same warm-up as the device-timed steps
-        fn(lat, pos_host, ids, nl)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    calls = []
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        c0 = time.perf_counter()
-        e, f, st = fn(lat, pos_host, ids, nl)
-        calls.append(time.perf_counter() - c0)
-    t_e2e = (time.perf_counter() - t0) / args.e2e_steps
-    if dist:
-        t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    names = [("Cu", "Ni")[t] for t in ids.tolist()]
+
+    def e2e_loop(types, n):
+        for _ in range(args.warmup):   # the same warm-up as the device-timed steps
+            fn(lat, pos_host, types, nl)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        calls = []
+        t0 = time.perf_counter()
+        for _ in range(n):
+            c0 = time.perf_counter()
+            r_ = fn(lat, pos_host, types, nl)
+            calls.append(time.perf_counter() - c0)
+        t_ = (time.perf_counter() - t0) / n
+        if dist:
+            tt = torch.tensor([t_], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t_ = float(tt.item())
+        return t_, calls, r_
+
+    t_e2e, calls, (e, f, st) = e2e_loop(names, args.e2e_steps)
+    t_ids, calls_ids, _ = e2e_loop(ids, args.e2e_steps)
+    # per call: positions in (the species ids are uploaded once: an
+    # unchanged list maps to the same ids and is not sent again; the lattice
+    # is compared on the host), forces out plus one copy of energy, virial
+    # and the two device status words
     e2e = {"value": world * n_atoms / t_e2e, "unit": "atoms/s",
-           "h2d_bytes_per_step": n_atoms * (24 + 4), "d2h_bytes_per_step": n_atoms * 24 + 8 + 72,
+           "h2d_bytes_per_step": n_atoms * 24, "d2h_bytes_per_step": n_atoms * 24 + 8 * (1 + 9 + 2),
            "ms_per_step": t_e2e * 1e3,
            "ms_per_call_min_median_max": [round(1e3 * float(np.min(calls)), 4),
                                           round(1e3 * float(np.median(calls)), 4),
                                           round(1e3 * float(np.max(calls)), 4)],
-           "path": "force_fn(lattice, numpy positions, species ids, NeighbourList) -> numpy"}
+           "path": "force_fn(lattice, numpy positions, list of species names, NeighbourList) -> numpy "
+                   "(the reference's call form)",
+           "with_int_ids": {"value": world * n_atoms / t_ids, "ms_per_step": t_ids * 1e3,
+                            "path": "the same call with an int32 species-id array"}}
 
     cpu = None
+    oracle_res = []
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        t_cpu, threads = time_reference(lat, pos, ids, steps=2, warmup=1)
+        t_cpu, threads = time_reference(lat, pos, ids, steps=2, warmup=1, result=oracle_res)
         cpu = {"value": n_atoms / t_cpu, "unit": "atoms/s", "cores": threads, "kind": "port",
                "sample": "2 full force calls of the same structure (after 1 warm-up), oracle port "
                          "of the reference's numba EAM path, prebuilt neighbour list"}
+
+    # each result's error: against the float64 oracle (the CPU port, same
+    # pairs) when it ran, and mixed against the float64 GPU path always
+    vol = abs(float(np.linalg.det(lat)))
+
+    def err(a, b):
+        return {"max_force_eVA": float(np.abs(a[1] - b[1]).max()),
+                "energy_per_atom_eV": abs(a[0] - b[0]) / n_atoms,
+                "stress_eVA3": float(np.abs((np.asarray(a[2]) - np.asarray(b[2])).reshape(-1)).max()) / vol}
+
+    res = {args.precision: res_main, other: res_other}
+    errors = {"tolerance": {"max_force_eVA": 1e-5, "energy_per_atom_eV": 1e-6, "stress_eVA3": 1e-5,
+                            "fp64_relative": 1e-10},
+              "mixed_vs_fp64_gpu": err(res["mixed"], res["fp64"])}
+    if oracle_res:
+        e0, f0, s0 = oracle_res[0]
+        ref = (e0, f0, np.asarray(s0) * vol)   # the oracle's stress is already / V
+        errors["mixed_vs_fp64_oracle"] = err(res["mixed"], ref)
+        errors["fp64_gpu_vs_fp64_oracle"] = err(res["fp64"], ref)
+    ms64 = ms if args.precision == "fp64" else ms_o
+    fp64_gpu = {"ms_per_step": ms64, "value": world * n_atoms / (ms64 * 1e-3),
+                "mixed_speedup": (ms_o / ms) if args.precision == "mixed" else (ms / ms_o),
+                "note": "the float64 GPU path on the same inputs and list, CUDA events, L2 flushed"}
+
+    subs = None
+    if world == 1 and not args.no_sub_records:
+        subs = sub_records(args)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -1249,10 +1237,56 @@ def main():
             "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
             "config": cfg, "gpu_launches": int(round(launches_per_step * args.steps)),
             "gpu_launches_per_step": launches_per_step, "clocks": clocks, "roofline": roof, "nl_build": nl_build,
-            "e2e": e2e, "cpu_baseline": cpu,
-            "check": {"energy_per_atom": e / n_atoms, "max_abs_force_sum": float(np.abs(f.sum(0)).max())}}
+            "fp64_gpu": fp64_gpu, "errors": errors, "e2e": e2e, "cpu_baseline": cpu,
+            "check": {"energy_per_atom": e / n_atoms, "max_abs_force_sum": float(np.abs(f.sum(0)).max())},
+            "configs": subs}
     print(json.dumps(line), flush=True)
     return 0
+
+
+# The other configurations, measured inside the default run and attached to
+# its line (steps kept small so the whole run stays within a few minutes).
+SUB_RECORDS = (
+    ("fit_sic256", {"steps": 10, "warmup": 3, "e2e_steps": 10}),
+    ("batched_si512", {"steps": 10, "warmup": 3, "e2e_steps": 5}),
+    ("md_tersoff_si4096", {"steps": 10, "warmup": 3, "e2e_steps": 1}),
+    ("md_sw_si64k", {"steps": 5, "warmup": 3, "e2e_steps": 1}),
+)
+
+
+def _summary(line):
+    keep = ("metric", "value", "unit", "ms_per_step", "ms_per_md_step", "dtype", "structures_per_s",
+            "per_structure_launches", "gpu_launches_per_step", "energy", "atom_force_evals_per_s",
+            "n_variables", "check")
+    out = {k: line[k] for k in keep if k in line}
+    out["workload"] = line["config"].get("workload")
+    e = line.get("e2e") or {}
+    out["e2e"] = {k: e.get(k) for k in ("value", "unit", "ms_per_step", "h2d_bytes_per_step",
+                                          "d2h_bytes_per_step", "path")}
+    c = line.get("cpu_baseline")
+    if c:
+        out["cpu_baseline"] = c
+        out["vs_cpu_port"] = line["value"] / c["value"]
+    return out
+
+
+def sub_records(args):
+    out = {}
+    for wl, over in SUB_RECORDS:
+        a = argparse.Namespace(**vars(args))
+        a.workload, a.collect, a.precision, a.precision_given = wl, [], "mixed", False
+        a.skip_singles = False
+        for k, v in over.items():
+            setattr(a, k, v)
+        t0 = time.perf_counter()
+        try:
+            fn = run_fit if wl in FIT_WORKLOADS else run_md if wl in MD_WORKLOADS else run_batched
+            fn(a, 1, 0, 0)
+            out[wl] = _summary(a.collect[0])
+        except Exception as exc:  # a failed sub-record is reported, not fatal
+            out[wl] = {"error": f"{type(exc).__name__}: {exc}"}
+        out[wl]["wall_s"] = round(time.perf_counter() - t0, 2)
+    return out
 
 
 if __name__ == "__main__":

@@ -10,7 +10,7 @@
  * Each entry point replaces one interface of the reference (akitsushima
  * 0.4.0a4, Python + numba); the citation is given beside it.  The reference
  * has no native ABI of its own, so these functions are what a ctypes / cffi
- * binding from its Python layer would call (see INTEGRATION.md).
+ * binding from its Python layer would call.
  *
  * Units: A, eV, eV/A; the virial returned is sum over pairs of -f (x) r
  * (eV), NOT divided by the volume -- the caller divides, as the reference does
@@ -164,7 +164,8 @@ size_t mbf_eval_workspace_bytes(int n_atoms, long long n_slots, int n_chunks);
 
 /* Status words of the last evaluation that used `workspace` (host_words[4],
  * synchronises `stream`): word 0 device error bits, word 1 the site of the
- * first failed index check (0 = none), word 2 the index that failed. */
+ * first failed index check (0 = none), word 2 the index that failed or the
+ * atom whose row held it. */
 int mbf_eval_status(const void *workspace, int *host_words, void *stream);
 
 /* ---- EAM --------------------------------------------------------------
@@ -196,14 +197,22 @@ typedef struct mbf_eam_tables {
     const int *phi_f;
     double r_cut;
     /* 1 when every function is a Zhou form (codes 3..6) sharing one switch
-     * (r_c, width) and ns <= 8: the kernels then evaluate an element's
+     * (r_c, width), each pair row holds its elements' density-row
+     * parameters, and ns <= 8: the kernels then evaluate an element's
      * density and pair function from shared exponentials.  0: generic. */
     int zhou_fused;
+    /* Optional HOST copies of P, rho_f and phi_f (all three, or NULL).  With
+     * them a fused Zhou table of one or two elements runs its fastest path:
+     * the element constants are passed as kernel arguments and both
+     * elements are evaluated for every pair without a branch.  The copies
+     * are read during the call only. */
+    const double *P_host;
+    const int *rho_f_host;
+    const int *phi_f_host;
 } mbf_eam_tables;
 
 /* lanes_per_atom: lanes of one atom's group in the density and force
- * passes, 1, 2, 4, 8, 16 or 32 (0 = 8); 2 is fastest on B200 for the
- * 256,000-atom Cu-Ni benchmark in both precisions. */
+ * passes, 1, 2, 4 or 8 (0 = 8; other values: MBF_ERR_ARGUMENT). */
 int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
                  const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
                  void *workspace, size_t workspace_bytes,
@@ -232,6 +241,13 @@ int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_table
 int mbf_eam_eval_static(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
                         const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
                         double *forces, double *energy, double *virial, void *stream);
+
+/* The status words of the last mbf_eam_eval_static on the current device,
+ * as mbf_eval_status gives them for a workspace (host_words[4]; synchronises
+ * `stream`): the no-allocation entry's callers hold no workspace pointer,
+ * so this is how they learn of a failed index check.  No counterpart in the
+ * reference.                                                              */
+int mbf_eam_eval_static_status(int *host_words, void *stream);
 
 /* Zhou EAM adjoint for fitting: the vector-Jacobian product of (energy,
  * forces, virial) with respect to the function rows P (nf, 43) of an

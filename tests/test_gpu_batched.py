@@ -21,7 +21,7 @@ def _structures(n, seed, amp=0.03, rattle=0.1):
     rng = np.random.default_rng(seed)
     out = []
     for k in range(n):
-        na, nb, nc = rng.integers(1, 4, size=3)
+        na, nb, nc = rng.integers(1, 5, size=3)   # {1..4} cells per axis, as the benchmark set
         cells = np.array([[i, j, l] for i in range(na) for j in range(nb) for l in range(nc)])
         frac = (np.asarray(DIAMOND, float)[None] + cells[:, None]).reshape(-1, 3)
         lat = np.diag([na, nb, nc]).astype(float) * 5.431

@@ -129,3 +129,60 @@ def test_build_staging_widths_agree(cuda_device, case):
         for k in range(4):
             np.testing.assert_array_equal(o[k], outs[0][k])
     np.testing.assert_array_equal(outs[0][2], ref.nbr[:ref.n_slots].cpu().numpy())
+
+
+def _criterion(lat0, ref, lat, pos, r_list, r_cut):
+    """The reference's decision (engine/neighborlist.py:653-673), restated."""
+    if np.allclose(lat, lat0, atol=1e-12):
+        sigma_min, M = 1.0, np.eye(3)
+    else:
+        M = np.linalg.inv(lat0) @ lat
+        sigma_min = float(np.linalg.svd(M, compute_uv=False)[-1])
+    dr = pos - ref @ M
+    frac = dr @ np.linalg.inv(lat)
+    frac -= np.round(frac)
+    d_max = float(np.max(np.linalg.norm(frac @ lat, axis=1)))
+    return sigma_min * r_list - 2.0 * d_max <= r_cut
+
+
+def test_check_and_rebuild_under_lattice_change(cuda_device):
+    """The skin criterion with the cell deforming between builds
+    (engine/neighborlist.py:653-668): sigma_min(inv(L_build) L_now) r_list
+    - 2 max|MIC(r - r_ref M)| <= r_cut.  An affine strain that keeps
+    sigma_min r_list above r_cut does not rebuild (the old rule rebuilt on
+    any lattice change), a compression beyond it does, and a small strain
+    plus a non-affine move crosses over where the restated criterion does;
+    a move across the strained cell's face is not motion."""
+    lat0, pos0, _ = cubic(DIAMOND, 5.431, 4, ["Si"] * 8, rattle=0.05, seed=2)
+    r_cut, skin = 3.0, 0.5
+    nl = ak.NeighbourList(r_cut, skin_width=skin)
+    assert nl.check_and_rebuild(lat0, pos0) is True
+    # 1 % affine strain: sigma_min ~ 0.99, 0.99 * 3.5 > 3: no rebuild
+    M = np.eye(3) + np.array([[0.01, 0.004, 0.0], [0.004, -0.008, 0.002], [0.0, 0.002, 0.005]])
+    lat1, pos1 = lat0 @ M, pos0 @ M
+    assert _criterion(lat0, pos0, lat1, pos1, r_cut + skin, r_cut) is False
+    assert nl.check_and_rebuild(lat1, pos1) is False
+    # the same strain with one atom moved 0.1 A (2 d = 0.2 < 0.99*3.5 - 3): no
+    # rebuild; 0.3 A: rebuild
+    moved = pos1.copy()
+    moved[7] += [0.1, 0.0, 0.0]
+    assert _criterion(lat0, pos0, lat1, moved, 3.5, 3.0) is False
+    assert nl.check_and_rebuild(lat1, moved) is False
+    moved[7] += [0.2, 0.0, 0.0]
+    assert _criterion(lat0, pos0, lat1, moved, 3.5, 3.0) is True
+    assert nl.check_and_rebuild(lat1, moved) is True
+    # after that rebuild the reference frame is lat1: a 15 % compression
+    # (sigma_min 0.85, 0.85 * 3.5 < 3) rebuilds with no atom moving
+    lat2, pos2 = lat1 * 0.85, moved * 0.85
+    assert nl.check_and_rebuild(lat2, pos2) is True
+    assert nl.rebuild_count == 3
+    # random strains and moves: the device decision equals the restated one
+    rng = np.random.default_rng(4)
+    for _ in range(12):
+        nl.build(lat0, pos0)
+        e = rng.uniform(-0.04, 0.04, (3, 3))
+        Mk = np.eye(3) + 0.5 * (e + e.T)
+        pk = pos0 @ Mk + rng.normal(0.0, 0.03, pos0.shape)
+        pk[rng.integers(len(pk))] += lat0[0] @ Mk   # a periodic image, not a move
+        want = _criterion(lat0, pos0, lat0 @ Mk, pk, 3.5, 3.0)
+        assert nl.needs_rebuild(lat0 @ Mk, pk) is want

@@ -341,3 +341,32 @@ def test_batch_of_structures_matches_single_calls():
         e0, f0, s0 = pot.compute(lat, pos, ["Si"] * len(pos))
         assert abs(e[k] - e0) < 1e-9
         assert np.abs(f[off[k]:off[k + 1]] - f0).max() < 1e-10
+
+
+def test_exp_clamp_beyond_500_matches_oracle():
+    """The Tersoff zeta exponential exp(lambda3^3 (r_ij - r_ik)^3) driven past
+    both clamps of the reference's _nb_exp (engine/_numba_common.py:12-33:
+    x > 500 -> exp(500), x < -500 -> 0): lambda3 = 40 on a rattled Si cell
+    gives arguments of both signs beyond 500; the float64 GPU path equals
+    the oracle, which restates the clamp, on the same pairs."""
+    lat, pos, types = cubic(DIAMOND, 5.431, 4, ["Si"] * 8, rattle=0.1, seed=11)
+    p = dict(TERSOFF_SI, lambda3=40.0)
+    nl = ak.NeighbourList(p["R"] + p["D"], skin_width=0.3)
+    nl.build(lat, pos)
+    i, j = nl.get_candidate_pairs()
+    d = pos[j] - pos[i]
+    s = d @ np.linalg.inv(lat)
+    s -= np.round(s)
+    r = np.linalg.norm(s @ lat, axis=1)
+    inside = r < p["R"] + p["D"]
+    rows = {}
+    for a, b, rr in zip(i[inside], j[inside], r[inside]):
+        rows.setdefault(a, []).append(rr)
+        rows.setdefault(b, []).append(rr)
+    spread = max(max(v) - min(v) for v in rows.values())
+    assert (40.0 * spread) ** 3 > 500.0   # both signs occur: (r_ij - r_ik) and (r_ik - r_ij)
+    fn = ak.force_fn_from_config({"type": "Tersoff", "species": ["Si"], "params": p})
+    res = fn(lat, pos, types, nl)
+    ref = oracle.tersoff_single(p, lat, pos, (i, j))
+    assert np.all(np.isfinite(res[1]))
+    _assert_rel(res, ref, 1e-10)

@@ -7,8 +7,11 @@ cudaMalloc / cudaFree can).  Its scratch is a fixed device array inside the
 library.  These tests call it through the C ABI and check that it returns
 what mbf_eam_eval (caller-provided workspace) returns, on two calls in a row
 with different positions -- the array keeps the previous call's contents, so
-the second call shows that nothing leaks from the first -- and that a
-structure too large for the array is refused without any work.
+the second call shows that nothing leaks from the first -- with its index
+check words, read through mbf_eam_eval_static_status (these callers hold
+no workspace pointer), clear after each call; and that a structure too
+large for the array, or a reduction plan with fewer chunks than
+structures, is refused without any work.
 
 This file is collected last so that a run stopping at the first failure has
 already run every other test.
@@ -55,6 +58,12 @@ def _static_call(torch, _lib, pot, batch, dl, precision):
                                         _lib.ptr(forces), _lib.ptr(energy), _lib.ptr(virial),
                                         torch.cuda.current_stream(dev).cuda_stream)
     _lib.check(rc, "mbf_eam_eval_static")
+    # the index-check words of that call, read through the entry point made
+    # for these callers (they hold no workspace pointer): all clear
+    words = (ctypes.c_int * 4)()
+    _lib.check(_lib.lib().mbf_eam_eval_static_status(words, torch.cuda.current_stream(dev).cuda_stream),
+               "mbf_eam_eval_static_status")
+    assert list(words)[:3] == [0, 0, 0], list(words)
     torch.cuda.synchronize()
     return energy.cpu().numpy(), forces.cpu().numpy(), virial.cpu().numpy()
 
@@ -82,6 +91,22 @@ def test_static_entry_matches_workspace_entry_on_two_calls(cuda_device, precisio
             assert abs(float(e1[0]) - float(g["energy"])) / 500 < 1e-10
 
 
+def test_static_entry_refuses_a_short_reduction_plan(cuda_device):
+    """A plan with fewer chunks than structures would clear completion
+    counters past their region (past the fixed array, here): refused."""
+    torch, _lib, g, pot, batch, dl = _setup("fp64")
+    dummy = torch.empty(1, dtype=torch.float64, device=batch.device)
+    sysd = batch.mbf_system()
+    two = _lib.MbfSystem(sysd.n_atoms, 2, sysd.positions, sysd.types, sysd.atom_struct, sysd.struct_off,
+                         sysd.cells, sysd.orthorhombic)
+    rc = _lib.lib().mbf_eam_eval_static(two, dl.mbf_nlist(), pot.tables(batch.device)[0],
+                                        _lib.MbfReducePlan(1, batch.reduce_plan().chunk,
+                                                           batch.reduce_plan().chunk_first),
+                                        _lib.MBF_FP64, 2, _lib.ptr(dummy), _lib.ptr(dummy), _lib.ptr(dummy),
+                                        torch.cuda.current_stream().cuda_stream)
+    assert rc == -1
+
+
 def test_static_entry_refuses_oversized_structure(cuda_device):
     torch, _lib, g, pot, batch, dl = _setup("fp64")
     L = _lib.lib()
@@ -100,5 +125,3 @@ def test_static_entry_refuses_oversized_structure(cuda_device):
     assert rc == -6
     assert "no-allocation" in L.mbf_error_string(rc).decode()
 
-
-_ = ctypes
