@@ -4,23 +4,20 @@
 // Replaces engine/eam.py:174-256 and engine/_eam_kernels.py:231-307.  The
 // reference visits each half pair once per phase in four serial phases
 // (density, embedding, pair forces, scatter).  Here every pass is a lane
-// group per atom over its own row:
-//   eam_density   each unordered pair once (the upper half of every row):
-//                 rho_{s_j}(r) is added to atom i's sum and rho_{s_i}(r) is
-//                 left in j's own slot (j -> i) = rev(i -> j);
-//   eam_embed     rho-bar_i = i's own sum + the shares in i's lower slots
-//                 (contiguous), clamped at 0; F and F' in float64; the record
+// group (or a thread) per atom over its own row:
+//   eam_density   rho-bar_i = sum over i's full row of rho_{s_j}(r) (owner
+//                 computes: a pair's density is evaluated from both sides,
+//                 each side only the other atom's species, and nothing is
+//                 scattered);
+//   eam_embed     rho-bar clamped at 0, F and F' in float64, and the record
 //                 {x, y, z, F'} every neighbour gathers in the force pass;
-//   eam_force     each unordered pair once: the pair's force coefficient
-//                 c / r, c = phi' + F'_i rho'_{s_j} + F'_j rho'_{s_i}; its force,
-//                 energy and virial go to i, the coefficient to j's slot;
-//   eam_gather_reduce  F_j = j's own upper-pair sum + coefficient x
-//                 minimum-image vector over j's lower slots, fused with the
-//                 per-structure energy / virial sums.
-// The minimum image used here is odd in the displacement (round half to even
-// and every product are), so the product j adds is the exact negative of the
-// one i added for the same pair.  rho-bar and F(rho-bar) are float64 in both
-// precisions.
+//   eam_force     each unordered pair once (the upper half of every row): its
+//                 force, energy and virial go to i, the negated force to j's
+//                 own slot (j -> i) = rev(i -> j);
+//   eam_gather_reduce  F_j = j's upper-pair sum + the forces its lower
+//                 neighbours left in its lower slots (contiguous), fused with
+//                 the per-structure energy / virial sums.
+// rho-bar and F(rho-bar) are float64 in both precisions.
 #include <mutex>
 
 #include "mbf_util.cuh"
@@ -348,12 +345,15 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
     return y;
 }
 
-// One element's constants (x = r / r_e).  exp(-beta (x - 1)) is
-// 2^(eb0 + eb1 r) with eb0 = beta log2(e), eb1 = -beta log2(e) / r_e (the
-// float32 form); likewise alpha.
+// One element's constants (x = r / r_e).  In float32 exp(-beta (x - 1)) is
+// 2^(eb (r - r_e)) with eb = -beta log2(e) / r_e: r - r_e is exact for r
+// within a factor two of r_e (Sterbenz), so near the equilibrium distance,
+// where the terms are largest, the argument carries only eb's own rounding
+// times a small number -- no cancellation between two large constants;
+// likewise alpha (ea).
 template <typename T>
 struct ZEl {
-    T ire, lam, kap, beta, alpha, eb0, eb1, ea0, ea1, fe, fe_ire, A, B;
+    T ire, re, lam, kap, beta, alpha, eb, ea, fe, fe_ire, A, B;
 };
 
 template <typename T>
@@ -366,16 +366,17 @@ struct ZK {
 // g = exp(-expo (x - 1)) / (1 + (x - shift)^20) and h with dg/dr = -g h / r_e,
 // h = expo + 20 (x - shift)^19 / (1 + (x - shift)^20) (engine/eam_zhou.py's
 // decay and its derivative).
-__device__ __forceinline__ void zdec(float r, float ire, float shift, float e0, float e1, float expo,
+// dre = r - r_e, el = the float32 exponent factor (eb or ea).
+__device__ __forceinline__ void zdec(float r, float dre, float ire, float shift, float el, float expo,
                                      float &g, float &h) {
     float u = fmaf(r, ire, -shift);
     float u2 = u * u, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8;
     float u19 = u16 * u2 * u;
     float rd = rcp_approx(fmaf(u16, u4, 1.0f));
-    g = ex2_approx(fmaf(e1, r, e0)) * rd;
+    g = ex2_approx(el * dre) * rd;
     h = fmaf(20.0f * u19, rd, expo);
 }
-__device__ __forceinline__ void zdec(double r, double ire, double shift, double, double, double expo,
+__device__ __forceinline__ void zdec(double r, double, double ire, double shift, double, double expo,
                                      double &g, double &h) {
     double x = r * ire, u = x - shift;
     double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8;
@@ -384,12 +385,12 @@ __device__ __forceinline__ void zdec(double r, double ire, double shift, double,
     g = exp(-expo * (x - 1.0)) * rd;
     h = expo + 20.0 * u19 * rd;
 }
-__device__ __forceinline__ float zval(float r, float ire, float shift, float e0, float e1, float) {
+__device__ __forceinline__ float zval(float r, float dre, float ire, float shift, float el, float) {
     float u = fmaf(r, ire, -shift);
     float u2 = u * u, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8;
-    return ex2_approx(fmaf(e1, r, e0)) * rcp_approx(fmaf(u16, u4, 1.0f));
+    return ex2_approx(el * dre) * rcp_approx(fmaf(u16, u4, 1.0f));
 }
-__device__ __forceinline__ double zval(double r, double ire, double shift, double, double, double expo) {
+__device__ __forceinline__ double zval(double r, double, double ire, double shift, double, double expo) {
     double x = r * ire, u = x - shift;
     double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8;
     return exp(-expo * (x - 1.0)) / (1.0 + u16 * u4);
@@ -408,8 +409,7 @@ __device__ __forceinline__ void dist_ir(double r2, double &r, double &ir) {
 // ---- evaluation policies ----------------------------------------------------
 // A policy gives, for a pair inside the cutoff at squared distance r2 of
 // species (si, sj):
-//   dens: the switched densities the pair puts on atom i, rho_{s_j}(r), and on
-//         atom j, rho_{s_i}(r);
+//   dens1: the switched density rho_{s_j}(r) neighbour j puts on atom i;
 //   pair: the switched pair function phi_{s_i s_j}(r) and its r-derivative,
 //         the r-derivatives of the switched rho_{s_j} and rho_{s_i}, and 1 / r.
 // PolGeneric reads any table (splines and every Zhou form, per call);
@@ -421,13 +421,10 @@ template <typename T>
 struct PolGeneric {
     EamDev E;
     __device__ __forceinline__ void setup(ZTab<T> &) const {}
-    __device__ __forceinline__ void dens(const ZTab<T> &, int si, int sj, double r2, T &to_i, T &to_j) const {
-        double rr = sqrt(r2);
+    __device__ __forceinline__ T dens1(const ZTab<T> &, int sj, double r2) const {
         T v, dv;
-        feval<T>(E, E.rho_f[sj], rr, v, dv);
-        to_i = v;
-        if (si != sj) feval<T>(E, E.rho_f[si], rr, v, dv);
-        to_j = v;
+        feval<T>(E, E.rho_f[sj], sqrt(r2), v, dv);
+        return v;
     }
     __device__ __forceinline__ void pair(const ZTab<T> &, int si, int sj, double r2, T &phi, T &dphi, T &drj,
                                          T &dri, T &ir) const {
@@ -450,12 +447,11 @@ template <typename T>
 struct PolZSmem {
     EamDev E;
     __device__ __forceinline__ void setup(ZTab<T> &Z) const { load_ztab<T>(E, Z); }
-    __device__ __forceinline__ void dens(const ZTab<T> &Z, int si, int sj, double r2, T &to_i, T &to_j) const {
+    __device__ __forceinline__ T dens1(const ZTab<T> &Z, int sj, double r2) const {
         T r = pair_dist<T>(r2);
         T S, dS;
         zswitch_fast<T>(r, Z, S, dS);
-        to_i = zdens_only<T>(Z.sp[sj], r) * S;
-        to_j = si == sj ? to_i : zdens_only<T>(Z.sp[si], r) * S;
+        return zdens_only<T>(Z.sp[sj], r) * S;
     }
     __device__ __forceinline__ void pair(const ZTab<T> &Z, int si, int sj, double r2, T &phi, T &dphi, T &drj,
                                          T &dri, T &ir) const {
@@ -485,28 +481,24 @@ struct PolZ2 {
     // f = f_e gB, phi_aa = A gA - B gB and their r-derivatives, unswitched.
     __device__ __forceinline__ void element(const ZEl<T> &p, T r, T &f, T &df, T &ph, T &dph) const {
         T gB, hB, gA, hA;
-        zdec(r, p.ire, p.lam, p.eb0, p.eb1, p.beta, gB, hB);
-        zdec(r, p.ire, p.kap, p.ea0, p.ea1, p.alpha, gA, hA);
+        const T dre = r - p.re;
+        zdec(r, dre, p.ire, p.lam, p.eb, p.beta, gB, hB);
+        zdec(r, dre, p.ire, p.kap, p.ea, p.alpha, gA, hA);
         f = p.fe * gB;
         df = -p.fe_ire * gB * hB;
         T a = p.A * gA, b = p.B * gB;
         ph = a - b;
         dph = -p.ire * (a * hA - b * hB);
     }
-    __device__ __forceinline__ void dens(const ZTab<T> &, int si, int sj, double r2, T &to_i, T &to_j) const {
+    // one element's switched density, its constants selected by species
+    __device__ __forceinline__ T dens1(const ZTab<T> &, int sj, double r2) const {
         T r, ir;
         dist_ir(r2, r, ir);
-        T S = sw_val(r);
-        const ZEl<T> &a = K.el[0];
-        T f0 = a.fe * S * zval(r, a.ire, a.lam, a.eb0, a.eb1, a.beta);
-        if (NS == 1) {
-            to_i = to_j = f0;
-            return;
-        }
-        const ZEl<T> &b = K.el[1];
-        T f1 = b.fe * S * zval(r, b.ire, b.lam, b.eb0, b.eb1, b.beta);
-        to_i = sj == 0 ? f0 : f1;
-        to_j = si == 0 ? f0 : f1;
+        const ZEl<T> &a = K.el[0], &b = K.el[1];
+        const bool one = NS == 1 || sj == 0;
+        const T re = one ? a.re : b.re, ire = one ? a.ire : b.ire, lam = one ? a.lam : b.lam;
+        const T eb = one ? a.eb : b.eb, beta = one ? a.beta : b.beta, fe = one ? a.fe : b.fe;
+        return fe * sw_val(r) * zval(r, r - re, ire, lam, eb, beta);
     }
     __device__ __forceinline__ void pair(const ZTab<T> &, int si, int sj, double r2, T &phi, T &dphi, T &drj,
                                          T &dri, T &ir) const {
@@ -594,18 +586,15 @@ __device__ __forceinline__ double3 ld_pos(const double *__restrict__ pos, int j)
     return make_double3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
 }
 
-// Density over the upper half of every row: each unordered pair once.  Atom
-// i sums rho_{s_j}(r) over its upper pairs (into aux[2 i]); rho_{s_i}(r), the
-// pair's share of j's density, goes to j's own slot (j -> i) = rev(i -> j), so
-// j's embedding pass reads its lower slots contiguously.  Every upper slot
-// writes its reverse slot (0 beyond the cutoff), so every lower slot of the
-// list is written.  Slot indices are loaded two iterations ahead, the
-// neighbour's position and species one ahead.
+// rho-bar_i = sum over i's full row of the switched rho_{s_j}(r) (owner
+// computes, engine/_eam_kernels.py:241-273: the density at an atom comes
+// from its neighbours' species functions), accumulated in float64 into
+// aux[2 i].  Slot indices are loaded two iterations ahead, the neighbour's
+// position and species one ahead.
 template <typename T, int LPA, class Pol, bool ORTHO>
 __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB : 1)
-    eam_density(SysView S, const int *__restrict__ row_off, const int *__restrict__ upper,
-                const int *__restrict__ nbr, const int *__restrict__ rev, Pol P, double rc2,
-                T *__restrict__ share, double *__restrict__ aux, Chk ck) {
+    eam_density(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr, Pol P, double rc2,
+                double *__restrict__ aux, Chk ck) {
     __shared__ ZTab<T> Z;
     P.setup(Z);
     const int sub = threadIdx.x & (LPA - 1);
@@ -615,50 +604,34 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB 
         double acc = 0.0;
         if (i < S.n_atoms) {
             int flag = 0;
-            int up = upper[i], end = row_off[i + 1];
-            if (!row_ok(row_off[i], up, end, ck.n_slots)) {
+            int beg = row_off[i], end = row_off[i + 1];
+            if (!row_ok(beg, beg, end, ck.n_slots)) {
                 flag = 1;
-                up = end = 0;
+                beg = end = 0;
             }
-            const int si = chk_idx(__ldg(S.types + i), ck.ns, 0, flag);
             CellView<ORTHO> cv;
             cv.load(S, i);
             const double3 pi = ld_pos(S.pos, i);
-            int s = up + sub;
-            int j0 = i, v0 = 0, j1 = i, v1 = 0;
-            if (s < end) {
-                j0 = nbr[s];
-                v0 = rev[s];
-            }
-            if (s + LPA < end) {
-                j1 = nbr[s + LPA];
-                v1 = rev[s + LPA];
-            }
+            int s = beg + sub;
+            int j0 = i, j1 = i;
+            if (s < end) j0 = nbr[s];
+            if (s + LPA < end) j1 = nbr[s + LPA];
             j0 = chk_idx(j0, ck.n_atoms, i, flag);
             double3 pn = ld_pos(S.pos, j0);
             int tn = __ldg(S.types + j0);
             for (; s < end; s += LPA) {
                 const double3 pj = pn;
                 const int sj = chk_idx(tn, ck.ns, 0, flag);
-                const int rs = v0;
                 if (s + LPA < end) {
                     j1 = chk_idx(j1, ck.n_atoms, i, flag);
                     pn = ld_pos(S.pos, j1);
                     tn = __ldg(S.types + j1);
                 }
-                v0 = v1;
-                if (s + 2 * LPA < end) {
-                    j1 = nbr[s + 2 * LPA];
-                    v1 = rev[s + 2 * LPA];
-                }
+                if (s + 2 * LPA < end) j1 = nbr[s + 2 * LPA];
                 double dx, dy, dz;
                 cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
                 const double r2 = dx * dx + dy * dy + dz * dz;
-                T to_i = T(0), to_j = T(0);
-                if (r2 < rc2 && r2 > 1e-24) P.dens(Z, si, sj, r2, to_i, to_j);
-                acc += (double)to_i;
-                if ((unsigned)rs < (unsigned)ck.n_slots) share[rs] = to_j;
-                else flag = 1;
+                if (r2 < rc2 && r2 > 1e-24) acc += (double)P.dens1(Z, sj, r2);
             }
             chk_flush(ck, flag, 11, i);
         }
@@ -667,33 +640,18 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB 
     }
 }
 
-// rho-bar_a = a's upper-pair sum + the shares in a's lower slots, clamped at
-// 0 (engine/_eam_kernels.py:268-274); F(rho-bar) and F'(rho-bar) in float64;
-// the record {x, y, z, F'} every neighbour reads in the force pass.  A thread
-// per atom: its lower slots are one contiguous run, so the shares arrive
-// sector by sector, and the embedding's branches run on full warps.
-template <typename T>
-__global__ void __launch_bounds__(256, 4) eam_embed(SysView S, const int *__restrict__ row_off,
-                                                    const int *__restrict__ upper, EamDev E,
-                                                    const T *__restrict__ share, double4 *__restrict__ pk,
+// F(rho-bar) and F'(rho-bar) in float64, rho-bar clamped at 0
+// (engine/_eam_kernels.py:268-274), and the record {x, y, z, F'} every
+// neighbour reads in the force pass (one 32-byte sector per gather); a
+// thread per atom, kept out of the density loop so the float64 pow / log of
+// the embedding does not set that kernel's register count.
+__global__ void __launch_bounds__(256, 4) eam_embed(SysView S, EamDev E, double4 *__restrict__ pk,
                                                     double *__restrict__ aux, Chk ck) {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= S.n_atoms) return;
     int flag = 0;
-    int beg = row_off[a], up = upper[a];
-    if (!row_ok(beg, up, row_off[a + 1], ck.n_slots)) {
-        flag = 1;
-        beg = up = 0;
-    }
-    double s0 = 0.0, s1 = 0.0;
-    int q = beg;
-    for (; q + 1 < up; q += 2) {
-        s0 += (double)share[q];
-        s1 += (double)share[q + 1];
-    }
-    if (q < up) s0 += (double)share[q];
     const int t = chk_idx(__ldg(S.types + a), ck.ns, 0, flag);
-    double rb = aux[2 * (size_t)a] + (s0 + s1);
+    double rb = aux[2 * (size_t)a];
     rb = rb > 0.0 ? rb : 0.0;
     double F, dF;
     embed64(E, E.F_f[t], rb, F, dF);
@@ -704,19 +662,34 @@ __global__ void __launch_bounds__(256, 4) eam_embed(SysView S, const int *__rest
     chk_flush(ck, flag, 41, a);
 }
 
+// The pair force one atom leaves in its partner's reverse slot: float4 in
+// the mixed path (one aligned 16-byte store and load), double3 in float64.
+template <typename T> struct SlotVec;
+template <> struct SlotVec<double> {
+    typedef double3 type;
+    static __device__ __forceinline__ type make(double x, double y, double z) { return make_double3(x, y, z); }
+};
+template <> struct SlotVec<float> {
+    typedef float4 type;
+    static __device__ __forceinline__ type make(double x, double y, double z) {
+        return make_float4((float)x, (float)y, (float)z, 0.0f);
+    }
+};
+
 // Force pass over the upper half of every row: each unordered pair once.
-// The pair's force coefficient sc = c / r (c = phi' + F'_i rho'_{s_j} +
-// F'_j rho'_{s_i}) gives i the force sc d (d = r_j - r_i, minimum image), the
-// pair energy and the virial -sc d (x) d; sc goes to j's own slot (j -> i) =
-// rev(i -> j) (0 beyond the cutoff), from which j's gather rebuilds its share.
-// T is float in the mixed path (a per-pair term, accumulated in float64) and
-// double in the float64 path.
+// c = phi' + F'_i rho'_{s_j} + F'_j rho'_{s_i}; the pair force (c / r) d on i
+// (d = r_j - r_i, minimum image), the pair energy and the virial -f (x) d go
+// to i, the lower index; -f goes to j's own slot (j -> i) = rev(i -> j), so
+// j's gather reads its row contiguously (0 beyond the cutoff).  T is float
+// in the mixed path (a per-pair term, accumulated in float64) and double in
+// the float64 path.
 template <typename T, int LPA, class Pol, bool ORTHO>
 __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
     eam_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ upper,
               const int *__restrict__ nbr, const int *__restrict__ rev, Pol P, double rc2,
-              const double4 *__restrict__ pk, const double *__restrict__ aux, T *__restrict__ coef,
-              double *__restrict__ f_local, double *__restrict__ per_atom, Chk ck) {
+              const double4 *__restrict__ pk, const double *__restrict__ aux,
+              typename SlotVec<T>::type *__restrict__ slot_f, double *__restrict__ f_local,
+              double *__restrict__ per_atom, Chk ck) {
     __shared__ ZTab<T> Z;
     P.setup(Z);
     const int sub = threadIdx.x & (LPA - 1);
@@ -768,15 +741,16 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
                 double dx, dy, dz;
                 cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
                 const double r2 = dx * dx + dy * dy + dz * dz;
-                T sc = T(0);
+                double px = 0.0, py = 0.0, pz = 0.0;
                 if (r2 < rc2 && r2 > 1e-24) {
                     npair += 1;
                     T phi, dphi, drj, dri, ir;
                     P.pair(Z, si, sj, r2, phi, dphi, drj, dri, ir);
                     const T c = dphi + Fp_i * drj + (T)pj.w * dri;
-                    sc = c * ir;
-                    const double scd = (double)sc;
-                    const double px = scd * dx, py = scd * dy, pz = scd * dz;
+                    const double scd = (double)(c * ir);
+                    px = scd * dx;
+                    py = scd * dy;
+                    pz = scd * dz;
                     fx += px;
                     fy += py;
                     fz += pz;
@@ -788,7 +762,7 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
                     vxz -= px * dz;
                     vyz -= py * dz;
                 }
-                if ((unsigned)rs < (unsigned)ck.n_slots) coef[rs] = sc;
+                if ((unsigned)rs < (unsigned)ck.n_slots) slot_f[rs] = SlotVec<T>::make(-px, -py, -pz);
                 else flag = 1;
             }
             chk_flush(ck, flag, 21, i);
@@ -818,16 +792,15 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
     }
 }
 
-// F_a = (pairs above a, from the force pass) + sum over a's lower slots of
-// coefficient x minimum-image vector to that neighbour (contiguous reads of
-// the row), fused with the per-structure sums (ChunkSums): a block per chunk
-// of the reduction plan, 8 lanes per atom; besides its atom's force each
-// group adds the atom's record (entries sub and sub + 8 of its 8 lanes), and
-// the block finishes the chunk's and, if last, the structure's sums.
-template <typename T, int NT, bool ORTHO>
-__global__ void __launch_bounds__(NT) eam_gather_reduce(SysView S, const int *__restrict__ row_off,
-                                                        const int *__restrict__ upper, const int *__restrict__ nbr,
-                                                        const T *__restrict__ coef, const double4 *__restrict__ pk,
+// F_a = (pairs above a) + the forces its lower neighbours left in a's own
+// lower slots (contiguous reads), fused with the per-structure sums
+// (ChunkSums): a block per chunk of the reduction plan, 8 lanes per atom;
+// besides its atom's force each group adds the atom's record (entries sub
+// and sub + 8 of its 8 lanes), and the block finishes the chunk's and, if
+// last, the structure's sums.
+template <typename V3, int NT>
+__global__ void __launch_bounds__(NT) eam_gather_reduce(int n_slots, const int *__restrict__ row_off,
+                                                        const int *__restrict__ upper, const V3 *__restrict__ slot_f,
                                                         const double *__restrict__ f_local,
                                                         double *__restrict__ forces, ChunkSums cs, Chk ck) {
     constexpr int LPA = 8, G = NT / LPA;
@@ -853,26 +826,17 @@ __global__ void __launch_bounds__(NT) eam_gather_reduce(SysView S, const int *__
         }
         double fx = 0, fy = 0, fz = 0;
         if (a < a1) {
-            int flag = 0;
-            if (!row_ok(beg, up, rend, ck.n_slots)) {
-                flag = 1;
+            if (!row_ok(beg, up, rend, n_slots)) {
+                chk_flush(ck, 1, 31, a);
                 beg = up = 0;
             }
-            CellView<ORTHO> cv;
-            cv.load(S, a);
-            const double4 pa = ld_pack(pk, a);
 #pragma unroll 4
             for (int q = beg + sub; q < up; q += LPA) {
-                const int j = chk_idx(nbr[q], ck.n_atoms, a, flag);
-                const double cq = (double)coef[q];
-                const double4 pj = ld_pack(pk, j);
-                double dx, dy, dz;
-                cv.mic(pj.x - pa.x, pj.y - pa.y, pj.z - pa.z, dx, dy, dz);
-                fx += cq * dx;
-                fy += cq * dy;
-                fz += cq * dz;
+                const V3 w = slot_f[q];
+                fx += (double)w.x;
+                fy += (double)w.y;
+                fz += (double)w.z;
             }
-            chk_flush(ck, flag, 31, a);
             const double *rec = cs.per_atom + (size_t)a * ATOM_ACC;
             r0 += rec[sub];
             if (sub < ATOM_ACC - LPA) r1 += rec[LPA + sub];
@@ -951,30 +915,34 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_site(SysView S, const int *__re
 struct EamBufs {
     double4 *pk;
     double *aux;
-    void *slot;  // per-slot density shares, then force coefficients (T each)
+    void *slot;  // per-slot pair forces (SlotVec<T>)
     double *f_local;
     double *forces;
     double *per_atom;
 };
 
+// The density pass walks full rows (twice the force pass's upper halves),
+// so it takes twice the force pass's lanes per atom, at most 8.
 template <typename T, int LPA, class Pol, bool ORTHO>
 static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const EamDev &E, double rc2,
                       const EamBufs &B, Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks,
                       cudaStream_t st) {
-    T *slot = static_cast<T *>(B.slot);
-    const int gpb = EAM_BLOCK / LPA;
-    const int blocks = (S.n_atoms + gpb - 1) / gpb;
-    int g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_density<T, LPA, Pol, ORTHO>);
+    typedef typename SlotVec<T>::type V3;
+    constexpr int DLPA = LPA >= 4 ? 8 : 2 * LPA;
+    V3 *slot = static_cast<V3 *>(B.slot);
+    const int dgpb = EAM_BLOCK / DLPA;
+    int g = persistent_grid((S.n_atoms + dgpb - 1) / dgpb, EAM_BLOCK,
+                            (const void *)eam_density<T, DLPA, Pol, ORTHO>);
     PROF_BEGIN("eam_density", st);
-    eam_density<T, LPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, P, rc2,
-                                                             slot, B.aux, ck);
+    eam_density<T, DLPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, rc2, B.aux, ck);
     PROF_END("eam_density", st);
     MBF_CHECK_LAUNCH();
     PROF_BEGIN("eam_embed", st);
-    eam_embed<T><<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S, nl->row_off, nl->upper, E, slot, B.pk, B.aux, ck);
+    eam_embed<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S, E, B.pk, B.aux, ck);
     PROF_END("eam_embed", st);
     MBF_CHECK_LAUNCH();
-    g = persistent_grid(blocks, EAM_BLOCK, (const void *)eam_force<T, LPA, Pol, ORTHO>);
+    const int gpb = EAM_BLOCK / LPA;
+    g = persistent_grid((S.n_atoms + gpb - 1) / gpb, EAM_BLOCK, (const void *)eam_force<T, LPA, Pol, ORTHO>);
     PROF_BEGIN("eam_force", st);
     eam_force<T, LPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, P, rc2,
                                                            B.pk, B.aux, slot, B.f_local, B.per_atom, ck);
@@ -983,14 +951,14 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const
     PROF_BEGIN("eam_gather_reduce", st);
     const int nt = chunk_block(S.n_atoms, n_chunks);
     if (nt == 128)
-        eam_gather_reduce<T, 128, ORTHO><<<n_chunks, 128, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, slot, B.pk,
-                                                                   B.f_local, B.forces, cs, ck);
+        eam_gather_reduce<V3, 128><<<n_chunks, 128, 0, st>>>(ck.n_slots, nl->row_off, nl->upper, slot, B.f_local,
+                                                             B.forces, cs, ck);
     else if (nt == 256)
-        eam_gather_reduce<T, 256, ORTHO><<<n_chunks, 256, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, slot, B.pk,
-                                                                   B.f_local, B.forces, cs, ck);
+        eam_gather_reduce<V3, 256><<<n_chunks, 256, 0, st>>>(ck.n_slots, nl->row_off, nl->upper, slot, B.f_local,
+                                                             B.forces, cs, ck);
     else
-        eam_gather_reduce<T, 512, ORTHO><<<n_chunks, 512, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, slot, B.pk,
-                                                                   B.f_local, B.forces, cs, ck);
+        eam_gather_reduce<V3, 512><<<n_chunks, 512, 0, st>>>(ck.n_slots, nl->row_off, nl->upper, slot, B.f_local,
+                                                             B.forces, cs, ck);
     PROF_END("eam_gather_reduce", st);
     MBF_CHECK_LAUNCH();
     if (so.e) {
@@ -1039,14 +1007,13 @@ static bool make_zk(const mbf_eam_tables *tab, ZK<T> &K) {
         const double re = p[0], fe = p[1], alpha = p[4], beta = p[5];
         ZEl<T> &q = K.el[s];
         q.ire = (T)(1.0 / re);
+        q.re = (T)re;
         q.lam = (T)p[9];
         q.kap = (T)p[8];
         q.beta = (T)beta;
         q.alpha = (T)alpha;
-        q.eb0 = (T)(beta * LOG2E);
-        q.eb1 = (T)(-beta * LOG2E / re);
-        q.ea0 = (T)(alpha * LOG2E);
-        q.ea1 = (T)(-alpha * LOG2E / re);
+        q.eb = (T)(-beta * LOG2E / re);
+        q.ea = (T)(-alpha * LOG2E / re);
         q.fe = (T)fe;
         q.fe_ire = (T)(fe / re);
         q.A = (T)p[6];

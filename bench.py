@@ -1207,7 +1207,7 @@ def main():
     def err(a, b):
         return {"max_force_eVA": float(np.abs(a[1] - b[1]).max()),
                 "energy_per_atom_eV": abs(a[0] - b[0]) / n_atoms,
-                "stress_eVA3": float(np.abs((np.asarray(a[2]) - np.asarray(b[2])).reshape(-1)).max()) / vol}
+                "stress_eVA3": float(np.abs(np.asarray(a[2]).reshape(-1) - np.asarray(b[2]).reshape(-1)).max()) / vol}
 
     res = {args.precision: res_main, other: res_other}
     errors = {"tolerance": {"max_force_eVA": 1e-5, "energy_per_atom_eV": 1e-6, "stress_eVA3": 1e-5,
