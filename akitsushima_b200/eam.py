@@ -284,8 +284,8 @@ class EAMPotential(DevicePotential):
 
     sites_entry = "mbf_eam_eval_sites"
     lane_choices = (1, 2, 4, 8)
-    # lanes of one atom's group: 2 measured fastest on B200 (256k Cu-Ni, both precisions)
-    lanes_per_atom = 2
+    # lanes of one atom's group in the force pass: 4 measured fastest on B200 (256k Cu-Ni)
+    lanes_per_atom = 4
 
     def _call(self, L, sysd, nld, tabs, plan, prec, ws, nbytes, forces, energy, virial, stream):
         return L.mbf_eam_eval(sysd, nld, tabs[0], plan, prec, int(self.lanes_per_atom), ws, nbytes,

@@ -953,7 +953,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--cells", type=int, default=40)
-    ap.add_argument("--lanes", type=int, default=2, help="EAM lanes per atom (1, 2, 4 or 8)")
+    ap.add_argument("--lanes", type=int, default=4, help="EAM lanes per atom (1, 2, 4 or 8)")
     ap.add_argument("--no-sub-records", action="store_true",
                     help="default workload: skip the other configurations' sub-records")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1112,7 +1112,7 @@ def main():
     del pi, pj, d, s, r, inside, cross
     force_flops = roofline.eam_force_flops(n_in - n_cross, n_cross)
     force_bytes = roofline.eam_force_bytes(n_atoms, dnl.n_slots)
-    dom = "eam_force"
+    dom = "eam_force_gather"
     cnt, tot = prof.get(dom, (1, float("nan")))
     t_dom = tot / cnt * 1e-3
     scratch = torch.empty(148 * 8 * 256 * 8 * 4, dtype=torch.uint8, device=dev)
