@@ -717,23 +717,30 @@ __device__ __forceinline__ void st_release(int *p, int v) {
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// ctr[0] next tile, ctr[1] next chunk, ctr[2] done prefix (every tile below
-// it is done); flag[t] = 1 once tile t is done.  Zero at launch.
+// ctr[0] next tile, ctr[1] next chunk; gcnt[k] counts the done tiles of
+// tile group k (TILE_GROUP tiles each); flag[t] = 1 once tile t is done.
+// All zero at launch.
+constexpr int TILE_GROUP = 32;
 struct Sched {
     int *ctr;
+    int *gcnt;
     int *flag;
     int n_tiles;
 };
 
-// Advance the shared done prefix over the tiles whose flags are set
-// (thread 0); returns the prefix it saw last.
-__device__ __forceinline__ int advance_prefix(const Sched &sc) {
-    int p = ld_acquire(sc.ctr + 2);
-    while (p < sc.n_tiles && ld_acquire(sc.flag + p) != 0) {
-        const int q = atomicCAS(sc.ctr + 2, p, p + 1);
-        p = (q == p) ? p + 1 : q;
-    }
-    return p;
+// Called by every thread of the block: true once every tile below `need`
+// is done.  Whole groups are checked by their counters, the remainder by
+// its flags, all threads loading in parallel (one round trip, not one per
+// tile); `known` caches the groups this block has seen complete.
+__device__ __forceinline__ bool tiles_done(const Sched &sc, int need, int &known) {
+    const int full = need / TILE_GROUP, rem = need - full * TILE_GROUP;
+    bool ok = true;
+    for (int k = known + (int)threadIdx.x; k < full; k += blockDim.x)
+        ok = ok && ld_acquire(sc.gcnt + k) == TILE_GROUP;
+    for (int k = threadIdx.x; k < rem; k += blockDim.x) ok = ok && ld_acquire(sc.flag + full * TILE_GROUP + k) != 0;
+    ok = __syncthreads_and(ok) != 0;
+    if (ok && full > known) known = full;
+    return ok;
 }
 
 // Polls of a bounded wait (each at least 128 ns apart: a quarter second or
@@ -914,62 +921,51 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
     __shared__ int s_work;
     P.setup(Z);
     constexpr int gpb = EAM_BLOCK / LPA;
-    bool tiles_left = true;
+    int known = 0;  // tile groups this block has seen complete (same in every thread)
     for (;;) {
-        if (tiles_left) {
-            if (threadIdx.x == 0) s_work = atomicAdd(sc.ctr, 1);
-            __syncthreads();
-            const int t = s_work;
-            __syncthreads();
-            if (t < sc.n_tiles) {
-                force_tile<T, LPA, Pol, ORTHO>(S, row_off, upper, nbr, rev, P, Z, rc2, pk, aux, slot_f, f_local,
-                                               per_atom, ck, t * gpb + (int)(threadIdx.x / LPA));
-                __threadfence();
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    st_release(sc.flag + t, 1);
-                    advance_prefix(sc);
-                }
-                // any chunk whose tiles are all done, without waiting
-                for (;;) {
-                    if (threadIdx.x == 0) {
-                        int g = -1;
-                        const int c = ld_acquire(sc.ctr + 1);
-                        if (c < n_chunks) {
-                            const int need = (cs.chunk[3 * c + 2] + gpb - 1) / gpb;
-                            if (advance_prefix(sc) >= need && atomicCAS(sc.ctr + 1, c, c + 1) == c) g = c;
-                        }
-                        s_work = g;
-                    }
-                    __syncthreads();
-                    const int g = s_work;
-                    __syncthreads();
-                    if (g < 0) break;
-                    gather_chunk<V3>(ck.n_slots, row_off, upper, slot_f, f_local, forces, cs, ck, g);
-                }
-                continue;
-            }
-            tiles_left = false;
-        }
-        // every tile is claimed: take the remaining chunks, waiting for each
+        if (threadIdx.x == 0) s_work = atomicAdd(sc.ctr, 1);
+        __syncthreads();
+        const int t = s_work;
+        __syncthreads();
+        if (t >= sc.n_tiles) break;
+        force_tile<T, LPA, Pol, ORTHO>(S, row_off, upper, nbr, rev, P, Z, rc2, pk, aux, slot_f, f_local, per_atom,
+                                       ck, t * gpb + (int)(threadIdx.x / LPA));
+        __threadfence();
+        __syncthreads();
         if (threadIdx.x == 0) {
-            int g = atomicAdd(sc.ctr + 1, 1);
-            if (g < n_chunks) {
-                const int need = (cs.chunk[3 * g + 2] + gpb - 1) / gpb;
-                long long k = 0;
-                while (advance_prefix(sc) < need && ++k < EAM_WAIT_POLLS) __nanosleep(128);
-                if (k >= EAM_WAIT_POLLS) {
-                    atomicOr(ck.err, MBF_DEV_WAIT_LIMIT);
-                    g = -2;
-                }
-            }
-            s_work = g;
+            st_release(sc.flag + t, 1);
+            atomicAdd(sc.gcnt + t / TILE_GROUP, 1);
         }
+        // any chunk whose tiles are all done, without waiting
+        for (;;) {
+            if (threadIdx.x == 0) s_work = ld_acquire(sc.ctr + 1);
+            __syncthreads();
+            const int c = s_work;
+            __syncthreads();
+            if (c >= n_chunks || !tiles_done(sc, (cs.chunk[3 * c + 2] + gpb - 1) / gpb, known)) break;
+            if (threadIdx.x == 0) s_work = atomicCAS(sc.ctr + 1, c, c + 1) == c;
+            __syncthreads();
+            const int mine = s_work;
+            __syncthreads();
+            if (!mine) break;
+            gather_chunk<V3>(ck.n_slots, row_off, upper, slot_f, f_local, forces, cs, ck, c);
+        }
+    }
+    // every tile is claimed: take the remaining chunks, waiting for each
+    for (;;) {
+        if (threadIdx.x == 0) s_work = atomicAdd(sc.ctr + 1, 1);
         __syncthreads();
-        const int g = s_work;
+        const int c = s_work;
         __syncthreads();
-        if (g == -2 || g >= n_chunks) break;
-        gather_chunk<V3>(ck.n_slots, row_off, upper, slot_f, f_local, forces, cs, ck, g);
+        if (c >= n_chunks) break;
+        const int need = (cs.chunk[3 * c + 2] + gpb - 1) / gpb;
+        long long k = 0;
+        while (!tiles_done(sc, need, known) && ++k < EAM_WAIT_POLLS) __nanosleep(128);
+        if (k >= EAM_WAIT_POLLS) {
+            if (threadIdx.x == 0) atomicOr(ck.err, MBF_DEV_WAIT_LIMIT);
+            break;
+        }
+        gather_chunk<V3>(ck.n_slots, row_off, upper, slot_f, f_local, forces, cs, ck, c);
     }
 }
 
@@ -1064,10 +1060,13 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const
     MBF_CHECK_LAUNCH();
     const int gpb = EAM_BLOCK / LPA;
     Sched sc;
-    sc.ctr = B.sched;
-    sc.flag = B.sched + 4;
     sc.n_tiles = (S.n_atoms + gpb - 1) / gpb;
-    if (cudaMemsetAsync(B.sched, 0, sizeof(int) * (size_t)(sc.n_tiles + 4), st) != cudaSuccess) return MBF_ERR_CUDA;
+    const int n_groups = (sc.n_tiles + TILE_GROUP - 1) / TILE_GROUP;
+    sc.ctr = B.sched;
+    sc.gcnt = B.sched + 4;
+    sc.flag = sc.gcnt + n_groups;
+    if (cudaMemsetAsync(B.sched, 0, sizeof(int) * (size_t)(4 + n_groups + sc.n_tiles), st) != cudaSuccess)
+        return MBF_ERR_CUDA;
     g = persistent_grid(sc.n_tiles, EAM_BLOCK, (const void *)eam_force_gather<T, LPA, Pol, ORTHO>);
     PROF_BEGIN("eam_force_gather", st);
     eam_force_gather<T, LPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, P,
