@@ -12,7 +12,6 @@
 // Device error word bits (workspace word 0 of each call's error block).
 #define MBF_DEV_ROW_TOO_LONG 1
 #define MBF_DEV_BAD_INDEX 2
-#define MBF_DEV_WAIT_LIMIT 4   /* a bounded wait of a persistent kernel gave up */
 
 #define MBF_CHECK_LAUNCH()                                   \
     do {                                                     \

@@ -20,7 +20,6 @@
 //                 the per-structure energy / virial sums.
 // rho-bar and F(rho-bar) are float64 in both precisions.
 #include <mutex>
-#include <type_traits>
 
 #include "mbf_util.cuh"
 
@@ -664,206 +663,153 @@ __global__ void __launch_bounds__(256, 4) eam_embed(SysView S, EamDev E, double4
     chk_flush(ck, flag, 41, a);
 }
 
-// ---- force pass and force gather, one persistent kernel ---------------------
-//
-// Force tiles: the atoms [t g, (t + 1) g), g = EAM_BLOCK / LPA, each atom's
-// upper row by its lane group.  Each unordered pair is evaluated once:
-// c = phi' + F'_i rho'_{s_j} + F'_j rho'_{s_i}; the pair force (c / r) d on i
-// (d = r_j - r_i, minimum image), the pair energy and the virial -f (x) d go
-// to i, the lower index, and -f to j's own slot (j -> i) = rev(i -> j) (0
-// beyond the cutoff).  T is float in the mixed path (a per-pair term,
-// accumulated in float64) and double in the float64 path.
-//
-// Gather units: the chunks of the reduction plan.  F_a = a's upper-pair sum
-// + the forces its lower neighbours left in a's lower slots (contiguous),
-// then the chunk's (and, if last, the structure's) energy / virial sums.  A
-// chunk's lower neighbours all lie below its last atom, so it can be
-// gathered as soon as every tile below that atom is done.
-//
-// Blocks claim tiles in atom order from a counter and, between tiles, claim
-// any chunk that is ready; when the tiles run out they claim the remaining
-// chunks and wait for them.  The pair forces in flight then span only the
-// tiles being worked on plus the list's index reach, a few tens of MB that
-// stay in L2 between the scattered write and the gather, instead of the
-// whole list's forces going to HBM and back.  A block waits only for tiles
-// already claimed, and a claimed tile never waits, so the waits end; each is
-// still bounded and reports MBF_DEV_WAIT_LIMIT if it gives up.
-
 // The pair force one atom leaves in its partner's reverse slot: float4 in
 // the mixed path (one aligned 16-byte store and load), double3 in float64.
 template <typename T> struct SlotVec;
 template <> struct SlotVec<double> {
     typedef double3 type;
     static __device__ __forceinline__ type make(double x, double y, double z) { return make_double3(x, y, z); }
-    static __device__ __forceinline__ type load_l2(const type *p) {
-        const double *q = reinterpret_cast<const double *>(p);
-        return make_double3(__ldcg(q), __ldcg(q + 1), __ldcg(q + 2));
-    }
 };
 template <> struct SlotVec<float> {
     typedef float4 type;
     static __device__ __forceinline__ type make(double x, double y, double z) {
         return make_float4((float)x, (float)y, (float)z, 0.0f);
     }
-    static __device__ __forceinline__ type load_l2(const type *p) { return __ldcg(p); }
 };
 
-__device__ __forceinline__ int ld_acquire(const int *p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release(int *p, int v) {
-    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// ctr[0] next tile, ctr[1] next chunk; gcnt[k] counts the done tiles of
-// tile group k (TILE_GROUP tiles each); flag[t] = 1 once tile t is done.
-// All zero at launch.
-constexpr int TILE_GROUP = 32;
-struct Sched {
-    int *ctr;
-    int *gcnt;
-    int *flag;
-    int n_tiles;
-};
-
-// Called by every thread of the block: true once every tile below `need`
-// is done.  Whole groups are checked by their counters, the remainder by
-// its flags, all threads loading in parallel (one round trip, not one per
-// tile); `known` caches the groups this block has seen complete.
-__device__ __forceinline__ bool tiles_done(const Sched &sc, int need, int &known) {
-    const int full = need / TILE_GROUP, rem = need - full * TILE_GROUP;
-    bool ok = true;
-    for (int k = known + (int)threadIdx.x; k < full; k += blockDim.x)
-        ok = ok && ld_acquire(sc.gcnt + k) == TILE_GROUP;
-    for (int k = threadIdx.x; k < rem; k += blockDim.x) ok = ok && ld_acquire(sc.flag + full * TILE_GROUP + k) != 0;
-    ok = __syncthreads_and(ok) != 0;
-    if (ok && full > known) known = full;
-    return ok;
-}
-
-// Polls of a bounded wait (each at least 128 ns apart: a quarter second or
-// more, far beyond the longest legitimate wait, the whole force pass).
-constexpr long long EAM_WAIT_POLLS = 1LL << 21;
-
+// Force pass over the upper half of every row: each unordered pair once.
+// c = phi' + F'_i rho'_{s_j} + F'_j rho'_{s_i}; the pair force (c / r) d on i
+// (d = r_j - r_i, minimum image), the pair energy and the virial -f (x) d go
+// to i, the lower index; -f goes to j's own slot (j -> i) = rev(i -> j), so
+// j's gather reads its row contiguously (0 beyond the cutoff).  T is float
+// in the mixed path (a per-pair term, accumulated in float64) and double in
+// the float64 path.
 template <typename T, int LPA, class Pol, bool ORTHO>
-__device__ __forceinline__ void force_tile(const SysView &S, const int *__restrict__ row_off,
-                                           const int *__restrict__ upper, const int *__restrict__ nbr,
-                                           const int *__restrict__ rev, const Pol &P, const ZTab<T> &Z, double rc2,
-                                           const double4 *__restrict__ pk, const double *__restrict__ aux,
-                                           typename SlotVec<T>::type *__restrict__ slot_f,
-                                           double *__restrict__ f_local, double *__restrict__ per_atom,
-                                           const Chk &ck, int i) {
+__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
+    eam_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ upper,
+              const int *__restrict__ nbr, const int *__restrict__ rev, Pol P, double rc2,
+              const double4 *__restrict__ pk, const double *__restrict__ aux,
+              typename SlotVec<T>::type *__restrict__ slot_f, double *__restrict__ f_local,
+              double *__restrict__ per_atom, Chk ck) {
+    __shared__ ZTab<T> Z;
+    P.setup(Z);
     const int sub = threadIdx.x & (LPA - 1);
-    double fx = 0, fy = 0, fz = 0, e = 0;
-    int npair = 0;
-    double vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
-    if (i < S.n_atoms) {
-        int flag = 0;
-        int up = upper[i], end = row_off[i + 1];
-        if (!row_ok(row_off[i], up, end, ck.n_slots)) {
-            flag = 1;
-            up = end = 0;
-        }
-        const int si = chk_idx(__ldg(S.types + i), ck.ns, 0, flag);
-        const double4 pi = ld_pack(pk, i);
-        const T Fp_i = (T)pi.w;
-        CellView<ORTHO> cv;
-        cv.load(S, i);
-        int s = up + sub;
-        int j0 = i, v0 = 0, j1 = i, v1 = 0;
-        if (s < end) {
-            j0 = nbr[s];
-            v0 = rev[s];
-        }
-        if (s + LPA < end) {
-            j1 = nbr[s + LPA];
-            v1 = rev[s + LPA];
-        }
-        j0 = chk_idx(j0, ck.n_atoms, i, flag);
-        double4 pn = ld_pack(pk, j0);
-        int tn = __ldg(S.types + j0);
-        for (; s < end; s += LPA) {
-            const double4 pj = pn;
-            const int sj = chk_idx(tn, ck.ns, 0, flag);
-            const int rs = v0;
+    const int gpb = EAM_BLOCK / LPA;
+    for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
+        const int i = base + threadIdx.x / LPA;
+        double fx = 0, fy = 0, fz = 0, e = 0;
+        int npair = 0;
+        double vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+        if (i < S.n_atoms) {
+            int flag = 0;
+            int up = upper[i], end = row_off[i + 1];
+            if (!row_ok(row_off[i], up, end, ck.n_slots)) {
+                flag = 1;
+                up = end = 0;
+            }
+            const int si = chk_idx(__ldg(S.types + i), ck.ns, 0, flag);
+            const double4 pi = ld_pack(pk, i);
+            const T Fp_i = (T)pi.w;
+            CellView<ORTHO> cv;
+            cv.load(S, i);
+            int s = up + sub;
+            int j0 = i, v0 = 0, j1 = i, v1 = 0;
+            if (s < end) {
+                j0 = nbr[s];
+                v0 = rev[s];
+            }
             if (s + LPA < end) {
-                j1 = chk_idx(j1, ck.n_atoms, i, flag);
-                pn = ld_pack(pk, j1);
-                tn = __ldg(S.types + j1);
+                j1 = nbr[s + LPA];
+                v1 = rev[s + LPA];
             }
-            v0 = v1;
-            if (s + 2 * LPA < end) {
-                j1 = nbr[s + 2 * LPA];
-                v1 = rev[s + 2 * LPA];
+            j0 = chk_idx(j0, ck.n_atoms, i, flag);
+            double4 pn = ld_pack(pk, j0);
+            int tn = __ldg(S.types + j0);
+            for (; s < end; s += LPA) {
+                const double4 pj = pn;
+                const int sj = chk_idx(tn, ck.ns, 0, flag);
+                const int rs = v0;
+                if (s + LPA < end) {
+                    j1 = chk_idx(j1, ck.n_atoms, i, flag);
+                    pn = ld_pack(pk, j1);
+                    tn = __ldg(S.types + j1);
+                }
+                v0 = v1;
+                if (s + 2 * LPA < end) {
+                    j1 = nbr[s + 2 * LPA];
+                    v1 = rev[s + 2 * LPA];
+                }
+                double dx, dy, dz;
+                cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                double px = 0.0, py = 0.0, pz = 0.0;
+                if (r2 < rc2 && r2 > 1e-24) {
+                    npair += 1;
+                    T phi, dphi, drj, dri, ir;
+                    P.pair(Z, si, sj, r2, phi, dphi, drj, dri, ir);
+                    const T c = dphi + Fp_i * drj + (T)pj.w * dri;
+                    const double scd = (double)(c * ir);
+                    px = scd * dx;
+                    py = scd * dy;
+                    pz = scd * dz;
+                    fx += px;
+                    fy += py;
+                    fz += pz;
+                    e += (double)phi;
+                    vxx -= px * dx;
+                    vyy -= py * dy;
+                    vzz -= pz * dz;
+                    vxy -= px * dy;
+                    vxz -= px * dz;
+                    vyz -= py * dz;
+                }
+                if ((unsigned)rs < (unsigned)ck.n_slots) slot_f[rs] = SlotVec<T>::make(-px, -py, -pz);
+                else flag = 1;
             }
-            double dx, dy, dz;
-            cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            double px = 0.0, py = 0.0, pz = 0.0;
-            if (r2 < rc2 && r2 > 1e-24) {
-                npair += 1;
-                T phi, dphi, drj, dri, ir;
-                P.pair(Z, si, sj, r2, phi, dphi, drj, dri, ir);
-                const T c = dphi + Fp_i * drj + (T)pj.w * dri;
-                const double scd = (double)(c * ir);
-                px = scd * dx;
-                py = scd * dy;
-                pz = scd * dz;
-                fx += px;
-                fy += py;
-                fz += pz;
-                e += (double)phi;
-                vxx -= px * dx;
-                vyy -= py * dy;
-                vzz -= pz * dz;
-                vxy -= px * dy;
-                vxz -= px * dz;
-                vyz -= py * dz;
-            }
-            if ((unsigned)rs < (unsigned)ck.n_slots) slot_f[rs] = SlotVec<T>::make(-px, -py, -pz);
-            else flag = 1;
+            chk_flush(ck, flag, 21, i);
         }
-        chk_flush(ck, flag, 21, i);
-    }
-    fx = group_sum<LPA>(fx);
-    fy = group_sum<LPA>(fy);
-    fz = group_sum<LPA>(fz);
-    e = group_sum<LPA>(e);
-    vxx = group_sum<LPA>(vxx);
-    vyy = group_sum<LPA>(vyy);
-    vzz = group_sum<LPA>(vzz);
-    vxy = group_sum<LPA>(vxy);
-    vxz = group_sum<LPA>(vxz);
-    vyz = group_sum<LPA>(vyz);
-    npair = group_sum<LPA>(npair);
-    if (sub == 0 && i < S.n_atoms) {
-        f_local[3 * (size_t)i] = fx;
-        f_local[3 * (size_t)i + 1] = fy;
-        f_local[3 * (size_t)i + 2] = fz;
-        double *pa = per_atom + (size_t)i * ATOM_ACC;
-        pa[0] = e + aux[2 * (size_t)i + 1];
-        pa[1] = vxx; pa[2] = vxy; pa[3] = vxz;
-        pa[4] = vxy; pa[5] = vyy; pa[6] = vyz;
-        pa[7] = vxz; pa[8] = vyz; pa[9] = vzz;
-        pa[10] = (double)npair;
+        fx = group_sum<LPA>(fx);
+        fy = group_sum<LPA>(fy);
+        fz = group_sum<LPA>(fz);
+        e = group_sum<LPA>(e);
+        vxx = group_sum<LPA>(vxx);
+        vyy = group_sum<LPA>(vyy);
+        vzz = group_sum<LPA>(vzz);
+        vxy = group_sum<LPA>(vxy);
+        vxz = group_sum<LPA>(vxz);
+        vyz = group_sum<LPA>(vyz);
+        npair = group_sum<LPA>(npair);
+        if (sub == 0 && i < S.n_atoms) {
+            f_local[3 * (size_t)i] = fx;
+            f_local[3 * (size_t)i + 1] = fy;
+            f_local[3 * (size_t)i + 2] = fz;
+            double *pa = per_atom + (size_t)i * ATOM_ACC;
+            pa[0] = e + aux[2 * (size_t)i + 1];
+            pa[1] = vxx; pa[2] = vxy; pa[3] = vxz;
+            pa[4] = vxy; pa[5] = vyy; pa[6] = vyz;
+            pa[7] = vxz; pa[8] = vyz; pa[9] = vzz;
+            pa[10] = (double)npair;
+        }
     }
 }
 
-// One chunk of the reduction plan, 8 lanes per atom, the next atom's row
-// bounds loaded one iteration ahead; everything the force tiles wrote is
-// read through L2 (they ran on other SMs).
-template <typename V3>
-__device__ __forceinline__ void gather_chunk(int n_slots, const int *__restrict__ row_off,
-                                             const int *__restrict__ upper, const V3 *__restrict__ slot_f,
-                                             const double *__restrict__ f_local, double *__restrict__ forces,
-                                             const ChunkSums &cs, const Chk &ck, int c) {
-    constexpr int LPA = 8, G = EAM_BLOCK / LPA;
-    typedef SlotVec<typename std::conditional<sizeof(V3) == 16, float, double>::type> SV;
+// F_a = (pairs above a) + the forces its lower neighbours left in a's own
+// lower slots (contiguous reads), fused with the per-structure sums
+// (ChunkSums): a block per chunk of the reduction plan, 8 lanes per atom;
+// besides its atom's force each group adds the atom's record (entries sub
+// and sub + 8 of its 8 lanes), and the block finishes the chunk's and, if
+// last, the structure's sums.
+template <typename V3, int NT>
+__global__ void __launch_bounds__(NT) eam_gather_reduce(int n_slots, const int *__restrict__ row_off,
+                                                        const int *__restrict__ upper, const V3 *__restrict__ slot_f,
+                                                        const double *__restrict__ f_local,
+                                                        double *__restrict__ forces, ChunkSums cs, Chk ck) {
+    constexpr int LPA = 8, G = NT / LPA;
+    const int c = blockIdx.x;
     const int s = cs.chunk[3 * c], a0 = cs.chunk[3 * c + 1], a1 = cs.chunk[3 * c + 2];
     const int sub = threadIdx.x & (LPA - 1), grp = threadIdx.x / LPA;
     double r0 = 0.0, r1 = 0.0;
+    // the next atom's row bounds are loaded one iteration ahead
     int nb = 0, nu = 0, ne = 0;
     if (a0 + grp < a1) {
         nb = row_off[a0 + grp];
@@ -887,86 +833,25 @@ __device__ __forceinline__ void gather_chunk(int n_slots, const int *__restrict_
             }
 #pragma unroll 4
             for (int q = beg + sub; q < up; q += LPA) {
-                const V3 w = SV::load_l2(slot_f + q);
+                const V3 w = slot_f[q];
                 fx += (double)w.x;
                 fy += (double)w.y;
                 fz += (double)w.z;
             }
             const double *rec = cs.per_atom + (size_t)a * ATOM_ACC;
-            r0 += __ldcg(rec + sub);
-            if (sub < ATOM_ACC - LPA) r1 += __ldcg(rec + LPA + sub);
+            r0 += rec[sub];
+            if (sub < ATOM_ACC - LPA) r1 += rec[LPA + sub];
         }
         fx = group_sum<LPA>(fx);
         fy = group_sum<LPA>(fy);
         fz = group_sum<LPA>(fz);
         if (sub == 0 && a < a1) {
-            forces[3 * (size_t)a] = __ldcg(f_local + 3 * (size_t)a) + fx;
-            forces[3 * (size_t)a + 1] = __ldcg(f_local + 3 * (size_t)a + 1) + fy;
-            forces[3 * (size_t)a + 2] = __ldcg(f_local + 3 * (size_t)a + 2) + fz;
+            forces[3 * (size_t)a] = f_local[3 * (size_t)a] + fx;
+            forces[3 * (size_t)a + 1] = f_local[3 * (size_t)a + 1] + fy;
+            forces[3 * (size_t)a + 2] = f_local[3 * (size_t)a + 2] + fz;
         }
     }
-    chunk_sums_finish<EAM_BLOCK>(cs, c, s, r0, r1);
-}
-
-template <typename T, int LPA, class Pol, bool ORTHO>
-__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
-    eam_force_gather(SysView S, const int *__restrict__ row_off, const int *__restrict__ upper,
-                     const int *__restrict__ nbr, const int *__restrict__ rev, Pol P, double rc2,
-                     const double4 *__restrict__ pk, const double *__restrict__ aux,
-                     typename SlotVec<T>::type *__restrict__ slot_f, double *__restrict__ f_local,
-                     double *__restrict__ per_atom, double *__restrict__ forces, ChunkSums cs, int n_chunks,
-                     Sched sc, Chk ck) {
-    typedef typename SlotVec<T>::type V3;
-    __shared__ ZTab<T> Z;
-    __shared__ int s_work;
-    P.setup(Z);
-    constexpr int gpb = EAM_BLOCK / LPA;
-    int known = 0;  // tile groups this block has seen complete (same in every thread)
-    for (;;) {
-        if (threadIdx.x == 0) s_work = atomicAdd(sc.ctr, 1);
-        __syncthreads();
-        const int t = s_work;
-        __syncthreads();
-        if (t >= sc.n_tiles) break;
-        force_tile<T, LPA, Pol, ORTHO>(S, row_off, upper, nbr, rev, P, Z, rc2, pk, aux, slot_f, f_local, per_atom,
-                                       ck, t * gpb + (int)(threadIdx.x / LPA));
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            st_release(sc.flag + t, 1);
-            atomicAdd(sc.gcnt + t / TILE_GROUP, 1);
-        }
-        // any chunk whose tiles are all done, without waiting
-        for (;;) {
-            if (threadIdx.x == 0) s_work = ld_acquire(sc.ctr + 1);
-            __syncthreads();
-            const int c = s_work;
-            __syncthreads();
-            if (c >= n_chunks || !tiles_done(sc, (cs.chunk[3 * c + 2] + gpb - 1) / gpb, known)) break;
-            if (threadIdx.x == 0) s_work = atomicCAS(sc.ctr + 1, c, c + 1) == c;
-            __syncthreads();
-            const int mine = s_work;
-            __syncthreads();
-            if (!mine) break;
-            gather_chunk<V3>(ck.n_slots, row_off, upper, slot_f, f_local, forces, cs, ck, c);
-        }
-    }
-    // every tile is claimed: take the remaining chunks, waiting for each
-    for (;;) {
-        if (threadIdx.x == 0) s_work = atomicAdd(sc.ctr + 1, 1);
-        __syncthreads();
-        const int c = s_work;
-        __syncthreads();
-        if (c >= n_chunks) break;
-        const int need = (cs.chunk[3 * c + 2] + gpb - 1) / gpb;
-        long long k = 0;
-        while (!tiles_done(sc, need, known) && ++k < EAM_WAIT_POLLS) __nanosleep(128);
-        if (k >= EAM_WAIT_POLLS) {
-            if (threadIdx.x == 0) atomicOr(ck.err, MBF_DEV_WAIT_LIMIT);
-            break;
-        }
-        gather_chunk<V3>(ck.n_slots, row_off, upper, slot_f, f_local, forces, cs, ck, c);
-    }
+    chunk_sums_finish<NT>(cs, c, s, r0, r1);
 }
 
 // Site terms (engine/site_terms.py:440-479): U_i = F_i(rho-bar_i) + 1/2
@@ -1035,7 +920,6 @@ struct EamBufs {
     double *f_local;
     double *forces;
     double *per_atom;
-    int *sched;  // (n_atoms + 64) ints: the persistent kernel's counters and flags
 };
 
 // The density pass walks full rows (twice the force pass's upper halves);
@@ -1059,20 +943,24 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const
     PROF_END("eam_embed", st);
     MBF_CHECK_LAUNCH();
     const int gpb = EAM_BLOCK / LPA;
-    Sched sc;
-    sc.n_tiles = (S.n_atoms + gpb - 1) / gpb;
-    const int n_groups = (sc.n_tiles + TILE_GROUP - 1) / TILE_GROUP;
-    sc.ctr = B.sched;
-    sc.gcnt = B.sched + 4;
-    sc.flag = sc.gcnt + n_groups;
-    if (cudaMemsetAsync(B.sched, 0, sizeof(int) * (size_t)(4 + n_groups + sc.n_tiles), st) != cudaSuccess)
-        return MBF_ERR_CUDA;
-    g = persistent_grid(sc.n_tiles, EAM_BLOCK, (const void *)eam_force_gather<T, LPA, Pol, ORTHO>);
-    PROF_BEGIN("eam_force_gather", st);
-    eam_force_gather<T, LPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, P,
-                                                                  rc2, B.pk, B.aux, slot, B.f_local, B.per_atom,
-                                                                  B.forces, cs, n_chunks, sc, ck);
-    PROF_END("eam_force_gather", st);
+    g = persistent_grid((S.n_atoms + gpb - 1) / gpb, EAM_BLOCK, (const void *)eam_force<T, LPA, Pol, ORTHO>);
+    PROF_BEGIN("eam_force", st);
+    eam_force<T, LPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, P, rc2,
+                                                           B.pk, B.aux, slot, B.f_local, B.per_atom, ck);
+    PROF_END("eam_force", st);
+    MBF_CHECK_LAUNCH();
+    PROF_BEGIN("eam_gather_reduce", st);
+    const int nt = chunk_block(S.n_atoms, n_chunks);
+    if (nt == 128)
+        eam_gather_reduce<V3, 128><<<n_chunks, 128, 0, st>>>(ck.n_slots, nl->row_off, nl->upper, slot, B.f_local,
+                                                             B.forces, cs, ck);
+    else if (nt == 256)
+        eam_gather_reduce<V3, 256><<<n_chunks, 256, 0, st>>>(ck.n_slots, nl->row_off, nl->upper, slot, B.f_local,
+                                                             B.forces, cs, ck);
+    else
+        eam_gather_reduce<V3, 512><<<n_chunks, 512, 0, st>>>(ck.n_slots, nl->row_off, nl->upper, slot, B.f_local,
+                                                             B.forces, cs, ck);
+    PROF_END("eam_gather_reduce", st);
     MBF_CHECK_LAUNCH();
     if (so.e) {
         g = persistent_grid((S.n_atoms + 15) / 16, EAM_BLOCK, (const void *)eam_site<T, Pol, ORTHO>);
@@ -1204,7 +1092,6 @@ static int eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
     B.f_local = ws_at<double>(workspace, L.f_local);
     B.forces = forces;
     B.per_atom = ws_at<double>(workspace, L.per_atom);
-    B.sched = ws_at<int>(workspace, L.sched);
     ChunkSums cs = {plan->chunk, plan->chunk_first, B.per_atom, ws_at<double>(workspace, L.partial), energy, virial,
                     ws_at<unsigned>(workspace, L.sdone)};
     if (cudaMemsetAsync(cs.sdone, 0, sizeof(unsigned) * (size_t)sys->n_struct, st) != cudaSuccess)

@@ -122,10 +122,8 @@ constexpr int ERR_CLEAR_BYTES = 16;
 //   slot_b   (n_slots, 2) doubles (Tersoff bond order and its derivative)
 //   partial  (n_chunks, ATOM_ACC) doubles
 //   sdone    (n_chunks,) completion counters of the per-structure sums
-//   sched    (n_atoms + 64) ints: work counters and per-tile completion
-//            flags of a persistent kernel that claims work in order
 struct EvalLayout {
-    size_t err, per_atom, f_local, atom_aux, pack, slot, slot_b, partial, sdone, sched, total;
+    size_t err, per_atom, f_local, atom_aux, pack, slot, slot_b, partial, sdone, total;
 };
 
 static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -151,8 +149,6 @@ static inline EvalLayout eval_layout(int n_atoms, long long n_slots, int n_chunk
     o = align256(o + sizeof(double) * (size_t)(n_chunks > 0 ? n_chunks : 1) * ATOM_ACC);
     L.sdone = o;
     o = align256(o + sizeof(unsigned) * (size_t)(n_chunks > 0 ? n_chunks : 1));
-    L.sched = o;
-    o = align256(o + sizeof(int) * ((size_t)(n_atoms > 0 ? n_atoms : 0) + 64));
     L.total = o;
     return L;
 }

@@ -1112,7 +1112,7 @@ def main():
     del pi, pj, d, s, r, inside, cross
     force_flops = roofline.eam_force_flops(n_in - n_cross, n_cross)
     force_bytes = roofline.eam_force_bytes(n_atoms, dnl.n_slots)
-    dom = "eam_force_gather"
+    dom = "eam_force"
     cnt, tot = prof.get(dom, (1, float("nan")))
     t_dom = tot / cnt * 1e-3
     scratch = torch.empty(148 * 8 * 256 * 8 * 4, dtype=torch.uint8, device=dev)
