@@ -34,9 +34,9 @@ constexpr int EAM_BLOCK = 128;
 #ifndef MBF_EAM_MINB
 #define MBF_EAM_MINB 5
 #endif
-// The same for the float32 density kernel.
+// The same for the float32 density kernel (48 registers, no spills).
 #ifndef MBF_EAM_DENS_MINB
-#define MBF_EAM_DENS_MINB 8
+#define MBF_EAM_DENS_MINB 10
 #endif
 
 enum { F_SPLINE = 1, F_SPLINE_R = 2, F_Z_DENS = 3, F_Z_PAIR = 4, F_Z_CROSS = 5, F_Z_EMB = 6 };
@@ -798,9 +798,14 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
 // (ChunkSums): a block per chunk of the reduction plan, 8 lanes per atom;
 // besides its atom's force each group adds the atom's record (entries sub
 // and sub + 8 of its 8 lanes), and the block finishes the chunk's and, if
-// last, the structure's sums.
+// last, the structure's sums.  The kernel waits on memory, so every load of
+// an atom is issued before any is used: its first GATHER_UNROLL x 8 lower
+// slots (an fcc row's lower half is about 40), its record and its
+// upper-pair force, with the next atom's row bounds one iteration ahead.
+constexpr int GATHER_UNROLL = 5;
+
 template <typename V3, int NT>
-__global__ void __launch_bounds__(NT) eam_gather_reduce(int n_slots, const int *__restrict__ row_off,
+__global__ void __launch_bounds__(NT, 1024 / NT) eam_gather_reduce(int n_slots, const int *__restrict__ row_off,
                                                         const int *__restrict__ upper, const V3 *__restrict__ slot_f,
                                                         const double *__restrict__ f_local,
                                                         double *__restrict__ forces, ChunkSums cs, Chk ck) {
@@ -809,7 +814,6 @@ __global__ void __launch_bounds__(NT) eam_gather_reduce(int n_slots, const int *
     const int s = cs.chunk[3 * c], a0 = cs.chunk[3 * c + 1], a1 = cs.chunk[3 * c + 2];
     const int sub = threadIdx.x & (LPA - 1), grp = threadIdx.x / LPA;
     double r0 = 0.0, r1 = 0.0;
-    // the next atom's row bounds are loaded one iteration ahead
     int nb = 0, nu = 0, ne = 0;
     if (a0 + grp < a1) {
         nb = row_off[a0 + grp];
@@ -825,30 +829,50 @@ __global__ void __launch_bounds__(NT) eam_gather_reduce(int n_slots, const int *
             ne = row_off[a + G + 1];
             nu = upper[a + G];
         }
-        double fx = 0, fy = 0, fz = 0;
+        double fx = 0, fy = 0, fz = 0, fl = 0.0;
         if (a < a1) {
             if (!row_ok(beg, up, rend, n_slots)) {
                 chk_flush(ck, 1, 31, a);
                 beg = up = 0;
             }
-#pragma unroll 4
-            for (int q = beg + sub; q < up; q += LPA) {
-                const V3 w = slot_f[q];
-                fx += (double)w.x;
-                fy += (double)w.y;
-                fz += (double)w.z;
-            }
             const double *rec = cs.per_atom + (size_t)a * ATOM_ACC;
-            r0 += rec[sub];
-            if (sub < ATOM_ACC - LPA) r1 += rec[LPA + sub];
+            const double ra = rec[sub];
+            const double rb = sub < ATOM_ACC - LPA ? rec[LPA + sub] : 0.0;
+            if (sub < 3) fl = f_local[3 * (size_t)a + sub];
+            V3 w[GATHER_UNROLL];
+#pragma unroll
+            for (int k = 0; k < GATHER_UNROLL; ++k) {
+                const int q = beg + sub + k * LPA;
+                if (q < up) w[k] = slot_f[q];
+            }
+#pragma unroll
+            for (int k = 0; k < GATHER_UNROLL; ++k) {
+                if (beg + sub + k * LPA < up) {
+                    fx += (double)w[k].x;
+                    fy += (double)w[k].y;
+                    fz += (double)w[k].z;
+                }
+            }
+            for (int q = beg + sub + GATHER_UNROLL * LPA; q < up; q += LPA) {
+                const V3 v = slot_f[q];
+                fx += (double)v.x;
+                fy += (double)v.y;
+                fz += (double)v.z;
+            }
+            r0 += ra;
+            r1 += rb;
         }
         fx = group_sum<LPA>(fx);
         fy = group_sum<LPA>(fy);
         fz = group_sum<LPA>(fz);
+        // lane k (k < 3) of the group holds component k of the upper-pair sum
+        const double gx = __shfl_sync(MBF_FULL, fl, 0, LPA);
+        const double gy = __shfl_sync(MBF_FULL, fl, 1, LPA);
+        const double gz = __shfl_sync(MBF_FULL, fl, 2, LPA);
         if (sub == 0 && a < a1) {
-            forces[3 * (size_t)a] = f_local[3 * (size_t)a] + fx;
-            forces[3 * (size_t)a + 1] = f_local[3 * (size_t)a + 1] + fy;
-            forces[3 * (size_t)a + 2] = f_local[3 * (size_t)a + 2] + fz;
+            forces[3 * (size_t)a] = gx + fx;
+            forces[3 * (size_t)a + 1] = gy + fy;
+            forces[3 * (size_t)a + 2] = gz + fz;
         }
     }
     chunk_sums_finish<NT>(cs, c, s, r0, r1);
