@@ -517,6 +517,25 @@ def run_md(args, world, rank, local):
            "job_ms": [round(1e3 * j, 3) for j in jobs],
            "path": f"md.NVE(numpy in) + run({n_e2e}) + results() + positions (graph captured inside), "
                    "mean of 3 jobs"}
+    # energy conservation over drift_ps picoseconds (dt 1 fs) in both
+    # precisions: the slope of E_tot per atom against time, against the
+    # reference's bar for a mixed-precision GPU path (<= 1e-5 eV/atom/ps over
+    # 10 ps, docs/adr/0016-gpu-support.md:115-123)
+    drift_rec = None
+    if getattr(args, "drift_ps", 0) > 0:
+        n_dr = int(round(args.drift_ps * 1000))
+        drift_rec = {"ps": args.drift_ps, "steps": n_dr, "bar_mixed_eV_per_atom_per_ps": 1e-5}
+        for prec in ("mixed", "fp64"):
+            s3 = md.NVE(_md_potential(kind, prec), lat, pos, types, temperature=300.0, seed=0,
+                        steps_per_graph=50, device=dev)
+            s3.run(n_dr)
+            r3 = s3.results()
+            t_ps = np.arange(1, len(r3["e_tot"]) + 1) * 1e-3
+            slope = float(np.polyfit(t_ps, r3["e_tot"] / n_atoms, 1)[0])
+            drift_rec[prec] = {"drift_eV_per_atom_per_ps": slope,
+                               "max_abs_deviation_eV_per_atom": float(np.abs(r3["drift"]).max() / n_atoms),
+                               "rebuilds": int(r3["rebuilds"])}
+            del s3
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         n = 3 if n_atoms > 10000 else 10
@@ -543,6 +562,7 @@ def run_md(args, world, rank, local):
                        "final_drift_ev_per_atom": float(drift[-1] / n_atoms),
                        "max_skin_displacement": float(res["skin_displacement"].max()),
                        "rebuilds": int(res["rebuilds"])},
+            "nve_drift": drift_rec,
             "e2e": e2e, "cpu_baseline": cpu, "roofline": None}
     emit(args, line)
     return 0
@@ -954,6 +974,8 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--cells", type=int, default=40)
     ap.add_argument("--lanes", type=int, default=4, help="EAM lanes per atom (1, 2, 4 or 8)")
+    ap.add_argument("--drift-ps", type=float, default=0.0,
+                    help="MD workloads: also run this many ps (dt 1 fs) in both precisions for the drift")
     ap.add_argument("--no-sub-records", action="store_true",
                     help="default workload: skip the other configurations' sub-records")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1249,15 +1271,15 @@ def main():
 SUB_RECORDS = (
     ("fit_sic256", {"steps": 10, "warmup": 3, "e2e_steps": 10}),
     ("batched_si512", {"steps": 10, "warmup": 3, "e2e_steps": 5}),
-    ("md_tersoff_si4096", {"steps": 10, "warmup": 3, "e2e_steps": 1}),
-    ("md_sw_si64k", {"steps": 5, "warmup": 3, "e2e_steps": 1}),
+    ("md_tersoff_si4096", {"steps": 10, "warmup": 3, "e2e_steps": 1, "drift_ps": 10.0}),
+    ("md_sw_si64k", {"steps": 5, "warmup": 3, "e2e_steps": 1, "drift_ps": 10.0}),
 )
 
 
 def _summary(line):
     keep = ("metric", "value", "unit", "ms_per_step", "ms_per_md_step", "dtype", "structures_per_s",
             "per_structure_launches", "gpu_launches_per_step", "energy", "atom_force_evals_per_s",
-            "n_variables", "check")
+            "n_variables", "check", "nve_drift")
     out = {k: line[k] for k in keep if k in line}
     out["workload"] = line["config"].get("workload")
     e = line.get("e2e") or {}

@@ -164,3 +164,27 @@ def test_fused_kicks_equal_separate_launches(cuda_device, graph):
     for key in ("e_pot", "e_kin", "skin_displacement"):
         np.testing.assert_array_equal(rb[key], rs[key])
     assert rb["rebuilds"] == rs["rebuilds"]
+
+
+def drift_per_ps(e_tot, n_atoms, dt_fs=1.0):
+    """Least-squares slope of the total energy per atom against time, eV /
+    atom / ps (the NVE drift measure of the reference's GPU plan)."""
+    t_ps = np.arange(1, len(e_tot) + 1) * dt_fs * 1e-3
+    return float(np.polyfit(t_ps, np.asarray(e_tot) / n_atoms, 1)[0])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_nve_drift_over_10_ps(cuda_device, precision):
+    """Mixed-precision NVE conserves energy to the reference's bar for a GPU
+    path: drift <= 1e-5 eV/atom/ps over 10 ps (docs/adr/0016-gpu-support.md
+    :115-123 of the reference).  Stillinger-Weber Si, 8^3 cells (4096 atoms),
+    displacements 0.1 A, 300 K, dt 1 fs, 10,000 steps with the criterion
+    rebuilds; float64 alongside for comparison."""
+    lat, pos, types = cubic(DIAMOND, 5.431, 8, ["Si"] * 8, rattle=0.1, seed=3)
+    pot = ak.StillingerWeberPotential(SW_SI, species=["Si"], precision=precision)
+    sim = md.NVE(pot, lat, pos, types, temperature=300.0, seed=0, steps_per_graph=50)
+    sim.run(10_000)
+    res = sim.results()
+    assert len(res["e_tot"]) == 10_000
+    slope = drift_per_ps(res["e_tot"], len(pos))
+    assert abs(slope) <= 1e-5, slope
