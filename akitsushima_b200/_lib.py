@@ -106,6 +106,12 @@ _SIGS = {
                                  ctypes.POINTER(MbfEamTables), ctypes.POINTER(MbfReducePlan), _i, _i,
                                  _vp, _vp, _vp, _vp]),
     "mbf_eam_eval_static_status": (_i, [ctypes.POINTER(_i), _vp]),
+    "mbf_eam_embedding": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
+                               ctypes.POINTER(MbfEamTables), ctypes.POINTER(MbfReducePlan), _i, _i,
+                               _vp, _sz, _vp, _vp]),
+    "mbf_eam_forces": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
+                            ctypes.POINTER(MbfEamTables), ctypes.POINTER(MbfReducePlan), _i, _i,
+                            _vp, _sz, _vp, _vp, _vp, _vp, _vp]),
     "mbf_tersoff_eval": (_i, [ctypes.POINTER(MbfSystem), ctypes.POINTER(MbfNlist),
                               ctypes.POINTER(MbfTersoffTables), ctypes.POINTER(MbfReducePlan), _i, _i,
                               _vp, _sz, _vp, _vp, _vp, _vp]),

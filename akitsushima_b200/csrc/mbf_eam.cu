@@ -946,26 +946,34 @@ struct EamBufs {
     double *per_atom;
 };
 
+// Phases of an evaluation: the density and embedding passes (F'(rho-bar)
+// of every atom), then the force pass and the gather.  A spatially split
+// structure runs them apart, with the halo atoms' F' exchanged in between.
+enum { PH_EMBED = 1, PH_FORCE = 2, PH_ALL = 3 };
+
 // The density pass walks full rows (twice the force pass's upper halves);
 // it takes 4 lanes per atom, or the force pass's lanes when that is more.
 template <typename T, int LPA, class Pol, bool ORTHO>
 static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const EamDev &E, double rc2,
                       const EamBufs &B, Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks,
-                      cudaStream_t st) {
+                      int phases, cudaStream_t st) {
     typedef typename SlotVec<T>::type V3;
     constexpr int DLPA = LPA >= 4 ? LPA : 4;
     V3 *slot = static_cast<V3 *>(B.slot);
-    const int dgpb = EAM_BLOCK / DLPA;
-    int g = persistent_grid((S.n_atoms + dgpb - 1) / dgpb, EAM_BLOCK,
-                            (const void *)eam_density<T, DLPA, Pol, ORTHO>);
-    PROF_BEGIN("eam_density", st);
-    eam_density<T, DLPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, rc2, B.aux, ck);
-    PROF_END("eam_density", st);
-    MBF_CHECK_LAUNCH();
-    PROF_BEGIN("eam_embed", st);
-    eam_embed<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S, E, B.pk, B.aux, ck);
-    PROF_END("eam_embed", st);
-    MBF_CHECK_LAUNCH();
+    int g = 0;
+    if (phases & PH_EMBED) {
+        const int dgpb = EAM_BLOCK / DLPA;
+        g = persistent_grid((S.n_atoms + dgpb - 1) / dgpb, EAM_BLOCK, (const void *)eam_density<T, DLPA, Pol, ORTHO>);
+        PROF_BEGIN("eam_density", st);
+        eam_density<T, DLPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, rc2, B.aux, ck);
+        PROF_END("eam_density", st);
+        MBF_CHECK_LAUNCH();
+        PROF_BEGIN("eam_embed", st);
+        eam_embed<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S, E, B.pk, B.aux, ck);
+        PROF_END("eam_embed", st);
+        MBF_CHECK_LAUNCH();
+    }
+    if (!(phases & PH_FORCE)) return MBF_OK;
     const int gpb = EAM_BLOCK / LPA;
     g = persistent_grid((S.n_atoms + gpb - 1) / gpb, EAM_BLOCK, (const void *)eam_force<T, LPA, Pol, ORTHO>);
     PROF_BEGIN("eam_force", st);
@@ -997,8 +1005,8 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const
 template <typename T, class Pol, bool ORTHO>
 static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const Pol &P, const EamDev &E,
                             double rc2, const EamBufs &B, Chk ck, const SiteOut &so, const ChunkSums &cs,
-                            int n_chunks, cudaStream_t st) {
-#define MBF_EAM_LAUNCH(L) eam_launch<T, L, Pol, ORTHO>(S, nl, P, E, rc2, B, ck, so, cs, n_chunks, st)
+                            int n_chunks, int phases, cudaStream_t st) {
+#define MBF_EAM_LAUNCH(L) eam_launch<T, L, Pol, ORTHO>(S, nl, P, E, rc2, B, ck, so, cs, n_chunks, phases, st)
     switch (lpa) {
         case 1: return MBF_EAM_LAUNCH(1);
         case 2: return MBF_EAM_LAUNCH(2);
@@ -1012,9 +1020,9 @@ static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, cons
 template <typename T, class Pol>
 static int eam_dispatch(const Pol &P, int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E, double rc2,
                         const EamBufs &B, Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks,
-                        cudaStream_t st) {
-    return S.ortho ? eam_dispatch_lpa<T, Pol, true>(lpa, S, nl, P, E, rc2, B, ck, so, cs, n_chunks, st)
-                   : eam_dispatch_lpa<T, Pol, false>(lpa, S, nl, P, E, rc2, B, ck, so, cs, n_chunks, st);
+                        int phases, cudaStream_t st) {
+    return S.ortho ? eam_dispatch_lpa<T, Pol, true>(lpa, S, nl, P, E, rc2, B, ck, so, cs, n_chunks, phases, st)
+                   : eam_dispatch_lpa<T, Pol, false>(lpa, S, nl, P, E, rc2, B, ck, so, cs, n_chunks, phases, st);
 }
 
 // The constants of the one- and two-element Zhou path from the host copies
@@ -1059,26 +1067,35 @@ static bool make_zk(const mbf_eam_tables *tab, ZK<T> &K) {
 template <typename T>
 static int eam_select(const mbf_eam_tables *tab, int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E,
                       double rc2, const EamBufs &B, Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks,
-                      cudaStream_t st) {
+                      int ph, cudaStream_t st) {
     ZK<T> K;
     if (make_zk<T>(tab, K)) {
-        if (tab->ns == 1) return eam_dispatch<T>(PolZ2<T, 1>{K}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, st);
-        return eam_dispatch<T>(PolZ2<T, 2>{K}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, st);
+        if (tab->ns == 1)
+            return eam_dispatch<T>(PolZ2<T, 1>{K}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, ph, st);
+        return eam_dispatch<T>(PolZ2<T, 2>{K}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, ph, st);
     }
     if (tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP)
-        return eam_dispatch<T>(PolZSmem<T>{E}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, st);
-    return eam_dispatch<T>(PolGeneric<T>{E}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, st);
+        return eam_dispatch<T>(PolZSmem<T>{E}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, ph, st);
+    return eam_dispatch<T>(PolGeneric<T>{E}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, ph, st);
 }
 
 }  // namespace mbf
 
 using namespace mbf;
 
+// The evaluation's phases (PH_*): with PH_EMBED alone F'(rho-bar) of every
+// atom is copied to fprime_out; with PH_FORCE alone fprime_in replaces F'
+// before the force pass (the workspace must hold the same list's embedding
+// pass); both: the whole evaluation.
 static int eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
                     const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
                     size_t workspace_bytes, double *forces, double *energy, double *virial, const SiteOut &so,
-                    void *stream) {
-    if (!sys || !nl || !tab || !plan || !workspace || !forces || !energy || !virial) return MBF_ERR_ARGUMENT;
+                    void *stream, int phases = PH_ALL, double *fprime_out = nullptr,
+                    const double *fprime_in = nullptr) {
+    if (!sys || !nl || !tab || !plan || !workspace) return MBF_ERR_ARGUMENT;
+    if ((phases & PH_FORCE) && (!forces || !energy || !virial)) return MBF_ERR_ARGUMENT;
+    if (phases == PH_EMBED && !fprime_out) return MBF_ERR_ARGUMENT;
+    if (phases == PH_FORCE && !fprime_in) return MBF_ERR_ARGUMENT;
     if (precision != MBF_FP64 && precision != MBF_MIXED) return MBF_ERR_ARGUMENT;
     if (nl->n_atoms != sys->n_atoms || tab->ns <= 0 || sys->n_struct <= 0) return MBF_ERR_ARGUMENT;
     if (nl->n_slots < 0 || nl->n_slots > 0x7fffff00LL) return MBF_ERR_ARGUMENT;
@@ -1095,8 +1112,9 @@ static int eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
     ck.n_atoms = sys->n_atoms;
     ck.n_slots = (int)nl->n_slots;
     ck.ns = tab->ns;
-    if (cudaMemsetAsync(ck.err, 0, ERR_CLEAR_BYTES, st) != cudaSuccess) return MBF_ERR_CUDA;
+    if ((phases & PH_EMBED) && cudaMemsetAsync(ck.err, 0, ERR_CLEAR_BYTES, st) != cudaSuccess) return MBF_ERR_CUDA;
     if (sys->n_atoms == 0) {
+        if (!(phases & PH_FORCE)) return MBF_OK;
         if (cudaMemsetAsync(energy, 0, sizeof(double) * sys->n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
         if (cudaMemsetAsync(virial, 0, sizeof(double) * 9 * sys->n_struct, st) != cudaSuccess) return MBF_ERR_CUDA;
         return MBF_OK;
@@ -1118,12 +1136,45 @@ static int eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
     B.per_atom = ws_at<double>(workspace, L.per_atom);
     ChunkSums cs = {plan->chunk, plan->chunk_first, B.per_atom, ws_at<double>(workspace, L.partial), energy, virial,
                     ws_at<unsigned>(workspace, L.sdone)};
-    if (cudaMemsetAsync(cs.sdone, 0, sizeof(unsigned) * (size_t)sys->n_struct, st) != cudaSuccess)
-        return MBF_ERR_CUDA;
+    const size_t n = (size_t)sys->n_atoms;
+    if (phases & PH_FORCE) {
+        if (cudaMemsetAsync(cs.sdone, 0, sizeof(unsigned) * (size_t)sys->n_struct, st) != cudaSuccess)
+            return MBF_ERR_CUDA;
+        // F' of every atom into the records the force pass gathers (column 3
+        // of pk, column 0 of aux), strided copies on the stream
+        if (!(phases & PH_EMBED) &&
+            (cudaMemcpy2DAsync(reinterpret_cast<double *>(B.pk) + 3, sizeof(double4), fprime_in, sizeof(double),
+                               sizeof(double), n, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+             cudaMemcpy2DAsync(B.aux, 2 * sizeof(double), fprime_in, sizeof(double), sizeof(double), n,
+                               cudaMemcpyDeviceToDevice, st) != cudaSuccess))
+            return MBF_ERR_CUDA;
+    }
     const double rc2 = tab->r_cut * tab->r_cut;
-    if (precision == MBF_FP64)
-        return eam_select<double>(tab, lpa, S, nl, E, rc2, B, ck, so, cs, plan->n_chunks, st);
-    return eam_select<float>(tab, lpa, S, nl, E, rc2, B, ck, so, cs, plan->n_chunks, st);
+    int rc = precision == MBF_FP64
+                 ? eam_select<double>(tab, lpa, S, nl, E, rc2, B, ck, so, cs, plan->n_chunks, phases, st)
+                 : eam_select<float>(tab, lpa, S, nl, E, rc2, B, ck, so, cs, plan->n_chunks, phases, st);
+    if (rc != MBF_OK || phases != PH_EMBED) return rc;
+    if (cudaMemcpy2DAsync(fprime_out, sizeof(double), B.aux, 2 * sizeof(double), sizeof(double), n,
+                          cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return MBF_ERR_CUDA;
+    return MBF_OK;
+}
+
+extern "C" int mbf_eam_embedding(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                                 const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
+                                 size_t workspace_bytes, double *fprime, void *stream) {
+    SiteOut none = {nullptr, nullptr, nullptr};
+    return eam_eval(sys, nl, tab, plan, precision, lanes_per_atom, workspace, workspace_bytes, nullptr, nullptr,
+                    nullptr, none, stream, PH_EMBED, fprime, nullptr);
+}
+
+extern "C" int mbf_eam_forces(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                              const mbf_reduce_plan *plan, int precision, int lanes_per_atom, void *workspace,
+                              size_t workspace_bytes, const double *fprime, double *forces, double *energy,
+                              double *virial, void *stream) {
+    SiteOut none = {nullptr, nullptr, nullptr};
+    return eam_eval(sys, nl, tab, plan, precision, lanes_per_atom, workspace, workspace_bytes, forces, energy,
+                    virial, none, stream, PH_FORCE, nullptr, fprime);
 }
 
 extern "C" int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,

@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .potential import DevicePotential
+from .potential import DevicePotential, EvalResult, _set_last_ws, precision_code, workspace
 
 ZHOU_KEYS = ("r_e", "f_e", "rho_e", "rho_s", "alpha", "beta", "A", "B", "kappa", "lambda",
              "Fn0", "Fn1", "Fn2", "Fn3", "F0", "F1", "F2", "F3", "eta", "F_e")
@@ -286,6 +286,55 @@ class EAMPotential(DevicePotential):
     lane_choices = (1, 2, 4, 8)
     # lanes of one atom's group in the force pass: 4 measured fastest on B200 (256k Cu-Ni)
     lanes_per_atom = 4
+
+    # ---- the evaluation in two halves (a structure split over ranks) --------
+    def _split_ws(self, batch, dlist, ws):
+        nbytes = int(_lib.lib().mbf_eval_workspace_bytes(batch.n_atoms, dlist.n_slots, batch.n_chunks))
+        if ws is None:
+            return workspace(batch.device, nbytes)
+        if ws.numel() < nbytes:
+            raise ValueError(f"workspace of {ws.numel()} bytes, {nbytes} needed")
+        return ws
+
+    def embedding(self, batch, dlist, precision=None, ws=None):
+        """The density and embedding passes: F'(rho-bar) of every atom of
+        ``batch`` (a new device float64 tensor).  The values of atoms whose
+        neighbourhood lies inside the batch are exact; the caller replaces
+        the others' (a spatial split's halo atoms) by their owners' before
+        forces_from_embedding, which must get the same ``ws``
+        (mbf_eam_embedding)."""
+        prec = precision_code(precision or self.precision)
+        ws = self._split_ws(batch, dlist, ws)
+        fp = torch.empty(batch.n_atoms, dtype=torch.float64, device=batch.device)
+        L = _lib.lib()
+        rc = L.mbf_eam_embedding(batch.mbf_system(), dlist.mbf_nlist(), self.tables(batch.device)[0],
+                                 batch.reduce_plan(), prec, int(self.lanes_per_atom), _lib.ptr(ws), ws.numel(),
+                                 _lib.ptr(fp), torch.cuda.current_stream(batch.device).cuda_stream)
+        _lib.check(rc, "EAMPotential.embedding")
+        _set_last_ws(self, ws)
+        return fp
+
+    def forces_from_embedding(self, batch, dlist, fprime, precision=None, ws=None, out=None):
+        """The force pass and the gather with the given F'(rho-bar) per atom
+        (mbf_eam_forces); ``ws`` the workspace of the embedding call.
+        Returns EvalResult; the energy and virial are the sums of the
+        records the batch's reduction plan covers."""
+        prec = precision_code(precision or self.precision)
+        ws = self._split_ws(batch, dlist, ws)
+        dev = batch.device
+        if out is None:
+            out = EvalResult(torch.empty(batch.n_struct, dtype=torch.float64, device=dev),
+                             torch.empty((batch.n_atoms, 3), dtype=torch.float64, device=dev),
+                             torch.empty((batch.n_struct, 9), dtype=torch.float64, device=dev))
+        fp = fprime.to(device=dev, dtype=torch.float64).contiguous()
+        L = _lib.lib()
+        rc = L.mbf_eam_forces(batch.mbf_system(), dlist.mbf_nlist(), self.tables(dev)[0], batch.reduce_plan(), prec,
+                              int(self.lanes_per_atom), _lib.ptr(ws), ws.numel(), _lib.ptr(fp),
+                              _lib.ptr(out.forces), _lib.ptr(out.energy), _lib.ptr(out.virial),
+                              torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(rc, "EAMPotential.forces_from_embedding")
+        _set_last_ws(self, ws)
+        return out
 
     def _call(self, L, sysd, nld, tabs, plan, prec, ws, nbytes, forces, energy, virial, stream):
         return L.mbf_eam_eval(sysd, nld, tabs[0], plan, prec, int(self.lanes_per_atom), ws, nbytes,

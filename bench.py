@@ -1000,6 +1000,8 @@ def main():
         return run_fit(args, world, rank, local)
     if args.workload in ("eam_setfl_cuni_256k", "sw_gesn_64k"):
         return run_perf_path(args, world, rank, local)
+    if world > 1 and args.impl != "reference":
+        return run_eam_spatial(args, world, rank, local)
     lat, pos, ids = make_cuni(args.cells)
     n_atoms = len(pos)
     workload = f"eam_zhou_cuni_fcc{args.cells}^3_{n_atoms}_atoms"
@@ -1262,6 +1264,119 @@ def main():
             "fp64_gpu": fp64_gpu, "errors": errors, "e2e": e2e, "cpu_baseline": cpu,
             "check": {"energy_per_atom": e / n_atoms, "max_abs_force_sum": float(np.abs(f.sum(0)).max())},
             "configs": subs}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_eam_spatial(args, world, rank, local):
+    """The headline alloy on N GPUs, weak scaling: fcc Cu-Ni of 40 x 40 x
+    40 N cells (256,000 N atoms, the same generator), one slab of 256,000
+    atoms per rank along z with a halo of one list radius.  A step is one
+    distributed evaluation: the embedding pass, the exchange of the halo
+    atoms' F'(rho-bar) (an NCCL all-gather of each rank's boundary block),
+    the force pass and gather, and the all-reduce of energy and virial; the
+    forces stay with their owners, as they would in a spatially split MD
+    run.  Timed with CUDA events, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    import akitsushima_b200 as ak
+    from akitsushima_b200 import _lib
+    from akitsushima_b200.spatial import SlabState, exchange_fprime
+    backend = os.environ.get("MBF_BENCH_BACKEND", "nccl")
+    n_dev = torch.cuda.device_count()
+    torch.cuda.set_device(local % n_dev)
+    dist.init_process_group(backend, timeout=timedelta(seconds=120))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    rng = np.random.default_rng(0)
+    a, c = 3.58, args.cells
+    frac = (np.asarray([[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0]], float)[None]
+            + np.stack(np.meshgrid(np.arange(c), np.arange(c), np.arange(c * world), indexing="ij"),
+                       -1).reshape(-1, 3)[:, None]).reshape(-1, 3)
+    pos = frac * a + rng.normal(0.0, 0.08, frac.shape)
+    ids = np.random.default_rng(1).integers(0, 2, len(pos)).astype(np.int32)
+    lat = np.diag([a * c, a * c, a * c * world])
+    n_atoms = len(pos)
+    fn = ak.force_fn_from_config({"type": "EAM", "form": "zhou2004", "elements": ["Cu", "Ni"]},
+                                 precision=args.precision)
+    pot = fn.engine.potentials[0]
+    pot.lanes_per_atom = args.lanes
+    st = SlabState(pot, lat, pos, ids, rank, world, 0.3, dev)
+    st.batch.set_positions(pos[st.local], check=False)
+    out = None
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    ew = torch.zeros(10, dtype=torch.float64, device=dev)
+
+    def step():
+        nonlocal out
+        fp = pot.embedding(st.batch, st.dlist, ws=st.ws)
+        fp = exchange_fprime(fp, st.plan)
+        out = pot.forces_from_embedding(st.batch, st.dlist, fp, ws=st.ws, out=out)
+        ew[0] = out.energy[0]
+        ew[1:] = out.virial[0]
+        dist.all_reduce(ew)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    _lib.profile_begin()
+    step()
+    prof = _lib.profile_end()
+    with ClockSampler(local % n_dev) as clk:
+        dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            step()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        dist.barrier()
+    ms = sum(x.elapsed_time(y) for x, y in ev) / args.steps
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    e_total = float(ew[0].item())
+    # end to end: host arrays in, every rank the whole result back
+    sfn = ak.SpatialForceFn(pot, skin=0.3, device=dev)
+    types = [("Cu", "Ni")[k] for k in ids.tolist()]
+    sfn(lat, pos, types)
+    dist.barrier()
+    t0 = time.perf_counter()
+    n_e2e = max(1, min(args.e2e_steps, 10))
+    for _ in range(n_e2e):
+        e_, F_, s_ = sfn(lat, pos, types)
+    t_e2e = (time.perf_counter() - t0) / n_e2e
+    tt = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    t_e2e = float(tt.item())
+    clocks = clk.summary()
+    n_local = len(st.local)
+    dist.barrier()
+    del st, sfn
+    dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": n_atoms / (ms * 1e-3), "unit": "atoms/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+            "data": "synthetic",
+            "config": {"workload": f"eam_zhou_cuni_fcc{c}x{c}x{c * world}_{n_atoms}_atoms_spatial",
+                       "potential": "Zhou 2004 EAM Cu-Ni", "n_atoms": n_atoms, "atoms_per_gpu": n_atoms // world,
+                       "a": a, "sigma": 0.08, "skin": 0.3, "precision": args.precision,
+                       "l2": "256 MB scratch write between steps, outside the timed events",
+                       "parallelism": f"spatial{world}: z slabs, halo of one list radius, F' all-gather "
+                                      f"({backend}), energy / virial all-reduce"},
+            "gpu_launches": int(sum(c_ for c_, _ in prof.values()) * args.steps),
+            "kernels": {k: {"launches": c_, "ms_per_launch": t_ / c_} for k, (c_, t_) in prof.items()},
+            "halo": {"local_atoms_rank0": n_local, "owned_atoms_rank0": n_atoms // world},
+            "clocks": clocks, "check": {"energy_per_atom": e_total / n_atoms},
+            "e2e": {"value": n_atoms / t_e2e, "unit": "atoms/s", "h2d_bytes_per_step": n_atoms * 24,
+                    "d2h_bytes_per_step": n_atoms * 24 + 80, "ms_per_step": t_e2e * 1e3,
+                    "path": "SpatialForceFn(lattice, numpy positions, species names) on every rank -> "
+                            "the whole (E, F, stress) on every rank"},
+            "cpu_baseline": None, "roofline": None}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -218,6 +218,26 @@ int mbf_eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_table
                  void *workspace, size_t workspace_bytes,
                  double *forces, double *energy, double *virial, void *stream);
 
+/* The same evaluation in its two halves, for a structure split over ranks
+ * (a slab per GPU with a halo of one list radius): the reference's phases 1-2
+ * and 3-4 (engine/_eam_kernels.py:241-274 and :276-307).
+ * mbf_eam_embedding runs the density and embedding passes and writes
+ * F'(rho-bar) of every atom to fprime (n_atoms doubles, device).  The
+ * owned atoms' values are exact; a halo atom's neighbourhood is cut, so
+ * the caller replaces its F' by the value its owner computed.
+ * mbf_eam_forces then takes that array, runs the force pass and the
+ * gather, and writes forces, energy and virial as mbf_eam_eval does (the
+ * reduction plan chooses whose records are summed).  Both calls use the
+ * same workspace, list and tables; the workspace keeps rho-bar, F and the
+ * positions between them.                                                 */
+int mbf_eam_embedding(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                      const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
+                      void *workspace, size_t workspace_bytes, double *fprime, void *stream);
+int mbf_eam_forces(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_tables *tab,
+                   const mbf_reduce_plan *plan, int precision, int lanes_per_atom,
+                   void *workspace, size_t workspace_bytes, const double *fprime,
+                   double *forces, double *energy, double *virial, void *stream);
+
 /* mbf_eam_eval without a workspace argument: no counterpart in the reference.
  * For callers that cannot allocate device memory -- a host program that
  * owns the whole device memory budget and gives its plug-ins only their
