@@ -235,7 +235,7 @@ class SlabState:
             fp = self.pot.embedding(b, self.dlist, ws=self.ws)
             if exchange_fn is not None:
                 fp = exchange_fn(self, fp)
-            else:
+            elif self.world > 1:
                 fp = exchange_fprime(fp, self.plan, group)
             res = self.pot.forces_from_embedding(b, self.dlist, fp, ws=self.ws)
         else:
