@@ -19,6 +19,7 @@
 //                 neighbours left in its lower slots (contiguous), fused with
 //                 the per-structure energy / virial sums.
 // rho-bar and F(rho-bar) are float64 in both precisions.
+#include <cstring>
 #include <mutex>
 
 #include "mbf_util.cuh"
@@ -534,6 +535,147 @@ struct PolZ2 {
         dri = si == 0 ? d0 : d1;
     }
 };
+
+// ---- the two-element float32 path on packed pairs ---------------------------
+// Blackwell's paired float32 instructions (add / mul / fma .f32x2) run one
+// operation on two values at once.  The two elements' decays are the same
+// instruction sequence with different constants, so the pair evaluation
+// packs element 0 and element 1 into the two halves of a 64-bit register:
+// the polynomial and product steps take half the instructions; the
+// exponentials and reciprocals stay per element (no paired form).
+
+typedef unsigned long long f2x;
+__device__ __forceinline__ f2x pk2(float lo, float hi) {
+    f2x r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void up2(f2x v, float &lo, float &hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2x fma2(f2x a, f2x b, f2x c) {
+    f2x d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f2x mul2(f2x a, f2x b) {
+    f2x d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2x add2(f2x a, f2x b) {
+    f2x d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// Packed constants (element 0 low, element 1 high), built on the host.
+struct ZK2x {
+    f2x ire, nre, nlam, nkap, eb, ea, beta, alpha, fe, nfe_ire, A, nB, nire, one, twenty;
+};
+
+static inline f2x pack_host(float lo, float hi) {
+    unsigned int a, b;
+    memcpy(&a, &lo, 4);
+    memcpy(&b, &hi, 4);
+    return (f2x)a | ((f2x)b << 32);
+}
+
+// g and h of both elements' decays with the same exponent / shift pairs.
+__device__ __forceinline__ void zdec2(f2x r2, f2x dre, f2x ire, f2x nshift, f2x el, f2x expo, f2x twenty, f2x one,
+                                      f2x &g, f2x &h) {
+    const f2x u = fma2(r2, ire, nshift);
+    const f2x u2 = mul2(u, u), u4 = mul2(u2, u2), u8 = mul2(u4, u4), u16 = mul2(u8, u8);
+    const f2x u19 = mul2(mul2(u16, u2), u);
+    const f2x d = fma2(u16, u4, one);
+    const f2x arg = mul2(el, dre);
+    float d0, d1, a0, a1;
+    up2(d, d0, d1);
+    up2(arg, a0, a1);
+    const f2x rd = pk2(rcp_approx(d0), rcp_approx(d1));
+    g = mul2(pk2(ex2_approx(a0), ex2_approx(a1)), rd);
+    h = fma2(mul2(twenty, u19), rd, expo);
+}
+
+struct PolZ2x {
+    ZK<float> K;
+    ZK2x X;
+    __device__ __forceinline__ void setup(ZTab<float> &) const {}
+    __device__ __forceinline__ float sw_val(float r) const {
+        float s = (r - K.r0) * K.iw;
+        s = s < 0.f ? 0.f : (s > 1.f ? 1.f : s);
+        return 1.f - s * s * s * (10.f - 15.f * s + 6.f * s * s);
+    }
+    __device__ __forceinline__ float dens1(const ZTab<float> &, int sj, double r2) const {
+        float r, ir;
+        dist_ir(r2, r, ir);
+        const ZEl<float> &a = K.el[0], &b = K.el[1];
+        const bool one = sj == 0;
+        const float re = one ? a.re : b.re, ire = one ? a.ire : b.ire, lam = one ? a.lam : b.lam;
+        const float eb = one ? a.eb : b.eb, beta = one ? a.beta : b.beta, fe = one ? a.fe : b.fe;
+        return fe * sw_val(r) * zval(r, r - re, ire, lam, eb, beta);
+    }
+    __device__ __forceinline__ void pair(const ZTab<float> &, int si, int sj, double r2, float &phi, float &dphi,
+                                         float &drj, float &dri, float &ir) const {
+        float r;
+        dist_ir(r2, r, ir);
+        float s = (r - K.r0) * K.iw;
+        s = s < 0.f ? 0.f : (s > 1.f ? 1.f : s);
+        const float s2 = s * s, om = 1.f - s;
+        const float S = 1.f - s2 * s * (10.f - 15.f * s + 6.f * s2);
+        const float dS = K.m30iw * s2 * om * om;
+        const f2x rr = pk2(r, r);
+        const f2x dre = add2(rr, X.nre);
+        f2x gB, hB, gA, hA;
+        zdec2(rr, dre, X.ire, X.nlam, X.eb, X.beta, X.twenty, X.one, gB, hB);
+        zdec2(rr, dre, X.ire, X.nkap, X.ea, X.alpha, X.twenty, X.one, gA, hA);
+        const f2x f = mul2(X.fe, gB);
+        const f2x df = mul2(mul2(X.nfe_ire, gB), hB);
+        const f2x av = mul2(X.A, gA), nb = mul2(X.nB, gB);
+        const f2x ph = add2(av, nb);
+        const f2x dph = mul2(X.nire, fma2(nb, hB, mul2(av, hA)));
+        float f0, f1, df0, df1, p0, p1, dp0, dp1;
+        up2(f, f0, f1);
+        up2(df, df0, df1);
+        up2(ph, p0, p1);
+        up2(dph, dp0, dp1);
+        // cross pair phi_01 = chi / 2 (q phi_00 + phi_11 / q), q = f_1 / f_0,
+        // from the unswitched functions (engine/eam_zhou.py:128-207)
+        const float inv = rcp_approx(f0 * f1);
+        const float q = f1 * f1 * inv, rq = f0 * f0 * inv, rf0 = f1 * inv;
+        const float dq = (df1 - q * df0) * rf0;
+        const float v = K.half_chi * (q * p0 + p1 * rq);
+        const float dv = K.half_chi * (dq * p0 + q * dp0 + (dp1 - p1 * dq * rq) * rq);
+        const bool cross = si != sj;
+        const float pv = cross ? v : (si == 0 ? p0 : p1);
+        const float pdv = cross ? dv : (si == 0 ? dp0 : dp1);
+        phi = pv * S;
+        dphi = pdv * S + pv * dS;
+        const float d0 = df0 * S + f0 * dS, d1 = df1 * S + f1 * dS;
+        drj = sj == 0 ? d0 : d1;
+        dri = si == 0 ? d0 : d1;
+    }
+};
+
+static bool make_zk2x(const ZK<float> &K, ZK2x &X) {
+    const ZEl<float> &a = K.el[0], &b = K.el[1];
+    X.ire = pack_host(a.ire, b.ire);
+    X.nre = pack_host(-a.re, -b.re);
+    X.nlam = pack_host(-a.lam, -b.lam);
+    X.nkap = pack_host(-a.kap, -b.kap);
+    X.eb = pack_host(a.eb, b.eb);
+    X.ea = pack_host(a.ea, b.ea);
+    X.beta = pack_host(a.beta, b.beta);
+    X.alpha = pack_host(a.alpha, b.alpha);
+    X.fe = pack_host(a.fe, b.fe);
+    X.nfe_ire = pack_host(-a.fe_ire, -b.fe_ire);
+    X.A = pack_host(a.A, b.A);
+    X.nB = pack_host(-a.B, -b.B);
+    X.nire = pack_host(-a.ire, -b.ire);
+    X.one = pack_host(1.0f, 1.0f);
+    X.twenty = pack_host(20.0f, 20.0f);
+    return true;
+}
 
 // Minimum image for the force kernels (fused multiply-add allowed).
 __device__ __forceinline__ void mic_fast(const double *__restrict__ c, double rx, double ry, double rz,
@@ -1072,7 +1214,13 @@ static int eam_select(const mbf_eam_tables *tab, int lpa, const SysView &S, cons
     if (make_zk<T>(tab, K)) {
         if (tab->ns == 1)
             return eam_dispatch<T>(PolZ2<T, 1>{K}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, ph, st);
-        return eam_dispatch<T>(PolZ2<T, 2>{K}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, ph, st);
+        if constexpr (sizeof(T) == 4) {
+            ZK2x X;
+            make_zk2x(K, X);
+            return eam_dispatch<T>(PolZ2x{K, X}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, ph, st);
+        } else {
+            return eam_dispatch<T>(PolZ2<T, 2>{K}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, ph, st);
+        }
     }
     if (tab->zhou_fused != 0 && tab->ns <= EAM_MAXSP)
         return eam_dispatch<T>(PolZSmem<T>{E}, lpa, S, nl, E, rc2, B, ck, so, cs, n_chunks, ph, st);
