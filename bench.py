@@ -327,6 +327,12 @@ def run_batched(args, world, rank, local):
     # end to end: host positions in (pinned staging), per-structure forces,
     # energies and stresses out, through the evaluator's public calls
     host_pos = [np.ascontiguousarray(ev.batch.pos.cpu().numpy()) for ev in evs]
+    for ev in evs:
+        ev.capture()               # results() then replays the evaluator's graph
+    for _ in range(args.warmup):   # the staging and result blocks are allocated on first use
+        for ev, hp in zip(evs, host_pos):
+            ev.batch.set_positions(hp)
+            ev.results()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
@@ -343,7 +349,7 @@ def run_batched(args, world, rank, local):
     d2h = sum(ev.n_atoms * 24 + ev.n_structures * (8 + 72) for ev in evs)
     e2e = {"value": 2 * total_atoms / t_e2e, "unit": "atoms/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "ms_per_step": t_e2e * 1e3,
-           "path": "BatchedEvaluator: batch.set_positions(numpy) + results() -> numpy, "
+           "path": "BatchedEvaluator (captured): batch.set_positions(numpy) + results() -> numpy, "
                    "Tersoff and SW"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1385,7 +1391,7 @@ def run_eam_spatial(args, world, rank, local):
 # its line (steps kept small so the whole run stays within a few minutes).
 SUB_RECORDS = (
     ("fit_sic256", {"steps": 10, "warmup": 3, "e2e_steps": 10}),
-    ("batched_si512", {"steps": 10, "warmup": 3, "e2e_steps": 5}),
+    ("batched_si512", {"steps": 10, "warmup": 3, "e2e_steps": 20}),
     ("md_tersoff_si4096", {"steps": 10, "warmup": 3, "e2e_steps": 1, "drift_ps": 10.0}),
     ("md_sw_si64k", {"steps": 5, "warmup": 3, "e2e_steps": 1, "drift_ps": 10.0}),
 )
