@@ -825,12 +825,7 @@ template <> struct SlotVec<float> {
 // to i, the lower index; -f goes to j's own slot (j -> i) = rev(i -> j), so
 // j's gather reads its row contiguously (0 beyond the cutoff).  T is float
 // in the mixed path (a per-pair term, accumulated in float64) and double in
-// the float64 path.  A warp takes 32 consecutive atoms and runs them in LPA
-// rounds of 32 / LPA, longest upper half first: upper halves range from
-// none to the whole row in a spatially ordered structure, and a round
-// lasts as long as its longest row, so ranking the window makes the rows
-// of a round alike (fcc 256k: 78 % -> 92 % of lanes busy) while the atoms
-// stay neighbours.
+// the float64 path.
 template <typename T, int LPA, class Pol, bool ORTHO>
 __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
     eam_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ upper,
@@ -839,120 +834,103 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
               typename SlotVec<T>::type *__restrict__ slot_f, double *__restrict__ f_local,
               double *__restrict__ per_atom, Chk ck) {
     __shared__ ZTab<T> Z;
-    __shared__ int perm_s[EAM_BLOCK];
     P.setup(Z);
-    const int sub = threadIdx.x & (LPA - 1), lane = threadIdx.x & 31;
-    int *perm = perm_s + (threadIdx.x & ~31);
-    const int warp = (blockIdx.x * EAM_BLOCK + threadIdx.x) >> 5, n_warps = gridDim.x * (EAM_BLOCK / 32);
-    for (int wbase = warp * 32; wbase < S.n_atoms; wbase += n_warps * 32) {  // uniform over the warp
-        {
-            const int a = wbase + lane;
-            const int c = a < S.n_atoms ? row_off[a + 1] - upper[a] : -1;  // a sort key only
-            int rank = 0;
-#pragma unroll 8
-            for (int q = 0; q < 32; ++q) {
-                const int cq = __shfl_sync(MBF_FULL, c, q);
-                rank += (cq > c || (cq == c && q < lane)) ? 1 : 0;
+    const int sub = threadIdx.x & (LPA - 1);
+    const int gpb = EAM_BLOCK / LPA;
+    for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
+        const int i = base + threadIdx.x / LPA;
+        double fx = 0, fy = 0, fz = 0, e = 0;
+        int npair = 0;
+        double vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+        if (i < S.n_atoms) {
+            int flag = 0;
+            int up = upper[i], end = row_off[i + 1];
+            if (!row_ok(row_off[i], up, end, ck.n_slots)) {
+                flag = 1;
+                up = end = 0;
             }
-            __syncwarp();
-            perm[rank] = a;
-            __syncwarp();
-        }
-        for (int round = 0; round < LPA; ++round) {
-            const int i = perm[round * (32 / LPA) + lane / LPA];
-            double fx = 0, fy = 0, fz = 0, e = 0;
-            int npair = 0;
-            double vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
-            if (i < S.n_atoms) {
-                int flag = 0;
-                int up = upper[i], end = row_off[i + 1];
-                if (!row_ok(row_off[i], up, end, ck.n_slots)) {
-                    flag = 1;
-                    up = end = 0;
-                }
-                const int si = chk_idx(__ldg(S.types + i), ck.ns, 0, flag);
-                const double4 pi = ld_pack(pk, i);
-                const T Fp_i = (T)pi.w;
-                CellView<ORTHO> cv;
-                cv.load(S, i);
-                int s = up + sub;
-                int j0 = i, v0 = 0, j1 = i, v1 = 0;
-                if (s < end) {
-                    j0 = nbr[s];
-                    v0 = rev[s];
-                }
+            const int si = chk_idx(__ldg(S.types + i), ck.ns, 0, flag);
+            const double4 pi = ld_pack(pk, i);
+            const T Fp_i = (T)pi.w;
+            CellView<ORTHO> cv;
+            cv.load(S, i);
+            int s = up + sub;
+            int j0 = i, v0 = 0, j1 = i, v1 = 0;
+            if (s < end) {
+                j0 = nbr[s];
+                v0 = rev[s];
+            }
+            if (s + LPA < end) {
+                j1 = nbr[s + LPA];
+                v1 = rev[s + LPA];
+            }
+            j0 = chk_idx(j0, ck.n_atoms, i, flag);
+            double4 pn = ld_pack(pk, j0);
+            int tn = __ldg(S.types + j0);
+            for (; s < end; s += LPA) {
+                const double4 pj = pn;
+                const int sj = chk_idx(tn, ck.ns, 0, flag);
+                const int rs = v0;
                 if (s + LPA < end) {
-                    j1 = nbr[s + LPA];
-                    v1 = rev[s + LPA];
+                    j1 = chk_idx(j1, ck.n_atoms, i, flag);
+                    pn = ld_pack(pk, j1);
+                    tn = __ldg(S.types + j1);
                 }
-                j0 = chk_idx(j0, ck.n_atoms, i, flag);
-                double4 pn = ld_pack(pk, j0);
-                int tn = __ldg(S.types + j0);
-                for (; s < end; s += LPA) {
-                    const double4 pj = pn;
-                    const int sj = chk_idx(tn, ck.ns, 0, flag);
-                    const int rs = v0;
-                    if (s + LPA < end) {
-                        j1 = chk_idx(j1, ck.n_atoms, i, flag);
-                        pn = ld_pack(pk, j1);
-                        tn = __ldg(S.types + j1);
-                    }
-                    v0 = v1;
-                    if (s + 2 * LPA < end) {
-                        j1 = nbr[s + 2 * LPA];
-                        v1 = rev[s + 2 * LPA];
-                    }
-                    double dx, dy, dz;
-                    cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
-                    const double r2 = dx * dx + dy * dy + dz * dz;
-                    double px = 0.0, py = 0.0, pz = 0.0;
-                    if (r2 < rc2 && r2 > 1e-24) {
-                        npair += 1;
-                        T phi, dphi, drj, dri, ir;
-                        P.pair(Z, si, sj, r2, phi, dphi, drj, dri, ir);
-                        const T c = dphi + Fp_i * drj + (T)pj.w * dri;
-                        const double scd = (double)(c * ir);
-                        px = scd * dx;
-                        py = scd * dy;
-                        pz = scd * dz;
-                        fx += px;
-                        fy += py;
-                        fz += pz;
-                        e += (double)phi;
-                        vxx -= px * dx;
-                        vyy -= py * dy;
-                        vzz -= pz * dz;
-                        vxy -= px * dy;
-                        vxz -= px * dz;
-                        vyz -= py * dz;
-                    }
-                    if ((unsigned)rs < (unsigned)ck.n_slots) slot_f[rs] = SlotVec<T>::make(-px, -py, -pz);
-                    else flag = 1;
+                v0 = v1;
+                if (s + 2 * LPA < end) {
+                    j1 = nbr[s + 2 * LPA];
+                    v1 = rev[s + 2 * LPA];
                 }
-                chk_flush(ck, flag, 21, i);
+                double dx, dy, dz;
+                cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                double px = 0.0, py = 0.0, pz = 0.0;
+                if (r2 < rc2 && r2 > 1e-24) {
+                    npair += 1;
+                    T phi, dphi, drj, dri, ir;
+                    P.pair(Z, si, sj, r2, phi, dphi, drj, dri, ir);
+                    const T c = dphi + Fp_i * drj + (T)pj.w * dri;
+                    const double scd = (double)(c * ir);
+                    px = scd * dx;
+                    py = scd * dy;
+                    pz = scd * dz;
+                    fx += px;
+                    fy += py;
+                    fz += pz;
+                    e += (double)phi;
+                    vxx -= px * dx;
+                    vyy -= py * dy;
+                    vzz -= pz * dz;
+                    vxy -= px * dy;
+                    vxz -= px * dz;
+                    vyz -= py * dz;
+                }
+                if ((unsigned)rs < (unsigned)ck.n_slots) slot_f[rs] = SlotVec<T>::make(-px, -py, -pz);
+                else flag = 1;
             }
-            fx = group_sum<LPA>(fx);
-            fy = group_sum<LPA>(fy);
-            fz = group_sum<LPA>(fz);
-            e = group_sum<LPA>(e);
-            vxx = group_sum<LPA>(vxx);
-            vyy = group_sum<LPA>(vyy);
-            vzz = group_sum<LPA>(vzz);
-            vxy = group_sum<LPA>(vxy);
-            vxz = group_sum<LPA>(vxz);
-            vyz = group_sum<LPA>(vyz);
-            npair = group_sum<LPA>(npair);
-            if (sub == 0 && i < S.n_atoms) {
-                f_local[3 * (size_t)i] = fx;
-                f_local[3 * (size_t)i + 1] = fy;
-                f_local[3 * (size_t)i + 2] = fz;
-                double *pa = per_atom + (size_t)i * ATOM_ACC;
-                pa[0] = e + aux[2 * (size_t)i + 1];
-                pa[1] = vxx; pa[2] = vxy; pa[3] = vxz;
-                pa[4] = vxy; pa[5] = vyy; pa[6] = vyz;
-                pa[7] = vxz; pa[8] = vyz; pa[9] = vzz;
-                pa[10] = (double)npair;
-            }
+            chk_flush(ck, flag, 21, i);
+        }
+        fx = group_sum<LPA>(fx);
+        fy = group_sum<LPA>(fy);
+        fz = group_sum<LPA>(fz);
+        e = group_sum<LPA>(e);
+        vxx = group_sum<LPA>(vxx);
+        vyy = group_sum<LPA>(vyy);
+        vzz = group_sum<LPA>(vzz);
+        vxy = group_sum<LPA>(vxy);
+        vxz = group_sum<LPA>(vxz);
+        vyz = group_sum<LPA>(vyz);
+        npair = group_sum<LPA>(npair);
+        if (sub == 0 && i < S.n_atoms) {
+            f_local[3 * (size_t)i] = fx;
+            f_local[3 * (size_t)i + 1] = fy;
+            f_local[3 * (size_t)i + 2] = fz;
+            double *pa = per_atom + (size_t)i * ATOM_ACC;
+            pa[0] = e + aux[2 * (size_t)i + 1];
+            pa[1] = vxx; pa[2] = vxy; pa[3] = vxz;
+            pa[4] = vxy; pa[5] = vyy; pa[6] = vyz;
+            pa[7] = vxz; pa[8] = vyz; pa[9] = vzz;
+            pa[10] = (double)npair;
         }
     }
 }
@@ -1138,7 +1116,8 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const
         MBF_CHECK_LAUNCH();
     }
     if (!(phases & PH_FORCE)) return MBF_OK;
-    g = persistent_grid((S.n_atoms + EAM_BLOCK - 1) / EAM_BLOCK, EAM_BLOCK, (const void *)eam_force<T, LPA, Pol, ORTHO>);
+    const int gpb = EAM_BLOCK / LPA;
+    g = persistent_grid((S.n_atoms + gpb - 1) / gpb, EAM_BLOCK, (const void *)eam_force<T, LPA, Pol, ORTHO>);
     PROF_BEGIN("eam_force", st);
     eam_force<T, LPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, P, rc2,
                                                            B.pk, B.aux, slot, B.f_local, B.per_atom, ck);
