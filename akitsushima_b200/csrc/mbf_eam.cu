@@ -19,8 +19,10 @@
 //                 neighbours left in its lower slots (contiguous), fused with
 //                 the per-structure energy / virial sums.
 // rho-bar and F(rho-bar) are float64 in both precisions.
+#include <cmath>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 
 #include "mbf_util.cuh"
 
@@ -346,6 +348,14 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+// x clamped to [0, 1]: a saturating multiply in float32
+__device__ __forceinline__ float sat01(float x) { return __saturatef(x); }
+__device__ __forceinline__ double sat01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }
 
 // One element's constants (x = r / r_e).  In float32 exp(-beta (x - 1)) is
 // 2^(eb (r - r_e)) with eb = -beta log2(e) / r_e: r - r_e is exact for r
@@ -356,6 +366,7 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
 template <typename T>
 struct ZEl {
     T ire, re, lam, kap, beta, alpha, eb, ea, fe, fe_ire, A, B;
+    T lfe;  // log2 f_e (f_e > 0): the density's prefactor moved into its exponent
 };
 
 template <typename T>
@@ -421,6 +432,7 @@ __device__ __forceinline__ void dist_ir(double r2, double &r, double &ir) {
 
 template <typename T>
 struct PolGeneric {
+    static constexpr bool species_addresses = true;  // species index the tables
     EamDev E;
     __device__ __forceinline__ void setup(ZTab<T> &) const {}
     __device__ __forceinline__ T dens1(const ZTab<T> &, int sj, double r2) const {
@@ -447,6 +459,7 @@ template <> __device__ __forceinline__ float pair_dist<float>(double r2) { retur
 
 template <typename T>
 struct PolZSmem {
+    static constexpr bool species_addresses = true;  // species index the tables
     EamDev E;
     __device__ __forceinline__ void setup(ZTab<T> &Z) const { load_ztab<T>(E, Z); }
     __device__ __forceinline__ T dens1(const ZTab<T> &Z, int sj, double r2) const {
@@ -463,19 +476,37 @@ struct PolZSmem {
     }
 };
 
+// The float32 switched density rho_{s_j}(r) of the one- and two-element
+// paths: S(r) 2^(eb (r - r_e) + log2 f_e) / (1 + (r / r_e - lambda)^20),
+// the prefactor in the exponent (one multiply fewer per slot), r from one
+// sqrt.approx (no 1 / r needed here), the switch's clamp a saturation, its
+// polynomial 1 - s^3 (10 - 15 s + 6 s^2) in Horner form.
+template <int NS>
+__device__ __forceinline__ float zdens_f32(const ZK<float> &K, int sj, double r2) {
+    const float r = sqrt_approx((float)r2);
+    const ZEl<float> &a = K.el[0], &b = K.el[1];
+    const bool one = NS == 1 || sj == 0;
+    const float re = one ? a.re : b.re, ire = one ? a.ire : b.ire, lam = one ? a.lam : b.lam;
+    const float eb = one ? a.eb : b.eb, lfe = one ? a.lfe : b.lfe;
+    const float s = sat01((r - K.r0) * K.iw), s2 = s * s;
+    const float S = fmaf(-s2 * s, fmaf(6.f, s2, fmaf(-15.f, s, 10.f)), 1.f);
+    const float u = fmaf(r, ire, -lam);
+    const float u2 = u * u, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8;
+    return S * ex2_approx(fmaf(eb, r - re, lfe)) * rcp_approx(fmaf(u16, u4, 1.f));
+}
+
 template <typename T, int NS>
 struct PolZ2 {
+    static constexpr bool species_addresses = false;  // species only compared, never an index
     ZK<T> K;
     __device__ __forceinline__ void setup(ZTab<T> &) const {}
 
     __device__ __forceinline__ T sw_val(T r) const {
-        T s = (r - K.r0) * K.iw;
-        s = s < T(0) ? T(0) : (s > T(1) ? T(1) : s);
+        const T s = sat01((r - K.r0) * K.iw);
         return T(1) - s * s * s * (T(10) - T(15) * s + T(6) * s * s);
     }
     __device__ __forceinline__ void sw(T r, T &S, T &dS) const {
-        T s = (r - K.r0) * K.iw;
-        s = s < T(0) ? T(0) : (s > T(1) ? T(1) : s);
+        const T s = sat01((r - K.r0) * K.iw);
         T s2 = s * s, om = T(1) - s;
         S = T(1) - s2 * s * (T(10) - T(15) * s + T(6) * s2);
         dS = K.m30iw * s2 * om * om;
@@ -494,13 +525,17 @@ struct PolZ2 {
     }
     // one element's switched density, its constants selected by species
     __device__ __forceinline__ T dens1(const ZTab<T> &, int sj, double r2) const {
-        T r, ir;
-        dist_ir(r2, r, ir);
-        const ZEl<T> &a = K.el[0], &b = K.el[1];
-        const bool one = NS == 1 || sj == 0;
-        const T re = one ? a.re : b.re, ire = one ? a.ire : b.ire, lam = one ? a.lam : b.lam;
-        const T eb = one ? a.eb : b.eb, beta = one ? a.beta : b.beta, fe = one ? a.fe : b.fe;
-        return fe * sw_val(r) * zval(r, r - re, ire, lam, eb, beta);
+        if constexpr (std::is_same<T, float>::value) {
+            return zdens_f32<NS>(K, sj, r2);
+        } else {
+            T r, ir;
+            dist_ir(r2, r, ir);
+            const ZEl<T> &a = K.el[0], &b = K.el[1];
+            const bool one = NS == 1 || sj == 0;
+            const T re = one ? a.re : b.re, ire = one ? a.ire : b.ire, lam = one ? a.lam : b.lam;
+            const T eb = one ? a.eb : b.eb, beta = one ? a.beta : b.beta, fe = one ? a.fe : b.fe;
+            return fe * sw_val(r) * zval(r, r - re, ire, lam, eb, beta);
+        }
     }
     __device__ __forceinline__ void pair(const ZTab<T> &, int si, int sj, double r2, T &phi, T &dphi, T &drj,
                                          T &dri, T &ir) const {
@@ -598,29 +633,18 @@ __device__ __forceinline__ void zdec2(f2x r2, f2x dre, f2x ire, f2x nshift, f2x 
 }
 
 struct PolZ2x {
+    static constexpr bool species_addresses = false;  // species only compared, never an index
     ZK<float> K;
     ZK2x X;
     __device__ __forceinline__ void setup(ZTab<float> &) const {}
-    __device__ __forceinline__ float sw_val(float r) const {
-        float s = (r - K.r0) * K.iw;
-        s = s < 0.f ? 0.f : (s > 1.f ? 1.f : s);
-        return 1.f - s * s * s * (10.f - 15.f * s + 6.f * s * s);
-    }
     __device__ __forceinline__ float dens1(const ZTab<float> &, int sj, double r2) const {
-        float r, ir;
-        dist_ir(r2, r, ir);
-        const ZEl<float> &a = K.el[0], &b = K.el[1];
-        const bool one = sj == 0;
-        const float re = one ? a.re : b.re, ire = one ? a.ire : b.ire, lam = one ? a.lam : b.lam;
-        const float eb = one ? a.eb : b.eb, beta = one ? a.beta : b.beta, fe = one ? a.fe : b.fe;
-        return fe * sw_val(r) * zval(r, r - re, ire, lam, eb, beta);
+        return zdens_f32<2>(K, sj, r2);
     }
     __device__ __forceinline__ void pair(const ZTab<float> &, int si, int sj, double r2, float &phi, float &dphi,
                                          float &drj, float &dri, float &ir) const {
         float r;
         dist_ir(r2, r, ir);
-        float s = (r - K.r0) * K.iw;
-        s = s < 0.f ? 0.f : (s > 1.f ? 1.f : s);
+        const float s = sat01((r - K.r0) * K.iw);
         const float s2 = s * s, om = 1.f - s;
         const float S = 1.f - s2 * s * (10.f - 15.f * s + 6.f * s2);
         const float dS = K.m30iw * s2 * om * om;
@@ -764,7 +788,9 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB 
             int tn = __ldg(S.types + j0);
             for (; s < end; s += LPA) {
                 const double3 pj = pn;
-                const int sj = chk_idx(tn, ck.ns, 0, flag);
+                // a species that indexes no memory needs no check here: the
+                // embedding pass checks every atom's species
+                const int sj = Pol::species_addresses ? chk_idx(tn, ck.ns, 0, flag) : tn;
                 if (s + LPA < end) {
                     j1 = chk_idx(j1, ck.n_atoms, i, flag);
                     pn = ld_pos(S.pos, j1);
@@ -869,7 +895,9 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
             int tn = __ldg(S.types + j0);
             for (; s < end; s += LPA) {
                 const double4 pj = pn;
-                const int sj = chk_idx(tn, ck.ns, 0, flag);
+                // a species that indexes no memory needs no check here: the
+                // embedding pass checks every atom's species
+                const int sj = Pol::species_addresses ? chk_idx(tn, ck.ns, 0, flag) : tn;
                 const int rs = v0;
                 if (s + LPA < end) {
                     j1 = chk_idx(j1, ck.n_atoms, i, flag);
@@ -1189,8 +1217,10 @@ static bool make_zk(const mbf_eam_tables *tab, ZK<T> &K) {
         q.alpha = (T)alpha;
         q.eb = (T)(-beta * LOG2E / re);
         q.ea = (T)(-alpha * LOG2E / re);
+        if (!(fe > 0.0)) return false;
         q.fe = (T)fe;
         q.fe_ire = (T)(fe / re);
+        q.lfe = (T)std::log2(fe);
         q.A = (T)p[6];
         q.B = (T)p[7];
     }
