@@ -840,9 +840,7 @@ template <> struct SlotVec<double> {
 };
 template <> struct SlotVec<float> {
     typedef float4 type;
-    static __device__ __forceinline__ type make(double x, double y, double z) {
-        return make_float4((float)x, (float)y, (float)z, 0.0f);
-    }
+    static __device__ __forceinline__ type make(float x, float y, float z) { return make_float4(x, y, z, 0.0f); }
 };
 
 // Force pass over the upper half of every row: each unordered pair once.
@@ -865,9 +863,11 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
     const int gpb = EAM_BLOCK / LPA;
     for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
         const int i = base + threadIdx.x / LPA;
-        double fx = 0, fy = 0, fz = 0, e = 0;
+        // this lane's sums over its pairs (T: at most a row's upper half / LPA
+        // terms in float32 in the mixed path), float64 from the lane sums on
+        T afx = 0, afy = 0, afz = 0, ae = 0;
+        T axx = 0, ayy = 0, azz = 0, axy = 0, axz = 0, ayz = 0;
         int npair = 0;
-        double vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
         if (i < S.n_atoms) {
             int flag = 0;
             int up = upper[i], end = row_off[i + 1];
@@ -912,32 +912,36 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
                 double dx, dy, dz;
                 cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
                 const double r2 = dx * dx + dy * dy + dz * dz;
-                double px = 0.0, py = 0.0, pz = 0.0;
+                T qx = 0, qy = 0, qz = 0;  // the pair force on j
                 if (r2 < rc2 && r2 > 1e-24) {
                     npair += 1;
                     T phi, dphi, drj, dri, ir;
                     P.pair(Z, si, sj, r2, phi, dphi, drj, dri, ir);
                     const T c = dphi + Fp_i * drj + (T)pj.w * dri;
-                    const double scd = (double)(c * ir);
-                    px = scd * dx;
-                    py = scd * dy;
-                    pz = scd * dz;
-                    fx += px;
-                    fy += py;
-                    fz += pz;
-                    e += (double)phi;
-                    vxx -= px * dx;
-                    vyy -= py * dy;
-                    vzz -= pz * dz;
-                    vxy -= px * dy;
-                    vxz -= px * dz;
-                    vyz -= py * dz;
+                    const T sc = c * ir;
+                    const T ex = (T)dx, ey = (T)dy, ez = (T)dz;
+                    const T px = sc * ex, py = sc * ey, pz = sc * ez;
+                    afx += px;
+                    afy += py;
+                    afz += pz;
+                    ae += phi;
+                    axx -= px * ex;
+                    ayy -= py * ey;
+                    azz -= pz * ez;
+                    axy -= px * ey;
+                    axz -= px * ez;
+                    ayz -= py * ez;
+                    qx = -px;
+                    qy = -py;
+                    qz = -pz;
                 }
-                if ((unsigned)rs < (unsigned)ck.n_slots) slot_f[rs] = SlotVec<T>::make(-px, -py, -pz);
+                if ((unsigned)rs < (unsigned)ck.n_slots) slot_f[rs] = SlotVec<T>::make(qx, qy, qz);
                 else flag = 1;
             }
             chk_flush(ck, flag, 21, i);
         }
+        double fx = afx, fy = afy, fz = afz, e = ae;
+        double vxx = axx, vyy = ayy, vzz = azz, vxy = axy, vxz = axz, vyz = ayz;
         fx = group_sum<LPA>(fx);
         fy = group_sum<LPA>(fy);
         fz = group_sum<LPA>(fz);
