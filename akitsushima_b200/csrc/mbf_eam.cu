@@ -761,7 +761,7 @@ __device__ __forceinline__ double3 ld_pos(const double *__restrict__ pos, int j)
 template <typename T, int LPA, class Pol, bool ORTHO>
 __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB : 1)
     eam_density(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr, Pol P, double rc2,
-                const double4 *__restrict__ rec, double *__restrict__ aux, Chk ck) {
+                double *__restrict__ aux, Chk ck) {
     __shared__ ZTab<T> Z;
     P.setup(Z);
     const int sub = threadIdx.x & (LPA - 1);
@@ -784,16 +784,17 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB 
             if (s < end) j0 = nbr[s];
             if (s + LPA < end) j1 = nbr[s + LPA];
             j0 = chk_idx(j0, ck.n_atoms, i, flag);
-            double4 pn = ld_pack(rec, j0);
+            double3 pn = ld_pos(S.pos, j0);
+            int tn = __ldg(S.types + j0);
             for (; s < end; s += LPA) {
-                const double4 pj = pn;
+                const double3 pj = pn;
                 // a species that indexes no memory needs no check here: the
                 // embedding pass checks every atom's species
-                const int tn = (int)__double_as_longlong(pj.w);
                 const int sj = Pol::species_addresses ? chk_idx(tn, ck.ns, 0, flag) : tn;
                 if (s + LPA < end) {
                     j1 = chk_idx(j1, ck.n_atoms, i, flag);
-                    pn = ld_pack(rec, j1);
+                    pn = ld_pos(S.pos, j1);
+                    tn = __ldg(S.types + j1);
                 }
                 if (s + 2 * LPA < end) j1 = nbr[s + 2 * LPA];
                 double dx, dy, dz;
@@ -806,18 +807,6 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB 
         acc = group_sum<LPA>(acc);
         if (sub == 0 && i < S.n_atoms) aux[2 * (size_t)i] = acc;
     }
-}
-
-// The density pass's neighbour record {x, y, z, species bits}: one aligned
-// 32-byte sector per neighbour, read as two 16-byte loads, where the
-// positions (24 bytes, across sector boundaries) and the species took four
-// loads -- that pass is bound by L1 throughput.  The embedding pass then
-// rewrites the record as {x, y, z, F'} for the force pass.
-__global__ void __launch_bounds__(256) eam_pack(SysView S, double4 *__restrict__ rec) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= S.n_atoms) return;
-    const double3 p = ld_pos(S.pos, a);
-    rec[a] = make_double4(p.x, p.y, p.z, __longlong_as_double((long long)__ldg(S.types + a)));
 }
 
 // F(rho-bar) and F'(rho-bar) in float64, rho-bar clamped at 0
@@ -1149,13 +1138,8 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const
     if (phases & PH_EMBED) {
         const int dgpb = EAM_BLOCK / DLPA;
         g = persistent_grid((S.n_atoms + dgpb - 1) / dgpb, EAM_BLOCK, (const void *)eam_density<T, DLPA, Pol, ORTHO>);
-        PROF_BEGIN("eam_pack", st);
-        eam_pack<<<(S.n_atoms + 255) / 256, 256, 0, st>>>(S, B.pk);
-        PROF_END("eam_pack", st);
-        MBF_CHECK_LAUNCH();
         PROF_BEGIN("eam_density", st);
-        eam_density<T, DLPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, rc2, B.pk, B.aux,
-                                                                  ck);
+        eam_density<T, DLPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, rc2, B.aux, ck);
         PROF_END("eam_density", st);
         MBF_CHECK_LAUNCH();
         PROF_BEGIN("eam_embed", st);
