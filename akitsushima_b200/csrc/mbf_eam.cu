@@ -976,10 +976,7 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
 // an atom is issued before any is used: its first GATHER_UNROLL x 8 lower
 // slots (an fcc row's lower half is about 40), its record and its
 // upper-pair force, with the next atom's row bounds one iteration ahead.
-#ifndef MBF_GATHER_UNROLL
-#define MBF_GATHER_UNROLL 5
-#endif
-constexpr int GATHER_UNROLL = MBF_GATHER_UNROLL;
+constexpr int GATHER_UNROLL = 5;
 
 template <typename V3, int NT>
 __global__ void __launch_bounds__(NT, 1024 / NT) eam_gather_reduce(int n_slots, const int *__restrict__ row_off,
@@ -1030,21 +1027,11 @@ __global__ void __launch_bounds__(NT, 1024 / NT) eam_gather_reduce(int n_slots, 
                     fz += (double)w[k].z;
                 }
             }
-            // rows longer than GATHER_UNROLL x 8 slots (up to twice that in a
-            // spatially ordered structure): the rest in batches of four
-            // loads a lane, each batch issued before any is used
-            for (int q0 = beg + sub + GATHER_UNROLL * LPA; q0 < up; q0 += 4 * LPA) {
-                V3 u[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if (q0 + k * LPA < up) u[k] = slot_f[q0 + k * LPA];
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if (q0 + k * LPA < up) {
-                        fx += (double)u[k].x;
-                        fy += (double)u[k].y;
-                        fz += (double)u[k].z;
-                    }
+            for (int q = beg + sub + GATHER_UNROLL * LPA; q < up; q += LPA) {
+                const V3 v = slot_f[q];
+                fx += (double)v.x;
+                fy += (double)v.y;
+                fz += (double)v.z;
             }
             r0 += ra;
             r1 += rb;
