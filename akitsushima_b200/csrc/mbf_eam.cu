@@ -414,10 +414,6 @@ __device__ __forceinline__ void dist_ir(double r2, float &r, float &ir) {
     ir = rsqrt_approx(q);
     r = q * ir;
 }
-__device__ __forceinline__ void dist_ir(float r2, float &r, float &ir) {
-    ir = rsqrt_approx(r2);
-    r = r2 * ir;
-}
 __device__ __forceinline__ void dist_ir(double r2, double &r, double &ir) {
     r = sqrt(r2);
     ir = 1.0 / r;
@@ -437,7 +433,6 @@ __device__ __forceinline__ void dist_ir(double r2, double &r, double &ir) {
 template <typename T>
 struct PolGeneric {
     static constexpr bool species_addresses = true;  // species index the tables
-    static constexpr bool zero_at_cutoff = false;    // splines: no such promise
     EamDev E;
     __device__ __forceinline__ void setup(ZTab<T> &) const {}
     __device__ __forceinline__ T dens1(const ZTab<T> &, int sj, double r2) const {
@@ -465,7 +460,6 @@ template <> __device__ __forceinline__ float pair_dist<float>(double r2) { retur
 template <typename T>
 struct PolZSmem {
     static constexpr bool species_addresses = true;  // species index the tables
-    static constexpr bool zero_at_cutoff = false;    // takes r^2 in float64
     EamDev E;
     __device__ __forceinline__ void setup(ZTab<T> &Z) const { load_ztab<T>(E, Z); }
     __device__ __forceinline__ T dens1(const ZTab<T> &Z, int sj, double r2) const {
@@ -504,7 +498,6 @@ __device__ __forceinline__ float zdens_f32(const ZK<float> &K, int sj, double r2
 template <typename T, int NS>
 struct PolZ2 {
     static constexpr bool species_addresses = false;  // species only compared, never an index
-    static constexpr bool zero_at_cutoff = true;      // Zhou switch: S = dS = 0 at r_c
     ZK<T> K;
     __device__ __forceinline__ void setup(ZTab<T> &) const {}
 
@@ -544,8 +537,7 @@ struct PolZ2 {
             return fe * sw_val(r) * zval(r, r - re, ire, lam, eb, beta);
         }
     }
-    template <typename R>
-    __device__ __forceinline__ void pair(const ZTab<T> &, int si, int sj, R r2, T &phi, T &dphi, T &drj,
+    __device__ __forceinline__ void pair(const ZTab<T> &, int si, int sj, double r2, T &phi, T &dphi, T &drj,
                                          T &dri, T &ir) const {
         T r;
         dist_ir(r2, r, ir);
@@ -642,15 +634,13 @@ __device__ __forceinline__ void zdec2(f2x r2, f2x dre, f2x ire, f2x nshift, f2x 
 
 struct PolZ2x {
     static constexpr bool species_addresses = false;  // species only compared, never an index
-    static constexpr bool zero_at_cutoff = true;      // Zhou switch: S = dS = 0 at r_c
     ZK<float> K;
     ZK2x X;
     __device__ __forceinline__ void setup(ZTab<float> &) const {}
     __device__ __forceinline__ float dens1(const ZTab<float> &, int sj, double r2) const {
         return zdens_f32<2>(K, sj, r2);
     }
-    template <typename R>
-    __device__ __forceinline__ void pair(const ZTab<float> &, int si, int sj, R r2, float &phi, float &dphi,
+    __device__ __forceinline__ void pair(const ZTab<float> &, int si, int sj, double r2, float &phi, float &dphi,
                                          float &drj, float &dri, float &ir) const {
         float r;
         dist_ir(r2, r, ir);
@@ -869,9 +859,6 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
               double *__restrict__ per_atom, Chk ck) {
     __shared__ ZTab<T> Z;
     P.setup(Z);
-    constexpr bool F32R2 = sizeof(T) == 4 && Pol::zero_at_cutoff;
-    typedef typename std::conditional<F32R2, float, double>::type R2;
-    const R2 rc2r = (R2)rc2;
     const int sub = threadIdx.x & (LPA - 1);
     const int gpb = EAM_BLOCK / LPA;
     for (int base = blockIdx.x * gpb; base < S.n_atoms; base += gridDim.x * gpb) {
@@ -924,18 +911,15 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
                 }
                 double dx, dy, dz;
                 cv.mic(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, dx, dy, dz);
-                const T ex = (T)dx, ey = (T)dy, ez = (T)dz;
-                // r^2 in float32 from the float32 displacement where the
-                // functions vanish with their derivatives at the cutoff (a
-                // pair within a rounding of it contributes nothing either way)
-                const R2 r2 = F32R2 ? (R2)(ex * ex + ey * ey + ez * ez) : (R2)(dx * dx + dy * dy + dz * dz);
+                const double r2 = dx * dx + dy * dy + dz * dz;
                 T qx = 0, qy = 0, qz = 0;  // the pair force on j
-                if (r2 < rc2r && r2 > (R2)1e-24) {
+                if (r2 < rc2 && r2 > 1e-24) {
                     npair += 1;
                     T phi, dphi, drj, dri, ir;
                     P.pair(Z, si, sj, r2, phi, dphi, drj, dri, ir);
                     const T c = dphi + Fp_i * drj + (T)pj.w * dri;
                     const T sc = c * ir;
+                    const T ex = (T)dx, ey = (T)dy, ez = (T)dz;
                     const T px = sc * ex, py = sc * ey, pz = sc * ez;
                     afx += px;
                     afy += py;
