@@ -72,11 +72,25 @@ class BatchedEvaluator:
         nbytes = int(_lib.lib().mbf_eval_workspace_bytes(self.batch.n_atoms, self.dlist.n_slots,
                                                          self.batch.n_chunks))
         self._ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=dev)
+        # results() reads one block: energies / reps (S), virials / volume
+        # (S, 9), the original atoms' forces (n0, 3)
+        S, n0 = self.batch.n_struct, int(sum(self.n_orig))
+        self._packed = torch.empty(10 * S + 3 * n0, dtype=torch.float64, device=dev)
         self._graph = None
 
     def _eval(self):
         return self.pot.evaluate(self.batch, self.dlist, precision=self.precision, out=self.out,
                                  ws=self._ws)
+
+    def _pack(self):
+        S, n0, out, p = self.batch.n_struct, int(sum(self.n_orig)), self.out, self._packed
+        torch.mul(out.energy, self._inv_reps, out=p[:S])
+        torch.div(out.virial, self._vol[:, None], out=p[S:10 * S].view(S, 9))
+        torch.index_select(out.forces, 0, self._orig_index, out=p[10 * S:].view(n0, 3))
+
+    def _eval_and_pack(self):
+        self._eval()
+        self._pack()
 
     @property
     def n_structures(self):
@@ -98,24 +112,26 @@ class BatchedEvaluator:
     def capture(self):
         """Capture one evaluation in a CUDA graph; later run() calls replay
         it (positions, lattices and species are read from the batch's device
-        arrays, so updating those in place keeps the graph valid)."""
-        self._eval()
-        self._graph = capture_graph(self._eval, self.device)
+        arrays, so updating those in place keeps the graph valid).  The graph
+        also packs the per-structure results into the block results() copies
+        to the host."""
+        self._eval_and_pack()
+        self._graph = capture_graph(self._eval_and_pack, self.device)
         torch.cuda.synchronize(self.device)
         return self
 
     def results(self):
         """Per-structure (energies (S,), forces list of (N_s, 3), stresses
-        (S, 3, 3)) of the ORIGINAL structures, on the host: one device-side
-        gather into a fresh pinned block and one copy (the arrays returned
-        are views of that block, which the caller's references keep)."""
-        out = self.run()
+        (S, 3, 3)) of the ORIGINAL structures, on the host: the results packed
+        into one device block (inside the captured graph, if any) and one
+        copy into a fresh pinned block (the arrays returned are views of it,
+        which the caller's references keep)."""
+        self.run()
+        if self._graph is None:
+            self._pack()
         S, n0 = self.batch.n_struct, int(sum(self.n_orig))
-        dev_buf = torch.cat([(out.energy * self._inv_reps),
-                             (out.virial / self._vol[:, None]).reshape(-1),
-                             out.forces.index_select(0, self._orig_index).reshape(-1)])
-        host = torch.empty(dev_buf.numel(), dtype=torch.float64, pin_memory=True)
-        host.copy_(dev_buf, non_blocking=True)
+        host = torch.empty(self._packed.numel(), dtype=torch.float64, pin_memory=True)
+        host.copy_(self._packed, non_blocking=True)
         torch.cuda.current_stream(self.device).synchronize()
         h = host.numpy()
         e = h[:S]
