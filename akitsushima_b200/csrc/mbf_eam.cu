@@ -1086,9 +1086,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 // true once the phase of `parity` has completed; false after the limit
-// (2^18 polls, far beyond a batch's microsecond or two)
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (int k = 0; k < (1 << 18); ++k)
+    for (int k = 0; k < (1 << 20); ++k)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -1157,7 +1156,6 @@ __global__ void __launch_bounds__(NT, 1024 / NT)
     };
     double r0 = 0.0, r1 = 0.0;
     uint32_t par0 = 0u, par1 = 0u;  // the phase each buffer's barrier waits for next
-    bool gave_up = false;           // after one wait that ran out, no more waits
     if (nb > 0) issue(0, 0);
     if (nb > 1) issue(1, 1);
     for (int b = 0; b < nb; ++b) {
@@ -1174,10 +1172,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT)
         const bool staged = tot > 0 && tot <= GB_CAP;
         if (staged) {
             const uint32_t bar = smem_u32(&gbar[X]);
-            if (!gave_up && !mbar_wait(bar, X ? par1 : par0)) {
+            if (!mbar_wait(bar, X ? par1 : par0)) {
                 chk_flush(ck, 1, 32, a0);
                 mbar_wait(bar, X ? par1 : par0);  // once more for the copies still in flight
-                gave_up = true;
             }
             if (X) par1 ^= 1u;
             else par0 ^= 1u;
