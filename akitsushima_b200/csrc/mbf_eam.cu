@@ -1052,162 +1052,6 @@ __global__ void __launch_bounds__(NT, 1024 / NT) eam_gather_reduce(int n_slots, 
     chunk_sums_finish<NT>(cs, c, s, r0, r1);
 }
 
-// ---- the mixed force gather through bulk asynchronous copies -------------
-// The same sums as eam_gather_reduce<float4, 512> in the same order, with
-// each atom's partner-slot run (contiguous float4s, 16-byte aligned, a
-// multiple of 16 bytes) brought into shared memory by one cp.async.bulk
-// per atom: the loads of a 64-atom batch are in flight in the copy engine,
-// not in registers, two batches ahead (double buffer, one mbarrier each,
-// completion by transaction bytes).  A batch whose runs exceed the buffer
-// reads them from global memory instead.  Waits are bounded: a wait that
-// runs out sets status site 32 and the batch's sums are then not trusted.
-constexpr int GB_CAP = 3072;  // float4 entries per buffer (48 KB)
-constexpr size_t GB_SMEM = 2 * GB_CAP * sizeof(float4);
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// true once the phase of `parity` has completed; false after the limit
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (int k = 0; k < (1 << 20); ++k)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
-template <int NT>
-__global__ void __launch_bounds__(NT, 1024 / NT)
-    eam_gather_bulk(int n_slots, const int *__restrict__ row_off, const int *__restrict__ upper,
-                    const float4 *__restrict__ slot_f, const double *__restrict__ f_local,
-                    double *__restrict__ forces, ChunkSums cs, Chk ck) {
-    constexpr int LPA = 8, G = NT / LPA;
-    static_assert(G % 32 == 0 && G <= 64, "eam_gather_bulk: one or two warps of atoms per batch");
-    extern __shared__ __align__(16) float4 gbuf[];  // [2][GB_CAP]
-    __shared__ __align__(8) unsigned long long gbar[2];
-    __shared__ int goff[2][G + 1], gbeg[2][G], glen[2][G], gws[2];
-    const int c = blockIdx.x;
-    const int s = cs.chunk[3 * c], a0 = cs.chunk[3 * c + 1], a1 = cs.chunk[3 * c + 2];
-    const int t = threadIdx.x, sub = t & (LPA - 1), grp = t / LPA;
-    const int nb = (a1 - a0 + G - 1) / G;
-    if (t == 0) {
-        mbar_init(smem_u32(&gbar[0]), 1);
-        mbar_init(smem_u32(&gbar[1]), 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    // batch b's run bounds and offsets into buffer X, and its copies when
-    // they fit (every thread calls it)
-    auto issue = [&](int b, int X) {
-        int len = 0;
-        if (t < G) {
-            const int a = a0 + b * G + t;
-            int beg = 0, up = 0;
-            if (a < a1) {
-                beg = row_off[a];
-                up = upper[a];
-                if (!row_ok(beg, up, row_off[a + 1], n_slots)) {
-                    chk_flush(ck, 1, 31, a);
-                    beg = up = 0;
-                }
-            }
-            len = up - beg;
-            gbeg[X][t] = beg;
-            glen[X][t] = len;
-            int incl = len;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(MBF_FULL, incl, o);
-                if ((t & 31) >= o) incl += v;
-            }
-            if ((t & 31) == 31) gws[t >> 5] = incl;
-            goff[X][t] = incl - len;  // within the warp for now
-        }
-        __syncthreads();
-        if (t < G) {
-            const int add = (t >> 5) ? gws[0] : 0;
-            goff[X][t] += add;
-            if (t == G - 1) goff[X][G] = goff[X][t] + len;
-        }
-        __syncthreads();
-        const int tot = goff[X][G];
-        if (tot > 0 && tot <= GB_CAP) {
-            const uint32_t bar = smem_u32(&gbar[X]);
-            if (t == 0) mbar_expect_tx(bar, (uint32_t)tot * 16u);
-            if (t < G && len > 0)
-                bulk_g2s(smem_u32(gbuf + X * GB_CAP + goff[X][t]), slot_f + gbeg[X][t], (uint32_t)len * 16u, bar);
-        }
-    };
-    double r0 = 0.0, r1 = 0.0;
-    uint32_t par0 = 0u, par1 = 0u;  // the phase each buffer's barrier waits for next
-    if (nb > 0) issue(0, 0);
-    if (nb > 1) issue(1, 1);
-    for (int b = 0; b < nb; ++b) {
-        const int X = b & 1;
-        const int a = a0 + b * G + grp;
-        double fx = 0, fy = 0, fz = 0, fl = 0.0, ra = 0.0, rb = 0.0;
-        if (a < a1) {
-            const double *rec = cs.per_atom + (size_t)a * ATOM_ACC;
-            ra = rec[sub];
-            rb = sub < ATOM_ACC - LPA ? rec[LPA + sub] : 0.0;
-            if (sub < 3) fl = f_local[3 * (size_t)a + sub];
-        }
-        const int tot = goff[X][G];
-        const bool staged = tot > 0 && tot <= GB_CAP;
-        if (staged) {
-            const uint32_t bar = smem_u32(&gbar[X]);
-            if (!mbar_wait(bar, X ? par1 : par0)) {
-                chk_flush(ck, 1, 32, a0);
-                mbar_wait(bar, X ? par1 : par0);  // once more for the copies still in flight
-            }
-            if (X) par1 ^= 1u;
-            else par0 ^= 1u;
-        }
-        if (a < a1) {
-            const int len = glen[X][grp];
-            const float4 *w = staged ? gbuf + X * GB_CAP + goff[X][grp] : slot_f + gbeg[X][grp];
-            for (int q = sub; q < len; q += LPA) {
-                const float4 v = w[q];
-                fx += (double)v.x;
-                fy += (double)v.y;
-                fz += (double)v.z;
-            }
-            r0 += ra;
-            r1 += rb;
-        }
-        fx = group_sum<LPA>(fx);
-        fy = group_sum<LPA>(fy);
-        fz = group_sum<LPA>(fz);
-        const double gx = __shfl_sync(MBF_FULL, fl, 0, LPA);
-        const double gy = __shfl_sync(MBF_FULL, fl, 1, LPA);
-        const double gz = __shfl_sync(MBF_FULL, fl, 2, LPA);
-        if (sub == 0 && a < a1) {
-            forces[3 * (size_t)a] = gx + fx;
-            forces[3 * (size_t)a + 1] = gy + fy;
-            forces[3 * (size_t)a + 2] = gz + fz;
-        }
-        __syncthreads();  // buffer X and its offsets are free again
-        if (b + 2 < nb) issue(b + 2, X);
-    }
-    chunk_sums_finish<NT>(cs, c, s, r0, r1);
-}
-
 // Site terms (engine/site_terms.py:440-479): U_i = F_i(rho-bar_i) + 1/2
 // sum_j phi_ij and dU_i/dv_ij = (F'_i rho'_{s_j}(r) + 1/2 phi'(r)) v / r over
 // the full row, after the density and embedding passes; v for every slot.
@@ -1281,23 +1125,6 @@ struct EamBufs {
 // structure runs them apart, with the halo atoms' F' exchanged in between.
 enum { PH_EMBED = 1, PH_FORCE = 2, PH_ALL = 3 };
 
-// eam_gather_bulk's 96 KB of dynamic shared memory, allowed once per device
-// (the attribute belongs to the device's context); false if refused, and
-// the launch then takes eam_gather_reduce.
-static bool gather_bulk_ready() {
-    static std::mutex mu;
-    static signed char state[64] = {0};  // 0 unknown, 1 set, -1 refused
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
-    std::lock_guard<std::mutex> lock(mu);
-    if (state[dev] == 0)
-        state[dev] = cudaFuncSetAttribute((const void *)eam_gather_bulk<512>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GB_SMEM) == cudaSuccess
-                         ? 1
-                         : -1;
-    return state[dev] > 0;
-}
-
 // The density pass walks full rows (twice the force pass's upper halves);
 // it takes 4 lanes per atom, or the force pass's lanes when that is more.
 template <typename T, int LPA, class Pol, bool ORTHO>
@@ -1330,15 +1157,6 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const
     MBF_CHECK_LAUNCH();
     PROF_BEGIN("eam_gather_reduce", st);
     const int nt = chunk_block(S.n_atoms, n_chunks);
-    if constexpr (std::is_same<V3, float4>::value) {
-        if (nt == 512 && gather_bulk_ready()) {
-            eam_gather_bulk<512><<<n_chunks, 512, GB_SMEM, st>>>(ck.n_slots, nl->row_off, nl->upper, slot, B.f_local,
-                                                                B.forces, cs, ck);
-            PROF_END("eam_gather_reduce", st);
-            MBF_CHECK_LAUNCH();
-            goto gathered;
-        }
-    }
     if (nt == 128)
         eam_gather_reduce<V3, 128><<<n_chunks, 128, 0, st>>>(ck.n_slots, nl->row_off, nl->upper, slot, B.f_local,
                                                              B.forces, cs, ck);
@@ -1350,7 +1168,6 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const
                                                              B.forces, cs, ck);
     PROF_END("eam_gather_reduce", st);
     MBF_CHECK_LAUNCH();
-gathered:
     if (so.e) {
         g = persistent_grid((S.n_atoms + 15) / 16, EAM_BLOCK, (const void *)eam_site<T, Pol, ORTHO>);
         eam_site<T, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, rc2, B.pk, B.aux, so, ck);
