@@ -742,6 +742,12 @@ struct CellView {
 
 // ---- kernels --------------------------------------------------------------
 
+// The gather reads each pair force once: a streaming load (evict-first),
+// so the forces do not displace the per-atom records from the caches
+// (60 against 66.6 us at 256k).
+__device__ __forceinline__ float4 ld_slot(const float4 *p) { return __ldcs(p); }
+__device__ __forceinline__ double3 ld_slot(const double3 *p) { return *p; }
+
 __device__ __forceinline__ double4 ld_pack(const double4 *__restrict__ pk, int j) {
     const double2 *p = reinterpret_cast<const double2 *>(pk + j);
     double2 a = __ldg(p), b = __ldg(p + 1);
@@ -1017,7 +1023,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) eam_gather_reduce(int n_slots, 
 #pragma unroll
             for (int k = 0; k < GATHER_UNROLL; ++k) {
                 const int q = beg + sub + k * LPA;
-                if (q < up) w[k] = slot_f[q];
+                if (q < up) w[k] = ld_slot(slot_f + q);
             }
 #pragma unroll
             for (int k = 0; k < GATHER_UNROLL; ++k) {
@@ -1028,7 +1034,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) eam_gather_reduce(int n_slots, 
                 }
             }
             for (int q = beg + sub + GATHER_UNROLL * LPA; q < up; q += LPA) {
-                const V3 v = slot_f[q];
+                const V3 v = ld_slot(slot_f + q);
                 fx += (double)v.x;
                 fy += (double)v.y;
                 fz += (double)v.z;
