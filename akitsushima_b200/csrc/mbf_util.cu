@@ -149,11 +149,12 @@ __global__ void __launch_bounds__(NT) gather_reduce_rows(const int *__restrict__
         }
         double fx = 0, fy = 0, fz = 0;
         if (a < a1) {
+            // each slot force is read once: streaming (evict-first) loads
 #pragma unroll 4
             for (int q = beg + sub; q < end; q += LPA) {
-                fx += G[3 * (size_t)q];
-                fy += G[3 * (size_t)q + 1];
-                fz += G[3 * (size_t)q + 2];
+                fx += __ldcs(G + 3 * (size_t)q);
+                fy += __ldcs(G + 3 * (size_t)q + 1);
+                fz += __ldcs(G + 3 * (size_t)q + 2);
             }
             const double *pa = cs.per_atom + (size_t)a * ATOM_ACC;
             r0 += pa[sub];
