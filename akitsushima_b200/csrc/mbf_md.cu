@@ -278,96 +278,6 @@ __global__ void __launch_bounds__(MD_BLOCK) md_kick_kick_drift_check(
     *done = 0u;
 }
 
-// md_kick_kick_drift_check for one small structure (at most MD_1B_MAXP
-// chunks) in one block: the chunks one after another, each with the
-// per-atom arithmetic and the chunk sum of the multi-block kernel, the
-// partials kept in shared memory and summed as md_thermo_body sums them,
-// the displacement maximum reduced in the block -- the same bits, without
-// the completion counter, the global maxima and the last block's serial
-// tail (at 4096 atoms the kernel is latency, not work).
-constexpr int MD_1B_MAXP = 16;
-
-__global__ void __launch_bounds__(MD_BLOCK) md_kick_kick_drift_check_1b(
-    SysView S, double *__restrict__ pos, double *__restrict__ vel, const double *__restrict__ F,
-    const double *__restrict__ im, double dt, int P, const double *__restrict__ energy, double *__restrict__ thermo,
-    int rows, int *__restrict__ tcounter, const double *__restrict__ ref, double r_list, double r_cut,
-    double *__restrict__ d_log, int *__restrict__ scounter, int *__restrict__ gate, unsigned long long cond) {
-    __shared__ double sh[MD_BLOCK / 32];
-    __shared__ double part[MD_1B_MAXP];
-    __shared__ unsigned long long wmax[MD_BLOCK / 32];
-    const int end = S.n_atoms;
-    const double *c = S.cells;
-    unsigned long long bits = 0ull;
-    for (int b = 0; b < P; ++b) {
-        double acc = 0.0;
-        const int first = b * MD_CHUNK;
-#pragma unroll
-        for (int k = 0; k < MD_ITEMS; ++k) {
-            int a = first + k * MD_BLOCK + threadIdx.x;
-            if (a < end) {
-                size_t o = 3 * (size_t)a;
-                double w = im[a];
-                double h = 0.5 * dt * w;
-                double fx = F[o], fy = F[o + 1], fz = F[o + 2];
-                double vx = vel[o] + h * fx, vy = vel[o + 1] + h * fy, vz = vel[o + 2] + h * fz;
-                acc += (vx * vx + vy * vy + vz * vz) / w;
-                vx = vx + h * fx;
-                vy = vy + h * fy;
-                vz = vz + h * fz;
-                double x = pos[o] + dt * vx, y = pos[o + 1] + dt * vy, z = pos[o + 2] + dt * vz;
-                double s0 = x * c[9] + y * c[12] + z * c[15];
-                double s1 = x * c[10] + y * c[13] + z * c[16];
-                double s2 = x * c[11] + y * c[14] + z * c[17];
-                s0 -= floor(s0);
-                s1 -= floor(s1);
-                s2 -= floor(s2);
-                if (s0 >= 1.0) s0 = 0.0;
-                if (s1 >= 1.0) s1 = 0.0;
-                if (s2 >= 1.0) s2 = 0.0;
-                double px = s0 * c[0] + s1 * c[3] + s2 * c[6];
-                double py = s0 * c[1] + s1 * c[4] + s2 * c[7];
-                double pz = s0 * c[2] + s1 * c[5] + s2 * c[8];
-                pos[o] = px;
-                pos[o + 1] = py;
-                pos[o + 2] = pz;
-                vel[o] = vx;
-                vel[o + 1] = vy;
-                vel[o + 2] = vz;
-                double dx, dy, dz;
-                mic_exact(c, px - ref[o], py - ref[o + 1], pz - ref[o + 2], dx, dy, dz);
-                unsigned long long u = (unsigned long long)__double_as_longlong(sqrt(dx * dx + dy * dy + dz * dz));
-                bits = u > bits ? u : bits;
-            }
-        }
-        acc = block_sum<MD_BLOCK>(acc, sh);
-        if (threadIdx.x == 0) part[b] = acc;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        unsigned long long u = __shfl_xor_sync(MBF_FULL, bits, o);
-        bits = u > bits ? u : bits;
-    }
-    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = bits;
-    __syncthreads();
-    double v = 0.0;
-    for (int k = threadIdx.x; k < P; k += MD_BLOCK) v += part[k];
-    v = block_sum<MD_BLOCK>(v, sh);
-    if (threadIdx.x != 0) return;
-    const int trow = *tcounter % rows;
-    thermo[2 * (size_t)trow] = energy[0];
-    thermo[2 * (size_t)trow + 1] = 0.5 * v;
-    *tcounter += 1;
-    unsigned long long m = 0ull;
-    for (int w = 0; w < MD_BLOCK / 32; ++w) m = wmax[w] > m ? wmax[w] : m;
-    const double d = __longlong_as_double((long long)m);
-    const int row = *scounter % rows;
-    d_log[row] = d;
-    const int need = r_list - 2.0 * d <= r_cut ? 1 : 0;
-    *gate = need;
-    if (cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, need ? 1u : 0u);
-    *scounter += 1;
-}
-
 // With inv_mass = conv / m the partials hold sum m v^2 / conv, so the
 // kinetic energy is half their sum, in eV (the reference's
 // 0.5 sum m v^2 / EV_ANG_TO_AMU_ANG_FS2, :243-244).
@@ -463,14 +373,9 @@ int mbf_md_kick_kick_drift_check(const mbf_system *sys, double *positions, doubl
     cudaStream_t st = (cudaStream_t)stream;
     int P = mbf_md_partial_count(sys->n_atoms);
     PROF_BEGIN("md_kick_kick_drift", st);
-    if (sys->n_struct == 1 && P <= MD_1B_MAXP)
-        md_kick_kick_drift_check_1b<<<1, MD_BLOCK, 0, st>>>(S, positions, velocities, forces, inv_mass, dt, P, energy,
-                                                            thermo, thermo_rows, thermo_counter, ref_positions,
-                                                            r_list, r_cut, d_log, skin_counter, gate, cond_handle);
-    else
-        md_kick_kick_drift_check<<<dim3(P, sys->n_struct), MD_BLOCK, 0, st>>>(
-            S, positions, velocities, forces, inv_mass, dt, P, partial, energy, thermo, thermo_rows, thermo_counter,
-            ref_positions, d_max, r_list, r_cut, d_log, skin_counter, gate, cond_handle, done);
+    md_kick_kick_drift_check<<<dim3(P, sys->n_struct), MD_BLOCK, 0, st>>>(
+        S, positions, velocities, forces, inv_mass, dt, P, partial, energy, thermo, thermo_rows, thermo_counter,
+        ref_positions, d_max, r_list, r_cut, d_log, skin_counter, gate, cond_handle, done);
     PROF_END("md_kick_kick_drift", st);
     MBF_CHECK_LAUNCH();
     return MBF_OK;
