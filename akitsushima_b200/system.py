@@ -103,8 +103,6 @@ def default_device():
 
 
 _IDS_CACHE = {}
-# host positions go up in at most four pieces of at least this many rows
-_STAGE_PIECE_ROWS = 16384
 
 
 def species_ids(atom_types, species):
@@ -219,11 +217,10 @@ class Batch:
         """Copy new positions in place: one (N, 3) array or tensor for the
         whole batch, or a sequence of (N_s, 3) arrays, one per structure.
         Host arrays go through a page-locked staging buffer kept by the
-        batch, filled by torch's threaded host copy in up to four pieces,
-        each piece's upload (asynchronous, on the current stream) starting
-        while the next is copied, so the caller's next launches queue behind
-        it instead of the host waiting for a pageable copy (0.35 ms for 6 MB
-        on a B200 host).  The buffer
+        batch: torch's threaded host copy fills it (0.02 ms for 6 MB on a
+        B200 host) and the upload is asynchronous on the current stream, so
+        the caller's next launches queue behind it instead of the host
+        waiting for a pageable copy (0.35 ms for the same 6 MB).  The buffer
         is refilled only after the previous upload from it has finished.
         check: refuse NaN / inf in host arrays (no kernel depends on it -- a
         non-finite coordinate only gives non-finite results)."""
@@ -252,12 +249,8 @@ class Batch:
             self._stage_done = torch.cuda.Event()
         else:
             self._stage_done.synchronize()
-        # in pieces, so each piece's upload overlaps the host copy of the next
-        n = src.shape[0]
-        step = max(_STAGE_PIECE_ROWS, -(-n // 4))
-        for a in range(0, n, step):
-            stage[a:a + step].copy_(src[a:a + step])
-            self.pos[a:a + step].copy_(stage[a:a + step], non_blocking=True)
+        stage.copy_(src)
+        self.pos.copy_(stage, non_blocking=True)
         self._stage_done.record(torch.cuda.current_stream(self.device))
 
     def forces_to_host(self, forces):
