@@ -26,7 +26,8 @@ _sz = ctypes.c_size_t
 
 class MbfSystem(ctypes.Structure):
     _fields_ = [("n_atoms", _i), ("n_struct", _i), ("positions", _vp), ("types", _vp),
-                ("atom_struct", _vp), ("struct_off", _vp), ("cells", _vp), ("orthorhombic", _i)]
+                ("atom_struct", _vp), ("struct_off", _vp), ("cells", _vp), ("orthorhombic", _i),
+                ("cells_host", _vp)]
 
 
 class MbfNlist(ctypes.Structure):

@@ -30,6 +30,8 @@ struct SysView {
     const int *struct_off;
     const double *cells;
     int ortho;
+    int boxed;      // 1: one diagonal cell, its lengths and inverses in box
+    double box[6];  // L0 L1 L2 1/L0 1/L1 1/L2 (only with boxed)
 };
 
 static inline SysView make_view(const mbf_system *s) {
@@ -42,6 +44,8 @@ static inline SysView make_view(const mbf_system *s) {
     v.struct_off = s->struct_off;
     v.cells = s->cells;
     v.ortho = s->orthorhombic;
+    v.boxed = 0;
+    for (int k = 0; k < 6; ++k) v.box[k] = 0.0;
     return v;
 }
 

@@ -37,6 +37,14 @@ constexpr int EAM_BLOCK = 128;
 #ifndef MBF_EAM_MINB
 #define MBF_EAM_MINB 5
 #endif
+// With the cell as a launch argument (CellView<2>) the kernels need fewer
+// registers: 84 for the force pass, 40 for the density pass.
+#ifndef MBF_EAM_MINB_BOX
+#define MBF_EAM_MINB_BOX 6
+#endif
+#ifndef MBF_EAM_DENS_MINB_BOX
+#define MBF_EAM_DENS_MINB_BOX 12
+#endif
 // The same for the float32 density kernel (48 registers, no spills).
 #ifndef MBF_EAM_DENS_MINB
 #define MBF_EAM_DENS_MINB 10
@@ -715,22 +723,34 @@ __device__ __forceinline__ void mic_fast(const double *__restrict__ c, double rx
     dz = sx * c[2] + sy * c[5] + sz * c[8];
 }
 
-// The cell of one atom as the force kernels need it: a diagonal cell keeps
-// six scalars (lengths and inverse lengths) instead of the 3x3 pair.
-template <bool ORTHO>
+// The cell of one atom as the force kernels need it.  CM 0: any cell (the
+// 3x3 pair from global memory); CM 1: a diagonal cell, six scalars
+// (lengths and inverse lengths) in registers; CM 2: one diagonal cell whose
+// six scalars came with the launch (SysView::box, read from the parameter
+// space where they are used: twelve registers fewer, so more resident warps).
+template <int CM>
 struct CellView {
     const double *c;
     double L0, L1, L2, i0, i1, i2;
+    const SysView *S_;
     __device__ __forceinline__ void load(const SysView &S, int atom) {
+        if (CM == 2) {
+            S_ = &S;
+            return;
+        }
         c = cell_of(S, atom);
-        if (ORTHO) {
+        if (CM == 1) {
             L0 = c[0]; L1 = c[4]; L2 = c[8];
             i0 = c[9]; i1 = c[13]; i2 = c[17];
         }
     }
     __device__ __forceinline__ void mic(double rx, double ry, double rz, double &dx, double &dy,
                                         double &dz) const {
-        if (ORTHO) {
+        if (CM == 2) {
+            dx = rx - S_->box[0] * rint_shift(rx * S_->box[3]);
+            dy = ry - S_->box[1] * rint_shift(ry * S_->box[4]);
+            dz = rz - S_->box[2] * rint_shift(rz * S_->box[5]);
+        } else if (CM == 1) {
             dx = rx - L0 * rint_shift(rx * i0);
             dy = ry - L1 * rint_shift(ry * i1);
             dz = rz - L2 * rint_shift(rz * i2);
@@ -764,8 +784,8 @@ __device__ __forceinline__ double3 ld_pos(const double *__restrict__ pos, int j)
 // from its neighbours' species functions), accumulated in float64 into
 // aux[2 i].  Slot indices are loaded two iterations ahead, the neighbour's
 // position and species one ahead.
-template <typename T, int LPA, class Pol, bool ORTHO>
-__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB : 1)
+template <typename T, int LPA, class Pol, int CM>
+__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? (CM == 2 ? MBF_EAM_DENS_MINB_BOX : MBF_EAM_DENS_MINB) : 1)
     eam_density(SysView S, const int *__restrict__ row_off, const int *__restrict__ nbr, Pol P, double rc2,
                 double *__restrict__ aux, Chk ck) {
     __shared__ ZTab<T> Z;
@@ -782,7 +802,7 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_DENS_MINB 
                 flag = 1;
                 beg = end = 0;
             }
-            CellView<ORTHO> cv;
+            CellView<CM> cv;
             cv.load(S, i);
             const double3 pi = ld_pos(S.pos, i);
             int s = beg + sub;
@@ -856,8 +876,8 @@ template <> struct SlotVec<float> {
 // j's gather reads its row contiguously (0 beyond the cutoff).  T is float
 // in the mixed path (a per-pair term, accumulated in float64) and double in
 // the float64 path.
-template <typename T, int LPA, class Pol, bool ORTHO>
-__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
+template <typename T, int LPA, class Pol, int CM>
+__global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? (CM == 2 ? MBF_EAM_MINB_BOX : MBF_EAM_MINB) : 1)
     eam_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ upper,
               const int *__restrict__ nbr, const int *__restrict__ rev, Pol P, double rc2,
               const double4 *__restrict__ pk, const double *__restrict__ aux,
@@ -884,7 +904,7 @@ __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? MBF_EAM_MINB : 1)
             const int si = chk_idx(__ldg(S.types + i), ck.ns, 0, flag);
             const double4 pi = ld_pack(pk, i);
             const T Fp_i = (T)pi.w;
-            CellView<ORTHO> cv;
+            CellView<CM> cv;
             cv.load(S, i);
             int s = up + sub;
             int j0 = i, v0 = 0, j1 = i, v1 = 0;
@@ -1082,7 +1102,7 @@ __global__ void __launch_bounds__(EAM_BLOCK) eam_site(SysView S, const int *__re
                 beg = end = 0;
             }
             const int si = chk_idx(__ldg(S.types + i), ck.ns, 0, flag);
-            CellView<ORTHO> cv;
+            CellView<ORTHO ? 1 : 0> cv;
             cv.load(S, i);
             const double4 pi = ld_pack(pk, i);
             const double Fp = aux[2 * (size_t)i];
@@ -1133,7 +1153,7 @@ enum { PH_EMBED = 1, PH_FORCE = 2, PH_ALL = 3 };
 
 // The density pass walks full rows (twice the force pass's upper halves);
 // it takes 4 lanes per atom, or the force pass's lanes when that is more.
-template <typename T, int LPA, class Pol, bool ORTHO>
+template <typename T, int LPA, class Pol, int CM>
 static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const EamDev &E, double rc2,
                       const EamBufs &B, Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks,
                       int phases, cudaStream_t st) {
@@ -1143,9 +1163,9 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const
     int g = 0;
     if (phases & PH_EMBED) {
         const int dgpb = EAM_BLOCK / DLPA;
-        g = persistent_grid((S.n_atoms + dgpb - 1) / dgpb, EAM_BLOCK, (const void *)eam_density<T, DLPA, Pol, ORTHO>);
+        g = persistent_grid((S.n_atoms + dgpb - 1) / dgpb, EAM_BLOCK, (const void *)eam_density<T, DLPA, Pol, CM>);
         PROF_BEGIN("eam_density", st);
-        eam_density<T, DLPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, rc2, B.aux, ck);
+        eam_density<T, DLPA, Pol, CM><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, rc2, B.aux, ck);
         PROF_END("eam_density", st);
         MBF_CHECK_LAUNCH();
         PROF_BEGIN("eam_embed", st);
@@ -1155,9 +1175,9 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const
     }
     if (!(phases & PH_FORCE)) return MBF_OK;
     const int gpb = EAM_BLOCK / LPA;
-    g = persistent_grid((S.n_atoms + gpb - 1) / gpb, EAM_BLOCK, (const void *)eam_force<T, LPA, Pol, ORTHO>);
+    g = persistent_grid((S.n_atoms + gpb - 1) / gpb, EAM_BLOCK, (const void *)eam_force<T, LPA, Pol, CM>);
     PROF_BEGIN("eam_force", st);
-    eam_force<T, LPA, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, P, rc2,
+    eam_force<T, LPA, Pol, CM><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, P, rc2,
                                                            B.pk, B.aux, slot, B.f_local, B.per_atom, ck);
     PROF_END("eam_force", st);
     MBF_CHECK_LAUNCH();
@@ -1175,18 +1195,18 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const
     PROF_END("eam_gather_reduce", st);
     MBF_CHECK_LAUNCH();
     if (so.e) {
-        g = persistent_grid((S.n_atoms + 15) / 16, EAM_BLOCK, (const void *)eam_site<T, Pol, ORTHO>);
-        eam_site<T, Pol, ORTHO><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, rc2, B.pk, B.aux, so, ck);
+        g = persistent_grid((S.n_atoms + 15) / 16, EAM_BLOCK, (const void *)eam_site<T, Pol, CM != 0>);
+        eam_site<T, Pol, CM != 0><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->nbr, P, rc2, B.pk, B.aux, so, ck);
         MBF_CHECK_LAUNCH();
     }
     return MBF_OK;
 }
 
-template <typename T, class Pol, bool ORTHO>
+template <typename T, class Pol, int CM>
 static int eam_dispatch_lpa(int lpa, const SysView &S, const mbf_nlist *nl, const Pol &P, const EamDev &E,
                             double rc2, const EamBufs &B, Chk ck, const SiteOut &so, const ChunkSums &cs,
                             int n_chunks, int phases, cudaStream_t st) {
-#define MBF_EAM_LAUNCH(L) eam_launch<T, L, Pol, ORTHO>(S, nl, P, E, rc2, B, ck, so, cs, n_chunks, phases, st)
+#define MBF_EAM_LAUNCH(L) eam_launch<T, L, Pol, CM>(S, nl, P, E, rc2, B, ck, so, cs, n_chunks, phases, st)
     switch (lpa) {
         case 1: return MBF_EAM_LAUNCH(1);
         case 2: return MBF_EAM_LAUNCH(2);
@@ -1201,8 +1221,11 @@ template <typename T, class Pol>
 static int eam_dispatch(const Pol &P, int lpa, const SysView &S, const mbf_nlist *nl, const EamDev &E, double rc2,
                         const EamBufs &B, Chk ck, const SiteOut &so, const ChunkSums &cs, int n_chunks,
                         int phases, cudaStream_t st) {
-    return S.ortho ? eam_dispatch_lpa<T, Pol, true>(lpa, S, nl, P, E, rc2, B, ck, so, cs, n_chunks, phases, st)
-                   : eam_dispatch_lpa<T, Pol, false>(lpa, S, nl, P, E, rc2, B, ck, so, cs, n_chunks, phases, st);
+    // the launch-argument box for the float32 one- and two-element Zhou path
+    if constexpr (sizeof(T) == 4 && !Pol::species_addresses)
+        if (S.boxed) return eam_dispatch_lpa<T, Pol, 2>(lpa, S, nl, P, E, rc2, B, ck, so, cs, n_chunks, phases, st);
+    return S.ortho ? eam_dispatch_lpa<T, Pol, 1>(lpa, S, nl, P, E, rc2, B, ck, so, cs, n_chunks, phases, st)
+                   : eam_dispatch_lpa<T, Pol, 0>(lpa, S, nl, P, E, rc2, B, ck, so, cs, n_chunks, phases, st);
 }
 
 // The constants of the one- and two-element Zhou path from the host copies
@@ -1309,6 +1332,22 @@ static int eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
     }
     if (!nl->upper || !nl->row_off || !nl->nbr || !nl->rev) return MBF_ERR_ARGUMENT;
     SysView S = make_view(sys);
+    // one diagonal cell known on the host: its lengths travel with the
+    // launch -- not inside a stream capture, whose graph must read the
+    // device cell at each replay (the lattice may change between replays)
+    if (sys->n_struct == 1 && sys->orthorhombic && sys->cells_host) {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone) {
+            const double *c = sys->cells_host;
+            S.boxed = 1;
+            S.box[0] = c[0];
+            S.box[1] = c[4];
+            S.box[2] = c[8];
+            S.box[3] = c[9];
+            S.box[4] = c[13];
+            S.box[5] = c[17];
+        }
+    }
     EamDev E;
     E.ns = tab->ns; E.nf = tab->nf; E.nX = tab->nX;
     E.codes = tab->codes; E.P = tab->P; E.xo = tab->xo; E.nx = tab->nx;

@@ -180,7 +180,8 @@ class Batch:
         invs = np.linalg.inv(self.lattices)
         cells = np.concatenate([self.lattices.reshape(-1, 9), invs.reshape(-1, 9)], axis=1)
         dev = self.device
-        self.cells = torch.as_tensor(np.ascontiguousarray(cells), device=dev)
+        self._cells_np = np.ascontiguousarray(cells)   # the host copy the C view points to
+        self.cells = torch.as_tensor(self._cells_np, device=dev)
         self.struct_off = torch.as_tensor(off.astype(np.int32), device=dev)
         self.atom_struct = torch.as_tensor(
             np.repeat(np.arange(self.n_struct, dtype=np.int32), counts), device=dev)
@@ -301,12 +302,13 @@ class Batch:
         self.lattices[s] = lat
         self.volumes[s] = abs(np.linalg.det(lat))
         row = np.concatenate([lat.reshape(9), np.linalg.inv(lat).reshape(9)])
+        self._cells_np[s] = row
         self.cells[s].copy_(torch.from_numpy(row))
 
     def mbf_system(self):
-        """The C ABI's view of the batch (device pointers and the diagonal
-        cell flag), built once and again only after a lattice change: the
-        device arrays keep their addresses."""
+        """The C ABI's view of the batch (device pointers, the diagonal
+        cell flag and a host copy of the cells), built once and again only
+        after a lattice change: the device arrays keep their addresses."""
         sysd = getattr(self, "_sysd", None)
         if sysd is None:
             off = self.lattices - np.einsum("sij,ij->sij", self.lattices, np.eye(3))
@@ -314,6 +316,7 @@ class Batch:
             sysd = _lib.MbfSystem(self.n_atoms, self.n_struct, _lib.ptr(self.pos), _lib.ptr(self.types),
                                   _lib.ptr(self.atom_struct), _lib.ptr(self.struct_off),
                                   _lib.ptr(self.cells), ortho)
+            sysd.cells_host = self._cells_np.ctypes.data   # the rows uploaded to self.cells
             self._sysd = sysd
         return sysd
 

@@ -61,6 +61,13 @@ typedef struct mbf_system {
     int orthorhombic;          /* 1 if every lattice is diagonal (off-diagonal
                                   entries exactly 0): kernels use a 3-axis
                                   minimum image; 0 for general cells */
+    const double *cells_host;  /* optional HOST copy of `cells` (n_struct, 18),
+                                  equal to it, or NULL.  For one orthorhombic
+                                  structure the mixed Zhou EAM evaluation then
+                                  takes the cell as a launch argument (fewer
+                                  registers, more resident warps) when the
+                                  stream is not capturing; captured launches
+                                  read `cells` at each replay. */
 } mbf_system;
 
 typedef struct mbf_nlist {
