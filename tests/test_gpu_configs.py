@@ -190,3 +190,22 @@ def test_sic256_fit_loss_and_gradient(cuda_device):
         xm[q] -= h
         fd[q] = (f.loss(xp) - f.loss(xm)) / (2 * h)
     np.testing.assert_allclose(grad, fd, rtol=1e-6, atol=1e-6 * np.abs(fd).max())
+
+
+def test_eam_launch_argument_cell_equals_device_cell(cuda_device):
+    """One orthorhombic cell with a host copy goes with the launch (mixed
+    Zhou path); the same evaluation reading the device cell gives the same
+    bits."""
+    lat, pos, ids = workloads.make_cuni(10)
+    types = list(np.array(["Cu", "Ni"])[ids])
+    fn = ak.force_fn_from_config(EAM_CFG, precision="mixed")
+    nl = ak.NeighbourList(fn.r_cut, skin_width=0.3)
+    nl.build(lat, pos)
+    e1, f1, s1 = fn(lat, pos, types, nl)
+    sysd = nl._batch.mbf_system()
+    assert sysd.cells_host
+    sysd.cells_host = None          # the cached view: the device cell only
+    e2, f2, s2 = fn(lat, pos, types, nl)
+    assert e1 == e2
+    np.testing.assert_array_equal(f1, f2)
+    np.testing.assert_array_equal(s1, s2)
