@@ -406,11 +406,6 @@ __device__ __forceinline__ void zdec(double r, double, double ire, double shift,
     g = exp(-expo * (x - 1.0)) * rd;
     h = expo + 20.0 * u19 * rd;
 }
-__device__ __forceinline__ float zval(float r, float dre, float ire, float shift, float el, float) {
-    float u = fmaf(r, ire, -shift);
-    float u2 = u * u, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8;
-    return ex2_approx(el * dre) * rcp_approx(fmaf(u16, u4, 1.0f));
-}
 __device__ __forceinline__ double zval(double r, double, double ire, double shift, double, double expo) {
     double x = r * ire, u = x - shift;
     double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4, u16 = u8 * u8;
