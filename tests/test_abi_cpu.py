@@ -194,3 +194,22 @@ def test_neighbour_list_api_rejects_cpu_backends():
 
 
 _ = (ctypes, FCC)
+
+
+def test_batch_view_carries_host_cells():
+    """The C view's optional host copy of the cells holds the rows uploaded
+    to the device array, before and after a lattice change."""
+    import torch
+    from akitsushima_b200.system import Batch
+    lat, pos, _ = cubic(FCC, 3.58, 3, ["Cu"] * 4, rattle=0.05, seed=2)
+    b = Batch([lat], [pos], [np.zeros(len(pos), np.int32)], device=torch.device("cpu"))
+
+    def host_rows():
+        sysd = b.mbf_system()
+        assert sysd.cells_host
+        return np.ctypeslib.as_array((ctypes.c_double * (18 * b.n_struct)).from_address(sysd.cells_host))
+
+    np.testing.assert_array_equal(host_rows(), b.cells.numpy().reshape(-1))
+    b.set_lattice(0, np.asarray(lat) * 1.01)
+    np.testing.assert_array_equal(host_rows(), b.cells.numpy().reshape(-1))
+    np.testing.assert_array_equal(host_rows()[:9], (np.asarray(lat) * 1.01).reshape(-1))
