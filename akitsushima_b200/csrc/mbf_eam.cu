@@ -45,7 +45,7 @@ constexpr int EAM_BLOCK = 128;
 #ifndef MBF_EAM_DENS_MINB_BOX
 #define MBF_EAM_DENS_MINB_BOX 12
 #endif
-// The same for the float32 density kernel (48 registers, no spills).
+// The same for the float32 density kernel (47 registers, no spills).
 #ifndef MBF_EAM_DENS_MINB
 #define MBF_EAM_DENS_MINB 10
 #endif
@@ -869,8 +869,9 @@ template <> struct SlotVec<float> {
 // (d = r_j - r_i, minimum image), the pair energy and the virial -f (x) d go
 // to i, the lower index; -f goes to j's own slot (j -> i) = rev(i -> j), so
 // j's gather reads its row contiguously (0 beyond the cutoff).  T is float
-// in the mixed path (a per-pair term, accumulated in float64) and double in
-// the float64 path.
+// in the mixed path (the pair terms, and each lane's sums over its quarter
+// of the row, at most about 20 terms; float64 across lanes and in the
+// gather) and double in the float64 path.
 template <typename T, int LPA, class Pol, int CM>
 __global__ void __launch_bounds__(EAM_BLOCK, sizeof(T) == 4 ? (CM == 2 ? MBF_EAM_MINB_BOX : MBF_EAM_MINB) : 1)
     eam_force(SysView S, const int *__restrict__ row_off, const int *__restrict__ upper,
