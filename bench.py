@@ -31,6 +31,7 @@ structures ("weak": a fixed share per rank would be 512 each; here the set is
 split, "strong").
 """
 import argparse
+import gc
 import json
 import os
 import sys
@@ -1421,6 +1422,10 @@ def sub_records(args):
         a.skip_singles = False
         for k, v in over.items():
             setattr(a, k, v)
+        # the earlier workloads' objects (the 256k species-name lists among
+        # them) out of the collector's way: each record times its own calls
+        gc.collect()
+        gc.freeze()
         t0 = time.perf_counter()
         try:
             fn = run_fit if wl in FIT_WORKLOADS else run_md if wl in MD_WORKLOADS else run_batched
