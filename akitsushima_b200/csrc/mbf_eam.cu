@@ -1174,11 +1174,11 @@ static int eam_launch(const SysView &S, const mbf_nlist *nl, const Pol &P, const
     }
     if (!(phases & PH_FORCE)) return MBF_OK;
     const int gpb = EAM_BLOCK / LPA;
-    // one block per step (EAM_BLOCK / LPA atoms), not a persistent grid: upper halves
-    // differ in length, and blocks taken as others finish leave a shorter
-    // tail than a fixed share per resident block (126.6 against 133.7 us
-    // at 256k; the density pass, whose full rows are alike, keeps its
-    // persistent grid)
+    // one block per step of EAM_BLOCK / LPA atoms, not a persistent grid:
+    // upper halves differ in length, and blocks taken up as others finish
+    // leave a shorter tail than a fixed share per resident block (126.6
+    // against 133.7 us at 256k; the density pass, whose full rows are
+    // alike, keeps its persistent grid)
     g = (S.n_atoms + gpb - 1) / gpb;
     PROF_BEGIN("eam_force", st);
     eam_force<T, LPA, Pol, CM><<<g, EAM_BLOCK, 0, st>>>(S, nl->row_off, nl->upper, nl->nbr, nl->rev, P, rc2,
