@@ -855,7 +855,7 @@ def _perf_case(name, precision):
 
 def run_perf_path(args, world, rank, local):
     """One evaluation of a large structure through the spline-EAM or the
-    multi-species SW path (SURVEY next-row performance paths)."""
+    multi-species SW path (the performance paths beside the headline)."""
     import oracle
     lat, pos, types, pot, ref, desc = _perf_case(args.workload, args.precision)
     n_atoms = len(pos)
