@@ -1341,7 +1341,9 @@ static int eam_eval(const mbf_system *sys, const mbf_nlist *nl, const mbf_eam_ta
     // device cell at each replay (the lattice may change between replays)
     if (sys->n_struct == 1 && sys->orthorhombic && sys->cells_host) {
         cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-        if (cudaStreamIsCapturing(st, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone) {
+        const cudaError_t qe = cudaStreamIsCapturing(st, &cap);
+        if (qe != cudaSuccess) (void)cudaGetLastError();  // not a launch error: keep the cell in memory
+        if (qe == cudaSuccess && cap == cudaStreamCaptureStatusNone) {
             const double *c = sys->cells_host;
             S.boxed = 1;
             S.box[0] = c[0];
